@@ -1,0 +1,207 @@
+"""hphi_b200: B200 engine for HPhi's matrix-free H*v and the Lanczos / TPQ loops.
+
+The compute path is the CUDA shared library ``libhphi_b200.so`` built from
+``hphi_b200/csrc`` (see ``build.py``); this module is a thin ctypes binding over its
+C-ABI (``include/hphi_b200.h``).  Names follow the reference's operator set:
+
+  ========================  ==================================================
+  this module               reference (HPhi 3.5.2)
+  ========================  ==================================================
+  ``Hamiltonian(path)``     ReadDefFileNInt / ReadDefFileIdxPara, check, setmem_large
+                            (src/readdef.c:463,1006; src/check.c:51; src/xsetmem.c:153)
+  ``H.sz()``                sz (src/sz.c:62) -> list_1, list_2_1, list_2_2
+  ``H.diagonalcalc()``      diagonalcalc (src/diagonalcalc.c:84) -> list_Diagonal
+  ``H.mltply(v0, v1)``      mltply (src/mltply.c:56): v0 += H v1, returns prdct
+  ``H.calc_by_lanczos()``   CalcByLanczos (src/CalcByLanczos.c:55)
+  ``H.calc_by_tpq()``       CalcByTPQ (src/CalcByTPQ.c:52)
+  ========================  ==================================================
+
+Host vectors use HPhi's layout (complex128, length dim+1, element 0 unused).  There
+is no CPU fallback: if the library or a CUDA device is missing the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+__all__ = ["Hamiltonian", "HPhiError", "load_library", "library_path", "REAL64", "COMPLEX128",
+           "INFO_FIELDS", "EXPORTED_SYMBOLS"]
+
+REAL64 = 0
+COMPLEX128 = 1
+_HERE = os.path.dirname(os.path.abspath(__file__))
+INFO_FIELDS = ["dim", "nsite", "calc_model", "calc_type", "size_list_2_1", "size_list_2_2", "is_gc",
+               "vec_type", "n_offdiag", "n_diag", "lanczos_max", "num_ave"]
+EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi_close", "hphi_info",
+                    "hphi_sz", "hphi_diagonalcalc", "hphi_mltply", "hphi_mltply_device", "hphi_lanczos",
+                    "hphi_lanczos_eigenvector", "hphi_tpq", "hphi_run"]
+
+
+class HPhiError(RuntimeError):
+    """A C-ABI call returned an error status."""
+
+
+def library_path() -> str:
+    return os.environ.get("HPHI_B200_LIB", os.path.join(_HERE, "libhphi_b200.so"))
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def load_library() -> ctypes.CDLL:
+    """Loads libhphi_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise HPhiError(f"{path} not found: build it with `python -m hphi_b200.build` "
+                        "(there is no CPU fallback)")
+    lib = ctypes.CDLL(path)
+    P, I, D, VP = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+    pd = ctypes.POINTER(ctypes.c_double)
+    pu64 = ctypes.POINTER(ctypes.c_uint64)
+    pi64 = ctypes.POINTER(ctypes.c_int64)
+    lib.hphi_version.restype = ctypes.c_char_p
+    lib.hphi_last_error.restype = ctypes.c_char_p
+    lib.hphi_open_expert.argtypes = [ctypes.c_char_p, I, ctypes.POINTER(P)]
+    lib.hphi_close.argtypes = [P]
+    lib.hphi_close.restype = None
+    lib.hphi_info.argtypes = [P, pi64, I]
+    lib.hphi_sz.argtypes = [P, pu64, pu64, pu64]
+    lib.hphi_diagonalcalc.argtypes = [P, pd]
+    lib.hphi_mltply.argtypes = [P, pd, pd, pd]
+    lib.hphi_mltply_device.argtypes = [P, I, VP, VP, D, D, pd]
+    lib.hphi_lanczos.argtypes = [P, pd, ctypes.c_char_p, pd, I]
+    lib.hphi_lanczos_eigenvector.argtypes = [P, pd]
+    lib.hphi_tpq.argtypes = [P, pd, ctypes.c_char_p, pd, I]
+    lib.hphi_run.argtypes = [P, ctypes.c_char_p]
+    for name in EXPORTED_SYMBOLS:
+        if name not in ("hphi_version", "hphi_last_error", "hphi_close"):
+            getattr(lib, name).restype = I
+    _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise HPhiError(load_library().hphi_last_error().decode())
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _as_hphi_vector(v: np.ndarray, dim: int) -> np.ndarray:
+    v = np.ascontiguousarray(v, dtype=np.complex128)
+    if v.shape != (dim + 1,):
+        raise ValueError(f"expected an HPhi vector of length dim+1 = {dim + 1}, got {v.shape}")
+    return v
+
+
+class Hamiltonian:
+    """An expert-mode HPhi input resident on one CUDA device."""
+
+    def __init__(self, namelist_def: str, device: int = 0):
+        lib = load_library()
+        h = ctypes.c_void_p()
+        _check(lib.hphi_open_expert(os.fsencode(namelist_def), int(device), ctypes.byref(h)))
+        self._h = h
+        self.device = device
+        info = (ctypes.c_int64 * len(INFO_FIELDS))()
+        _check(lib.hphi_info(h, info, len(INFO_FIELDS)))
+        self.info = {k: int(info[i]) for i, k in enumerate(INFO_FIELDS)}
+        self.dim = self.info["dim"]
+
+    # -------------------------------------------------------------- lifecycle
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load_library().hphi_close(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    # ------------------------------------------------------------ reference ops
+    def sz(self):
+        """list_1 (length dim+1), list_2_1, list_2_2 as uint64 arrays (HPhi layout)."""
+        l1 = np.zeros(self.dim + 1, dtype=np.uint64)
+        l21 = np.zeros(self.info["size_list_2_1"], dtype=np.uint64)
+        l22 = np.zeros(self.info["size_list_2_2"], dtype=np.uint64)
+        pu = ctypes.POINTER(ctypes.c_uint64)
+        _check(load_library().hphi_sz(self._h, l1.ctypes.data_as(pu), l21.ctypes.data_as(pu),
+                                      l22.ctypes.data_as(pu)))
+        return l1, l21, l22
+
+    def diagonalcalc(self) -> np.ndarray:
+        d = np.zeros(self.dim + 1, dtype=np.float64)
+        _check(load_library().hphi_diagonalcalc(self._h, _dptr(d)))
+        return d
+
+    def mltply(self, v0: np.ndarray, v1: np.ndarray) -> complex:
+        """v0 += H v1 in place (HPhi layout, complex128); returns prdct = <v1|H|v1>."""
+        if not (isinstance(v0, np.ndarray) and v0.dtype == np.complex128 and v0.flags.c_contiguous):
+            raise TypeError("v0 must be a contiguous complex128 array (it is updated in place)")
+        _as_hphi_vector(v0, self.dim)
+        v1 = _as_hphi_vector(v1, self.dim)
+        pr = np.zeros(2)
+        _check(load_library().hphi_mltply(self._h, _dptr(v0.view(np.float64)), _dptr(v1.view(np.float64)),
+                                          _dptr(pr)))
+        return complex(pr[0], pr[1])
+
+    def mltply_device(self, v0_ptr: int, v1_ptr: int, vec_type: int, acc: float = 1.0,
+                      scale: float = 1.0) -> complex:
+        """Device form: v0 = acc*v0 + scale*H v1 on 0-based device arrays (raw pointers)."""
+        pr = np.zeros(2)
+        _check(load_library().hphi_mltply_device(self._h, int(vec_type), ctypes.c_void_p(v0_ptr),
+                                                 ctypes.c_void_p(v1_ptr), float(acc), float(scale), _dptr(pr)))
+        return complex(pr[0], pr[1])
+
+    def calc_by_lanczos(self, v_init: Optional[np.ndarray] = None, output_dir: Optional[str] = None) -> dict:
+        res = np.zeros(11)
+        vi = None if v_init is None else _as_hphi_vector(v_init, self.dim)
+        _check(load_library().hphi_lanczos(self._h, None if vi is None else _dptr(vi.view(np.float64)),
+                                           None if output_dir is None else os.fsencode(output_dir),
+                                           _dptr(res), len(res)))
+        keys = ["converged", "steps", "e_target", "e1", "e2", "e3", "e4", "energy", "var", "doublon", "sz"]
+        out = {k: float(res[i]) for i, k in enumerate(keys)}
+        out["converged"] = bool(res[0])
+        out["steps"] = int(res[1])
+        return out
+
+    def lanczos_eigenvector(self) -> np.ndarray:
+        v = np.zeros(self.dim + 1, dtype=np.complex128)
+        _check(load_library().hphi_lanczos_eigenvector(self._h, _dptr(v.view(np.float64))))
+        return v
+
+    def calc_by_tpq(self, v_init: Optional[Sequence[np.ndarray]] = None, output_dir: Optional[str] = None,
+                    nresult: Optional[int] = None) -> np.ndarray:
+        n = nresult or self.info["lanczos_max"]
+        res = np.zeros(n)
+        buf = None
+        if v_init is not None:
+            buf = np.ascontiguousarray(np.stack([_as_hphi_vector(v, self.dim) for v in v_init]))
+            if buf.shape[0] < self.info["num_ave"]:
+                raise ValueError("need one start vector per TPQ sample (NumAve)")
+        _check(load_library().hphi_tpq(self._h, None if buf is None else _dptr(buf.view(np.float64)),
+                                       None if output_dir is None else os.fsencode(output_dir), _dptr(res), n))
+        return res
+
+    def run(self, output_dir: str = "output") -> None:
+        _check(load_library().hphi_run(self._h, os.fsencode(output_dir)))

@@ -1,0 +1,245 @@
+// extern "C" entry points (include/hphi_b200.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hphi_b200.h"
+#include "driver.hpp"
+#include "engine.hpp"
+#include "model.hpp"
+
+namespace hphi {
+namespace {
+thread_local std::string g_err;
+}
+void set_error(const std::string &msg) { g_err = msg; }
+const char *get_error() { return g_err.c_str(); }
+}  // namespace hphi
+
+struct hphi_handle {
+  hphi::Sector *sector = nullptr;
+  hphi::LanczosResult last_lanczos;
+  double *d_scal = nullptr;  // coefficient / result slots for hphi_mltply*
+};
+
+using namespace hphi;
+
+namespace {
+#define CHECK_HANDLE(h)                        \
+  do {                                         \
+    if (!(h) || !(h)->sector) {                \
+      set_error("invalid handle");             \
+      return -1;                               \
+    }                                          \
+  } while (0)
+
+int cuda_fail(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return 0;
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return -1;
+}
+}  // namespace
+
+extern "C" {
+
+const char *hphi_version(void) { return "hphi_b200 0.1 (sm_100a)"; }
+
+const char *hphi_last_error(void) { return get_error(); }
+
+int hphi_open_expert(const char *namelist_def, int device, hphi_handle **out) {
+  if (!namelist_def || !out) { set_error("null argument"); return -1; }
+  *out = nullptr;
+  Model m;
+  std::string err;
+  if (read_expert(namelist_def, &m, &err) != 0) { set_error(err); return -1; }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("no CUDA device available");
+    return -1;
+  }
+  if (device < 0 || device >= ndev) { set_error("device index out of range"); return -1; }
+  Sector *s = nullptr;
+  if (sector_build(m, device, &s, &err) != 0) {
+    set_error(err);
+    sector_free(s);
+    return -1;
+  }
+  hphi_handle *h = new hphi_handle();
+  h->sector = s;
+  if (cuda_fail(cudaMalloc(&h->d_scal, sizeof(double) * 8), "alloc")) { hphi_close(h); return -1; }
+  *out = h;
+  return 0;
+}
+
+void hphi_close(hphi_handle *h) {
+  if (!h) return;
+  if (h->sector) {
+    cudaSetDevice(h->sector->device);
+    cudaFree(h->d_scal);
+    sector_free(h->sector);
+  }
+  delete h;
+}
+
+int hphi_info(const hphi_handle *h, int64_t *info, int n) {
+  CHECK_HANDLE(h);
+  const Sector &s = *h->sector;
+  int64_t v[HPHI_INFO_COUNT];
+  v[HPHI_INFO_DIM] = s.dim;
+  v[HPHI_INFO_NSITE] = s.model.nsite;
+  v[HPHI_INFO_CALC_MODEL] = s.model.calc_model;
+  v[HPHI_INFO_CALC_TYPE] = s.model.calc_type;
+  v[HPHI_INFO_SIZE_LIST_2_1] = s.size_list_2_1;
+  v[HPHI_INFO_SIZE_LIST_2_2] = s.size_list_2_2;
+  v[HPHI_INFO_IS_GC] = s.gc ? 1 : 0;
+  v[HPHI_INFO_VEC_TYPE] = default_vec_type(s);
+  v[HPHI_INFO_N_OFFDIAG] = s.nterms;
+  v[HPHI_INFO_N_DIAG] = s.ndterms;
+  v[HPHI_INFO_LANCZOS_MAX] = s.model.lanczos_max;
+  v[HPHI_INFO_NUM_AVE] = s.model.num_ave;
+  for (int i = 0; i < n && i < HPHI_INFO_COUNT; i++) info[i] = v[i];
+  return 0;
+}
+
+int hphi_sz(const hphi_handle *h, uint64_t *list_1, uint64_t *list_2_1, uint64_t *list_2_2) {
+  CHECK_HANDLE(h);
+  const Sector &s = *h->sector;
+  if (s.gc) { set_error("grand-canonical models have no sector lists"); return -1; }
+  cudaSetDevice(s.device);
+  if (list_1) {
+    list_1[0] = 0;
+    if (cuda_fail(cudaMemcpy(list_1 + 1, s.d_list_1, sizeof(uint64_t) * s.dim, cudaMemcpyDeviceToHost), "copy list_1"))
+      return -1;
+  }
+  if (list_2_1 || list_2_2) {
+    std::vector<uint32_t> tmp(std::max<uint64_t>(s.ihfbit, s.sdim));
+    if (list_2_1) {
+      if (cuda_fail(cudaMemcpy(tmp.data(), s.d_list_2_1, sizeof(uint32_t) * s.ihfbit, cudaMemcpyDeviceToHost), "copy"))
+        return -1;
+      for (int64_t i = 0; i < s.size_list_2_1; i++) list_2_1[i] = (uint64_t)i < s.ihfbit ? tmp[i] : 0;
+    }
+    if (list_2_2) {
+      if (cuda_fail(cudaMemcpy(tmp.data(), s.d_list_2_2, sizeof(uint32_t) * s.sdim, cudaMemcpyDeviceToHost), "copy"))
+        return -1;
+      for (int64_t i = 0; i < s.size_list_2_2; i++) list_2_2[i] = (uint64_t)i < s.sdim ? tmp[i] : 0;
+    }
+  }
+  return 0;
+}
+
+int hphi_diagonalcalc(const hphi_handle *h, double *list_diagonal) {
+  CHECK_HANDLE(h);
+  const Sector &s = *h->sector;
+  cudaSetDevice(s.device);
+  list_diagonal[0] = 0.0;
+  return cuda_fail(cudaMemcpy(list_diagonal + 1, s.d_diag, sizeof(double) * s.dim, cudaMemcpyDeviceToHost),
+                   "copy list_Diagonal");
+}
+
+int hphi_mltply_device(hphi_handle *h, int vec_type, void *d_v0, const void *d_v1, double acc, double scale,
+                       double *prdct) {
+  CHECK_HANDLE(h);
+  Sector *s = h->sector;
+  if (vec_type != HPHI_REAL64 && vec_type != HPHI_COMPLEX128) { set_error("bad vec_type"); return -1; }
+  cudaSetDevice(s->device);
+  const double coef[2] = {acc, scale};
+  if (cuda_fail(cudaMemcpyAsync(h->d_scal, coef, sizeof(coef), cudaMemcpyHostToDevice, s->stream), "coef")) return -1;
+  if (hv_launch(s, (VecType)vec_type, d_v1, d_v0, h->d_scal, h->d_scal + 2) != 0) return -1;
+  double out[2];
+  if (cuda_fail(cudaMemcpyAsync(out, h->d_scal + 2, sizeof(out), cudaMemcpyDeviceToHost, s->stream), "prdct")) return -1;
+  if (cuda_fail(cudaStreamSynchronize(s->stream), "sync")) return -1;
+  if (prdct) { prdct[0] = out[0]; prdct[1] = out[1]; }
+  return 0;
+}
+
+int hphi_mltply(hphi_handle *h, double *v0, const double *v1, double *prdct) {
+  CHECK_HANDLE(h);
+  Sector *s = h->sector;
+  cudaSetDevice(s->device);
+  const size_t bytes = sizeof(cplx) * (size_t)s->dim;
+  void *d0 = nullptr, *d1 = nullptr;
+  if (cuda_fail(cudaMalloc(&d0, bytes), "alloc v0")) return -1;
+  if (cuda_fail(cudaMalloc(&d1, bytes), "alloc v1")) { cudaFree(d0); return -1; }
+  int rc = vec_from_host_c128(s, kComplex128, v1, d1);
+  if (rc == 0) rc = vec_from_host_c128(s, kComplex128, v0, d0);
+  if (rc == 0) rc = hphi_mltply_device(h, HPHI_COMPLEX128, d0, d1, 1.0, 1.0, prdct);
+  if (rc == 0) rc = vec_to_host_c128(s, kComplex128, d0, v0);
+  cudaFree(d0);
+  cudaFree(d1);
+  return rc;
+}
+
+int hphi_lanczos(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult) {
+  CHECK_HANDLE(h);
+  Sector *s = h->sector;
+  const VecType vt = default_vec_type(*s);
+  std::vector<double> start;
+  if (!v_init) {
+    if (!single_element_start(*s, &start))
+      random_start(*s, 123432ull + (uint64_t)std::abs(s->model.initial_iv), vt == kComplex128, &start);
+    v_init = start.data();
+  }
+  LanczosOptions opt;
+  opt.eigenvector = (s->model.calc_eigenvec != -1);
+  opt.copy_eigenvector = opt.eigenvector;
+  LanczosResult &r = h->last_lanczos;
+  r = LanczosResult();
+  const int rc = lanczos_run(s, vt, v_init, opt, &r);
+  if (result && nresult > 0) {
+    double v[11] = {r.converged ? 1.0 : 0.0, (double)r.steps, r.e_target, 0, 0, 0, 0, r.energy, r.var, r.doublon, r.sz};
+    for (int q = 0; q < 4 && q < (int)r.energies.size(); q++) v[3 + q] = r.energies[q];
+    for (int i = 0; i < nresult && i < 11; i++) result[i] = v[i];
+  }
+  if (rc != 0) return -1;
+  if (output_dir && write_lanczos_outputs(*s, r, output_dir) != 0) return -1;
+  return 0;
+}
+
+int hphi_lanczos_eigenvector(hphi_handle *h, double *v) {
+  CHECK_HANDLE(h);
+  const auto &e = h->last_lanczos.eigenvector;
+  if (e.empty()) { set_error("no eigenvector: run hphi_lanczos with CalcEigenVec != -1 first"); return -1; }
+  std::memcpy(v, e.data(), sizeof(double) * e.size());
+  return 0;
+}
+
+int hphi_tpq(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult) {
+  CHECK_HANDLE(h);
+  Sector *s = h->sector;
+  const VecType vt = default_vec_type(*s);
+  const std::string out = output_dir ? output_dir : "output";
+  const int64_t stride = 2 * (s->dim + 1);
+  TpqResult r;
+  std::vector<double> start;
+  for (int rand_i = 0; rand_i < s->model.num_ave; rand_i++) {
+    const double *v = nullptr;
+    if (v_init) {
+      v = v_init + stride * rand_i;
+    } else {
+      random_start(*s, 123432ull + (uint64_t)(rand_i + 1) * (uint64_t)std::abs(s->model.initial_iv),
+                   vt == kComplex128, &start);
+      v = start.data();
+    }
+    if (tpq_run(s, vt, v, rand_i, out, &r) != 0) return -1;
+  }
+  if (result)
+    for (int i = 0; i < nresult && i < (int)r.energy.size(); i++) result[i] = r.energy[i];
+  return 0;
+}
+
+int hphi_run(hphi_handle *h, const char *output_dir) {
+  CHECK_HANDLE(h);
+  const std::string out = output_dir ? output_dir : "output";
+  switch (h->sector->model.calc_type) {
+    case kLanczos: return hphi_lanczos(h, nullptr, out.c_str(), nullptr, 0);
+    case kTPQ: return hphi_tpq(h, nullptr, out.c_str(), nullptr, 0);
+    default:
+      set_error("CalcType not supported by this engine (Lanczos = 0 and TPQ = 1 are)");
+      return -1;
+  }
+}
+
+}  // extern "C"

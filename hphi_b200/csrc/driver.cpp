@@ -1,0 +1,517 @@
+// Lanczos and TPQ drivers (host C++ over the device kernels) and HPhi-format output.
+//
+// Lanczos follows Lanczos_EigenValue (src/Lanczos_EigenValue.c:50-310): two-vector
+// recurrence without reorthogonalisation, eigenvalues of the stp x stp tridiagonal
+// matrix every step, stop when |(E_target - E_before)/E_target| < 10^-LanczosEps or
+// beta < 1e-14, E_target = E[LanczosTarget] (0-based).  The eigenvector pass replays
+// the recurrence (Lanczos_EigenVector, src/Lanczos_EigenVector.c:46-208) and energy /
+// variance follow expec_energy_flct (src/expec_energy_flct.c:34-179).  TPQ follows
+// CalcByTPQ / FirstMultiply / Multiply (src/CalcByTPQ.c:52-294, src/FirstMultiply.c:41-85,
+// src/Multiply.c:42-68).
+//
+// Device recurrence per Lanczos step (q_k = s*Q, P holds q_{k-1} scaled):
+//   hv:     P <- acc*P + s*H Q  (acc = -beta_{k-1} s_{k-1}),  raw = <Q|HQ>
+//   scalar: alpha_k = s^2 raw
+//   sweep:  P <- P - alpha_k s Q,  |P|^2
+//   scalar: beta_k = |P|; swap(P, Q); s = 1/beta_k
+// Scalars stay on the device; the host reads alpha/beta every few steps to run the
+// reference's convergence test step by step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <sys/stat.h>
+#include <vector>
+
+#include "driver.hpp"
+#include "engine.hpp"
+
+namespace hphi {
+namespace {
+
+// ---------------------------------------------------------------- tridiagonal
+// Number of eigenvalues of the symmetric tridiagonal (a[0..n), b[0..n-1)) below x
+// (Sturm sequence of the LDL^T factorisation of T - x).
+int sturm_count(const double *a, const double *b, int n, double x) {
+  int cnt = 0;
+  double d = a[0] - x;
+  const double tiny = 1e-300;
+  if (d < 0) cnt++;
+  for (int i = 1; i < n; i++) {
+    if (std::fabs(d) < tiny) d = (d < 0) ? -tiny : tiny;
+    d = a[i] - x - b[i - 1] * b[i - 1] / d;
+    if (d < 0) cnt++;
+  }
+  return cnt;
+}
+
+// k-th smallest eigenvalue (0-based) by bisection to full double precision.
+double tridiag_eigenvalue(const double *a, const double *b, int n, int k) {
+  double lo = a[0], hi = a[0];
+  for (int i = 0; i < n; i++) {
+    const double r = (i > 0 ? std::fabs(b[i - 1]) : 0.0) + (i < n - 1 ? std::fabs(b[i]) : 0.0);
+    lo = std::min(lo, a[i] - r);
+    hi = std::max(hi, a[i] + r);
+  }
+  const double span = std::max(std::fabs(lo), std::fabs(hi));
+  lo -= 1e-12 * span + 1e-300;
+  hi += 1e-12 * span + 1e-300;
+  for (int it = 0; it < 200; it++) {
+    const double mid = 0.5 * (lo + hi);
+    if (mid <= lo || mid >= hi) break;
+    if (sturm_count(a, b, n, mid) > k) hi = mid;
+    else lo = mid;
+  }
+  return 0.5 * (lo + hi);
+}
+
+// Eigenvector of the tridiagonal matrix for eigenvalue lam by inverse iteration
+// (Gaussian elimination with partial pivoting on T - lam), normalised, with the
+// sign fixed so that the largest component is positive.
+void tridiag_eigenvector(const double *a, const double *b, int n, double lam, std::vector<double> *out) {
+  std::vector<double> x(n, 1.0);
+  if (n == 1) { out->assign(1, 1.0); return; }
+  const double eps = 1e-14 * (std::fabs(lam) + 1.0);
+  // Banded LU with partial pivoting: rows have up to 3 non-zeros after pivoting.
+  std::vector<double> d(n), du(n), du2(n), dl(n);
+  std::vector<int> piv(n);
+  for (int it = 0; it < 3; it++) {
+    for (int i = 0; i < n; i++) { d[i] = a[i] - lam; du[i] = (i < n - 1) ? b[i] : 0.0; dl[i] = (i < n - 1) ? b[i] : 0.0; du2[i] = 0.0; }
+    std::vector<double> rhs = x;
+    for (int i = 0; i < n - 1; i++) {
+      if (std::fabs(d[i]) >= std::fabs(dl[i])) {
+        piv[i] = 0;
+        if (std::fabs(d[i]) < eps) d[i] = eps;
+        const double f = dl[i] / d[i];
+        d[i + 1] -= f * du[i];
+        rhs[i + 1] -= f * rhs[i];
+        dl[i] = f;
+      } else {
+        piv[i] = 1;
+        const double f = d[i] / dl[i];
+        d[i] = dl[i];
+        const double t = d[i + 1];
+        d[i + 1] = du[i] - f * t;
+        du2[i] = (i < n - 2) ? du[i + 1] : 0.0;
+        if (i < n - 2) du[i + 1] = -f * du2[i];
+        du[i] = t;
+        std::swap(rhs[i], rhs[i + 1]);
+        rhs[i + 1] -= f * rhs[i];
+        dl[i] = f;
+      }
+    }
+    if (std::fabs(d[n - 1]) < eps) d[n - 1] = eps;
+    // back substitution
+    x[n - 1] = rhs[n - 1] / d[n - 1];
+    if (n >= 2) x[n - 2] = (rhs[n - 2] - du[n - 2] * x[n - 1]) / d[n - 2];
+    for (int i = n - 3; i >= 0; i--) x[i] = (rhs[i] - du[i] * x[i + 1] - du2[i] * x[i + 2]) / d[i];
+    double nrm = 0.0;
+    for (double v : x) nrm += v * v;
+    nrm = std::sqrt(nrm);
+    for (double &v : x) v /= nrm;
+  }
+  int imax = 0;
+  for (int i = 1; i < n; i++)
+    if (std::fabs(x[i]) > std::fabs(x[imax])) imax = i;
+  if (x[imax] < 0)
+    for (double &v : x) v = -v;
+  *out = x;
+}
+
+// ---------------------------------------------------------------- helpers
+struct DevBuf {
+  void *p = nullptr;
+  ~DevBuf() { if (p) cudaFree(p); }
+};
+
+int ensure_dir(const std::string &dir) {
+  if (dir.empty()) return 0;
+  struct stat st;
+  if (stat(dir.c_str(), &st) == 0) return 0;
+  if (mkdir(dir.c_str(), 0755) != 0) {
+    set_error("cannot create output directory " + dir);
+    return -1;
+  }
+  return 0;
+}
+
+std::string join(const std::string &dir, const std::string &name) {
+  if (dir.empty()) return name;
+  return dir + "/" + name;
+}
+
+int cuda_ok(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) {
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return -1;
+  }
+  return 0;
+}
+
+#define RET(x) do { if ((x) != 0) return -1; } while (0)
+
+}  // namespace
+
+VecType default_vec_type(const Sector &s) {
+  if (s.model.complex_terms) return kComplex128;
+  return (s.model.initial_vec_type == 1) ? kReal64 : kComplex128;
+}
+
+// Initial vector of SetInitialVector (src/Lanczos_EigenValue.c:499-611) for the
+// deterministic single-element mode (initial_iv > 0 on canonical models), in HPhi's
+// 1-based complex128 layout.  Returns false when the reference would use a random vector.
+bool single_element_start(const Sector &s, std::vector<double> *v) {
+  const Model &m = s.model;
+  if (s.gc || m.initial_iv <= 0) return false;
+  const uint64_t dim = (uint64_t)s.dim;
+  const uint64_t iv = (dim / 2 + (uint64_t)m.initial_iv) % dim + 1;
+  v->assign(2 * (dim + 1), 0.0);
+  if (iv < dim) {
+    if (m.initial_vec_type == 0) {
+      (*v)[2 * (iv + 1)] = 1.0 / std::sqrt(2.0);
+      (*v)[2 * (iv + 1) + 1] = 1.0 / std::sqrt(2.0);
+    } else {
+      (*v)[2 * (iv + 1)] = 1.0;
+    }
+  }
+  return true;
+}
+
+// Seeded uniform start in [-1, 1) (complex: both parts), normalised; 1-based complex128.
+void random_start(const Sector &s, uint64_t seed, bool complex_vec, std::vector<double> *v) {
+  const uint64_t dim = (uint64_t)s.dim;
+  v->assign(2 * (dim + 1), 0.0);
+  uint64_t z = seed * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+  auto next = [&]() {
+    z += 0x9E3779B97F4A7C15ull;
+    uint64_t x = z;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    x ^= x >> 31;
+    return (double)(x >> 11) * (1.0 / 9007199254740992.0);
+  };
+  double nrm = 0.0;
+  for (uint64_t i = 1; i <= dim; i++) {
+    const double re = 2.0 * (next() - 0.5);
+    const double im = complex_vec ? 2.0 * (next() - 0.5) : 0.0;
+    (*v)[2 * i] = re;
+    (*v)[2 * i + 1] = im;
+    nrm += re * re + im * im;
+  }
+  nrm = std::sqrt(nrm);
+  for (uint64_t i = 1; i <= dim; i++) { (*v)[2 * i] /= nrm; (*v)[2 * i + 1] /= nrm; }
+}
+
+// ------------------------------------------------------------------- Lanczos
+int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOptions &opt, LanczosResult *res) {
+  const Model &m = s->model;
+  const int64_t dim = s->dim;
+  const size_t esz = (vt == kReal64) ? sizeof(double) : sizeof(cplx);
+  RET(cuda_ok(cudaSetDevice(s->device), "cudaSetDevice"));
+  DevBuf P, Q, V0, ST, AL, BE;
+  RET(cuda_ok(cudaMalloc(&P.p, esz * dim), "alloc P"));
+  RET(cuda_ok(cudaMalloc(&Q.p, esz * dim), "alloc Q"));
+  RET(cuda_ok(cudaMalloc(&ST.p, sizeof(double) * 16), "alloc scalars"));
+  int max_steps = m.lanczos_max;
+  if ((int64_t)max_steps > dim) max_steps = (int)dim;
+  if (dim < m.lanczos_target) max_steps = (int)dim;
+  RET(cuda_ok(cudaMalloc(&AL.p, sizeof(double) * (max_steps + 2)), "alloc alpha"));
+  RET(cuda_ok(cudaMalloc(&BE.p, sizeof(double) * (max_steps + 2)), "alloc beta"));
+  RET(vec_from_host_c128(s, vt, h_init, Q.p));
+  const bool want_vec = opt.eigenvector;
+  if (want_vec) {
+    RET(cuda_ok(cudaMalloc(&V0.p, esz * dim), "alloc V0"));
+    RET(cuda_ok(cudaMemcpyAsync(V0.p, Q.p, esz * dim, cudaMemcpyDeviceToDevice, s->stream), "copy V0"));
+  }
+  double *st = (double *)ST.p;
+  const double init_st[6] = {0.0, 0.0, 0.0, 1.0, 0.0, 0.0};  // acc = 0, s = 1
+  RET(cuda_ok(cudaMemcpyAsync(st, init_st, sizeof(init_st), cudaMemcpyHostToDevice, s->stream), "init scalars"));
+  RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+
+  std::vector<double> alpha(max_steps + 2, 0.0), beta(max_steps + 2, 0.0);
+  void *pp = P.p, *qq = Q.p;
+  auto do_step = [&](int k) -> int {
+    RET(hv_launch(s, vt, qq, pp, st + 2, st + 0));
+    RET(lanczos_scalars(s, 0, k, st, (double *)AL.p, (double *)BE.p));
+    RET(vec_lanczos_sweep(s, vt, st + 4, pp, qq, st + 5));
+    RET(lanczos_scalars(s, 1, k, st, (double *)AL.p, (double *)BE.p));
+    std::swap(pp, qq);
+    return 0;
+  };
+
+  const int target = m.lanczos_target;
+  const double eps = std::pow(10.0, -m.lanczos_eps);
+  res->lines.clear();
+  res->converged = false;
+  res->steps = 0;
+  const int batch = opt.batch > 0 ? opt.batch : (dim >= (1 << 20) ? 1 : 16);
+  int done = 0;       // steps executed on the device
+  int checked = 1;    // steps examined on the host
+  double ebefor = 0.0;
+  std::vector<double> E(5, 0.0);
+  const double ns = (double)m.nsite;
+  char line[512];
+  if (dim == 1) {
+    RET(do_step(1));
+    RET(cuda_ok(cudaMemcpy(alpha.data(), AL.p, sizeof(double) * 2, cudaMemcpyDeviceToHost), "read alpha"));
+    res->converged = true;
+    res->steps = 1;
+    res->energies.assign(1, alpha[1]);
+    res->e_target = alpha[1];
+  }
+  while (dim > 1 && !res->converged && checked < max_steps) {
+    const int upto = std::min(max_steps, done + batch);
+    if (done == 0) { RET(do_step(1)); done = 1; }
+    while (done < upto) { done++; RET(do_step(done)); }
+    RET(cuda_ok(cudaMemcpyAsync(alpha.data(), AL.p, sizeof(double) * (done + 1), cudaMemcpyDeviceToHost, s->stream), "read alpha"));
+    RET(cuda_ok(cudaMemcpyAsync(beta.data(), BE.p, sizeof(double) * (done + 1), cudaMemcpyDeviceToHost, s->stream), "read beta"));
+    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+    for (int stp = checked + 1; stp <= done; stp++) {
+      checked = stp;
+      const double *a = alpha.data() + 1;
+      const double *b = beta.data() + 1;
+      if (stp == 2) {
+        E[1] = tridiag_eigenvalue(a, b, 2, 0);
+        E[2] = tridiag_eigenvalue(a, b, 2, 1);
+        res->lines.push_back(std::string("LanczosStep  E[1] E[2] E[3] E[4] Target:E[") + std::to_string(target + 1) +
+                             "] E_Max/Nsite\n");
+        if (target < 2) {
+          const double et = (target == 0) ? E[1] : E[2];
+          ebefor = et;
+          snprintf(line, sizeof(line), "stp = %d %.10lf %.10lf xxxxxxxxxx xxxxxxxxx %.10lf xxxxxxxxx \n", stp, E[1],
+                   E[2], et);
+        } else {
+          snprintf(line, sizeof(line), "stp = %d %.10lf %.10lf xxxxxxxxxx xxxxxxxxx xxxxxxxxx xxxxxxxxx \n", stp, E[1],
+                   E[2]);
+        }
+        res->lines.push_back(line);
+      }
+      if (stp > 2) {
+        for (int q = 0; q < 4; q++) E[q + 1] = (q < stp) ? tridiag_eigenvalue(a, b, stp, q) : 0.0;
+        E[0] = tridiag_eigenvalue(a, b, stp, stp - 1);
+        double et = 0.0;
+        if (stp > target) {
+          et = tridiag_eigenvalue(a, b, stp, target);
+          snprintf(line, sizeof(line), "stp=%d %.10lf %.10lf %.10lf %.10lf %.10lf %.10lf\n", stp, E[1], E[2], E[3],
+                   E[4], et, E[0] / ns);
+        } else {
+          snprintf(line, sizeof(line), "stp=%d %.10lf %.10lf %.10lf %.10lf xxxxxxxxx %.10lf\n", stp, E[1], E[2], E[3],
+                   E[4], E[0] / ns);
+        }
+        res->lines.push_back(line);
+        if (stp > target) {
+          if (std::fabs((et - ebefor) / et) < eps || std::fabs(beta[stp]) < 1e-14) {
+            res->converged = true;
+            res->steps = stp;
+            res->e_target = et;
+            break;
+          }
+          ebefor = et;
+        }
+      }
+    }
+  }
+  if (!res->converged) {
+    res->steps = checked;
+  }
+  const int itr = res->steps;
+  res->alpha.assign(alpha.begin() + 1, alpha.begin() + 1 + itr);
+  res->beta.assign(beta.begin() + 1, beta.begin() + 1 + itr);
+  res->energies.clear();
+  const int nev = std::min(itr, std::max(m.nvec, m.lanczos_target + 1));
+  for (int q = 0; q < nev && q < itr; q++) res->energies.push_back(tridiag_eigenvalue(res->alpha.data(), res->beta.data(), itr, q));
+  if (!res->converged) {
+    set_error("Lanczos Eigenvalue is not converged in this process.");
+    return -1;
+  }
+  if (!want_vec) return 0;
+
+  // ---- eigenvector: vg = sum_k c_k q_k with c the k_exct-th tridiagonal eigenvector
+  const int kx = m.k_exct - 1;
+  const double lam = tridiag_eigenvalue(res->alpha.data(), res->beta.data(), itr, kx);
+  res->e_tridiag = lam;
+  std::vector<double> c;
+  tridiag_eigenvector(res->alpha.data(), res->beta.data(), itr, lam, &c);
+  DevBuf VG;
+  RET(cuda_ok(cudaMalloc(&VG.p, esz * dim), "alloc VG"));
+  pp = P.p; qq = Q.p;
+  RET(cuda_ok(cudaMemcpyAsync(qq, V0.p, esz * dim, cudaMemcpyDeviceToDevice, s->stream), "copy"));
+  RET(cuda_ok(cudaMemcpyAsync(VG.p, V0.p, esz * dim, cudaMemcpyDeviceToDevice, s->stream), "copy"));
+  RET(vec_scale(s, vt, c[0], VG.p));
+  double sq = 1.0, acc = 0.0;
+  for (int k = 1; k < itr; k++) {
+    const double coef[2] = {acc, sq};
+    RET(cuda_ok(cudaMemcpyAsync(st + 8, coef, sizeof(coef), cudaMemcpyHostToDevice, s->stream), "coef"));
+    RET(hv_launch(s, vt, qq, pp, st + 8, st + 10));
+    const double ak = res->alpha[k - 1], bk = res->beta[k - 1];
+    RET(vec_replay_sweep(s, vt, ak * sq, c[k] / bk, pp, qq, VG.p));
+    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+    acc = -bk * sq;
+    sq = 1.0 / bk;
+    std::swap(pp, qq);
+  }
+  double nrm2 = 0.0;
+  RET(vec_norm2(s, vt, VG.p, st + 12));
+  RET(cuda_ok(cudaMemcpyAsync(&nrm2, st + 12, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "read"));
+  RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+  RET(vec_scale(s, vt, 1.0 / std::sqrt(nrm2), VG.p));
+  // expec_energy_flct: H vg -> E = <vg|H vg>, var = <H vg|H vg>
+  const double coef1[2] = {0.0, 1.0};
+  RET(cuda_ok(cudaMemcpyAsync(st + 8, coef1, sizeof(coef1), cudaMemcpyHostToDevice, s->stream), "coef"));
+  RET(hv_launch(s, vt, VG.p, pp, st + 8, st + 10));
+  RET(vec_norm2(s, vt, pp, st + 12));
+  RET(vec_diag_observables(s, vt, VG.p, st + 13));
+  double sc[10];
+  RET(cuda_ok(cudaMemcpyAsync(sc, st + 10, sizeof(double) * 9, cudaMemcpyDeviceToHost, s->stream), "read"));
+  RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+  res->energy = sc[0];
+  res->var = sc[2];
+  res->doublon = sc[3];
+  res->sz = sc[7];
+  res->eigenvector.assign(2 * (dim + 1), 0.0);
+  if (opt.copy_eigenvector) RET(vec_to_host_c128(s, vt, VG.p, res->eigenvector.data()));
+  else res->eigenvector.clear();
+  return 0;
+}
+
+int write_lanczos_outputs(const Sector &s, const LanczosResult &r, const std::string &outdir) {
+  RET(ensure_dir(outdir));
+  const Model &m = s.model;
+  const std::string step_file = join(outdir, m.data_head + "_Lanczos_Step.dat");
+  FILE *f = fopen(step_file.c_str(), "w");
+  if (!f) { set_error("cannot write " + step_file); return -1; }
+  for (const auto &l : r.lines) fputs(l.c_str(), f);
+  fclose(f);
+  if (m.calc_eigenvec == -1) return 0;
+  const std::string ef = join(outdir, m.data_head + "_energy.dat");
+  f = fopen(ef.c_str(), "w");
+  if (!f) { set_error("cannot write " + ef); return -1; }
+  fprintf(f, "Energy  %.16lf \n", r.energy);
+  fprintf(f, "Doublon  %.16lf \n", r.doublon);
+  fprintf(f, "Sz  %.16lf \n", r.sz);
+  fclose(f);
+  if (m.output_eigenvec && !r.eigenvector.empty()) {
+    // zvo_eigenvec_%d_rank_%d.dat: int step, long dim, complex128[dim+1] (src/CalcByLanczos.c:262-273)
+    char name[256];
+    snprintf(name, sizeof(name), "%s_eigenvec_%d_rank_%d.dat", m.data_head.c_str(), m.k_exct - 1, 0);
+    const std::string vf = join(outdir, name);
+    f = fopen(vf.c_str(), "wb");
+    if (!f) { set_error("cannot write " + vf); return -1; }
+    const int itr = r.steps;
+    const long dim = (long)s.dim;
+    fwrite(&itr, sizeof(int), 1, f);
+    fwrite(&dim, sizeof(long), 1, f);
+    fwrite(r.eigenvector.data(), sizeof(double), r.eigenvector.size(), f);
+    fclose(f);
+  }
+  return 0;
+}
+
+// ------------------------------------------------------------------------ TPQ
+int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::string &outdir, TpqResult *res) {
+  const Model &m = s->model;
+  const int64_t dim = s->dim;
+  const size_t esz = (vt == kReal64) ? sizeof(double) : sizeof(cplx);
+  const double Ns = (double)m.nsite;
+  const double L = m.large_value;
+  RET(cuda_ok(cudaSetDevice(s->device), "cudaSetDevice"));
+  DevBuf V, H, ST;
+  RET(cuda_ok(cudaMalloc(&V.p, esz * dim), "alloc V"));
+  RET(cuda_ok(cudaMalloc(&H.p, esz * dim), "alloc H"));
+  RET(cuda_ok(cudaMalloc(&ST.p, sizeof(double) * 32), "alloc scalars"));
+  double *st = (double *)ST.p;
+  // h_init is the un-normalised start vector; its norm is global_1st_norm.
+  RET(vec_from_host_c128(s, vt, h_init, V.p));
+  double n0 = 0.0;
+  RET(vec_norm2(s, vt, V.p, st + 0));
+  RET(cuda_ok(cudaMemcpyAsync(&n0, st, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "read"));
+  RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+  const double first_norm = std::sqrt(n0);
+  double sv = 1.0 / first_norm;  // V holds the current vector times 1/sv
+  RET(ensure_dir(outdir));
+  char name[256];
+  snprintf(name, sizeof(name), "SS_rand%d.dat", rand_i);
+  const std::string ss_file = join(outdir, name);
+  snprintf(name, sizeof(name), "Norm_rand%d.dat", rand_i);
+  const std::string norm_file = join(outdir, name);
+  snprintf(name, sizeof(name), "Flct_rand%d.dat", rand_i);
+  const std::string flct_file = join(outdir, name);
+  FILE *fss = fopen(ss_file.c_str(), "w"), *fnorm = fopen(norm_file.c_str(), "w"), *fflct = fopen(flct_file.c_str(), "w");
+  if (!fss || !fnorm || !fflct) {
+    if (fss) fclose(fss);
+    if (fnorm) fclose(fnorm);
+    if (fflct) fclose(fflct);
+    set_error("cannot write TPQ output files in " + outdir);
+    return -1;
+  }
+  fprintf(fss, " # inv_tmp, energy, phys_var, phys_doublon, phys_num, step_i\n");
+  fprintf(fnorm, " # inv_temp, global_norm, global_1st_norm, step_i \n");
+  fprintf(fflct, " # inv_temp, N, N^2, D, D^2, Sz, Sz^2, step_i \n");
+  // expec_energy_flct on the current vector (sv*V): observables, H = H*(sv V), E, var.
+  double ob[6], E = 0.0, var = 0.0;
+  auto expec = [&]() -> int {
+    RET(vec_diag_observables(s, vt, V.p, st + 16));
+    const double coef[2] = {0.0, sv};
+    RET(cuda_ok(cudaMemcpyAsync(st + 4, coef, sizeof(coef), cudaMemcpyHostToDevice, s->stream), "coef"));
+    RET(hv_launch(s, vt, V.p, H.p, st + 4, st + 6));
+    RET(vec_norm2(s, vt, H.p, st + 8));
+    double sc[3];
+    RET(cuda_ok(cudaMemcpyAsync(sc, st + 6, sizeof(double) * 3, cudaMemcpyDeviceToHost, s->stream), "read"));
+    RET(cuda_ok(cudaMemcpyAsync(ob, st + 16, sizeof(double) * 6, cudaMemcpyDeviceToHost, s->stream), "read"));
+    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+    const double w2 = sv * sv;
+    for (double &o : ob) o *= w2;
+    E = sc[0] * sv * sv;
+    var = sc[2];
+    return 0;
+  };
+  auto write_lines = [&](double inv_temp, double gnorm, int step, bool flct) {
+    fprintf(fss, "%.16lf  %.16lf %.16lf %.16lf %.16lf %d\n", inv_temp, E, var, ob[0], ob[2], step);
+    fprintf(fnorm, "%.16lf %.16lf %.16lf %d\n", inv_temp, gnorm, first_norm, step);
+    if (flct)
+      fprintf(fflct, "%.16lf %.16lf %.16lf %.16lf %.16lf %.16lf %.16lf %d\n", inv_temp, ob[2], ob[3], ob[0], ob[1],
+              ob[4], ob[5], step);
+  };
+  auto multiply = [&](double *gnorm) -> int {
+    // v = L*v - H v / Ns with v = sv V: V <- (L sv) V - (1/Ns) H, then normalise lazily.
+    RET(vec_tpq_sweep(s, vt, L * sv, 1.0 / Ns, V.p, H.p, st + 10));
+    double n2 = 0.0;
+    RET(cuda_ok(cudaMemcpyAsync(&n2, st + 10, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "read"));
+    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+    *gnorm = std::sqrt(n2);
+    sv = 1.0 / *gnorm;
+    return 0;
+  };
+  res->energy.clear();
+  res->inv_temp.clear();
+  // FirstMultiply: expec on the start vector, then v = (L - H/Ns) v normalised.
+  RET(expec());
+  double gnorm = 0.0;
+  RET(multiply(&gnorm));
+  write_lines(0.0, first_norm, 0, false);
+  res->energy.push_back(E);
+  res->inv_temp.push_back(0.0);
+  RET(expec());
+  int step = 1;
+  double inv_temp = (2.0 / Ns) / (L - E / Ns);
+  write_lines(inv_temp, gnorm, step, true);
+  res->energy.push_back(E);
+  res->inv_temp.push_back(inv_temp);
+  for (step = 2; step < m.lanczos_max; step++) {
+    RET(multiply(&gnorm));
+    RET(expec());
+    inv_temp = (2.0 * step / Ns) / (L - E / Ns);
+    write_lines(inv_temp, gnorm, step, true);
+    res->energy.push_back(E);
+    res->inv_temp.push_back(inv_temp);
+  }
+  fclose(fss);
+  fclose(fnorm);
+  fclose(fflct);
+  return 0;
+}
+
+}  // namespace hphi

@@ -1,0 +1,42 @@
+// Lanczos / TPQ drivers over a device Sector.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace hphi {
+
+struct LanczosOptions {
+  bool eigenvector = false;       // replay the recurrence for the k_exct-th eigenvector
+  bool copy_eigenvector = false;  // copy it back to the host (HPhi layout)
+  int batch = 0;                  // steps between host convergence checks (0: automatic)
+};
+
+struct LanczosResult {
+  bool converged = false;
+  int steps = 0;                     // X->Large.itr
+  double e_target = 0.0;             // X->Phys.Target_energy
+  double e_tridiag = 0.0;            // eigenvalue used for the eigenvector (Target_CG_energy)
+  std::vector<double> alpha, beta;   // alpha[0..steps), beta[0..steps)
+  std::vector<double> energies;      // lowest eigenvalues of the final tridiagonal matrix
+  std::vector<std::string> lines;    // zvo_Lanczos_Step.dat
+  double energy = 0.0, var = 0.0, doublon = 0.0, sz = 0.0;
+  std::vector<double> eigenvector;   // 1-based complex128 (HPhi layout) when requested
+};
+
+struct TpqResult {
+  std::vector<double> inv_temp, energy;
+};
+
+VecType default_vec_type(const Sector &s);
+bool single_element_start(const Sector &s, std::vector<double> *v);
+void random_start(const Sector &s, uint64_t seed, bool complex_vec, std::vector<double> *v);
+
+// h_init: normalised start vector in HPhi's 1-based complex128 layout.
+int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOptions &opt, LanczosResult *res);
+int write_lanczos_outputs(const Sector &s, const LanczosResult &r, const std::string &outdir);
+// h_init: start vector (any norm) of sample rand_i; writes SS/Norm/Flct_rand<rand_i>.dat.
+int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::string &outdir, TpqResult *res);
+
+}  // namespace hphi

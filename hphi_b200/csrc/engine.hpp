@@ -1,0 +1,89 @@
+// Device-resident sector ("Hilbert space") and the kernels that act on it.
+//
+// One Sector replaces HPhi's globally allocated state for one Hamiltonian
+// (list_1, list_2_1, list_2_2, list_Diagonal; src/include/global.h:34-50, allocated by
+// setmem_large, src/xsetmem.c:153-249).  Vectors are 0-based device arrays of length
+// dim (HPhi's 1-based host arrays carry an unused slot 0; the C-ABI converts at the
+// boundary).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "model.hpp"
+
+namespace hphi {
+
+// Real or complex double scalar for host/device code.
+struct cplx { double x, y; };
+
+enum VecType : int { kReal64 = 0, kComplex128 = 1 };
+
+struct Sector {
+  Model model;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool gc = false;                 // grand-canonical: configuration == row index
+  int64_t dim = 0;                 // idim_max (src/check.c:51-209)
+  int lo_bits = 0, hi_bits = 0;    // HPhi's half split: ihfbit = 2^lo_bits (src/bitcalc.c:45-62)
+  uint64_t ihfbit = 0, sdim = 0;   // sdim = number of upper-half configurations (src/check.c:296-328)
+  int64_t size_list_2_1 = 0, size_list_2_2 = 0;  // HPhi's allocation sizes (src/xsetmem.c:284-318)
+
+  // Device tables (canonical models).  list_2_1 / list_2_2 hold HPhi's values: the
+  // 0-based row of configuration c is list_2_1[c & (ihfbit-1)] + list_2_2[c >> lo_bits] - 3
+  // and a zero entry means "not in the sector" (src/bitcalc.c:195-223).
+  uint64_t *d_list_1 = nullptr;    // [dim] configurations in HPhi order
+  uint32_t *d_list_2_1 = nullptr;  // [ihfbit]
+  uint32_t *d_list_2_2 = nullptr;  // [sdim]
+  double *d_diag = nullptr;        // [dim] list_Diagonal
+  BitTerm *d_terms = nullptr;
+  int nterms = 0;
+  DiagTerm *d_dterms = nullptr;
+  int ndterms = 0;
+  double *d_red = nullptr;         // reduction partials
+  double *d_scal = nullptr;        // small device scalars (dot results)
+  int red_blocks = 0;
+  int num_sms = 0;
+};
+
+int sector_build(const Model &m, int device, Sector **out, std::string *err);
+void sector_free(Sector *s);
+
+// v0 = acc * v0 + s * (H v1) with (acc, s) = d_coef[0..1] read on the device, and the raw
+// sum_r conj(v1[r]) (H v1)[r] written to d_out[0..1] (re, im).  HPhi's mltply
+// (src/mltply.c:56-132) is acc = s = 1, prdct = d_out.  acc == 0 never reads v0.
+int hv_launch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out);
+
+// ---- vector kernels (vecops.cu); all reductions are deterministic (fixed grid).
+// d_out[0] = sum |x|^2
+int vec_norm2(Sector *s, VecType vt, const void *d_x, double *d_out);
+// d_out[0..1] = sum conj(x) y
+int vec_dot(Sector *s, VecType vt, const void *d_x, const void *d_y, double *d_out);
+// y = a*x + b*y  (real a, b)
+int vec_axpby(Sector *s, VecType vt, double a, const void *d_x, double b, void *d_y);
+// x *= a
+int vec_scale(Sector *s, VecType vt, double a, void *d_x);
+// Lanczos sweep: p = p - alpha*sq*q in place and d_out[0] = |p|^2 (one pass).
+int vec_lanczos_sweep(Sector *s, VecType vt, const double *d_alpha_scale, void *d_p, const void *d_q,
+                      double *d_out);
+// Diagonal observables of a vector: d_out[0] = sum |v|^2 n_up n_dn over sites (doublon),
+// d_out[1] = sum |v|^2 * Sz, d_out[2] = sum |v|^2 * N.
+int vec_diag_observables(Sector *s, VecType vt, const void *d_v, double *d_out);
+
+// Device-side Lanczos scalar update (see vecops.cu); st is a device array of >= 6 doubles.
+int lanczos_scalars(Sector *s, int phase, int k, double *st, double *alpha, double *beta);
+// p = p - a_sq*q; vg += c_over_b * p  (eigenvector replay)
+int vec_replay_sweep(Sector *s, VecType vt, double a_sq, double c_over_b, void *p, const void *q, void *vg);
+// v = cv*v - ch*h and d_out[0] = |v|^2 (TPQ step before normalisation)
+int vec_tpq_sweep(Sector *s, VecType vt, double cv, double ch, void *v, const void *h, double *d_out);
+
+// Copies between HPhi's 1-based complex128 host layout and a device vector.
+int vec_from_host_c128(Sector *s, VecType vt, const double *h_v_1based, void *d_v);
+int vec_to_host_c128(Sector *s, VecType vt, const void *d_v, double *h_v_1based);
+
+void set_error(const std::string &msg);
+const char *get_error();
+
+}  // namespace hphi

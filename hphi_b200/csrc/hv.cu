@@ -1,0 +1,112 @@
+// Matrix-free H*v, general path: every off-diagonal term in gather form.
+//
+// Replaces mltply (src/mltply.c:56-132) and the term passes it dispatches to
+// (mltplyHubbard / mltplyHubbardGC, src/mltplyHubbard.c:150-528; mltplyHalfSpin /
+// mltplyHalfSpinGC, src/mltplySpin.c:192-703).  The reference makes one full pass over
+// the vector per term and scatters v0[off(j)] += c * v1[j]; here each output row is
+// owned by one thread, which walks the compiled terms once, tests the row's
+// configuration against each term's pattern, and gathers the matching source element:
+//   s = c ^ flip,  row(s) = list_2_1[s & (ihfbit-1)] + list_2_2[s >> lo_bits] - 3,
+//   sign = (-1)^popcount(c & sign_mask)            (GetOffComp / SgnBit, src/bitcalc.c).
+// Output rows are written exactly once, so there are no races and no atomics, and the
+// fused <v1|H|v1> of the reference (X->Large.prdct) comes from a block reduction of
+// conj(v1[r]) * (H v1)[r].
+#include <cuda_runtime.h>
+
+#include "device_util.cuh"
+#include "engine.hpp"
+
+namespace hphi {
+namespace {
+
+constexpr int kHvThreads = 256;
+constexpr int kSmemTermMax = 1024;  // 48 KiB of BitTerm
+
+template <typename T, bool GC, bool SMEM>
+__global__ void __launch_bounds__(kHvThreads) hv_general_kernel(
+    int64_t dim, const uint64_t *__restrict__ list_1, const uint32_t *__restrict__ l21,
+    const uint32_t *__restrict__ l22, int lo_bits, uint64_t lo_mask, const BitTerm *__restrict__ gterms,
+    int nterms, const double *__restrict__ diag, const T *__restrict__ v1, T *__restrict__ v0,
+    const double *__restrict__ coef, double *__restrict__ part) {
+  const double acc = coef[0], scale = coef[1];
+  extern __shared__ BitTerm sterms[];
+  const BitTerm *terms = gterms;
+  if (SMEM) {
+    for (int k = threadIdx.x; k < nterms; k += blockDim.x) sterms[k] = gterms[k];
+    __syncthreads();
+    terms = sterms;
+  }
+  double pr[2] = {0.0, 0.0};
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < dim; r += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = GC ? (uint64_t)r : list_1[r];
+    const T x = v1[r];
+    T y = VT<T>::scale(diag[r], x);
+    for (int k = 0; k < nterms; k++) {
+      const BitTerm t = terms[k];
+      if ((c & t.cm) != t.cv) continue;
+      const uint64_t src = c ^ t.flip;
+      int64_t j;
+      if (GC) {
+        j = (int64_t)src;
+      } else {
+        const uint32_t a = l21[src & lo_mask];
+        const uint32_t b = l22[src >> lo_bits];
+        if (a == 0u || b == 0u) continue;
+        j = (int64_t)a + (int64_t)b - 3;
+      }
+      const double sg = (__popcll(c & t.sm) & 1) ? -t.re : t.re;
+      const double sgi = (__popcll(c & t.sm) & 1) ? -t.im : t.im;
+      y = VT<T>::add(y, VT<T>::cmul_re_im(sg, sgi, v1[j]));
+    }
+    pr[0] += VT<T>::conj_mul_re(x, y);
+    pr[1] += VT<T>::conj_mul_im(x, y);
+    y = VT<T>::scale(scale, y);
+    v0[r] = (acc == 0.0) ? y : VT<T>::add(VT<T>::scale(acc, v0[r]), y);
+  }
+  block_sum<2>(pr);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = pr[0];
+    part[2 * blockIdx.x + 1] = pr[1];
+  }
+}
+
+template <typename T, bool GC>
+void launch_general(Sector *s, const T *v1, T *v0, const double *coef) {
+  const int grid = s->red_blocks;
+  const uint64_t lo_mask = s->ihfbit - 1;
+  if (s->nterms <= kSmemTermMax) {
+    const size_t smem = sizeof(BitTerm) * (size_t)s->nterms;
+    hv_general_kernel<T, GC, true><<<grid, kHvThreads, smem, s->stream>>>(
+        s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, s->d_terms, s->nterms, s->d_diag,
+        v1, v0, coef, s->d_red);
+  } else {
+    hv_general_kernel<T, GC, false><<<grid, kHvThreads, 0, s->stream>>>(
+        s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, s->d_terms, s->nterms, s->d_diag,
+        v1, v0, coef, s->d_red);
+  }
+}
+
+}  // namespace
+
+int hv_launch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out) {
+  if (vt == kReal64 && s->model.complex_terms) {
+    set_error("H has complex coefficients: real vectors are not allowed");
+    return -1;
+  }
+  if (vt == kReal64) {
+    if (s->gc) launch_general<double, true>(s, (const double *)d_v1, (double *)d_v0, d_coef);
+    else launch_general<double, false>(s, (const double *)d_v1, (double *)d_v0, d_coef);
+  } else {
+    if (s->gc) launch_general<cplx, true>(s, (const cplx *)d_v1, (cplx *)d_v0, d_coef);
+    else launch_general<cplx, false>(s, (const cplx *)d_v1, (cplx *)d_v0, d_coef);
+  }
+  finalize_partials_kernel<2><<<1, 256, 0, s->stream>>>(s->d_red, s->red_blocks, d_out);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error(std::string("hv launch failed: ") + cudaGetErrorString(e));
+    return -1;
+  }
+  return 0;
+}
+
+}  // namespace hphi

@@ -1,0 +1,565 @@
+// Expert-mode reader and term compiler (host C++).
+//
+// File formats follow the reference reader (src/readdef.c):
+//   namelist.def   "Keyword file" lines; keywords src/readdef.c:46-71
+//   calcmod.def    "Key int" lines                          src/readdef.c:233-386
+//   modpara.def    8 header lines, then "Key value" lines   src/readdef.c:513-640
+//   locspn.def     5 header lines (2nd: "NlocalSpin n"), then "i S2" lines
+//   interactions   5 header lines (2nd: "N<kind> n"), then one entry per line
+// Sector parameters (Nup, Ndown, Ne, Total2Sz) are derived as in
+// src/readdef.c:880-960.  Hamiltonian semantics of each keyword:
+//   Trans        H += -t c+_{i s1} c_{j s2}               (src/mltplyHubbard.c:202; diagonal
+//                                                          entries become EDChemi, src/readdef.c:2185-2233)
+//   CoulombIntra H += U n_{i0} n_{i1}                     (src/diagonalcalc.c:260-355)
+//   CoulombInter H += V n_i n_j                           (src/diagonalcalc.c:543-787)
+//   Hund         H += -J (n_{i0} n_{j0} + n_{i1} n_{j1})   (src/diagonalcalc.c:788-1112)
+//   Ising        Hund(-J/2) + CoulombInter(-J/4)          (src/readdef.c:1320-1327)
+//   Exchange     Hubbard/Kondo: J (c+_{i0}c_{j0}c+_{j1}c_{i1} + h.c.) (src/mltplyHubbardCore.c:197-218, 472-526)
+//                Spin: J (|10><01| + |01><10|) on (i,j)   (src/mltplySpinCore.c:35-56, 273-307)
+//   PairHop      J (c+_{i0}c_{j0}c+_{i1}c_{j1}), stored with its (j,i) partner (src/readdef.c:1262-1283,
+//                src/mltplyHubbardCore.c:533-575)
+//   PairLift     SpinGC: J (|11><00| + |00><11|) on (i,j)  (src/mltplySpinCore.c:352-382)
+//   InterAll     V c+_{i s1} c_{j s2} c+_{k s3} c_{l s4}   (src/readdef.c:1373-1400, 2415-2549)
+// Spin models label a site's state by its bit value (sigma == bit), as the spin
+// element routines do (src/mltplySpinCore.c:239-266, src/diagonalcalc.c SetDiagonalChemi).
+#include "model.hpp"
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <tuple>
+
+namespace hphi {
+namespace {
+
+std::string lower(std::string s) {
+  for (auto &ch : s) ch = (char)std::tolower((unsigned char)ch);
+  return s;
+}
+
+bool open_def(const Model &m, const std::string &name, std::ifstream *f) {
+  f->open(name);
+  if (f->is_open()) return true;
+  if (!name.empty() && name[0] != '/' && !m.base_dir.empty()) {
+    f->clear();
+    f->open(m.base_dir + "/" + name);
+    return f->is_open();
+  }
+  return false;
+}
+
+int parity64(uint64_t x) { return __builtin_popcountll(x) & 1; }
+
+// Reads the count on the 2nd header line of an interaction file and the entry lines.
+bool read_table(const Model &m, const std::string &fname, std::vector<std::vector<double>> *rows,
+                int ncol, std::string *err) {
+  std::ifstream f;
+  if (!open_def(m, fname, &f)) { *err = "cannot open " + fname; return false; }
+  std::string line;
+  int count = -1;
+  for (int i = 0; i < 5; i++) {
+    if (!std::getline(f, line)) { *err = fname + ": truncated header"; return false; }
+    if (i == 1) {
+      std::istringstream ss(line);
+      std::string kw;
+      ss >> kw >> count;
+      if (ss.fail()) { *err = fname + ": bad header line 2"; return false; }
+    }
+  }
+  rows->clear();
+  while ((int)rows->size() < count && std::getline(f, line)) {
+    if (line.find_first_not_of(" \t\r\n") == std::string::npos) continue;
+    std::istringstream ss(line);
+    std::vector<double> r(ncol, 0.0);
+    int got = 0;
+    for (; got < ncol; got++) {
+      if (!(ss >> r[got])) break;
+    }
+    if (got < ncol) {
+      // Trans/InterAll may omit the imaginary part.
+      if (!(got == ncol - 1)) { *err = fname + ": malformed line: " + line; return false; }
+      r[ncol - 1] = 0.0;
+    }
+    rows->push_back(r);
+  }
+  if ((int)rows->size() != count) { *err = fname + ": fewer entries than the header count"; return false; }
+  return true;
+}
+
+// Compiles a fermion operator string (ops applied right to left) in the
+// Jordan-Wigner ordering of configuration bits.  Push form: a source s with
+// (s & req_mask) == req_val maps to s ^ flip with sign (-1)^(sign0 + popc(s & sm)).
+bool compile_fermion(const std::vector<FermionOp> &ops, uint64_t *req_mask, uint64_t *req_val,
+                     uint64_t *flip, uint64_t *sm, int *sign0) {
+  uint64_t rm = 0, rv = 0, fl = 0, s = 0;
+  int sg = 0;
+  for (int k = (int)ops.size() - 1; k >= 0; k--) {
+    const uint64_t b = 1ull << ops[k].bit;
+    const int need_now = ops[k].dag ? 0 : 1;
+    const int need_orig = need_now ^ ((fl & b) ? 1 : 0);
+    if (rm & b) {
+      if ((int)((rv & b) ? 1 : 0) != need_orig) return false;
+    } else {
+      rm |= b;
+      if (need_orig) rv |= b;
+    }
+    const uint64_t below = b - 1;
+    s ^= below;
+    sg ^= parity64(fl & below);
+    fl ^= b;
+  }
+  *req_mask = rm; *req_val = rv; *flip = fl; *sm = s; *sign0 = sg;
+  return true;
+}
+
+bool compile_spin(const std::vector<SpinOp> &ops, uint64_t *req_mask, uint64_t *req_val, uint64_t *flip) {
+  uint64_t rm = 0, rv = 0, fl = 0;
+  for (int k = (int)ops.size() - 1; k >= 0; k--) {
+    const uint64_t b = 1ull << ops[k].site;
+    const int need_orig = ops[k].from ^ ((fl & b) ? 1 : 0);
+    if (rm & b) {
+      if ((int)((rv & b) ? 1 : 0) != need_orig) return false;
+    } else {
+      rm |= b;
+      if (need_orig) rv |= b;
+    }
+    if (ops[k].to != ops[k].from) fl ^= b;
+  }
+  *req_mask = rm; *req_val = rv; *flip = fl;
+  return true;
+}
+
+void push_term(Model *m, uint64_t rm, uint64_t rv, uint64_t fl, uint64_t sm, int sign0,
+               std::complex<double> coef) {
+  if (sign0) coef = -coef;
+  if (fl == 0) {
+    m->diag.push_back(DiagTerm{rm, rv, coef.real()});
+    return;
+  }
+  // Pull form for the output configuration t = s ^ fl.
+  const uint64_t cv = rv ^ (fl & rm);
+  if (parity64(fl & sm)) coef = -coef;
+  m->offdiag.push_back(BitTerm{rm, cv, fl, sm, coef.real(), coef.imag()});
+}
+
+}  // namespace
+
+bool add_fermion_string(Model *m, const std::vector<FermionOp> &ops, std::complex<double> coef) {
+  uint64_t rm, rv, fl, sm;
+  int s0;
+  if (!compile_fermion(ops, &rm, &rv, &fl, &sm, &s0)) return false;
+  push_term(m, rm, rv, fl, sm, s0, coef);
+  return true;
+}
+
+bool add_spin_string(Model *m, const std::vector<SpinOp> &ops, std::complex<double> coef) {
+  uint64_t rm, rv, fl;
+  if (!compile_spin(ops, &rm, &rv, &fl)) return false;
+  push_term(m, rm, rv, fl, 0, 0, coef);
+  return true;
+}
+
+void canonicalize_terms(Model *m) {
+  std::map<std::tuple<uint64_t, uint64_t, uint64_t, uint64_t>, std::complex<double>> off;
+  std::vector<std::tuple<uint64_t, uint64_t, uint64_t, uint64_t>> order;
+  for (const auto &t : m->offdiag) {
+    auto key = std::make_tuple(t.flip, t.cm, t.cv, t.sm);
+    auto it = off.find(key);
+    if (it == off.end()) { off[key] = {t.re, t.im}; order.push_back(key); }
+    else it->second += std::complex<double>(t.re, t.im);
+  }
+  m->offdiag.clear();
+  m->complex_terms = false;
+  for (const auto &key : order) {
+    const auto c = off[key];
+    if (c == std::complex<double>(0.0, 0.0)) continue;
+    m->offdiag.push_back(BitTerm{std::get<1>(key), std::get<2>(key), std::get<0>(key),
+                                 std::get<3>(key), c.real(), c.imag()});
+    if (c.imag() != 0.0) m->complex_terms = true;
+  }
+  // Diagonal terms are summed in their input order by the device (no merging, so the
+  // per-configuration sum follows the reference's term order as closely as possible).
+  std::vector<DiagTerm> d;
+  for (const auto &t : m->diag)
+    if (t.v != 0.0) d.push_back(t);
+  m->diag.swap(d);
+}
+
+int read_expert(const std::string &namelist, Model *m, std::string *err) {
+  *m = Model();
+  {
+    const auto pos = namelist.find_last_of('/');
+    m->base_dir = (pos == std::string::npos) ? std::string(".") : namelist.substr(0, pos);
+  }
+  std::ifstream nl(namelist);
+  if (!nl.is_open()) { *err = "cannot open " + namelist; return -1; }
+  std::map<std::string, std::string> files;
+  std::string line;
+  static const char *known[] = {"calcmod", "modpara", "locspin", "trans", "coulombintra", "coulombinter",
+                                "hund", "pairhop", "exchange", "interall", "onebodyg", "twobodyg",
+                                "pairlift", "ising", "boost", "singleexcitation", "pairexcitation",
+                                "spectrumvec", "laser", "teonebody", "tetwobody", "threebodyg",
+                                "fourbodyg", "sixbodyg"};
+  while (std::getline(nl, line)) {
+    std::istringstream ss(line);
+    std::string kw, fn;
+    if (!(ss >> kw)) continue;
+    if (kw[0] == '#') continue;
+    if (!(ss >> fn)) { *err = "namelist.def: keyword without file: " + kw; return -1; }
+    const std::string k = lower(kw);
+    if (std::find(std::begin(known), std::end(known), k) == std::end(known)) {
+      *err = "namelist.def: unknown keyword " + kw;
+      return -1;
+    }
+    if (files.count(k)) { *err = "namelist.def: duplicate keyword " + kw; return -1; }
+    files[k] = fn;
+  }
+  for (const char *must : {"calcmod", "modpara", "locspin"})
+    if (!files.count(must)) { *err = std::string("namelist.def: missing ") + must; return -1; }
+  for (const char *unsupported : {"boost", "laser", "teonebody", "tetwobody", "singleexcitation",
+                                  "pairexcitation", "spectrumvec"})
+    if (files.count(unsupported)) {
+      *err = std::string("namelist.def: keyword not supported by this engine: ") + unsupported;
+      return -1;
+    }
+
+  // ---- calcmod.def
+  {
+    std::ifstream f;
+    if (!open_def(*m, files["calcmod"], &f)) { *err = "cannot open " + files["calcmod"]; return -1; }
+    while (std::getline(f, line)) {
+      std::istringstream ss(line);
+      std::string kw;
+      long v;
+      if (!(ss >> kw) || kw[0] == '#' || kw[0] == '=' || kw[0] == '-') continue;
+      if (!(ss >> v)) continue;
+      const std::string k = lower(kw);
+      if (k == "calctype") m->calc_type = (int)v;
+      else if (k == "calcmodel") m->calc_model = (int)v;
+      else if (k == "outputmode") m->output_mode = (int)v;
+      else if (k == "calceigenvec") m->calc_eigenvec = (int)v;
+      else if (k == "initialvectype") m->initial_vec_type = (int)v;
+      else if (k == "outputeigenvec" || k == "oev") m->output_eigenvec = (int)v;
+      else if (k == "inputeigenvec" || k == "iev") m->input_eigenvec = (int)v;
+      else if (k == "restart") m->restart = (int)v;
+      else if (k == "flgfinitetemperature") m->flg_finite_temperature = (int)v;
+      else if (k == "outputham" || k == "inputham" || k == "outputexcitedvec" || k == "outputexvec" ||
+               k == "calcspec" || k == "calcspectrum" || k == "ngpu" || k == "scalapack") {
+        if ((k == "calcspec" || k == "calcspectrum" || k == "inputham") && v != 0) {
+          *err = "calcmod.def: " + kw + " is not supported by this engine";
+          return -1;
+        }
+      } else {
+        *err = "calcmod.def: unknown keyword " + kw;
+        return -1;
+      }
+    }
+    if (m->calc_model < 0 || m->calc_model > 5) { *err = "calcmod.def: CalcModel out of range"; return -1; }
+    if (m->calc_type < 0 || m->calc_type > 5) { *err = "calcmod.def: CalcType out of range"; return -1; }
+  }
+  // ---- modpara.def
+  {
+    std::ifstream f;
+    if (!open_def(*m, files["modpara"], &f)) { *err = "cannot open " + files["modpara"]; return -1; }
+    for (int i = 0; i < 8; i++) {
+      if (!std::getline(f, line)) { *err = "modpara.def: truncated header"; return -1; }
+      std::istringstream ss(line);
+      std::string kw, v;
+      if (i == 5 && (ss >> kw >> v)) m->data_head = v;
+      if (i == 6 && (ss >> kw >> v)) m->para_head = v;
+    }
+    while (std::getline(f, line)) {
+      std::istringstream ss(line);
+      std::string kw;
+      double v = 0.0;
+      if (!(ss >> kw)) continue;
+      if (!(ss >> v)) { *err = "modpara.def: malformed line: " + line; return -1; }
+      const std::string k = lower(kw);
+      if (k == "nsite") m->nsite = (int)v;
+      else if (k == "nup") m->nup = (int)v;
+      else if (k == "ndown") { m->ndown = (int)v; m->total_2sz = m->nup - m->ndown; }
+      else if (k == "2sz") { m->total_2sz = (int)v; m->sz_conserved = true; }
+      else if (k == "ncond") {
+        if ((int)v < 0) { *err = "modpara.def: Ncond must be non-negative"; return -1; }
+        m->ncond = (int)v; m->read_ncond = true;
+      }
+      else if (k == "lanczos_max") m->lanczos_max = (int)v;
+      else if (k == "initial_iv") m->initial_iv = (int)v;
+      else if (k == "nvec") m->nvec = (int)v;
+      else if (k == "exct") m->k_exct = (int)v;
+      else if (k == "lanczoseps") m->lanczos_eps = (int)v;
+      else if (k == "lanczostarget") m->lanczos_target = (int)v;
+      else if (k == "largevalue") m->large_value = v;
+      else if (k == "numave") m->num_ave = (int)v;
+      else if (k == "expecinterval") m->expec_interval = (int)v;
+      else if (k == "calchs") m->read_hacker = (int)v;
+      else if (k == "timeslice" || k == "expandcoef" || k == "outputinterval" || k == "tinit" ||
+               k == "omegamax" || k == "omegamin" || k == "omegaim" || k == "omegaorg" || k == "nomega" ||
+               k == "targettpqrand" || k == "precg") {
+        // accepted and ignored: parameters of modes outside this engine
+      } else {
+        *err = "modpara.def: unknown keyword " + kw;
+        return -1;
+      }
+    }
+  }
+  // ---- locspn.def
+  {
+    std::ifstream f;
+    if (!open_def(*m, files["locspin"], &f)) { *err = "cannot open " + files["locspin"]; return -1; }
+    for (int i = 0; i < 5; i++) {
+      if (!std::getline(f, line)) { *err = "locspn.def: truncated header"; return -1; }
+      if (i == 1) {
+        std::istringstream ss(line);
+        std::string kw;
+        ss >> kw >> m->nlocspn;
+      }
+    }
+    if (m->nsite <= 0) { *err = "modpara.def: Nsite must be positive"; return -1; }
+    m->locspn.assign(m->nsite, -1);
+    int idx = 0;
+    while (std::getline(f, line)) {
+      std::istringstream ss(line);
+      int i, s;
+      if (!(ss >> i >> s)) continue;
+      if (idx == m->nsite || i < 0 || i >= m->nsite) { *err = "locspn.def: bad site index"; return -1; }
+      m->locspn[i] = s;
+      idx++;
+    }
+    for (int i = 0; i < m->nsite; i++)
+      if (m->locspn[i] < 0) { *err = "locspn.def: missing site"; return -1; }
+    for (int i = 0; i < m->nsite; i++) {
+      if (m->is_spin() && m->locspn[i] != 1) {
+        *err = "locspn.def: only S=1/2 spins (2S=1) are supported by this engine";
+        return -1;
+      }
+      if ((m->calc_model == kHubbard || m->calc_model == kHubbardGC) && m->locspn[i] != 0) {
+        *err = "locspn.def: Hubbard models need itinerant sites (0)";
+        return -1;
+      }
+    }
+  }
+  // ---- sector parameters (src/readdef.c:880-960)
+  switch (m->calc_model) {
+    case kSpin: case kHubbard: case kKondo:
+      if (m->read_ncond) {
+        if (m->calc_model == kSpin) { *err = "modpara.def: Ncond is not allowed for Spin"; return -1; }
+        if (m->sz_conserved) {
+          m->nup = (m->nlocspn + m->ncond + m->total_2sz) / 2;
+          m->ndown = (m->nlocspn + m->ncond - m->total_2sz) / 2;
+        } else if (m->calc_model == kHubbard) {
+          m->ne = m->ncond;
+          if (m->ne < 1) { *err = "modpara.def: Ncond must be positive"; return -1; }
+          m->calc_model = kHubbardNConserved;
+        } else {
+          *err = "modpara.def: Kondo needs 2Sz"; return -1;
+        }
+      } else if (m->sz_conserved) {
+        if (m->calc_model != kSpin) { *err = "modpara.def: Ncond is required"; return -1; }
+        m->nup = (m->nlocspn + m->total_2sz) / 2;
+        m->ndown = (m->nlocspn - m->total_2sz) / 2;
+      } else if (m->nup == 0 && m->ndown == 0) {
+        *err = "modpara.def: sector (2Sz / Ncond / Nup, Ndown) is not given"; return -1;
+      }
+      if (m->calc_model == kSpin) m->ne = m->nup;
+      else if (m->ne == 0) m->ne = m->nup + m->ndown;
+      break;
+    default:
+      break;
+  }
+  if (m->lanczos_max <= 0) { *err = "modpara.def: Lanczos_max must be positive"; return -1; }
+  if (m->lanczos_eps <= 0) { *err = "modpara.def: LanczosEps must be positive"; return -1; }
+  if (m->num_ave <= 0) { *err = "modpara.def: NumAve must be positive"; return -1; }
+  if (m->expec_interval <= 0) { *err = "modpara.def: ExpecInterval must be positive"; return -1; }
+  if (m->nvec == 0) m->nvec = m->lanczos_max;
+  if (m->nvec < m->k_exct) m->nvec = m->k_exct;
+  if (m->lanczos_target < m->k_exct) m->lanczos_target = m->k_exct;
+  if (m->k_exct < 1 || m->k_exct > m->nvec) { *err = "modpara.def: exct out of range"; return -1; }
+  if (m->calc_model == kKondo || m->calc_model == kKondoGC) {
+    *err = "Kondo models are not supported by this engine yet";
+    return -1;
+  }
+  const bool spin = m->is_spin();
+  m->nbits = spin ? m->nsite : 2 * m->nsite;
+  if (m->nbits > 64) { *err = "too many sites for 64-bit configurations"; return -1; }
+
+  auto fbit = [&](int site, int s) { return 2 * site + s; };
+  auto check_site = [&](int i) { return i >= 0 && i < m->nsite; };
+  std::vector<std::vector<double>> rows;
+
+  // ---- Trans
+  if (files.count("trans")) {
+    if (!read_table(*m, files["trans"], &rows, 6, err)) return -1;
+    // Merge duplicates (src/readdef.c:1139-1156), then check Hermiticity (CheckTransferHermite).
+    std::map<std::tuple<int, int, int, int>, std::complex<double>> tr;
+    std::vector<std::tuple<int, int, int, int>> order;
+    for (const auto &r : rows) {
+      const int i = (int)r[0], s1 = (int)r[1], j = (int)r[2], s2 = (int)r[3];
+      if (!check_site(i) || !check_site(j) || s1 < 0 || s1 > 1 || s2 < 0 || s2 > 1) {
+        *err = files["trans"] + ": bad site or spin index"; return -1;
+      }
+      if (i == j && s1 == s2 && std::fabs(r[5]) > 1e-12) {
+        *err = files["trans"] + ": diagonal transfer with an imaginary part"; return -1;
+      }
+      if (m->calc_model == kSpin && i != j) { *err = files["trans"] + ": Spin needs site-diagonal transfers"; return -1; }
+      if (m->calc_model == kSpinGC && i != j) { *err = files["trans"] + ": SpinGC needs site-diagonal transfers"; return -1; }
+      auto key = std::make_tuple(i, s1, j, s2);
+      if (!tr.count(key)) order.push_back(key);
+      tr[key] += std::complex<double>(r[4], r[5]);
+    }
+    for (const auto &key : order) {
+      int i, s1, j, s2;
+      std::tie(i, s1, j, s2) = key;
+      if (i == j && s1 == s2) continue;
+      auto it = tr.find(std::make_tuple(j, s2, i, s1));
+      if (it == tr.end() || std::abs(it->second - std::conj(tr[key])) > 1e-12) {
+        *err = files["trans"] + ": transfer integrals are not Hermitian"; return -1;
+      }
+    }
+    for (const auto &key : order) {
+      int i, s1, j, s2;
+      std::tie(i, s1, j, s2) = key;
+      const std::complex<double> t = tr[key];
+      if (spin) add_spin_string(m, {{i, s1, s2}}, -t);
+      else add_fermion_string(m, {{fbit(i, s1), true}, {fbit(j, s2), false}}, -t);
+    }
+    m->n_trans = (int)rows.size();
+  }
+  // ---- CoulombIntra
+  if (files.count("coulombintra")) {
+    if (!read_table(*m, files["coulombintra"], &rows, 2, err)) return -1;
+    for (const auto &r : rows) {
+      const int i = (int)r[0];
+      if (!check_site(i)) { *err = files["coulombintra"] + ": bad site"; return -1; }
+      if (!spin) {
+        const uint64_t msk = (1ull << fbit(i, 0)) | (1ull << fbit(i, 1));
+        m->diag.push_back(DiagTerm{msk, msk, r[1]});
+      }
+    }
+    m->n_coulomb_intra = (int)rows.size();
+  }
+  auto add_inter = [&](int i, int j, double V) {
+    if (spin) { m->diag.push_back(DiagTerm{0, 0, V}); return; }
+    for (int a = 0; a < 2; a++)
+      for (int b = 0; b < 2; b++) {
+        const uint64_t msk = (1ull << fbit(i, a)) | (1ull << fbit(j, b));
+        m->diag.push_back(DiagTerm{msk, msk, V});
+      }
+  };
+  auto add_hund = [&](int i, int j, double J) {  // H += -J (n_i0 n_j0 + n_i1 n_j1)
+    if (spin) {
+      const uint64_t msk = (1ull << i) | (1ull << j);
+      m->diag.push_back(DiagTerm{msk, msk, -J});
+      m->diag.push_back(DiagTerm{msk, 0, -J});
+      return;
+    }
+    for (int a = 0; a < 2; a++) {
+      const uint64_t msk = (1ull << fbit(i, a)) | (1ull << fbit(j, a));
+      m->diag.push_back(DiagTerm{msk, msk, -J});
+    }
+  };
+  // ---- CoulombInter
+  if (files.count("coulombinter")) {
+    if (!read_table(*m, files["coulombinter"], &rows, 3, err)) return -1;
+    for (const auto &r : rows) {
+      if (!check_site((int)r[0]) || !check_site((int)r[1])) { *err = files["coulombinter"] + ": bad site"; return -1; }
+      add_inter((int)r[0], (int)r[1], r[2]);
+    }
+    m->n_coulomb_inter = (int)rows.size();
+  }
+  // ---- Hund
+  if (files.count("hund")) {
+    if (!read_table(*m, files["hund"], &rows, 3, err)) return -1;
+    for (const auto &r : rows) {
+      if (!check_site((int)r[0]) || !check_site((int)r[1])) { *err = files["hund"] + ": bad site"; return -1; }
+      add_hund((int)r[0], (int)r[1], r[2]);
+    }
+    m->n_hund = (int)rows.size();
+  }
+  // ---- Ising: Hund(-J/2) + CoulombInter(-J/4)
+  if (files.count("ising")) {
+    if (!read_table(*m, files["ising"], &rows, 3, err)) return -1;
+    for (const auto &r : rows) {
+      if (!check_site((int)r[0]) || !check_site((int)r[1])) { *err = files["ising"] + ": bad site"; return -1; }
+      add_hund((int)r[0], (int)r[1], -r[2] / 2.0);
+      add_inter((int)r[0], (int)r[1], -r[2] / 4.0);
+    }
+    m->n_ising = (int)rows.size();
+  }
+  // ---- Exchange
+  if (files.count("exchange")) {
+    if (!read_table(*m, files["exchange"], &rows, 3, err)) return -1;
+    for (const auto &r : rows) {
+      const int i = (int)r[0], j = (int)r[1];
+      if (!check_site(i) || !check_site(j)) { *err = files["exchange"] + ": bad site"; return -1; }
+      if (i == j) continue;
+      const std::complex<double> J(r[2], 0.0);
+      if (spin) {
+        add_spin_string(m, {{i, 1, 0}, {j, 0, 1}}, J);
+        add_spin_string(m, {{i, 0, 1}, {j, 1, 0}}, J);
+      } else {
+        add_fermion_string(m, {{fbit(i, 0), true}, {fbit(j, 0), false}, {fbit(j, 1), true}, {fbit(i, 1), false}}, J);
+        add_fermion_string(m, {{fbit(j, 0), true}, {fbit(i, 0), false}, {fbit(i, 1), true}, {fbit(j, 1), false}}, J);
+      }
+    }
+    m->n_exchange = (int)rows.size();
+  }
+  // ---- PairHop
+  if (files.count("pairhop")) {
+    if (spin) { *err = "PairHop is not active in Spin and SpinGC"; return -1; }
+    if (!read_table(*m, files["pairhop"], &rows, 3, err)) return -1;
+    for (const auto &r : rows) {
+      const int i = (int)r[0], j = (int)r[1];
+      if (!check_site(i) || !check_site(j)) { *err = files["pairhop"] + ": bad site"; return -1; }
+      if (i == j) continue;
+      const std::complex<double> J(r[2], 0.0);
+      add_fermion_string(m, {{fbit(i, 0), true}, {fbit(j, 0), false}, {fbit(i, 1), true}, {fbit(j, 1), false}}, J);
+      add_fermion_string(m, {{fbit(j, 0), true}, {fbit(i, 0), false}, {fbit(j, 1), true}, {fbit(i, 1), false}}, J);
+    }
+    m->n_pairhop = (int)rows.size();
+  }
+  // ---- PairLift
+  if (files.count("pairlift")) {
+    if (!read_table(*m, files["pairlift"], &rows, 3, err)) return -1;
+    if (!rows.empty() && m->calc_model != kSpinGC) { *err = "PairLift is active only in SpinGC"; return -1; }
+    for (const auto &r : rows) {
+      const int i = (int)r[0], j = (int)r[1];
+      if (!check_site(i) || !check_site(j)) { *err = files["pairlift"] + ": bad site"; return -1; }
+      if (i == j) continue;
+      const std::complex<double> J(r[2], 0.0);
+      add_spin_string(m, {{i, 1, 0}, {j, 1, 0}}, J);
+      add_spin_string(m, {{i, 0, 1}, {j, 0, 1}}, J);
+    }
+    m->n_pairlift = (int)rows.size();
+  }
+  // ---- InterAll
+  if (files.count("interall")) {
+    if (!read_table(*m, files["interall"], &rows, 10, err)) return -1;
+    for (const auto &r : rows) {
+      int s[4], g[4];
+      for (int q = 0; q < 4; q++) { s[q] = (int)r[2 * q]; g[q] = (int)r[2 * q + 1]; }
+      for (int q = 0; q < 4; q++)
+        if (!check_site(s[q]) || g[q] < 0 || g[q] > 1) { *err = files["interall"] + ": bad index"; return -1; }
+      const std::complex<double> V(r[8], r[9]);
+      if (spin) {
+        if (s[0] != s[1] || s[2] != s[3]) {
+          *err = files["interall"] + ": spin InterAll needs i==j and k==l"; return -1;
+        }
+        add_spin_string(m, {{s[0], g[0], g[1]}, {s[2], g[2], g[3]}}, V);
+      } else {
+        add_fermion_string(m, {{fbit(s[0], g[0]), true}, {fbit(s[1], g[1]), false},
+                               {fbit(s[2], g[2]), true}, {fbit(s[3], g[3]), false}}, V);
+      }
+    }
+    m->n_interall = (int)rows.size();
+  }
+  canonicalize_terms(m);
+  return 0;
+}
+
+}  // namespace hphi

@@ -1,0 +1,90 @@
+// Host-side model description: HPhi expert-mode input compiled to bit-operator terms.
+//
+// Every Hamiltonian term that HPhi reads from its expert-mode .def files (Trans,
+// CoulombIntra, CoulombInter, Hund, Ising, Exchange, PairHop, PairLift, InterAll;
+// reader in src/readdef.c:1006-2059) is an operator string acting on the occupation
+// bits of a configuration.  On a basis configuration c such a string either gives
+// zero or a single configuration c ^ flip with a coefficient whose sign is
+// (-1)^popcount(c & sign_mask) times a constant.  That closed form is what the GPU
+// kernels evaluate; it reproduces the per-term element routines of
+// src/mltplyHubbardCore.c and src/mltplySpinCore.c (masks from the *_GetInfo
+// functions, fermion signs from SgnBit, src/bitcalc.c:338-352).
+#pragma once
+#include <complex>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace hphi {
+
+// CalcModel values of calcmod.def (include/DefCommon.h:21-39).  HubbardNConserved is
+// the internal model HPhi switches to when Hubbard is given Ncond without 2Sz
+// (src/readdef.c:905-912).
+enum CalcModel : int {
+  kHubbard = 0, kSpin = 1, kKondo = 2, kHubbardGC = 3, kSpinGC = 4, kKondoGC = 5,
+  kHubbardNConserved = 6
+};
+// CalcType values (include/DefCommon.h).
+enum CalcType : int { kLanczos = 0, kTPQ = 1, kFullDiag = 2, kCG = 3, kTimeEvolution = 4, kcTPQ = 5 };
+
+// Off-diagonal term in gather ("pull") form, for an output configuration t:
+//   applies iff (t & cm) == cv; source configuration s = t ^ flip;
+//   contribution = (re + i im) * (-1)^popcount(t & sm) * v[index(s)].
+struct BitTerm {
+  uint64_t cm, cv, flip, sm;
+  double re, im;
+};
+
+// Diagonal projector term: adds v iff (c & cm) == cv.
+struct DiagTerm {
+  uint64_t cm, cv;
+  double v;
+};
+
+struct Model {
+  // calcmod.def
+  int calc_type = 0, calc_model = 0, output_mode = 0, calc_eigenvec = 0, initial_vec_type = 0;
+  int output_eigenvec = 0, input_eigenvec = 0, restart = 0, flg_finite_temperature = 0;
+  // modpara.def
+  int nsite = 0, nup = 0, ndown = 0, ne = 0, total_2sz = 0, ncond = 0;
+  bool sz_conserved = false, read_ncond = false;
+  int lanczos_max = 0, initial_iv = 0, nvec = 0, k_exct = 0, lanczos_eps = 0, lanczos_target = 0;
+  int num_ave = 1, expec_interval = 1, read_hacker = 1;
+  double large_value = 0.0;
+  std::string data_head = "zvo", para_head = "zqp";
+  // locspn.def
+  int nlocspn = 0;
+  std::vector<int> locspn;
+  // Compiled Hamiltonian.
+  std::vector<BitTerm> offdiag;
+  std::vector<DiagTerm> diag;
+  bool complex_terms = false;   // any off-diagonal coefficient with a non-zero imaginary part
+  int nbits = 0;                // configuration bits: 2*Nsite (Hubbard/Kondo) or Nsite (spin)
+  // Raw term counts as read (for logs).
+  int n_trans = 0, n_coulomb_intra = 0, n_coulomb_inter = 0, n_hund = 0, n_exchange = 0;
+  int n_ising = 0, n_pairhop = 0, n_pairlift = 0, n_interall = 0;
+  std::string base_dir;
+
+  bool is_gc() const {
+    return calc_model == kHubbardGC || calc_model == kSpinGC || calc_model == kKondoGC;
+  }
+  bool is_spin() const { return calc_model == kSpin || calc_model == kSpinGC; }
+};
+
+// Reads namelist.def and every file it names (expert mode).  Returns 0 on success,
+// -1 with a message in *err otherwise.  Mirrors ReadDefFileNInt / ReadDefFileIdxPara
+// (src/readdef.c:463, 1006) for the keywords this engine supports.
+int read_expert(const std::string &namelist, Model *m, std::string *err);
+
+// Adds a literal operator string to the compiled model.  Fermion strings are lists
+// of (bit, dagger) applied right to left; spin strings are lists of (site, to, from)
+// single-site transitions |to><from|.  Returns false for an identically-zero string.
+struct FermionOp { int bit; bool dag; };
+struct SpinOp { int site, to, from; };
+bool add_fermion_string(Model *m, const std::vector<FermionOp> &ops, std::complex<double> coef);
+bool add_spin_string(Model *m, const std::vector<SpinOp> &ops, std::complex<double> coef);
+
+// Merges duplicate terms (same masks) by adding their coefficients, drops zeros.
+void canonicalize_terms(Model *m);
+
+}  // namespace hphi

@@ -1,0 +1,314 @@
+// Sector enumeration and diagonal on the device.
+//
+// Replaces sz() (src/sz.c:62-832, hacker paths omp_sz_hacker :993-1094 and
+// omp_sz_spin_hacker :1495-1546) and diagonalcalc() (src/diagonalcalc.c:84-187).
+//
+// HPhi orders the canonical sector by upper half ib (bits >= lo_bits) and, inside
+// a block, by increasing lower half ia.  Which ia are allowed depends only on the
+// particle-number class of ib, so
+//   list_2_1[ia] = rank of ia among lower halves of its class + 2   (0 if the class
+//                  is never needed by any ib),
+//   list_2_2[ib] = (number of rows in blocks before ib) + 1          (0 for empty blocks),
+//   list_1[jb + ja] = unrank(class, ja) | ib << lo_bits.
+// The serial list_jb prefix loop of the reference becomes a device scan; the per-block
+// snoob enumeration becomes a gather from a per-class unrank table.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "engine.hpp"
+
+namespace hphi {
+namespace {
+
+#define CK(call)                                                                  \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      *err = std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #call; \
+      return -1;                                                                  \
+    }                                                                             \
+  } while (0)
+
+__constant__ uint64_t c_binom[65][65];
+
+// Class of a half configuration: (n_even, n_odd) by global bit parity for Hubbard
+// (even bit = up, src/sz.c:1006-1015), popcount otherwise.  class id = a*(D+1)+b.
+__device__ __forceinline__ void half_counts(uint64_t x, int offset, int hubbard, int *a, int *b) {
+  if (!hubbard) { *a = __popcll(x); *b = 0; return; }
+  // global position offset + p is even (up) iff p has the parity of offset.
+  const uint64_t even_local = (offset & 1) ? 0xAAAAAAAAAAAAAAAAull : 0x5555555555555555ull;
+  *a = __popcll(x & even_local);
+  *b = __popcll(x & ~even_local);
+}
+
+// Rank of x among half configurations of the same class (increasing order).
+__device__ uint64_t half_rank(uint64_t x, int nbits, int offset, int hubbard) {
+  const uint64_t even_local = (offset & 1) ? 0xAAAAAAAAAAAAAAAAull : 0x5555555555555555ull;
+  uint64_t r = 0;
+  int need_a = 0, need_b = 0;  // class counts of x restricted to positions <= p
+  // walk from low to high so that need_* are the counts at and below p
+  for (int p = 0; p < nbits; p++) {
+    const uint64_t bit = 1ull << p;
+    const bool is_a = !hubbard || (even_local & bit);
+    if (x & bit) {
+      if (is_a) need_a++; else need_b++;
+      const uint64_t below = bit - 1;
+      int na, nb;
+      if (!hubbard) { na = p; nb = 0; }
+      else { na = __popcll(below & even_local); nb = __popcll(below & ~even_local); }
+      if (need_a <= na && need_b <= nb) r += c_binom[na][need_a] * c_binom[nb][need_b];
+    }
+  }
+  return r;
+}
+
+__global__ void lo_tables_kernel(uint64_t ihfbit, int lo_bits, int hubbard, int D,
+                                 const unsigned char *__restrict__ valid_cls,
+                                 const uint64_t *__restrict__ cls_off, uint32_t *__restrict__ list_2_1,
+                                 uint32_t *__restrict__ unrank) {
+  const uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (x >= ihfbit) return;
+  int a, b;
+  half_counts(x, 0, hubbard, &a, &b);
+  const int cls = a * (D + 1) + b;
+  const uint64_t r = half_rank(x, lo_bits, 0, hubbard);
+  list_2_1[x] = valid_cls[cls] ? (uint32_t)(r + 2) : 0u;
+  unrank[cls_off[cls] + r] = (uint32_t)x;
+}
+
+__global__ void hi_count_kernel(uint64_t sdim, int lo_bits, int hubbard, int D_lo, int ta, int tb,
+                                const uint64_t *__restrict__ cls_cnt, int max_a, int max_b,
+                                uint64_t *__restrict__ cnt, int *__restrict__ need) {
+  const uint64_t ib = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (ib >= sdim) return;
+  int a, b;
+  half_counts(ib, lo_bits, hubbard, &a, &b);
+  const int na = ta - a, nb = tb - b;
+  if (na < 0 || nb < 0 || na > max_a || nb > max_b) { cnt[ib] = 0; need[ib] = -1; return; }
+  const int cls = na * (D_lo + 1) + nb;
+  cnt[ib] = cls_cnt[cls];
+  need[ib] = cls;
+}
+
+// Exclusive scan of cnt into jb (single block, deterministic), total into *total.
+__global__ void scan_kernel(uint64_t n, const uint64_t *__restrict__ cnt, uint64_t *__restrict__ jb,
+                            uint64_t *__restrict__ total) {
+  __shared__ uint64_t warp_sums[32];
+  __shared__ uint64_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (uint64_t base = 0; base < n; base += blockDim.x) {
+    const uint64_t i = base + threadIdx.x;
+    const uint64_t v = (i < n) ? cnt[i] : 0;
+    uint64_t incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sums[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      const int nw = blockDim.x >> 5;
+      uint64_t w = (lane < nw) ? warp_sums[lane] : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t t = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += t;
+      }
+      if (lane < nw) warp_sums[lane] = w;
+    }
+    __syncthreads();
+    const uint64_t warp_prefix = (wid > 0) ? warp_sums[wid - 1] : 0;
+    if (i < n) jb[i] = carry + warp_prefix + incl - v;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry += warp_prefix + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void list_2_2_kernel(uint64_t sdim, const uint64_t *__restrict__ cnt, const uint64_t *__restrict__ jb,
+                                uint32_t *__restrict__ list_2_2) {
+  const uint64_t ib = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (ib >= sdim) return;
+  list_2_2[ib] = cnt[ib] ? (uint32_t)(jb[ib] + 1) : 0u;
+}
+
+// One block per upper half ib (grid-strided), threads over the block's rows.
+__global__ void list_1_kernel(uint64_t sdim, int lo_bits, const uint64_t *__restrict__ cnt,
+                              const uint64_t *__restrict__ jb, const int *__restrict__ need,
+                              const uint64_t *__restrict__ cls_off, const uint32_t *__restrict__ unrank,
+                              uint64_t *__restrict__ list_1) {
+  for (uint64_t ib = blockIdx.x; ib < sdim; ib += gridDim.x) {
+    const uint64_t n = cnt[ib];
+    if (!n) continue;
+    const uint64_t base = jb[ib];
+    const uint32_t *u = unrank + cls_off[need[ib]];
+    const uint64_t hi = ib << lo_bits;
+    for (uint64_t ja = threadIdx.x; ja < n; ja += blockDim.x) list_1[base + ja] = (uint64_t)u[ja] | hi;
+  }
+}
+
+__global__ void diag_kernel(int64_t dim, int gc, const uint64_t *__restrict__ list_1,
+                            const DiagTerm *__restrict__ terms, int nterms, double *__restrict__ diag) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < dim; r += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = gc ? (uint64_t)r : list_1[r];
+    double d = 0.0;
+    for (int k = 0; k < nterms; k++) {
+      const DiagTerm t = terms[k];
+      if ((c & t.cm) == t.cv) d += t.v;
+    }
+    diag[r] = d;
+  }
+}
+
+uint64_t binom_host(int n, int k) {
+  if (k < 0 || n < 0 || k > n) return 0;
+  uint64_t r = 1;
+  for (int i = 1; i <= k; i++) r = r * (uint64_t)(n - k + i) / (uint64_t)i;
+  return r;
+}
+
+}  // namespace
+
+int sector_build(const Model &m, int device, Sector **out, std::string *err) {
+  CK(cudaSetDevice(device));
+  Sector *s = new Sector();
+  s->model = m;
+  s->device = device;
+  CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  int nsm = 0;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  s->num_sms = nsm;
+  s->red_blocks = nsm * 8;
+  CK(cudaMalloc(&s->d_red, sizeof(double) * 8 * (size_t)s->red_blocks));
+  CK(cudaMalloc(&s->d_scal, sizeof(double) * 64));
+
+  const int nbits = m.nbits;
+  s->gc = m.is_gc();
+  // GetSplitBit (src/bitcalc.c:45-62): ihfbit = 2^((Nbits+1)/2).
+  s->lo_bits = (nbits + 1) / 2;
+  s->hi_bits = nbits - s->lo_bits;
+  s->ihfbit = 1ull << s->lo_bits;
+  s->sdim = 1ull << s->hi_bits;
+  // HPhi's list_2_* allocation sizes (GetlistSize, src/xsetmem.c:284-318).
+  s->size_list_2_2 = (int64_t)s->sdim + 2;
+  s->size_list_2_1 = (int64_t)s->ihfbit + 2;
+
+  if (s->gc) {
+    s->dim = (int64_t)(1ull << nbits);
+  } else {
+    const int hubbard = (m.calc_model == kHubbard) ? 1 : 0;
+    // Targets and class geometry.
+    int ta, tb, Dlo, Dhi, Alo, Ahi;
+    if (hubbard) {
+      ta = m.nup; tb = m.ndown;
+      Alo = (s->lo_bits + 1) / 2; Dlo = s->lo_bits / 2;  // lo half starts at an even position
+      const int off_odd = s->lo_bits & 1;
+      Ahi = off_odd ? s->hi_bits / 2 : (s->hi_bits + 1) / 2;
+      Dhi = s->hi_bits - Ahi;
+    } else {
+      ta = m.ne; tb = 0;
+      Alo = s->lo_bits; Dlo = 0; Ahi = s->hi_bits; Dhi = 0;
+    }
+    (void)Dhi; (void)Ahi;
+    const int ncls = (Alo + 1) * (Dlo + 1);
+    std::vector<uint64_t> cls_cnt(ncls), cls_off(ncls + 1, 0);
+    for (int a = 0; a <= Alo; a++)
+      for (int b = 0; b <= Dlo; b++) cls_cnt[a * (Dlo + 1) + b] = binom_host(Alo, a) * binom_host(Dlo, b);
+    for (int c = 0; c < ncls; c++) cls_off[c + 1] = cls_off[c] + cls_cnt[c];
+    // A lower-half class is used iff some upper half needs it.
+    std::vector<unsigned char> valid(ncls, 0);
+    for (int a = 0; a <= Ahi; a++)
+      for (int b = 0; b <= Dhi; b++) {
+        const int na = ta - a, nb = tb - b;
+        if (na < 0 || nb < 0 || na > Alo || nb > Dlo) continue;
+        if (!hubbard && b != 0) continue;
+        valid[na * (Dlo + 1) + nb] = 1;
+      }
+    std::vector<uint64_t> binom(65 * 65, 0);
+    for (int n = 0; n <= 64; n++)
+      for (int k = 0; k <= n; k++) binom[n * 65 + k] = binom_host(n, k);
+    CK(cudaMemcpyToSymbol(c_binom, binom.data(), sizeof(uint64_t) * 65 * 65));
+
+    unsigned char *d_valid;
+    uint64_t *d_cls_off, *d_cls_cnt, *d_cnt, *d_jb, *d_total;
+    uint32_t *d_unrank;
+    int *d_need;
+    CK(cudaMalloc(&d_valid, ncls));
+    CK(cudaMalloc(&d_cls_off, sizeof(uint64_t) * (ncls + 1)));
+    CK(cudaMalloc(&d_cls_cnt, sizeof(uint64_t) * ncls));
+    CK(cudaMalloc(&d_unrank, sizeof(uint32_t) * s->ihfbit));
+    CK(cudaMalloc(&d_cnt, sizeof(uint64_t) * s->sdim));
+    CK(cudaMalloc(&d_jb, sizeof(uint64_t) * s->sdim));
+    CK(cudaMalloc(&d_total, sizeof(uint64_t)));
+    CK(cudaMalloc(&d_need, sizeof(int) * s->sdim));
+    CK(cudaMalloc(&s->d_list_2_1, sizeof(uint32_t) * s->ihfbit));
+    CK(cudaMalloc(&s->d_list_2_2, sizeof(uint32_t) * s->sdim));
+    CK(cudaMemcpyAsync(d_valid, valid.data(), ncls, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(d_cls_off, cls_off.data(), sizeof(uint64_t) * (ncls + 1), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(d_cls_cnt, cls_cnt.data(), sizeof(uint64_t) * ncls, cudaMemcpyHostToDevice, s->stream));
+    const int T = 256;
+    lo_tables_kernel<<<(unsigned)((s->ihfbit + T - 1) / T), T, 0, s->stream>>>(
+        s->ihfbit, s->lo_bits, hubbard, Dlo, d_valid, d_cls_off, s->d_list_2_1, d_unrank);
+    hi_count_kernel<<<(unsigned)((s->sdim + T - 1) / T), T, 0, s->stream>>>(
+        s->sdim, s->lo_bits, hubbard, Dlo, ta, tb, d_cls_cnt, Alo, Dlo, d_cnt, d_need);
+    scan_kernel<<<1, 1024, 0, s->stream>>>(s->sdim, d_cnt, d_jb, d_total);
+    list_2_2_kernel<<<(unsigned)((s->sdim + T - 1) / T), T, 0, s->stream>>>(s->sdim, d_cnt, d_jb, s->d_list_2_2);
+    CK(cudaGetLastError());
+    uint64_t total = 0;
+    CK(cudaMemcpyAsync(&total, d_total, sizeof(uint64_t), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->dim = (int64_t)total;
+    // idim_max from check() (src/check.c:102-150).
+    uint64_t expect;
+    if (m.calc_model == kHubbard) expect = binom_host(m.nsite, m.nup) * binom_host(m.nsite, m.ndown);
+    else if (m.calc_model == kHubbardNConserved) expect = binom_host(2 * m.nsite, m.ne);
+    else expect = binom_host(m.nsite, m.ne);
+    if (total != expect || total == 0) {
+      *err = "sector size mismatch: enumerated " + std::to_string(total) + ", expected " + std::to_string(expect);
+      return -1;
+    }
+    if (total > 0xFFFFFFF0ull) { *err = "sector too large for 32-bit list_2 tables"; return -1; }
+    CK(cudaMalloc(&s->d_list_1, sizeof(uint64_t) * total));
+    const unsigned nb = (unsigned)std::min<uint64_t>(s->sdim, (uint64_t)nsm * 64);
+    list_1_kernel<<<nb, 256, 0, s->stream>>>(s->sdim, s->lo_bits, d_cnt, d_jb, d_need, d_cls_off, d_unrank,
+                                             s->d_list_1);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s->stream));
+    cudaFree(d_valid); cudaFree(d_cls_off); cudaFree(d_cls_cnt); cudaFree(d_unrank);
+    cudaFree(d_cnt); cudaFree(d_jb); cudaFree(d_total); cudaFree(d_need);
+  }
+
+  // Terms.
+  s->nterms = (int)m.offdiag.size();
+  s->ndterms = (int)m.diag.size();
+  if (s->nterms) {
+    CK(cudaMalloc(&s->d_terms, sizeof(BitTerm) * s->nterms));
+    CK(cudaMemcpyAsync(s->d_terms, m.offdiag.data(), sizeof(BitTerm) * s->nterms, cudaMemcpyHostToDevice, s->stream));
+  }
+  if (s->ndterms) {
+    CK(cudaMalloc(&s->d_dterms, sizeof(DiagTerm) * s->ndterms));
+    CK(cudaMemcpyAsync(s->d_dterms, m.diag.data(), sizeof(DiagTerm) * s->ndterms, cudaMemcpyHostToDevice, s->stream));
+  }
+  CK(cudaMalloc(&s->d_diag, sizeof(double) * (size_t)s->dim));
+  diag_kernel<<<nsm * 8, 256, 0, s->stream>>>(s->dim, s->gc ? 1 : 0, s->d_list_1, s->d_dterms, s->ndterms, s->d_diag);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s->stream));
+  *out = s;
+  return 0;
+}
+
+void sector_free(Sector *s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  cudaFree(s->d_list_1); cudaFree(s->d_list_2_1); cudaFree(s->d_list_2_2); cudaFree(s->d_diag);
+  cudaFree(s->d_terms); cudaFree(s->d_dterms); cudaFree(s->d_red); cudaFree(s->d_scal);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+}  // namespace hphi

@@ -1,0 +1,133 @@
+/*
+ * hphi_b200 - C-ABI of the B200 engine for HPhi's H*v / Lanczos / TPQ path.
+ *
+ * Plain C types only.  Complex vectors on the host use HPhi's layout: an array of
+ * (dim + 1) complex128 values stored as interleaved (re, im) doubles, element 0 unused
+ * (src/include/global.h:34-50, src/xsetmem.c:178-193); this is layout-compatible with
+ * C99 `double complex v[dim + 1]`.  Device vectors are 0-based arrays of dim elements
+ * of the given element type.
+ *
+ * Every entry point returns 0 on success and -1 on failure; hphi_last_error() then
+ * returns a message (per thread).  Nothing here calls exit().
+ */
+#ifndef HPHI_B200_H
+#define HPHI_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hphi_handle hphi_handle;
+
+/* Element types of device vectors. */
+#define HPHI_REAL64 0      /* double */
+#define HPHI_COMPLEX128 1  /* interleaved (re, im) doubles */
+
+/* Indices into the info array of hphi_info(). */
+#define HPHI_INFO_DIM 0          /* idim_max (src/check.c:51-209) */
+#define HPHI_INFO_NSITE 1
+#define HPHI_INFO_CALC_MODEL 2   /* CalcModel; 6 = Hubbard with Ncond only (HubbardNConserved) */
+#define HPHI_INFO_CALC_TYPE 3
+#define HPHI_INFO_SIZE_LIST_2_1 4 /* X->Large.SizeOflist_2_1 (src/xsetmem.c:284-318) */
+#define HPHI_INFO_SIZE_LIST_2_2 5 /* X->Large.SizeOflist_2_2 */
+#define HPHI_INFO_IS_GC 6
+#define HPHI_INFO_VEC_TYPE 7     /* element type the drivers use for this input */
+#define HPHI_INFO_N_OFFDIAG 8    /* compiled off-diagonal terms */
+#define HPHI_INFO_N_DIAG 9       /* compiled diagonal projector terms */
+#define HPHI_INFO_LANCZOS_MAX 10
+#define HPHI_INFO_NUM_AVE 11
+#define HPHI_INFO_COUNT 12
+
+/* Library version string. */
+const char *hphi_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *hphi_last_error(void);
+
+/*
+ * Reads an expert-mode input (namelist.def and the files it names) and builds the
+ * sector and diagonal on CUDA device `device`.
+ * Replaces: ReadDefFileNInt + ReadDefFileIdxPara (src/readdef.c:463, 1006), check
+ * (src/check.c:51), setmem_large (src/xsetmem.c:153), sz (src/sz.c:62) and
+ * diagonalcalc (src/diagonalcalc.c:84), as called from main (src/HPhiMain.c:223-288).
+ */
+int hphi_open_expert(const char *namelist_def, int device, hphi_handle **out);
+
+/* Frees the handle and its device memory. */
+void hphi_close(hphi_handle *h);
+
+/* Fills info[0 .. min(n, HPHI_INFO_COUNT)) with the HPHI_INFO_* values. */
+int hphi_info(const hphi_handle *h, int64_t *info, int n);
+
+/*
+ * Copies the sector tables in HPhi's layout: list_1[0 .. dim] (element 0 unused),
+ * list_2_1[0 .. SizeOflist_2_1), list_2_2[0 .. SizeOflist_2_2), as filled by
+ * sz() (src/sz.c:62-832).  Any pointer may be NULL.  Fails for grand-canonical models,
+ * which have no lists.
+ */
+int hphi_sz(const hphi_handle *h, uint64_t *list_1, uint64_t *list_2_1, uint64_t *list_2_2);
+
+/* Copies list_Diagonal[0 .. dim] (element 0 unused) as diagonalcalc computes it
+ * (src/diagonalcalc.c:84-187). */
+int hphi_diagonalcalc(const hphi_handle *h, double *list_diagonal);
+
+/*
+ * v0 += H v1 on host vectors in HPhi's layout, and *prdct = <v1|H|v1> (complex, 2 doubles).
+ * Replaces: int mltply(struct BindStruct *X, double complex *v0, double complex *v1)
+ * (src/mltply.c:56-132), whose X->Large.prdct is returned in prdct.
+ */
+int hphi_mltply(hphi_handle *h, double *v0, const double *v1, double *prdct);
+
+/*
+ * Device form of mltply: d_v0 = acc * d_v0 + scale * (H d_v1) on 0-based device vectors
+ * of element type vec_type (acc == 0 never reads d_v0), and prdct (host, 2 doubles) =
+ * sum conj(d_v1) (H d_v1).  Runs on the handle's stream and waits for it.
+ * Replaces: mltply (src/mltply.c:56-132) for callers that keep vectors on the device.
+ */
+int hphi_mltply_device(hphi_handle *h, int vec_type, void *d_v0, const void *d_v1, double acc, double scale,
+                       double *prdct);
+
+/*
+ * Lanczos ground state (and, with CalcEigenVec != -1, the eigenvector, its energy and
+ * variance).  v_init: normalised start vector in HPhi's layout, or NULL for the
+ * reference's own start (single element for initial_iv > 0 on canonical models, else a
+ * seeded random vector).  Writes zvo_Lanczos_Step.dat (and zvo_energy.dat with the
+ * eigenvector) into output_dir when it is not NULL.  result (may be NULL) receives
+ *   [0] converged (1/0)  [1] steps  [2] E_target  [3] E[1]  [4] E[2]  [5] E[3]  [6] E[4]
+ *   [7] energy <v|H|v>   [8] <Hv|Hv>  [9] doublon  [10] Sz
+ * Replaces: CalcByLanczos (src/CalcByLanczos.c:55-276) with Lanczos_EigenValue
+ * (src/Lanczos_EigenValue.c:50) and Lanczos_EigenVector (src/Lanczos_EigenVector.c:46).
+ */
+int hphi_lanczos(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult);
+
+/*
+ * Lanczos eigenvector copy-out: after hphi_lanczos with CalcEigenVec != -1, copies the
+ * eigenvector (HPhi layout, dim + 1 complex128) into v.
+ */
+int hphi_lanczos_eigenvector(hphi_handle *h, double *v);
+
+/*
+ * mTPQ: NumAve samples of Lanczos_max steps each.  v_init: NumAve start vectors in HPhi's
+ * layout, back to back ((dim + 1) complex128 each; any norm), or NULL for seeded random
+ * starts.  Writes SS_rand%d.dat, Norm_rand%d.dat, Flct_rand%d.dat into output_dir.
+ * result (may be NULL) receives the energies of the last sample, one per step
+ * (nresult values at most).
+ * Replaces: CalcByTPQ (src/CalcByTPQ.c:52-294), FirstMultiply (src/FirstMultiply.c:41),
+ * Multiply (src/Multiply.c:42), expec_energy_flct (src/expec_energy_flct.c:34).
+ */
+int hphi_tpq(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult);
+
+/*
+ * The whole expert-mode run of `HPhi -e namelist.def` for CalcType 0 (Lanczos) and
+ * 1 (TPQ), writing HPhi's output files into output_dir ("output" when NULL).
+ * Replaces: main (src/HPhiMain.c:178-358) for those modes.
+ */
+int hphi_run(hphi_handle *h, const char *output_dir);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPHI_B200_H */

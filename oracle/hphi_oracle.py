@@ -1,0 +1,469 @@
+"""CPU oracle for the H*v / Lanczos / TPQ path (TEST INFRASTRUCTURE ONLY).
+
+A numpy restatement of the reference's algorithms, used by the tests and by
+bench.py's cpu_baseline leg as the checker.  The product (hphi_b200/) never imports
+this module.  Each function mirrors the reference routine it cites, structured as the
+reference is: one vectorised pass over all rows per Hamiltonian term, push form
+``v0[off(j)] += coef * sgn * v1[j]``.
+
+Its outputs are pinned against dumps of the reference itself (oracle/_ref/HPhi_ref,
+built by oracle/Makefile from the reference sources) through the fixtures in
+tests/golden/.
+"""
+from __future__ import annotations
+
+import os
+from dataclasses import dataclass, field
+from math import comb
+from typing import Dict, List, Tuple
+
+import numpy as np
+
+HUBBARD, SPIN, KONDO, HUBBARDGC, SPINGC, KONDOGC, HUBBARD_NCONS = 0, 1, 2, 3, 4, 5, 6
+
+
+# ----------------------------------------------------------------------------- input
+@dataclass
+class Def:
+    """What ReadDefFileNInt / ReadDefFileIdxPara (src/readdef.c:463, 1006) store."""
+    calc_type: int = 0
+    calc_model: int = 0
+    calc_eigenvec: int = 0
+    initial_vec_type: int = 0
+    nsite: int = 0
+    nup: int = 0
+    ndown: int = 0
+    ne: int = 0
+    total_2sz: int = 0
+    ncond: int = 0
+    nlocspn: int = 0
+    lanczos_max: int = 0
+    initial_iv: int = 0
+    k_exct: int = 1
+    lanczos_eps: int = 14
+    lanczos_target: int = 2
+    large_value: float = 0.0
+    num_ave: int = 1
+    trans: List[Tuple[int, int, int, int, complex]] = field(default_factory=list)   # off-diagonal, Hermitian pairs
+    chemi: List[Tuple[int, int, float]] = field(default_factory=list)                # (site, spin, mu): -mu n
+    coulomb_intra: List[Tuple[int, float]] = field(default_factory=list)
+    coulomb_inter: List[Tuple[int, int, float]] = field(default_factory=list)
+    hund: List[Tuple[int, int, float]] = field(default_factory=list)
+    exchange: List[Tuple[int, int, float]] = field(default_factory=list)
+    pairhop: List[Tuple[int, int, float]] = field(default_factory=list)
+    pairlift: List[Tuple[int, int, float]] = field(default_factory=list)
+    interall_diag: List[Tuple[int, int, int, int, float]] = field(default_factory=list)
+    interall_off: List[Tuple[int, int, int, int, int, int, int, int, complex]] = field(default_factory=list)
+
+
+def _table(path: str) -> List[List[float]]:
+    with open(path) as f:
+        lines = f.read().splitlines()
+    n = int(lines[1].split()[1])
+    rows = [list(map(float, l.split())) for l in lines[5:] if l.strip()]
+    return rows[:n]
+
+
+def read_expert(namelist: str) -> Def:
+    """Expert-mode reader (src/readdef.c).  Diagonal transfers become chemical terms and
+    Ising becomes Hund(-J/2) + CoulombInter(-J/4) (src/readdef.c:1320-1327); InterAll
+    terms with i=j, k=l and equal spins per pair are diagonal (GetDiagonalInterAll,
+    src/readdef.c:2415-2549), the others stay as written."""
+    base = os.path.dirname(os.path.abspath(namelist))
+    files: Dict[str, str] = {}
+    for line in open(namelist):
+        p = line.split()
+        if len(p) >= 2 and not p[0].startswith("#"):
+            files[p[0].lower()] = os.path.join(base, p[1])
+    d = Def()
+    for line in open(files["calcmod"]):
+        p = line.split()
+        if len(p) < 2 or p[0].startswith("#"):
+            continue
+        k, v = p[0].lower(), int(p[1])
+        if k == "calctype": d.calc_type = v
+        elif k == "calcmodel": d.calc_model = v
+        elif k == "calceigenvec": d.calc_eigenvec = v
+        elif k == "initialvectype": d.initial_vec_type = v
+    sz_cons, read_ncond = False, False
+    for line in open(files["modpara"]).read().splitlines()[8:]:
+        p = line.split()
+        if len(p) < 2:
+            continue
+        k, v = p[0].lower(), float(p[1])
+        if k == "nsite": d.nsite = int(v)
+        elif k == "nup": d.nup = int(v)
+        elif k == "ndown": d.ndown = int(v); d.total_2sz = d.nup - d.ndown
+        elif k == "2sz": d.total_2sz = int(v); sz_cons = True
+        elif k == "ncond": d.ncond = int(v); read_ncond = True
+        elif k == "lanczos_max": d.lanczos_max = int(v)
+        elif k == "initial_iv": d.initial_iv = int(v)
+        elif k == "exct": d.k_exct = int(v)
+        elif k == "lanczoseps": d.lanczos_eps = int(v)
+        elif k == "lanczostarget": d.lanczos_target = int(v)
+        elif k == "largevalue": d.large_value = v
+        elif k == "numave": d.num_ave = int(v)
+    d.nlocspn = int(open(files["locspin"]).read().splitlines()[1].split()[1])
+    if d.calc_model in (SPIN, HUBBARD):
+        if read_ncond:
+            if sz_cons:
+                d.nup = (d.nlocspn + d.ncond + d.total_2sz) // 2
+                d.ndown = (d.nlocspn + d.ncond - d.total_2sz) // 2
+            else:
+                d.ne = d.ncond
+                d.calc_model = HUBBARD_NCONS
+        elif sz_cons:
+            d.nup = (d.nlocspn + d.total_2sz) // 2
+            d.ndown = (d.nlocspn - d.total_2sz) // 2
+        if d.calc_model == SPIN:
+            d.ne = d.nup
+        elif d.ne == 0:
+            d.ne = d.nup + d.ndown
+    if d.lanczos_target < d.k_exct:
+        d.lanczos_target = d.k_exct
+    if "trans" in files:
+        acc: Dict[Tuple[int, int, int, int], complex] = {}
+        for r in _table(files["trans"]):
+            key = (int(r[0]), int(r[1]), int(r[2]), int(r[3]))
+            acc[key] = acc.get(key, 0) + complex(r[4], r[5] if len(r) > 5 else 0.0)
+        for (i, s1, j, s2), t in acc.items():
+            if i == j and s1 == s2:
+                d.chemi.append((i, s1, t.real))
+            else:
+                d.trans.append((i, s1, j, s2, t))
+    if "coulombintra" in files:
+        d.coulomb_intra = [(int(r[0]), r[1]) for r in _table(files["coulombintra"])]
+    if "coulombinter" in files:
+        d.coulomb_inter = [(int(r[0]), int(r[1]), r[2]) for r in _table(files["coulombinter"])]
+    if "hund" in files:
+        d.hund = [(int(r[0]), int(r[1]), r[2]) for r in _table(files["hund"])]
+    if "ising" in files:
+        for r in _table(files["ising"]):
+            d.hund.append((int(r[0]), int(r[1]), -r[2] / 2.0))
+            d.coulomb_inter.append((int(r[0]), int(r[1]), -r[2] / 4.0))
+    if "exchange" in files:
+        d.exchange = [(int(r[0]), int(r[1]), r[2]) for r in _table(files["exchange"])]
+    if "pairhop" in files:
+        for r in _table(files["pairhop"]):
+            d.pairhop.append((int(r[0]), int(r[1]), r[2]))
+            d.pairhop.append((int(r[1]), int(r[0]), r[2]))
+    if "pairlift" in files:
+        d.pairlift = [(int(r[0]), int(r[1]), r[2]) for r in _table(files["pairlift"])]
+    if "interall" in files:
+        for r in _table(files["interall"]):
+            i, s1, j, s2, k, s3, l, s4 = (int(x) for x in r[:8])
+            v = complex(r[8], r[9] if len(r) > 9 else 0.0)
+            if i == j and k == l and s1 == s2 and s3 == s4:
+                d.interall_diag.append((i, s1, k, s3, v.real))
+            else:
+                d.interall_off.append((i, s1, j, s2, k, s3, l, s4, v))
+    return d
+
+
+# ------------------------------------------------------------------------- helpers
+def _is_spin(d: Def) -> bool:
+    return d.calc_model in (SPIN, SPINGC)
+
+
+def _is_gc(d: Def) -> bool:
+    return d.calc_model in (HUBBARDGC, SPINGC, KONDOGC)
+
+
+def nbits(d: Def) -> int:
+    return d.nsite if _is_spin(d) else 2 * d.nsite
+
+
+def split_bits(d: Def) -> Tuple[int, int, int]:
+    """GetSplitBit (src/bitcalc.c:45-62): (ihfbit, irght, ilft)."""
+    nb = nbits(d)
+    ihfbit = 1 << ((nb + 1) // 2)
+    irght = ihfbit - 1
+    ilft = ((1 << nb) - 1) ^ irght
+    return ihfbit, irght, ilft
+
+
+def sdim(d: Def) -> int:
+    """check() (src/check.c:296-328)."""
+    return (1 << d.nsite) if not _is_spin(d) else (1 << (d.nsite // 2))
+
+
+def _popcount(x: np.ndarray) -> np.ndarray:
+    x = x.astype(np.uint64)
+    c = np.zeros(x.shape, dtype=np.int64)
+    while np.any(x):
+        c += (x & np.uint64(1)).astype(np.int64)
+        x = x >> np.uint64(1)
+    return c
+
+
+def _parity(x: np.ndarray) -> np.ndarray:
+    """SgnBit (src/bitcalc.c:338-352) as 0/1 parity."""
+    x = x.astype(np.uint64)
+    for s in (1, 2, 4, 8, 16, 32):
+        x = x ^ (x >> np.uint64(s))
+    return (x & np.uint64(1)).astype(np.int64)
+
+
+# ---------------------------------------------------------------------------- sz
+def sz(d: Def):
+    """sz (src/sz.c:62-832), hacker enumeration omp_sz_hacker (:993-1094) /
+    omp_sz_spin_hacker (:1495-1546): blocks by upper half ib ascending, each block the
+    ascending lower halves ia whose particle numbers complete the sector."""
+    if _is_gc(d):
+        raise ValueError("grand-canonical models have no lists")
+    ihfbit, irght, ilft = split_bits(d)
+    sd = sdim(d)
+    lo = (nbits(d) + 1) // 2
+    size21 = sd * 2 + 2 if (d.calc_model == SPIN and d.nsite % 2 == 1) else sd + 2
+    list_2_1 = np.zeros(size21, dtype=np.uint64)
+    list_2_2 = np.zeros(sd + 2, dtype=np.uint64)
+    ia = np.arange(ihfbit, dtype=np.uint64)
+    even = np.uint64(0x5555555555555555)
+    if d.calc_model == HUBBARD:
+        a_up, a_dn = _popcount(ia & even), _popcount(ia & ~even)
+    else:
+        a_up, a_dn = _popcount(ia), np.zeros(ihfbit, dtype=np.int64)
+    blocks = []
+    jb = 0
+    cache: Dict[Tuple[int, int], np.ndarray] = {}
+    for ib in range(sd):
+        i = np.uint64(ib) * np.uint64(ihfbit)
+        if d.calc_model == HUBBARD:
+            nu, nd = int(_popcount(np.array([i & even]))[0]), int(_popcount(np.array([i & ~even]))[0])
+            key = (d.nup - nu, d.ndown - nd)
+            if key not in cache:
+                cache[key] = np.nonzero((a_up == key[0]) & (a_dn == key[1]))[0].astype(np.uint64)
+        else:
+            nu = int(_popcount(np.array([i]))[0])
+            target = d.ne
+            key = (target - nu, 0)
+            if key not in cache:
+                cache[key] = np.nonzero(a_up == key[0])[0].astype(np.uint64) if key[0] >= 0 else np.zeros(0, np.uint64)
+        sel = cache[key]
+        if sel.size:
+            blocks.append(sel + np.uint64(ib) * np.uint64(ihfbit))
+            list_2_1[sel] = np.arange(sel.size, dtype=np.uint64) + np.uint64(2)
+            list_2_2[ib] = jb + 1
+            jb += sel.size
+    list_1 = np.concatenate([np.zeros(1, dtype=np.uint64)] + blocks)
+    return list_1, list_2_1, list_2_2
+
+
+def configs(d: Def, lists) -> np.ndarray:
+    """Configuration of every row (1-based arrays: element 0 unused)."""
+    if _is_gc(d):
+        n = 1 << nbits(d)
+        return np.concatenate([np.zeros(1, np.uint64), np.arange(n, dtype=np.uint64)])
+    return lists[0]
+
+
+def get_off(d: Def, lists, c: np.ndarray) -> np.ndarray:
+    """GetOffComp (src/bitcalc.c:195-223): 1-based row of configuration c, 0 if absent."""
+    if _is_gc(d):
+        return c.astype(np.int64) + 1
+    ihfbit, irght, ilft = split_bits(d)
+    lo = (nbits(d) + 1) // 2
+    a = lists[1][(c & np.uint64(irght)).astype(np.int64)].astype(np.int64)
+    b = lists[2][(c >> np.uint64(lo)).astype(np.int64)].astype(np.int64)
+    return np.where((a == 0) | (b == 0), 0, a + b - 2)
+
+
+# ------------------------------------------------------------------------ diagonal
+def diagonalcalc(d: Def, lists) -> np.ndarray:
+    """diagonalcalc (src/diagonalcalc.c:84-187) in the reference's term order:
+    CoulombIntra, Chemi, CoulombInter, Hund, InterAll-diagonal."""
+    c = configs(d, lists)
+    diag = np.zeros(c.size)
+    bit = lambda pos: ((c >> np.uint64(pos)) & np.uint64(1)).astype(np.int64)
+    spin = _is_spin(d)
+    for i, U in d.coulomb_intra:   # SetDiagonalCoulombIntra :260-355 (zero for spin)
+        if not spin:
+            diag += U * (bit(2 * i) & bit(2 * i + 1))
+    for i, s, mu in d.chemi:       # SetDiagonalChemi :373-527, tmp_V = -mu
+        n = (bit(i) ^ (1 - s)) if spin else bit(2 * i + s)
+        diag += -mu * n
+    for i, j, V in d.coulomb_inter:  # SetDiagonalCoulombInter :543-787
+        if spin:
+            diag += V
+        else:
+            diag += V * (bit(2 * i) + bit(2 * i + 1)) * (bit(2 * j) + bit(2 * j + 1))
+    for i, j, J in d.hund:         # SetDiagonalHund :788-1112, tmp_V = -J
+        if spin:
+            diag += -J * (bit(i) == bit(j))
+        else:
+            diag += -J * (bit(2 * i) * bit(2 * j) + bit(2 * i + 1) * bit(2 * j + 1))
+    for i, s1, k, s3, V in d.interall_diag:  # SetDiagonalInterAll :1113-1415
+        if spin:
+            diag += V * ((bit(i) == s1) & (bit(k) == s3))
+        else:
+            diag += V * (bit(2 * i + s1) * bit(2 * k + s3))
+    diag[0] = 0.0
+    return diag
+
+
+# -------------------------------------------------------------------------- mltply
+def _hop(c: np.ndarray, b_to: int, b_from: int):
+    """c+_{to} c_{from} on configurations c (CisAjt, src/mltplyHubbardCore.c:305-347):
+    allowed iff 'to' empty and 'from' occupied (or to == from: n_from); returns
+    (allowed mask, new configurations, sign) with sign = (-1)^(occupied strictly between)."""
+    if b_to == b_from:
+        ok = ((c >> np.uint64(b_from)) & np.uint64(1)).astype(bool)
+        return ok, c, np.ones(c.size, dtype=np.int64)
+    m_to, m_from = np.uint64(1 << b_to), np.uint64(1 << b_from)
+    ok = ((c & m_to) == 0) & ((c & m_from) != 0)
+    lo_b, hi_b = min(b_to, b_from), max(b_to, b_from)
+    between = np.uint64(((1 << hi_b) - 1) ^ ((1 << (lo_b + 1)) - 1))
+    sgn = 1 - 2 * _parity(c & between)
+    return ok, c ^ (m_to | m_from), sgn
+
+
+def _spin_flip(c: np.ndarray, site: int, to: int, frm: int):
+    """|to><from| on spin site (child_exchange_spin_element / child_SpinGC_CisAit,
+    src/mltplySpinCore.c:203-266): sigma equals the bit value."""
+    b = (c >> np.uint64(site)) & np.uint64(1)
+    ok = b == np.uint64(frm)
+    if to == frm:
+        return ok, c
+    return ok, c ^ np.uint64(1 << site)
+
+
+def mltply(d: Def, lists, diag: np.ndarray, v0: np.ndarray, v1: np.ndarray):
+    """mltply (src/mltply.c:56-132): v0 += H v1 (1-based complex arrays) and
+    prdct = <v1|H|v1>; the diagonal pass first, then one pass per off-diagonal term in
+    the reference's order (mltplyHubbard src/mltplyHubbard.c:150-340, mltplyHalfSpin /
+    mltplyHalfSpinGC src/mltplySpin.c:192-703)."""
+    v0 = v0.astype(np.complex128).copy()
+    v1 = v1.astype(np.complex128)
+    c = configs(d, lists)
+    rows = np.arange(1, c.size, dtype=np.int64)
+    cj = c[1:]
+    x = v1[1:]
+    v0[1:] += diag[1:] * x
+    prdct = np.sum(diag[1:] * np.abs(x) ** 2)
+    spin = _is_spin(d)
+
+    def scatter(ok, target, coef):
+        nonlocal prdct
+        off = np.zeros(cj.size, dtype=np.int64)
+        off[ok] = get_off(d, lists, target[ok])
+        ok = ok & (off > 0)
+        dmv = coef[ok] * x[ok]
+        np.add.at(v0, off[ok], dmv)
+        prdct += np.sum(np.conj(v1[off[ok]]) * dmv)
+
+    if spin:
+        # InterAll off-diagonal (general_int_spin :1020-1051 / GC_general_int_spin :1058-1112)
+        for (i, s1, j, s2, k, s3, l, s4, V) in d.interall_off:
+            ok2, t2 = _spin_flip(cj, k, s3, s4)
+            ok1, t1 = _spin_flip(t2, i, s1, s2)
+            scatter(ok1 & ok2, t1, np.full(cj.size, V))
+        # transverse field (SpinGC Trans with s1 != s2; GC_CisAit, src/mltplySpin.c:500-560)
+        for (i, s1, j, s2, t) in d.trans:
+            ok, t1 = _spin_flip(cj, i, s1, s2)
+            scatter(ok, t1, np.full(cj.size, -t))
+        # Exchange (exchange_spin_element, src/mltplySpinCore.c:273-307): flip antiparallel pair
+        for (i, j, J) in d.exchange:
+            bi = (cj >> np.uint64(i)) & np.uint64(1)
+            bj = (cj >> np.uint64(j)) & np.uint64(1)
+            ok = bi != bj
+            scatter(ok, cj ^ np.uint64((1 << i) | (1 << j)), np.full(cj.size, complex(J)))
+        # PairLift (GC_pairlift_spin_element, src/mltplySpinCore.c:352-382): flip parallel pair
+        for (i, j, J) in d.pairlift:
+            bi = (cj >> np.uint64(i)) & np.uint64(1)
+            bj = (cj >> np.uint64(j)) & np.uint64(1)
+            ok = bi == bj
+            scatter(ok, cj ^ np.uint64((1 << i) | (1 << j)), np.full(cj.size, complex(J)))
+    else:
+        fb = lambda site, s: 2 * site + s
+        # Transfer (general_hopp / CisAjt): tmp_trans = -t  (src/mltplyHubbard.c:202)
+        for (i, s1, j, s2, t) in d.trans:
+            ok, t1, sg = _hop(cj, fb(i, s1), fb(j, s2))
+            scatter(ok, t1, -t * sg)
+        # InterAll off-diagonal: c+_i c_j c+_k c_l = (c+_i c_j)(c+_k c_l), right pair first
+        for (i, s1, j, s2, k, s3, l, s4, V) in d.interall_off:
+            ok2, t2, sg2 = _hop(cj, fb(k, s3), fb(l, s4))
+            ok1, t1, sg1 = _hop(t2, fb(i, s1), fb(j, s2))
+            scatter(ok1 & ok2, t1, V * sg1 * sg2)
+        # PairHop (pairhopp_element :533-575): J, i both empty, j both occupied
+        for (i, j, J) in d.pairhop:
+            if i == j:
+                continue
+            b = lambda p: ((cj >> np.uint64(p)) & np.uint64(1)).astype(bool)
+            ok = ~b(fb(i, 0)) & ~b(fb(i, 1)) & b(fb(j, 0)) & b(fb(j, 1))
+            m = np.uint64((1 << fb(i, 0)) | (1 << fb(i, 1)) | (1 << fb(j, 0)) | (1 << fb(j, 1)))
+            scatter(ok, cj ^ m, np.full(cj.size, complex(J)))
+        # Exchange (exchange_element :472-526): tmp_J = -J, (i dn, j up) <-> (i up, j dn)
+        for (i, j, J) in d.exchange:
+            if i == j:
+                continue
+            b = lambda p: ((cj >> np.uint64(p)) & np.uint64(1)).astype(bool)
+            ok = (~b(fb(i, 0)) & b(fb(i, 1)) & b(fb(j, 0)) & ~b(fb(j, 1))) | \
+                 (b(fb(i, 0)) & ~b(fb(i, 1)) & ~b(fb(j, 0)) & b(fb(j, 1)))
+            m = np.uint64((1 << fb(i, 0)) | (1 << fb(i, 1)) | (1 << fb(j, 0)) | (1 << fb(j, 1)))
+            scatter(ok, cj ^ m, np.full(cj.size, complex(-J)))
+    return v0, complex(prdct)
+
+
+# ------------------------------------------------------------------------- drivers
+def lanczos_eigenvalues(d: Def, lists, diag, v_init: np.ndarray, max_steps: int = None):
+    """Lanczos_EigenValue (src/Lanczos_EigenValue.c:50-310): two-vector recurrence,
+    dense tridiagonal eigenvalues every step, stop at |dE/E| < 10^-LanczosEps or
+    beta < 1e-14.  Returns (converged step, E_target, lowest eigenvalues, alpha, beta)."""
+    dim = v_init.size - 1
+    maxs = min(d.lanczos_max if max_steps is None else max_steps, dim)
+    eps = 10.0 ** (-d.lanczos_eps)
+    target = d.lanczos_target
+    v1 = v_init.astype(np.complex128).copy()
+    v0 = np.zeros_like(v1)
+    v0, pr = mltply(d, lists, diag, v0, v1)
+    alpha, beta = [0.0, pr.real], [0.0]
+    beta.append(float(np.sqrt(np.sum(np.abs(v0[1:] - alpha[1] * v1[1:]) ** 2))))
+    ebefor = 0.0
+    for stp in range(2, maxs + 1):
+        a1, b1 = alpha[-1], beta[-1]
+        tmp = v1.copy()
+        v1[1:] = (v0[1:] - a1 * v1[1:]) / b1
+        v0[1:] = -b1 * tmp[1:]
+        v0, pr = mltply(d, lists, diag, v0, v1)
+        alpha.append(pr.real)
+        beta.append(float(np.sqrt(np.sum(np.abs(v0[1:] - alpha[-1] * v1[1:]) ** 2))))
+        T = np.diag(alpha[1:stp + 1]) + np.diag(beta[1:stp], 1) + np.diag(beta[1:stp], -1)
+        E = np.linalg.eigvalsh(T)
+        if stp == 2 and target < 2:
+            ebefor = E[target]
+        if stp > 2 and stp > target:
+            et = E[target]
+            if abs((et - ebefor) / et) < eps or abs(beta[stp]) < 1e-14:
+                return stp, et, E, np.array(alpha[1:]), np.array(beta[1:])
+            ebefor = et
+    raise RuntimeError("Lanczos did not converge")
+
+
+def tpq_energies(d: Def, lists, diag, v_start: np.ndarray, nsteps: int):
+    """CalcByTPQ (src/CalcByTPQ.c:52-294) for one sample: returns the energies of the
+    SS_rand lines for steps 0 .. nsteps-1 (step 0 = the start vector itself)."""
+    ns = float(d.nsite)
+    L = d.large_value
+    v = v_start.astype(np.complex128) / np.sqrt(np.sum(np.abs(v_start[1:]) ** 2))
+    out = []
+    h, _ = mltply(d, lists, diag, np.zeros_like(v), v)
+    out.append(np.vdot(v[1:], h[1:]).real)
+    for step in range(1, nsteps):
+        w = L * v - h / ns
+        w[0] = 0
+        v = w / np.sqrt(np.sum(np.abs(w[1:]) ** 2))
+        h, _ = mltply(d, lists, diag, np.zeros_like(v), v)
+        out.append(np.vdot(v[1:], h[1:]).real)
+    return np.array(out)
+
+
+def dense_hamiltonian(d: Def, lists, diag) -> np.ndarray:
+    """Dense H from columns H e_j (small dims only)."""
+    dim = diag.size - 1
+    H = np.zeros((dim, dim), dtype=np.complex128)
+    for j in range(dim):
+        e = np.zeros(dim + 1, dtype=np.complex128)
+        e[j + 1] = 1.0
+        col, _ = mltply(d, lists, diag, np.zeros_like(e), e)
+        H[:, j] = col[1:]
+    return H
