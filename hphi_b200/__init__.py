@@ -27,7 +27,7 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-__all__ = ["Hamiltonian", "HPhiError", "load_library", "library_path", "REAL64", "COMPLEX128",
+__all__ = ["Hamiltonian", "HPhiError", "inspect_terms", "load_library", "library_path", "REAL64", "COMPLEX128",
            "INFO_FIELDS", "EXPORTED_SYMBOLS"]
 
 REAL64 = 0
@@ -37,7 +37,9 @@ INFO_FIELDS = ["dim", "nsite", "calc_model", "calc_type", "size_list_2_1", "size
                "vec_type", "n_offdiag", "n_diag", "lanczos_max", "num_ave"]
 EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi_close", "hphi_info",
                     "hphi_sz", "hphi_diagonalcalc", "hphi_mltply", "hphi_mltply_device", "hphi_lanczos",
-                    "hphi_lanczos_eigenvector", "hphi_tpq", "hphi_run"]
+                    "hphi_lanczos_eigenvector", "hphi_tpq", "hphi_run", "hphi_inspect_terms",
+                    "hphi_lanczos_tridiagonal", "hphi_mltply_device_async", "hphi_stream",
+                    "hphi_synchronize"]
 
 
 class HPhiError(RuntimeError):
@@ -79,8 +81,14 @@ def load_library() -> ctypes.CDLL:
     lib.hphi_lanczos_eigenvector.argtypes = [P, pd]
     lib.hphi_tpq.argtypes = [P, pd, ctypes.c_char_p, pd, I]
     lib.hphi_run.argtypes = [P, ctypes.c_char_p]
+    lib.hphi_mltply_device_async.argtypes = [P, I, VP, VP, VP, VP]
+    lib.hphi_stream.argtypes = [P]
+    lib.hphi_stream.restype = ctypes.c_void_p
+    lib.hphi_synchronize.argtypes = [P]
+    lib.hphi_lanczos_tridiagonal.argtypes = [P, pd, pd, I, ctypes.POINTER(I)]
+    lib.hphi_inspect_terms.argtypes = [ctypes.c_char_p, pu64, pd, I, pu64, pd, I, pi64]
     for name in EXPORTED_SYMBOLS:
-        if name not in ("hphi_version", "hphi_last_error", "hphi_close"):
+        if name not in ("hphi_version", "hphi_last_error", "hphi_close", "hphi_stream"):
             getattr(lib, name).restype = I
     _lib = lib
     return lib
@@ -100,6 +108,26 @@ def _as_hphi_vector(v: np.ndarray, dim: int) -> np.ndarray:
     if v.shape != (dim + 1,):
         raise ValueError(f"expected an HPhi vector of length dim+1 = {dim + 1}, got {v.shape}")
     return v
+
+
+def inspect_terms(namelist_def: str):
+    """Compiled terms of an expert-mode input, read on the host (no device needed).
+
+    Returns (masks[n_off, 4] = (cm, cv, flip, sign_mask), coefs[n_off] complex,
+    dmasks[n_diag, 2] = (cm, cv), dcoefs[n_diag])."""
+    lib = load_library()
+    counts = (ctypes.c_int64 * 2)()
+    path = os.fsencode(namelist_def)
+    _check(lib.hphi_inspect_terms(path, None, None, 0, None, None, 0, counts))
+    no, nd = int(counts[0]), int(counts[1])
+    masks = np.zeros((max(no, 1), 4), dtype=np.uint64)
+    coefs = np.zeros((max(no, 1), 2))
+    dmasks = np.zeros((max(nd, 1), 2), dtype=np.uint64)
+    dcoefs = np.zeros(max(nd, 1))
+    pu = ctypes.POINTER(ctypes.c_uint64)
+    _check(lib.hphi_inspect_terms(path, masks.ctypes.data_as(pu), _dptr(coefs), no, dmasks.ctypes.data_as(pu),
+                                  _dptr(dcoefs), nd, counts))
+    return masks[:no], coefs[:no, 0] + 1j * coefs[:no, 1], dmasks[:nd], dcoefs[:nd]
 
 
 class Hamiltonian:
@@ -173,6 +201,27 @@ class Hamiltonian:
                                                  ctypes.c_void_p(v1_ptr), float(acc), float(scale), _dptr(pr)))
         return complex(pr[0], pr[1])
 
+    def mltply_device_async(self, v0_ptr: int, v1_ptr: int, vec_type: int, coef_ptr: int, prdct_ptr: int) -> None:
+        """Enqueue v0 = coef[0]*v0 + coef[1]*H v1 on the handle's stream (all device pointers)."""
+        _check(load_library().hphi_mltply_device_async(self._h, int(vec_type), ctypes.c_void_p(v0_ptr),
+                                                       ctypes.c_void_p(v1_ptr), ctypes.c_void_p(coef_ptr),
+                                                       ctypes.c_void_p(prdct_ptr)))
+
+    def mltply_raw(self, v0_ptr: int, v1_ptr: int) -> complex:
+        """mltply on raw host pointers (HPhi layout, complex128, dim+1 elements each)."""
+        pr = np.zeros(2)
+        pd = ctypes.POINTER(ctypes.c_double)
+        _check(load_library().hphi_mltply(self._h, ctypes.cast(v0_ptr, pd), ctypes.cast(v1_ptr, pd), _dptr(pr)))
+        return complex(pr[0], pr[1])
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of the handle (as an integer), for external events / streams."""
+        return int(load_library().hphi_stream(self._h) or 0)
+
+    def synchronize(self) -> None:
+        _check(load_library().hphi_synchronize(self._h))
+
     def calc_by_lanczos(self, v_init: Optional[np.ndarray] = None, output_dir: Optional[str] = None) -> dict:
         res = np.zeros(11)
         vi = None if v_init is None else _as_hphi_vector(v_init, self.dim)
@@ -184,6 +233,15 @@ class Hamiltonian:
         out["converged"] = bool(res[0])
         out["steps"] = int(res[1])
         return out
+
+    def lanczos_tridiagonal(self):
+        """(alpha, beta) of the last calc_by_lanczos run (reference's alpha[1..itr], beta[1..itr])."""
+        steps = ctypes.c_int()
+        _check(load_library().hphi_lanczos_tridiagonal(self._h, None, None, 0, ctypes.byref(steps)))
+        n = steps.value
+        a, b = np.zeros(max(n, 1)), np.zeros(max(n, 1))
+        _check(load_library().hphi_lanczos_tridiagonal(self._h, _dptr(a), _dptr(b), n, ctypes.byref(steps)))
+        return a[:n], b[:n]
 
     def lanczos_eigenvector(self) -> np.ndarray:
         v = np.zeros(self.dim + 1, dtype=np.complex128)

@@ -22,6 +22,8 @@ struct hphi_handle {
   hphi::Sector *sector = nullptr;
   hphi::LanczosResult last_lanczos;
   double *d_scal = nullptr;  // coefficient / result slots for hphi_mltply*
+  void *d_stage0 = nullptr;  // device staging vectors of hphi_mltply (allocated on first use)
+  void *d_stage1 = nullptr;
 };
 
 using namespace hphi;
@@ -74,11 +76,33 @@ int hphi_open_expert(const char *namelist_def, int device, hphi_handle **out) {
   return 0;
 }
 
+int hphi_inspect_terms(const char *namelist_def, uint64_t *masks, double *coefs, int cap_off, uint64_t *dmasks,
+                       double *dcoefs, int cap_diag, int64_t *counts) {
+  if (!namelist_def || !counts) { set_error("null argument"); return -1; }
+  Model m;
+  std::string err;
+  if (read_expert(namelist_def, &m, &err) != 0) { set_error(err); return -1; }
+  counts[0] = (int64_t)m.offdiag.size();
+  counts[1] = (int64_t)m.diag.size();
+  for (int k = 0; k < (int)m.offdiag.size() && k < cap_off; k++) {
+    const BitTerm &t = m.offdiag[k];
+    if (masks) { masks[4 * k] = t.cm; masks[4 * k + 1] = t.cv; masks[4 * k + 2] = t.flip; masks[4 * k + 3] = t.sm; }
+    if (coefs) { coefs[2 * k] = t.re; coefs[2 * k + 1] = t.im; }
+  }
+  for (int k = 0; k < (int)m.diag.size() && k < cap_diag; k++) {
+    if (dmasks) { dmasks[2 * k] = m.diag[k].cm; dmasks[2 * k + 1] = m.diag[k].cv; }
+    if (dcoefs) dcoefs[k] = m.diag[k].v;
+  }
+  return 0;
+}
+
 void hphi_close(hphi_handle *h) {
   if (!h) return;
   if (h->sector) {
     cudaSetDevice(h->sector->device);
     cudaFree(h->d_scal);
+    cudaFree(h->d_stage0);
+    cudaFree(h->d_stage1);
     sector_free(h->sector);
   }
   delete h;
@@ -160,16 +184,36 @@ int hphi_mltply(hphi_handle *h, double *v0, const double *v1, double *prdct) {
   Sector *s = h->sector;
   cudaSetDevice(s->device);
   const size_t bytes = sizeof(cplx) * (size_t)s->dim;
-  void *d0 = nullptr, *d1 = nullptr;
-  if (cuda_fail(cudaMalloc(&d0, bytes), "alloc v0")) return -1;
-  if (cuda_fail(cudaMalloc(&d1, bytes), "alloc v1")) { cudaFree(d0); return -1; }
-  int rc = vec_from_host_c128(s, kComplex128, v1, d1);
-  if (rc == 0) rc = vec_from_host_c128(s, kComplex128, v0, d0);
-  if (rc == 0) rc = hphi_mltply_device(h, HPHI_COMPLEX128, d0, d1, 1.0, 1.0, prdct);
-  if (rc == 0) rc = vec_to_host_c128(s, kComplex128, d0, v0);
-  cudaFree(d0);
-  cudaFree(d1);
+  if (!h->d_stage0) {
+    if (cuda_fail(cudaMalloc(&h->d_stage0, bytes), "alloc v0")) return -1;
+    if (cuda_fail(cudaMalloc(&h->d_stage1, bytes), "alloc v1")) {
+      cudaFree(h->d_stage0);
+      h->d_stage0 = nullptr;
+      return -1;
+    }
+  }
+  int rc = vec_from_host_c128(s, kComplex128, v1, h->d_stage1);
+  if (rc == 0) rc = vec_from_host_c128(s, kComplex128, v0, h->d_stage0);
+  if (rc == 0) rc = hphi_mltply_device(h, HPHI_COMPLEX128, h->d_stage0, h->d_stage1, 1.0, 1.0, prdct);
+  if (rc == 0) rc = vec_to_host_c128(s, kComplex128, h->d_stage0, v0);
   return rc;
+}
+
+int hphi_mltply_device_async(hphi_handle *h, int vec_type, void *d_v0, const void *d_v1, const double *d_coef,
+                             double *d_prdct) {
+  CHECK_HANDLE(h);
+  Sector *s = h->sector;
+  if (vec_type != HPHI_REAL64 && vec_type != HPHI_COMPLEX128) { set_error("bad vec_type"); return -1; }
+  cudaSetDevice(s->device);
+  return hv_launch(s, (VecType)vec_type, d_v1, d_v0, d_coef, d_prdct);
+}
+
+void *hphi_stream(hphi_handle *h) { return (h && h->sector) ? (void *)h->sector->stream : nullptr; }
+
+int hphi_synchronize(hphi_handle *h) {
+  CHECK_HANDLE(h);
+  cudaSetDevice(h->sector->device);
+  return cuda_fail(cudaStreamSynchronize(h->sector->stream), "synchronize");
 }
 
 int hphi_lanczos(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult) {
@@ -195,6 +239,17 @@ int hphi_lanczos(hphi_handle *h, const double *v_init, const char *output_dir, d
   }
   if (rc != 0) return -1;
   if (output_dir && write_lanczos_outputs(*s, r, output_dir) != 0) return -1;
+  return 0;
+}
+
+int hphi_lanczos_tridiagonal(hphi_handle *h, double *alpha, double *beta, int cap, int *steps) {
+  CHECK_HANDLE(h);
+  const LanczosResult &r = h->last_lanczos;
+  if (steps) *steps = r.steps;
+  for (int i = 0; i < cap && i < (int)r.alpha.size(); i++) {
+    if (alpha) alpha[i] = r.alpha[i];
+    if (beta) beta[i] = r.beta[i];
+  }
   return 0;
 }
 

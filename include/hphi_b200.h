@@ -55,6 +55,20 @@ const char *hphi_last_error(void);
  */
 int hphi_open_expert(const char *namelist_def, int device, hphi_handle **out);
 
+/*
+ * Reads an expert-mode input on the host only (no device needed) and exports the
+ * compiled Hamiltonian: counts[0] = off-diagonal terms, counts[1] = diagonal terms.
+ * Off-diagonal term k (gather form, for an output configuration t): applies iff
+ * (t & masks[4k]) == masks[4k+1]; source s = t ^ masks[4k+2]; value
+ * (coefs[2k] + i coefs[2k+1]) * (-1)^popcount(t & masks[4k+3]) * v[row(s)].
+ * Diagonal term k adds dcoefs[k] iff (c & dmasks[2k]) == dmasks[2k+1].
+ * Arrays may be NULL (counts only); at most cap_off / cap_diag terms are written.
+ * Inspection aid with no counterpart in the reference (its terms live in
+ * struct DefineList, include/struct.h:43-300).
+ */
+int hphi_inspect_terms(const char *namelist_def, uint64_t *masks, double *coefs, int cap_off, uint64_t *dmasks,
+                       double *dcoefs, int cap_diag, int64_t *counts);
+
 /* Frees the handle and its device memory. */
 void hphi_close(hphi_handle *h);
 
@@ -90,6 +104,19 @@ int hphi_mltply_device(hphi_handle *h, int vec_type, void *d_v0, const void *d_v
                        double *prdct);
 
 /*
+ * Asynchronous device form for callers that launch back to back: d_v0 = acc * d_v0 +
+ * scale * (H d_v1) with (acc, scale) = d_coef[0..1] read on the device, and
+ * d_prdct[0..1] = sum conj(d_v1) (H d_v1), all device pointers; enqueued on the
+ * handle's stream (hphi_stream) without waiting.
+ */
+int hphi_mltply_device_async(hphi_handle *h, int vec_type, void *d_v0, const void *d_v1, const double *d_coef,
+                             double *d_prdct);
+
+/* The CUDA stream (cudaStream_t) the handle launches on, and a blocking wait on it. */
+void *hphi_stream(hphi_handle *h);
+int hphi_synchronize(hphi_handle *h);
+
+/*
  * Lanczos ground state (and, with CalcEigenVec != -1, the eigenvector, its energy and
  * variance).  v_init: normalised start vector in HPhi's layout, or NULL for the
  * reference's own start (single element for initial_iv > 0 on canonical models, else a
@@ -101,6 +128,13 @@ int hphi_mltply_device(hphi_handle *h, int vec_type, void *d_v0, const void *d_v
  * (src/Lanczos_EigenValue.c:50) and Lanczos_EigenVector (src/Lanczos_EigenVector.c:46).
  */
 int hphi_lanczos(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult);
+
+/*
+ * Tridiagonal coefficients of the last hphi_lanczos run: alpha[0 .. n) and beta[0 .. n)
+ * with n = min(cap, steps); *steps receives the step count.  These are the reference's
+ * alpha[1 .. itr] and beta[1 .. itr] (src/Lanczos_EigenValue.c:113-176).
+ */
+int hphi_lanczos_tridiagonal(hphi_handle *h, double *alpha, double *beta, int cap, int *steps);
 
 /*
  * Lanczos eigenvector copy-out: after hphi_lanczos with CalcEigenVec != -1, copies the

@@ -6,7 +6,8 @@
  * It never changes what the reference computes; it only records it:
  *
  *   HPHI_DUMP_DIR=<dir>      enables the dumps below (nothing is written otherwise)
- *   HPHI_DUMP_CALL=<k>       which mltply call to dump (0 = the first one)
+ *   HPHI_DUMP_CALL=<k>       which mltply call to dump (0 = the first one, -1 = none)
+ *   HPHI_DUMP_LISTS=0        skip the lists.bin / diag.bin dumps (timing runs)
  *
  *   <dir>/lists.bin   after sz():           int64 idim, n21, n22, then list_1[0..idim],
  *                                            list_2_1[0..n21), list_2_2[0..n22) as uint64
@@ -50,6 +51,11 @@ static FILE *open_dump(const char *name) {
   return fopen(path, "wb");
 }
 
+static int dump_lists(void) {
+  const char *d = getenv("HPHI_DUMP_LISTS");
+  return !(d && d[0] == '0');
+}
+
 static double now_s(void) {
   struct timespec ts;
   clock_gettime(CLOCK_MONOTONIC, &ts);
@@ -71,7 +77,7 @@ static void write_times(void) {
 int __wrap_sz(struct BindStruct *X, long unsigned int *a, long unsigned int *b, long unsigned int *c) {
   int r = __real_sz(X, a, b, c);
   /* grand-canonical models have no lists (GetlistSize, src/xsetmem.c:284-318) */
-  FILE *f = (a && b && c) ? open_dump("lists.bin") : NULL;
+  FILE *f = (a && b && c && dump_lists()) ? open_dump("lists.bin") : NULL;
   if (f) {
     long long idim = (long long)X->Check.idim_max;
     long long n21 = X->Large.SizeOflist_2_1, n22 = X->Large.SizeOflist_2_2;
@@ -86,7 +92,7 @@ int __wrap_sz(struct BindStruct *X, long unsigned int *a, long unsigned int *b, 
 
 int __wrap_diagonalcalc(struct BindStruct *X) {
   int r = __real_diagonalcalc(X);
-  FILE *f = open_dump("diag.bin");
+  FILE *f = dump_lists() ? open_dump("diag.bin") : NULL;
   if (f) {
     long long idim = (long long)X->Check.idim_max;
     fwrite(&idim, 8, 1, f);

@@ -1,0 +1,174 @@
+"""Generates the golden fixtures in tests/golden/ by running the reference HPhi.
+
+Each case directory holds the expert-mode input the reference ran (the .def files)
+and golden.npz with what the reference produced, read through the link-time hooks
+of oracle/ref_hooks.c:
+  list_1, list_2_1, list_2_2     sz() output (canonical models)
+  diag                           list_Diagonal after diagonalcalc()
+  hv0_v1, hv0_v0a, hv0_pr        the first mltply call (v0 = 0 before: the start vector in v1)
+  hv3_v1, hv3_v0b, hv3_v0a, hv3_pr  the 4th mltply call (accumulates into a non-zero v0)
+  steps, step_vals               zvo_Lanczos_Step.dat (Lanczos cases)
+  tpq                            SS_rand0.dat rows (TPQ cases)
+Large cases store only SHA-256 digests of the lists (sha_list_1 ...).
+
+Run in a container that has the reference sources and oracle/_ref/HPhi_ref
+(`make -C oracle`):  python tests/golden/make_golden.py [case ...]
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import shutil
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from hphi_b200 import expert  # noqa: E402
+import run_ref  # noqa: E402
+
+
+def _cases():
+    c = {}
+    # Heisenberg chain L=16, Sz=0, real vectors, random start (the CPU-runnable workload).
+    c["chain16"] = expert.heisenberg(16, expert.chain_bonds(16))
+    m = expert.j1j2_chain(14, 1.0, 0.45)
+    c["j1j2_14"] = m
+    # Odd number of sites: the lower half has more bits than the upper half.
+    c["chain13_sz1"] = expert.heisenberg(13, expert.chain_bonds(13), two_sz=1)
+    m = expert.hubbard(8, expert.square_bonds(2, 4), 1.0, 8.0, 4, 4)
+    c["hub2x4"] = m
+    m = expert.hubbard(8, expert.chain_bonds(8), 1.0, 4.0, 4, 4)
+    m.initial_vec_type = 0
+    c["hubchain8_complex"] = m
+    m = expert.hubbard(7, expert.chain_bonds(7), 1.0, 6.0, 3, 4)
+    c["hubchain7_odd"] = m
+    # Hubbard with Ncond only (HubbardNConserved).
+    m = expert.hubbard(6, expert.square_bonds(2, 3), 1.0, 4.0, 3, 3)
+    m.two_sz = None
+    c["hub2x3_ncons"] = m
+    # Grand-canonical Hubbard with chemical potential (diagonal transfers).
+    m = expert.ExpertModel(model="HubbardGC", nsite=4, two_sz=None, initial_vec_type=0)
+    for i, j in expert.chain_bonds(4):
+        for s in (0, 1):
+            m.trans += [(i, s, j, s, 1.0, 0.0), (j, s, i, s, 1.0, 0.0)]
+    m.trans += [(i, s, i, s, 0.7, 0.0) for i in range(4) for s in (0, 1)]
+    m.coulombintra = [(i, 3.0) for i in range(4)]
+    c["hubgc4"] = m
+    # Kitaev-Heisenberg honeycomb, SpinGC (Exchange + PairLift + Ising), complex vectors.
+    m = expert.kitaev_heisenberg(2, 2, -1.0, 0.2)
+    m.initial_vec_type = 0
+    c["kitaev2x2"] = m
+    # SpinGC with a transverse field (site-diagonal Trans with s1 != s2).
+    m = expert.heisenberg(8, expert.chain_bonds(8))
+    m.model, m.two_sz, m.initial_vec_type = "SpinGC", None, 0
+    m.trans = [(i, 0, i, 1, 0.3, 0.0) for i in range(8)] + [(i, 1, i, 0, 0.3, 0.0) for i in range(8)]
+    c["spingc_field8"] = m
+    # Canonical spin with random InterAll terms (complex coefficients).
+    m = expert.heisenberg(10, expert.chain_bonds(10))
+    m.initial_vec_type = 0
+    inter = [t for t in expert.random_interall_spin(10, 12, seed=7)
+             if (t[1] - t[3]) + (t[5] - t[7]) == 0]  # keep Sz-conserving strings
+    m.interall = inter
+    c["spin_interall10"] = m
+    # Hubbard with every two-body keyword and a complex hopping.
+    m = expert.hubbard(6, expert.chain_bonds(6), 1.0, 5.0, 3, 3)
+    m.initial_vec_type = 0
+    m.trans += [(0, 0, 2, 0, 0.3, 0.2), (2, 0, 0, 0, 0.3, -0.2), (0, 1, 2, 1, 0.3, 0.2), (2, 1, 0, 1, 0.3, -0.2)]
+    m.coulombinter = [(i, (i + 1) % 6, 0.8) for i in range(6)]
+    m.hund = [(i, (i + 1) % 6, 0.4) for i in range(6)]
+    m.exchange = [(i, (i + 1) % 6, 0.35) for i in range(6)]
+    m.pairhop = [(i, (i + 2) % 6, 0.25) for i in range(6)]
+    m.ising = [(0, 3, 0.5)]
+    m.interall = [(1, 0, 1, 0, 4, 1, 4, 1, 0.6, 0.0),
+                  (0, 0, 1, 0, 3, 1, 4, 1, 0.2, 0.1), (4, 1, 3, 1, 1, 0, 0, 0, 0.2, -0.1)]
+    c["hub6_allterms"] = m
+    # TPQ on a chain (one sample).
+    m = expert.heisenberg(12, expert.chain_bonds(12), calc_type="TPQ", lanczos_max=25, num_ave=1,
+                          large_value=4.5)
+    c["tpq_chain12"] = m
+    m = expert.hubbard(6, expert.chain_bonds(6), 1.0, 4.0, 3, 3, calc_type="TPQ", lanczos_max=20, num_ave=1,
+                       large_value=6.0)
+    m.initial_vec_type = 0
+    c["tpq_hub6"] = m
+    return c
+
+
+def _large_cases():
+    """Full-size sectors: only list digests are stored (the reference's own sz)."""
+    c = {}
+    m = expert.hubbard(16, expert.square_bonds(4, 4), 1.0, 8.0, 8, 8, lanczos_max=1)
+    c["hub4x4_lists"] = m
+    m = expert.heisenberg(24, expert.chain_bonds(24), lanczos_max=1)
+    c["chain24_lists"] = m
+    return c
+
+
+def _sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.uint64).tobytes()).hexdigest()
+
+
+def make_case(name: str, m, large: bool = False) -> None:
+    out = os.path.join(HERE, name)
+    shutil.rmtree(out, ignore_errors=True)
+    m.write(out)
+    data = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for f in os.listdir(out):
+            shutil.copy(os.path.join(out, f), tmp)
+        p = run_ref.run(tmp, threads=1 if not large else os.cpu_count(), dump_call=0)
+        # large cases stop after sz() output (Lanczos_max=1 does not converge and exits -1)
+        if p.returncode != 0 and not (large and os.path.exists(os.path.join(tmp, "lists.bin"))):
+            raise RuntimeError(f"{name}: reference failed\n{p.stdout[-3000:]}\n{p.stderr[-3000:]}")
+        if os.path.exists(os.path.join(tmp, "lists.bin")):
+            l1, l21, l22 = run_ref.read_lists(tmp)
+            if large:
+                data.update(sha_list_1=_sha(l1), sha_list_2_1=_sha(l21), sha_list_2_2=_sha(l22),
+                            dim=l1.size - 1, n21=l21.size, n22=l22.size)
+            else:
+                data.update(list_1=l1, list_2_1=l21, list_2_2=l22)
+        if large:
+            np.savez_compressed(os.path.join(out, "golden.npz"), **data)
+            return
+        data["diag"] = run_ref.read_diag(tmp)
+        v1, v0b, v0a, pr = run_ref.read_hv(tmp)
+        data.update(hv0_v1=v1, hv0_v0a=v0a, hv0_pr=np.array(pr))
+        if m.calc_type == "Lanczos":
+            steps = run_ref.lanczos_steps(tmp)
+            data["steps"] = np.array([s for s, _ in steps])
+            data["step_vals"] = np.array([[np.nan if v is None else v for v in (vals + [None] * 6)[:6]]
+                                          for _, vals in steps])
+        else:
+            data["tpq"] = run_ref.tpq_table(tmp, 0)
+    with tempfile.TemporaryDirectory() as tmp:
+        for f in os.listdir(out):
+            shutil.copy(os.path.join(out, f), tmp)
+        p = run_ref.run(tmp, threads=1, dump_call=3)
+        if p.returncode != 0:
+            raise RuntimeError(f"{name}: reference failed (call 3)")
+        if os.path.exists(os.path.join(tmp, "hv.bin")):
+            v1, v0b, v0a, pr = run_ref.read_hv(tmp)
+            data.update(hv3_v1=v1, hv3_v0b=v0b, hv3_v0a=v0a, hv3_pr=np.array(pr))
+    np.savez_compressed(os.path.join(out, "golden.npz"), **data)
+
+
+def main(argv) -> None:
+    if not run_ref.available():
+        raise SystemExit("oracle/_ref/HPhi_ref is missing: run `make -C oracle` first")
+    small, large = _cases(), _large_cases()
+    names = argv or list(small) + list(large)
+    for n in names:
+        print("case", n, flush=True)
+        if n in small:
+            make_case(n, small[n])
+        else:
+            make_case(n, large[n], large=True)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])
