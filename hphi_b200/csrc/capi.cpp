@@ -35,6 +35,7 @@ namespace {
       set_error("invalid handle");             \
       return -1;                               \
     }                                          \
+    cudaGetLastError();                        \
   } while (0)
 
 int cuda_fail(cudaError_t e, const char *what) {
@@ -57,6 +58,7 @@ int hphi_open_expert(const char *namelist_def, int device, hphi_handle **out) {
   std::string err;
   if (read_expert(namelist_def, &m, &err) != 0) { set_error(err); return -1; }
   int ndev = 0;
+  cudaGetLastError();
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
     set_error("no CUDA device available");

@@ -214,7 +214,7 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   DevBuf P, Q, V0, ST, AL, BE;
   RET(cuda_ok(cudaMalloc(&P.p, esz * dim), "alloc P"));
   RET(cuda_ok(cudaMalloc(&Q.p, esz * dim), "alloc Q"));
-  RET(cuda_ok(cudaMalloc(&ST.p, sizeof(double) * 16), "alloc scalars"));
+  RET(cuda_ok(cudaMalloc(&ST.p, sizeof(double) * 32), "alloc scalars"));  // slots used: [0, 19)
   int max_steps = m.lanczos_max;
   if ((int64_t)max_steps > dim) max_steps = (int)dim;
   if (dim < m.lanczos_target) max_steps = (int)dim;
