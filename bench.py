@@ -200,6 +200,7 @@ def main():
     finally:
         pass
     dim = H.dim
+    H_native = bool(H.info.get("native_order"))
     vt = hphi_b200.REAL64
     gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
     v1 = torch.rand(dim, dtype=torch.float64, device="cuda", generator=gen) - 0.5
@@ -238,6 +239,16 @@ def main():
     value = world * args.steps * balg / (t_max * 1e-3) / 1e9
     per_launch = t_ms / args.steps
     achieved = balg / (per_launch * 1e-3) / 1e9
+
+    # ---- the same H*v on HPhi-ordered device vectors (permutations to / from the native order included)
+    hphi_order_ms = None
+    if H.info.get("native_order"):
+        H.mltply_device(v0.data_ptr(), v1.data_ptr(), vt)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(3):
+            H.mltply_device(v0.data_ptr(), v1.data_ptr(), vt)
+        hphi_order_ms = (time.perf_counter() - t0) / 3 * 1e3
 
     # ---- e2e through the reference-facing host mltply (complex128, pinned host buffers)
     e2e = None
@@ -284,7 +295,9 @@ def main():
            "config": {"workload": args.workload, "desc": desc, "dim": dim, "vector": "real f64",
                       "step": "one v0 += H v1 (mltply)", "b_alg_bytes": balg,
                       "l2": "inputs larger than L2 (1.3 GB vectors), no flush",
-                      "parallelism": "replicas" if world > 1 else "single"},
+                      "parallelism": "replicas" if world > 1 else "single",
+                      "vector_order": "native (per-block up x down product order)" if H_native else "HPhi",
+                      "hphi_order_ms_per_step": hphi_order_ms},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak, "peak_kind": peak_kind,
                         "traffic": profile_traffic("hv", args.workload)},

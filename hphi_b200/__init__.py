@@ -34,12 +34,12 @@ REAL64 = 0
 COMPLEX128 = 1
 _HERE = os.path.dirname(os.path.abspath(__file__))
 INFO_FIELDS = ["dim", "nsite", "calc_model", "calc_type", "size_list_2_1", "size_list_2_2", "is_gc",
-               "vec_type", "n_offdiag", "n_diag", "lanczos_max", "num_ave"]
+               "vec_type", "n_offdiag", "n_diag", "lanczos_max", "num_ave", "native_order"]
 EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi_close", "hphi_info",
                     "hphi_sz", "hphi_diagonalcalc", "hphi_mltply", "hphi_mltply_device", "hphi_lanczos",
                     "hphi_lanczos_eigenvector", "hphi_tpq", "hphi_run", "hphi_inspect_terms",
                     "hphi_lanczos_tridiagonal", "hphi_mltply_device_async", "hphi_stream",
-                    "hphi_synchronize"]
+                    "hphi_synchronize", "hphi_to_native", "hphi_from_native"]
 
 
 class HPhiError(RuntimeError):
@@ -82,6 +82,8 @@ def load_library() -> ctypes.CDLL:
     lib.hphi_tpq.argtypes = [P, pd, ctypes.c_char_p, pd, I]
     lib.hphi_run.argtypes = [P, ctypes.c_char_p]
     lib.hphi_mltply_device_async.argtypes = [P, I, VP, VP, VP, VP]
+    lib.hphi_to_native.argtypes = [P, I, VP, VP]
+    lib.hphi_from_native.argtypes = [P, I, VP, VP]
     lib.hphi_stream.argtypes = [P]
     lib.hphi_stream.restype = ctypes.c_void_p
     lib.hphi_synchronize.argtypes = [P]
@@ -206,6 +208,15 @@ class Hamiltonian:
         _check(load_library().hphi_mltply_device_async(self._h, int(vec_type), ctypes.c_void_p(v0_ptr),
                                                        ctypes.c_void_p(v1_ptr), ctypes.c_void_p(coef_ptr),
                                                        ctypes.c_void_p(prdct_ptr)))
+
+    def to_native(self, in_ptr: int, out_ptr: int, vec_type: int) -> None:
+        """HPhi order -> the engine's native order (0-based device vectors, in != out)."""
+        _check(load_library().hphi_to_native(self._h, int(vec_type), ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr)))
+
+    def from_native(self, in_ptr: int, out_ptr: int, vec_type: int) -> None:
+        """Native order -> HPhi order (0-based device vectors, in != out)."""
+        _check(load_library().hphi_from_native(self._h, int(vec_type), ctypes.c_void_p(in_ptr),
+                                               ctypes.c_void_p(out_ptr)))
 
     def mltply_raw(self, v0_ptr: int, v1_ptr: int) -> complex:
         """mltply on raw host pointers (HPhi layout, complex128, dim+1 elements each)."""

@@ -24,6 +24,8 @@ struct hphi_handle {
   double *d_scal = nullptr;  // coefficient / result slots for hphi_mltply*
   void *d_stage0 = nullptr;  // device staging vectors of hphi_mltply (allocated on first use)
   void *d_stage1 = nullptr;
+  void *d_perm0 = nullptr;   // native-order scratch of the HPhi-order device entry points
+  void *d_perm1 = nullptr;
 };
 
 using namespace hphi;
@@ -105,6 +107,8 @@ void hphi_close(hphi_handle *h) {
     cudaFree(h->d_scal);
     cudaFree(h->d_stage0);
     cudaFree(h->d_stage1);
+    cudaFree(h->d_perm0);
+    cudaFree(h->d_perm1);
     sector_free(h->sector);
   }
   delete h;
@@ -126,6 +130,7 @@ int hphi_info(const hphi_handle *h, int64_t *info, int n) {
   v[HPHI_INFO_N_DIAG] = s.ndterms;
   v[HPHI_INFO_LANCZOS_MAX] = s.model.lanczos_max;
   v[HPHI_INFO_NUM_AVE] = s.model.num_ave;
+  v[HPHI_INFO_NATIVE_ORDER] = has_native_order(&s) ? 1 : 0;
   for (int i = 0; i < n && i < HPHI_INFO_COUNT; i++) info[i] = v[i];
   return 0;
 }
@@ -170,15 +175,51 @@ int hphi_mltply_device(hphi_handle *h, int vec_type, void *d_v0, const void *d_v
   CHECK_HANDLE(h);
   Sector *s = h->sector;
   if (vec_type != HPHI_REAL64 && vec_type != HPHI_COMPLEX128) { set_error("bad vec_type"); return -1; }
+  const VecType vt = (VecType)vec_type;
   cudaSetDevice(s->device);
   const double coef[2] = {acc, scale};
   if (cuda_fail(cudaMemcpyAsync(h->d_scal, coef, sizeof(coef), cudaMemcpyHostToDevice, s->stream), "coef")) return -1;
-  if (hv_launch(s, (VecType)vec_type, d_v1, d_v0, h->d_scal, h->d_scal + 2) != 0) return -1;
+  if (!has_native_order(s)) {
+    if (hv_launch(s, vt, d_v1, d_v0, h->d_scal, h->d_scal + 2) != 0) return -1;
+  } else {
+    // HPhi order in and out: permute to the native order around the native kernel
+    const size_t bytes = sizeof(cplx) * (size_t)s->dim;
+    if (!h->d_perm0) {
+      if (cuda_fail(cudaMalloc(&h->d_perm0, bytes), "alloc scratch")) return -1;
+      if (cuda_fail(cudaMalloc(&h->d_perm1, bytes), "alloc scratch")) {
+        cudaFree(h->d_perm0);
+        h->d_perm0 = nullptr;
+        return -1;
+      }
+    }
+    if (to_native(s, vt, d_v1, h->d_perm1) != 0) return -1;
+    if (acc != 0.0 && to_native(s, vt, d_v0, h->d_perm0) != 0) return -1;
+    if (hv_native(s, vt, h->d_perm1, h->d_perm0, h->d_scal, h->d_scal + 2) != 0) return -1;
+    if (from_native(s, vt, h->d_perm0, d_v0) != 0) return -1;
+  }
   double out[2];
   if (cuda_fail(cudaMemcpyAsync(out, h->d_scal + 2, sizeof(out), cudaMemcpyDeviceToHost, s->stream), "prdct")) return -1;
   if (cuda_fail(cudaStreamSynchronize(s->stream), "sync")) return -1;
   if (prdct) { prdct[0] = out[0]; prdct[1] = out[1]; }
   return 0;
+}
+
+int hphi_to_native(hphi_handle *h, int vec_type, const void *d_hphi, void *d_native) {
+  CHECK_HANDLE(h);
+  if (vec_type != HPHI_REAL64 && vec_type != HPHI_COMPLEX128) { set_error("bad vec_type"); return -1; }
+  if (d_hphi == d_native && has_native_order(h->sector)) { set_error("in-place permutation is not supported"); return -1; }
+  cudaSetDevice(h->sector->device);
+  if (to_native(h->sector, (VecType)vec_type, d_hphi, d_native) != 0) return -1;
+  return cuda_fail(cudaStreamSynchronize(h->sector->stream), "sync");
+}
+
+int hphi_from_native(hphi_handle *h, int vec_type, const void *d_native, void *d_hphi) {
+  CHECK_HANDLE(h);
+  if (vec_type != HPHI_REAL64 && vec_type != HPHI_COMPLEX128) { set_error("bad vec_type"); return -1; }
+  if (d_hphi == d_native && has_native_order(h->sector)) { set_error("in-place permutation is not supported"); return -1; }
+  cudaSetDevice(h->sector->device);
+  if (from_native(h->sector, (VecType)vec_type, d_native, d_hphi) != 0) return -1;
+  return cuda_fail(cudaStreamSynchronize(h->sector->stream), "sync");
 }
 
 int hphi_mltply(hphi_handle *h, double *v0, const double *v1, double *prdct) {
@@ -207,7 +248,7 @@ int hphi_mltply_device_async(hphi_handle *h, int vec_type, void *d_v0, const voi
   Sector *s = h->sector;
   if (vec_type != HPHI_REAL64 && vec_type != HPHI_COMPLEX128) { set_error("bad vec_type"); return -1; }
   cudaSetDevice(s->device);
-  return hv_launch(s, (VecType)vec_type, d_v1, d_v0, d_coef, d_prdct);
+  return hv_native(s, (VecType)vec_type, d_v1, d_v0, d_coef, d_prdct);
 }
 
 void *hphi_stream(hphi_handle *h) { return (h && h->sector) ? (void *)h->sector->stream : nullptr; }

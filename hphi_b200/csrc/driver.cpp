@@ -220,7 +220,9 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   if (dim < m.lanczos_target) max_steps = (int)dim;
   RET(cuda_ok(cudaMalloc(&AL.p, sizeof(double) * (max_steps + 2)), "alloc alpha"));
   RET(cuda_ok(cudaMalloc(&BE.p, sizeof(double) * (max_steps + 2)), "alloc beta"));
-  RET(vec_from_host_c128(s, vt, h_init, Q.p));
+  // start vector: HPhi order on the host -> native order on the device
+  RET(vec_from_host_c128(s, vt, h_init, P.p));
+  RET(to_native(s, vt, P.p, Q.p));
   const bool want_vec = opt.eigenvector;
   if (want_vec) {
     RET(cuda_ok(cudaMalloc(&V0.p, esz * dim), "alloc V0"));
@@ -234,7 +236,7 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   std::vector<double> alpha(max_steps + 2, 0.0), beta(max_steps + 2, 0.0);
   void *pp = P.p, *qq = Q.p;
   auto do_step = [&](int k) -> int {
-    RET(hv_launch(s, vt, qq, pp, st + 2, st + 0));
+    RET(hv_native(s, vt, qq, pp, st + 2, st + 0));
     RET(lanczos_scalars(s, 0, k, st, (double *)AL.p, (double *)BE.p));
     RET(vec_lanczos_sweep(s, vt, st + 4, pp, qq, st + 5));
     RET(lanczos_scalars(s, 1, k, st, (double *)AL.p, (double *)BE.p));
@@ -345,7 +347,7 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   for (int k = 1; k < itr; k++) {
     const double coef[2] = {acc, sq};
     RET(cuda_ok(cudaMemcpyAsync(st + 8, coef, sizeof(coef), cudaMemcpyHostToDevice, s->stream), "coef"));
-    RET(hv_launch(s, vt, qq, pp, st + 8, st + 10));
+    RET(hv_native(s, vt, qq, pp, st + 8, st + 10));
     const double ak = res->alpha[k - 1], bk = res->beta[k - 1];
     RET(vec_replay_sweep(s, vt, ak * sq, c[k] / bk, pp, qq, VG.p));
     RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
@@ -361,9 +363,9 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   // expec_energy_flct: H vg -> E = <vg|H vg>, var = <H vg|H vg>
   const double coef1[2] = {0.0, 1.0};
   RET(cuda_ok(cudaMemcpyAsync(st + 8, coef1, sizeof(coef1), cudaMemcpyHostToDevice, s->stream), "coef"));
-  RET(hv_launch(s, vt, VG.p, pp, st + 8, st + 10));
+  RET(hv_native(s, vt, VG.p, pp, st + 8, st + 10));
   RET(vec_norm2(s, vt, pp, st + 12));
-  RET(vec_diag_observables(s, vt, VG.p, st + 13));
+  RET(native_observables(s, vt, VG.p, st + 13));
   double sc[10];
   RET(cuda_ok(cudaMemcpyAsync(sc, st + 10, sizeof(double) * 9, cudaMemcpyDeviceToHost, s->stream), "read"));
   RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
@@ -372,8 +374,12 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   res->doublon = sc[3];
   res->sz = sc[7];
   res->eigenvector.assign(2 * (dim + 1), 0.0);
-  if (opt.copy_eigenvector) RET(vec_to_host_c128(s, vt, VG.p, res->eigenvector.data()));
-  else res->eigenvector.clear();
+  if (opt.copy_eigenvector) {
+    RET(from_native(s, vt, VG.p, pp));
+    RET(vec_to_host_c128(s, vt, pp, res->eigenvector.data()));
+  } else {
+    res->eigenvector.clear();
+  }
   return 0;
 }
 
@@ -424,7 +430,8 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
   RET(cuda_ok(cudaMalloc(&ST.p, sizeof(double) * 32), "alloc scalars"));
   double *st = (double *)ST.p;
   // h_init is the un-normalised start vector; its norm is global_1st_norm.
-  RET(vec_from_host_c128(s, vt, h_init, V.p));
+  RET(vec_from_host_c128(s, vt, h_init, H.p));
+  RET(to_native(s, vt, H.p, V.p));
   double n0 = 0.0;
   RET(vec_norm2(s, vt, V.p, st + 0));
   RET(cuda_ok(cudaMemcpyAsync(&n0, st, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "read"));
@@ -453,10 +460,10 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
   // expec_energy_flct on the current vector (sv*V): observables, H = H*(sv V), E, var.
   double ob[6], E = 0.0, var = 0.0;
   auto expec = [&]() -> int {
-    RET(vec_diag_observables(s, vt, V.p, st + 16));
+    RET(native_observables(s, vt, V.p, st + 16));
     const double coef[2] = {0.0, sv};
     RET(cuda_ok(cudaMemcpyAsync(st + 4, coef, sizeof(coef), cudaMemcpyHostToDevice, s->stream), "coef"));
-    RET(hv_launch(s, vt, V.p, H.p, st + 4, st + 6));
+    RET(hv_native(s, vt, V.p, H.p, st + 4, st + 6, false));
     RET(vec_norm2(s, vt, H.p, st + 8));
     double sc[3];
     RET(cuda_ok(cudaMemcpyAsync(sc, st + 6, sizeof(double) * 3, cudaMemcpyDeviceToHost, s->stream), "read"));

@@ -16,6 +16,8 @@
 
 namespace hphi {
 
+struct HubPlan;
+
 // Real or complex double scalar for host/device code.
 struct cplx { double x, y; };
 
@@ -46,6 +48,9 @@ struct Sector {
   double *d_scal = nullptr;        // small device scalars (dot results)
   int red_blocks = 0;
   int num_sms = 0;
+  // Optional specialised plan (canonical Hubbard).  When present, the drivers keep
+  // vectors in the plan's native order; see hv_native / to_native.
+  HubPlan *hub = nullptr;
 };
 
 int sector_build(const Model &m, int device, Sector **out, std::string *err);
@@ -55,6 +60,17 @@ void sector_free(Sector *s);
 // sum_r conj(v1[r]) (H v1)[r] written to d_out[0..1] (re, im).  HPhi's mltply
 // (src/mltply.c:56-132) is acc = s = 1, prdct = d_out.  acc == 0 never reads v0.
 int hv_launch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out);
+
+// Native vector order: HPhi order unless a specialised plan defines its own (then an
+// exact per-block permutation of it).  hv_native runs the fastest kernel on native
+// vectors; to_native / from_native convert (they copy when the orders coincide).
+bool has_native_order(const Sector *s);
+int hv_native(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out,
+              bool acc_read = true);
+int to_native(Sector *s, VecType vt, const void *d_hphi, void *d_native);
+int from_native(Sector *s, VecType vt, const void *d_native, void *d_hphi);
+// Diagonal observables of a native-order vector (as vec_diag_observables).
+int native_observables(Sector *s, VecType vt, const void *d_v, double *d_out);
 
 // ---- vector kernels (vecops.cu); all reductions are deterministic (fixed grid).
 // d_out[0] = sum |x|^2

@@ -15,6 +15,7 @@
 
 #include "device_util.cuh"
 #include "engine.hpp"
+#include "hv_hubbard.hpp"
 
 namespace hphi {
 namespace {
@@ -107,6 +108,39 @@ int hv_launch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double 
     return -1;
   }
   return 0;
+}
+
+bool has_native_order(const Sector *s) { return s->hub != nullptr; }
+
+int hv_native(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out,
+              bool acc_read) {
+  if (s->hub) return hub_hv_launch(s, vt, d_v1, d_v0, d_coef, d_out, acc_read);
+  return hv_launch(s, vt, d_v1, d_v0, d_coef, d_out);
+}
+
+int to_native(Sector *s, VecType vt, const void *in, void *out) {
+  if (s->hub) return hub_permute(s, vt, in, out, true);
+  const size_t esz = (vt == kReal64) ? sizeof(double) : sizeof(cplx);
+  if (in != out && cudaMemcpyAsync(out, in, esz * (size_t)s->dim, cudaMemcpyDeviceToDevice, s->stream) != cudaSuccess) {
+    set_error("to_native: copy failed");
+    return -1;
+  }
+  return 0;
+}
+
+int from_native(Sector *s, VecType vt, const void *in, void *out) {
+  if (s->hub) return hub_permute(s, vt, in, out, false);
+  const size_t esz = (vt == kReal64) ? sizeof(double) : sizeof(cplx);
+  if (in != out && cudaMemcpyAsync(out, in, esz * (size_t)s->dim, cudaMemcpyDeviceToDevice, s->stream) != cudaSuccess) {
+    set_error("from_native: copy failed");
+    return -1;
+  }
+  return 0;
+}
+
+int native_observables(Sector *s, VecType vt, const void *v, double *d_out) {
+  if (s->hub) return hub_observables(s, vt, v, d_out);
+  return vec_diag_observables(s, vt, v, d_out);
 }
 
 }  // namespace hphi

@@ -16,8 +16,10 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 
 #include "engine.hpp"
+#include "hv_hubbard.hpp"
 
 namespace hphi {
 namespace {
@@ -297,6 +299,11 @@ int sector_build(const Model &m, int device, Sector **out, std::string *err) {
   diag_kernel<<<nsm * 8, 256, 0, s->stream>>>(s->dim, s->gc ? 1 : 0, s->d_list_1, s->d_dterms, s->ndterms, s->d_diag);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(s->stream));
+  // Specialised kernels (HPHI_B200_KERNEL=general keeps the general kernel).
+  const char *kern = getenv("HPHI_B200_KERNEL");
+  if (!(kern && std::string(kern) == "general")) {
+    if (hub_plan_build(s, err) != 0) return -1;
+  }
   *out = s;
   return 0;
 }
@@ -307,6 +314,7 @@ void sector_free(Sector *s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   cudaFree(s->d_list_1); cudaFree(s->d_list_2_1); cudaFree(s->d_list_2_2); cudaFree(s->d_diag);
   cudaFree(s->d_terms); cudaFree(s->d_dterms); cudaFree(s->d_red); cudaFree(s->d_scal);
+  hub_plan_free(s->hub);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }

@@ -38,7 +38,8 @@ typedef struct hphi_handle hphi_handle;
 #define HPHI_INFO_N_DIAG 9       /* compiled diagonal projector terms */
 #define HPHI_INFO_LANCZOS_MAX 10
 #define HPHI_INFO_NUM_AVE 11
-#define HPHI_INFO_COUNT 12
+#define HPHI_INFO_NATIVE_ORDER 12 /* 1 if the engine's native vector order differs from HPhi's */
+#define HPHI_INFO_COUNT 13
 
 /* Library version string. */
 const char *hphi_version(void);
@@ -104,13 +105,25 @@ int hphi_mltply_device(hphi_handle *h, int vec_type, void *d_v0, const void *d_v
                        double *prdct);
 
 /*
- * Asynchronous device form for callers that launch back to back: d_v0 = acc * d_v0 +
- * scale * (H d_v1) with (acc, scale) = d_coef[0..1] read on the device, and
- * d_prdct[0..1] = sum conj(d_v1) (H d_v1), all device pointers; enqueued on the
- * handle's stream (hphi_stream) without waiting.
+ * Asynchronous device form for callers that launch back to back, on vectors in the
+ * engine's NATIVE order (see hphi_to_native): d_v0 = acc * d_v0 + scale * (H d_v1)
+ * with (acc, scale) = d_coef[0..1] read on the device, and d_prdct[0..1] =
+ * sum conj(d_v1) (H d_v1), all device pointers; enqueued on the handle's stream
+ * (hphi_stream) without waiting.  acc == 0 never reads d_v0.
+ * Replaces: mltply (src/mltply.c:56-132) inside device-resident solver loops.
  */
 int hphi_mltply_device_async(hphi_handle *h, int vec_type, void *d_v0, const void *d_v1, const double *d_coef,
                              double *d_prdct);
+
+/*
+ * Native vector order.  For canonical Hubbard inputs the engine stores each block of
+ * HPhi's sector (rows sharing the upper half of the configuration, src/sz.c:993-1094)
+ * as an (up, down) product matrix; otherwise the native order is HPhi's order.  These
+ * permute 0-based device vectors between the two orders (d_in != d_out); they copy
+ * when the orders coincide.  No counterpart in the reference (HPhi has one order).
+ */
+int hphi_to_native(hphi_handle *h, int vec_type, const void *d_hphi, void *d_native);
+int hphi_from_native(hphi_handle *h, int vec_type, const void *d_native, void *d_hphi);
 
 /* The CUDA stream (cudaStream_t) the handle launches on, and a blocking wait on it. */
 void *hphi_stream(hphi_handle *h);

@@ -1,0 +1,134 @@
+"""The specialised Hubbard block kernel against the general kernel (both on the GPU,
+the general one pinned to the reference by test_gpu_parity), native-order round trips,
+and full-size H*v properties."""
+import os
+
+import numpy as np
+import pytest
+
+import hphi_b200
+from hphi_b200 import expert
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _open(path, general=False):
+    old = os.environ.get("HPHI_B200_KERNEL")
+    if general:
+        os.environ["HPHI_B200_KERNEL"] = "general"
+    else:
+        os.environ.pop("HPHI_B200_KERNEL", None)
+    try:
+        return hphi_b200.Hamiltonian(path)
+    finally:
+        if old is None:
+            os.environ.pop("HPHI_B200_KERNEL", None)
+        else:
+            os.environ["HPHI_B200_KERNEL"] = old
+
+
+def _hv_device(H, v1, v0, vt, acc=1.0, scale=1.0):
+    out = v0.clone()
+    pr = H.mltply_device(out.data_ptr(), v1.data_ptr(), vt, acc=acc, scale=scale)
+    return out, pr
+
+
+MODELS = {
+    "hub3x4": lambda: expert.hubbard(12, expert.square_bonds(3, 4), 1.0, 8.0, 6, 6),
+    "hub4x2_doped": lambda: expert.hubbard(8, expert.square_bonds(4, 2), 1.0, 4.0, 3, 2),
+    "hubchain10_complex_t": lambda: _complex_chain(10),
+    "hub_inter": lambda: _with_inter(),
+}
+
+
+def _complex_chain(L):
+    m = expert.hubbard(L, expert.chain_bonds(L), 1.0, 3.0, L // 2, L // 2)
+    m.trans = []
+    for i, j in expert.chain_bonds(L):
+        for s in (0, 1):
+            m.trans += [(i, s, j, s, 0.8, 0.3), (j, s, i, s, 0.8, -0.3)]
+    m.trans += [(0, 0, 0, 0, 0.2, 0.0)]
+    return m
+
+
+def _with_inter():
+    m = expert.hubbard(8, expert.square_bonds(2, 4), 1.0, 6.0, 4, 4)
+    m.coulombinter = [(i, j, 0.7) for i, j in expert.square_bonds(2, 4)]
+    m.hund = [(0, 5, 0.3)]
+    return m
+
+
+@pytest.mark.parametrize("name", list(MODELS))
+def test_block_kernel_matches_general_kernel(name, tmp_path):
+    path = MODELS[name]().write(str(tmp_path))
+    Hf = _open(path)
+    Hg = _open(path, general=True)
+    try:
+        assert Hf.info["native_order"] == 1, "block kernel should apply to this input"
+        assert Hg.info["native_order"] == 0
+        dim = Hf.dim
+        g = torch.Generator(device="cuda").manual_seed(5)
+        cplx = Hf.info["vec_type"] == hphi_b200.COMPLEX128 or "complex" in name
+        dt = torch.complex128 if cplx else torch.float64
+        vt = hphi_b200.COMPLEX128 if cplx else hphi_b200.REAL64
+        v1 = torch.randn(dim, dtype=dt, device="cuda", generator=g)
+        v0 = torch.randn(dim, dtype=dt, device="cuda", generator=g)
+        for acc, scale in ((1.0, 1.0), (0.0, 1.0), (-0.75, 1.3)):
+            yf, pf = _hv_device(Hf, v1, v0, vt, acc, scale)
+            yg, pg = _hv_device(Hg, v1, v0, vt, acc, scale)
+            err = (yf - yg).abs().max().item() / yg.abs().max().item()
+            assert err < 1e-12, (acc, scale, err)
+            assert abs(pf - pg) < 1e-10 * abs(pg)
+        # native order round trip
+        nat = torch.empty_like(v1)
+        back = torch.empty_like(v1)
+        Hf.to_native(v1.data_ptr(), nat.data_ptr(), vt)
+        Hf.from_native(nat.data_ptr(), back.data_ptr(), vt)
+        assert torch.equal(back, v1)
+        assert not torch.equal(nat, v1)
+    finally:
+        Hf.close()
+        Hg.close()
+
+
+def test_block_kernel_lanczos_energy(tmp_path):
+    """Lanczos through the native-order driver gives the general kernel's ground state."""
+    path = MODELS["hub3x4"]().write(str(tmp_path))
+    rng = np.random.default_rng(3)
+    Hf = _open(path)
+    v = np.zeros(Hf.dim + 1, dtype=np.complex128)
+    v[1:] = rng.uniform(-1, 1, Hf.dim)
+    v[1:] /= np.linalg.norm(v[1:])
+    rf = Hf.calc_by_lanczos(v_init=v)
+    Hf.close()
+    Hg = _open(path, general=True)
+    rg = Hg.calc_by_lanczos(v_init=v)
+    Hg.close()
+    assert rf["converged"] and rg["converged"]
+    assert abs(rf["e1"] - rg["e1"]) < 1e-10
+    assert abs(rf["e1"] - (-5.8334842575)) < 1e-9   # reference HPhi, 3x4 U=8 half filling
+
+
+def test_full_size_hubbard4x4_block_vs_general(tmp_path):
+    """Half-filled 4x4 Hubbard (dim 165,636,900): block kernel == general kernel to 1e-12,
+    and H is Hermitian: <u|Hv> = conj(<v|Hu>)."""
+    path = expert.hubbard(16, expert.square_bonds(4, 4), 1.0, 8.0, 8, 8).write(str(tmp_path))
+    Hf = _open(path)
+    assert Hf.info["native_order"] == 1
+    dim = Hf.dim
+    g = torch.Generator(device="cuda").manual_seed(11)
+    u = torch.rand(dim, dtype=torch.float64, device="cuda", generator=g) - 0.5
+    v = torch.rand(dim, dtype=torch.float64, device="cuda", generator=g) - 0.5
+    zero = torch.zeros_like(u)
+    Hu, _ = _hv_device(Hf, u, zero, hphi_b200.REAL64, acc=0.0)
+    Hv, _ = _hv_device(Hf, v, zero, hphi_b200.REAL64, acc=0.0)
+    a = torch.dot(u, Hv).item()
+    b = torch.dot(v, Hu).item()
+    assert abs(a - b) < 1e-11 * (abs(a) + abs(b))
+    Hf.close()
+    Hg = _open(path, general=True)
+    Hug, _ = _hv_device(Hg, u, zero, hphi_b200.REAL64, acc=0.0)
+    Hg.close()
+    err = (Hu - Hug).abs().max().item() / Hug.abs().max().item()
+    assert err < 1e-12
