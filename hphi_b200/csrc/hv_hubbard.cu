@@ -38,18 +38,19 @@ constexpr int kThreads = 256;
 constexpr int kMaxBlockTerms = 128;   // per-block hi / cross term lists
 
 struct HubTermDev {       // upper-half or cross hop (pull form on the full configuration)
-  uint64_t cm, cv, flip, sm;
+  uint32_t cm_hi, cv_hi;  // condition on the upper half (bits of c >> N)
+  uint32_t flip_hi;       // flip of the upper half
+  uint32_t sm;            // sign mask on the full configuration
   double re, im;
-  int lo_bit;             // cross: bit index inside ua / da (-1 for upper-half hops)
-  int lo_need;            // cross: required value of that bit in the output configuration
-  int spin;               // 0 up, 1 down
-  int pad;
+  int lo_bit;             // cross hops: bit of ua / da that moves (-1 for upper-half hops)
+  int lo_need;            // cross hops: value of that bit in the output configuration
 };
 
 struct HubArgs {
-  int nsite, L, N;                 // N = Nsite = bits per half
+  int L, N;                        // N = Nsite = bits per half, L = N/2 sites per half
   int nup, ndn;
-  uint64_t sdim;
+  int nblocks;                     // non-empty blocks
+  const uint32_t *order[2];        // block processing order: [0] by (db, ub), [1] by (ub, db)
   const uint32_t *list_2_2;        // block offsets + 1 (HPhi's list_2_2), 0 = empty block
   const uint16_t *rank;            // [2^L] rank of x among L-bit numbers of its popcount
   const uint16_t *unrank;          // [2^L] grouped by popcount, offsets unrank_off
@@ -60,24 +61,16 @@ struct HubArgs {
   const uint32_t *csr_up;          // entries: r' | term << 16
   const int *csr_dn_ptr;
   const uint32_t *csr_dn;
-  const double *lo_coef;           // [n_lo_terms][2]
-  const uint64_t *lo_sm;           // [n_lo_terms]
-  const HubTermDev *hi_terms;      // upper-half hops
-  int n_hi;
-  const HubTermDev *cross_terms;   // cross hops
-  int n_cross;
+  int n_csr_up, n_csr_dn, n_lo;
+  const double *lo_coef;           // [n_lo][2]
+  const uint32_t *lo_sm;           // [n_lo]
+  const HubTermDev *terms[2];      // [0] up-spin upper-half + cross hops, [1] down-spin
+  int n_hi[2], n_cross[2];         // terms[s] = n_hi[s] upper-half hops, then n_cross[s] cross hops
   const double *d_lo;              // diagonal, lower-half terms, per class pair in native order
   const int *d_lo_off;             // [(L+1)*(L+1)] offset of class pair (ku, kd)
   const double *d_hi;              // [2^N] diagonal, upper-half terms
   const DiagTerm *d_cross;         // diagonal terms spanning both halves
   int n_dcross;
-};
-
-struct BlockTerm {  // a term resolved for the current output block
-  uint64_t sm;
-  double re, im;
-  int64_t src;      // first element of the source block
-  int lo_bit, lo_need, spin, nsrc;  // nsrc: C(L, k') of the changed species in the source block
 };
 
 template <typename T>
@@ -88,139 +81,184 @@ template <>
 __device__ __forceinline__ cplx coef_mul<cplx>(double re, double im, cplx x) {
   return cplx{re * x.x - im * x.y, re * x.y + im * x.x};
 }
+__device__ __forceinline__ double sgn_of(uint32_t c, uint32_t sm) { return (__popc(c & sm) & 1) ? -1.0 : 1.0; }
 
-template <typename T>
-__global__ void __launch_bounds__(kThreads) hv_hub_kernel(HubArgs a, const T *__restrict__ v1, T *__restrict__ v0,
-                                                          const double *__restrict__ coef, double *__restrict__ part) {
-  extern __shared__ unsigned char smem_raw[];
-  T *xs = reinterpret_cast<T *>(smem_raw);
-  __shared__ BlockTerm hi_list[kMaxBlockTerms];
-  __shared__ BlockTerm cr_list[kMaxBlockTerms];
-  __shared__ int n_hi_blk, n_cr_blk;
+// Per-block resolved terms (SoA in shared memory).
+struct BlockTerms {
+  int64_t src[kMaxBlockTerms];
+  uint32_t sm[kMaxBlockTerms];
+  double re[kMaxBlockTerms], im[kMaxBlockTerms];
+  int bit[kMaxBlockTerms], need[kMaxBlockTerms], nsrc[kMaxBlockTerms];
+  int n_hi, n_cr;
+};
+
+// Phase 0 (up spin) and phase 1 (down spin) of the native-order Hubbard H*v.
+//   phase 0: v0 = acc*v0 + scale*(D + H_lo + H_up,hi + H_up,cross) v1   blocks in (db, ub) order
+//   phase 1: v0 += scale*(H_dn,hi + H_dn,cross) v1                       blocks in (ub, db) order
+// The up-spin hops of a block only reach blocks with the same down part db (and the
+// down-spin hops only blocks with the same ub), so in each phase the source blocks of the
+// CTAs in flight form a few L2-resident columns (rows) of the block grid.
+template <typename T, int PHASE>
+__global__ void __launch_bounds__(kThreads) hv_hub_phase(HubArgs a, const T *__restrict__ v1, T *__restrict__ v0,
+                                                         const double *__restrict__ coef, double *__restrict__ part) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ BlockTerms bl;
+  const int L = a.L, N = a.N, nx = 1 << L;
+  // shared tables: rank, unrank, spread (+ lower-half CSR in phase 0), then the staged block
+  unsigned char *sp = smem_raw;
+  uint32_t *s_spread = reinterpret_cast<uint32_t *>(sp); sp += sizeof(uint32_t) * nx;
+  uint16_t *s_rank = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * nx;
+  uint16_t *s_unrank = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * nx;
+  int *s_uoff = reinterpret_cast<int *>(sp); sp += sizeof(int) * 32;
+  int *s_binom = reinterpret_cast<int *>(sp); sp += sizeof(int) * 32;
+  int *s_up_ptr = nullptr, *s_dn_ptr = nullptr;
+  uint32_t *s_up = nullptr, *s_dn = nullptr, *s_losm = nullptr;
+  double *s_locoef = nullptr;
+  T *xs = nullptr;
+  if (PHASE == 0) {
+    s_up_ptr = reinterpret_cast<int *>(sp); sp += sizeof(int) * (nx + 1);
+    s_dn_ptr = reinterpret_cast<int *>(sp); sp += sizeof(int) * (nx + 1);
+    s_up = reinterpret_cast<uint32_t *>(sp); sp += sizeof(uint32_t) * a.n_csr_up;
+    s_dn = reinterpret_cast<uint32_t *>(sp); sp += sizeof(uint32_t) * a.n_csr_dn;
+    s_losm = reinterpret_cast<uint32_t *>(sp); sp += sizeof(uint32_t) * a.n_lo;
+    sp = smem_raw + (((sp - smem_raw) + 15) & ~(size_t)15);
+    s_locoef = reinterpret_cast<double *>(sp); sp += sizeof(double) * 2 * a.n_lo;
+    xs = reinterpret_cast<T *>(sp);
+  }
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    s_spread[i] = a.spread[i]; s_rank[i] = a.rank[i]; s_unrank[i] = a.unrank[i];
+  }
+  for (int i = threadIdx.x; i <= L + 1 && i < 32; i += blockDim.x) {
+    s_uoff[i] = a.unrank_off[i];
+    if (i <= L) s_binom[i] = a.binom[i];
+  }
+  if (PHASE == 0) {
+    for (int i = threadIdx.x; i <= nx; i += blockDim.x) { s_up_ptr[i] = a.csr_up_ptr[i]; s_dn_ptr[i] = a.csr_dn_ptr[i]; }
+    for (int i = threadIdx.x; i < a.n_csr_up; i += blockDim.x) s_up[i] = a.csr_up[i];
+    for (int i = threadIdx.x; i < a.n_csr_dn; i += blockDim.x) s_dn[i] = a.csr_dn[i];
+    for (int i = threadIdx.x; i < a.n_lo; i += blockDim.x) {
+      s_losm[i] = a.lo_sm[i]; s_locoef[2 * i] = a.lo_coef[2 * i]; s_locoef[2 * i + 1] = a.lo_coef[2 * i + 1];
+    }
+  }
+  __syncthreads();
   const double acc = coef[0], scale = coef[1];
-  const int N = a.N, L = a.L;
-  const uint64_t even_mask = 0x5555555555555555ull & ((N >= 64) ? ~0ull : ((1ull << N) - 1));
+  const uint32_t even_mask = 0x55555555u & ((N >= 32) ? 0xFFFFFFFFu : ((1u << N) - 1u));
+  const HubTermDev *terms = a.terms[PHASE];
+  const int n_hi = a.n_hi[PHASE], n_all = a.n_hi[PHASE] + a.n_cross[PHASE];
   double pr[2] = {0.0, 0.0};
 
-  for (uint64_t ib = blockIdx.x; ib < a.sdim; ib += gridDim.x) {
-    const uint32_t l22 = a.list_2_2[ib];
-    if (l22 == 0u) continue;
-    const int64_t jb = (int64_t)l22 - 1;
-    const int pu = __popcll(ib & even_mask), pd = __popcll(ib & (even_mask << 1));
-    const int nu = a.nup - pu, nd = a.ndn - pd;
-    const int nua = a.binom[nu], nda = a.binom[nd];
+  for (int bi = blockIdx.x; bi < a.nblocks; bi += gridDim.x) {
+    const uint32_t ib = a.order[PHASE][bi];
+    const int64_t jb = (int64_t)a.list_2_2[ib] - 1;
+    const int nu = a.nup - __popc(ib & even_mask), nd = a.ndn - __popc(ib & (even_mask << 1));
+    const int nua = s_binom[nu], nda = s_binom[nd];
     const int n = nua * nda;
-    const uint64_t chi = ib << N;
-    // stage the source block
-    for (int p = threadIdx.x; p < n; p += blockDim.x) xs[p] = v1[jb + p];
-    // resolve the block's upper-half and cross terms
+    const uint32_t chi = ib << N;
+    if (PHASE == 0)
+      for (int p = threadIdx.x; p < n; p += blockDim.x) xs[p] = v1[jb + p];
     if (threadIdx.x < 32) {
       int nh = 0, nc = 0;
-      for (int base = 0; base < a.n_hi + a.n_cross; base += 32) {
+      for (int base = 0; base < n_all; base += 32) {
         const int t = base + (int)threadIdx.x;
         bool take = false;
-        const HubTermDev *tt = nullptr;
-        if (t < a.n_hi + a.n_cross) {
-          tt = (t < a.n_hi) ? &a.hi_terms[t] : &a.cross_terms[t - a.n_hi];
-          const uint64_t cm_hi = tt->cm & ~((N >= 64) ? ~0ull : ((1ull << N) - 1));
-          const uint64_t cv_hi = tt->cv & cm_hi;
-          take = (chi & cm_hi) == cv_hi;
+        HubTermDev tt;
+        if (t < n_all) {
+          tt = terms[t];
+          take = (ib & tt.cm_hi) == tt.cv_hi;
         }
-        const unsigned mask = __ballot_sync(0xffffffffu, take && t < a.n_hi);
-        const unsigned maskc = __ballot_sync(0xffffffffu, take && t >= a.n_hi);
+        const bool is_hi = t < n_hi;
+        const unsigned mh = __ballot_sync(0xffffffffu, take && is_hi);
+        const unsigned mc = __ballot_sync(0xffffffffu, take && !is_hi);
         if (take) {
-          const uint64_t src_ib = ib ^ (tt->flip >> N);
-          const uint32_t sl = a.list_2_2[src_ib];
-          BlockTerm bt;
-          bt.sm = tt->sm; bt.re = tt->re; bt.im = tt->im;
-          bt.src = (sl == 0u) ? -1 : (int64_t)sl - 1;
-          bt.lo_bit = tt->lo_bit; bt.lo_need = tt->lo_need; bt.spin = tt->spin;
-          if (t < a.n_hi) {
-            bt.nsrc = 0;
-            const int slot = nh + __popc(mask & ((1u << threadIdx.x) - 1));
-            if (slot < kMaxBlockTerms) hi_list[slot] = bt;
-          } else {
-            // source class of the changed species: one particle more or fewer in the lower half
-            const int k_src = (tt->spin == 0 ? nu : nd) + (tt->lo_need ? -1 : 1);
-            bt.nsrc = (k_src >= 0 && k_src <= L) ? a.binom[k_src] : 0;
-            const int slot = nc + __popc(maskc & ((1u << threadIdx.x) - 1));
-            if (slot < kMaxBlockTerms) cr_list[slot] = bt;
-          }
+          const uint32_t sl = a.list_2_2[ib ^ tt.flip_hi];
+          const int slot = is_hi ? nh + __popc(mh & ((1u << threadIdx.x) - 1))
+                                 : kMaxBlockTerms - 1 - (nc + __popc(mc & ((1u << threadIdx.x) - 1)));
+          bl.src[slot] = (sl == 0u) ? -1 : (int64_t)sl - 1;
+          bl.sm[slot] = tt.sm; bl.re[slot] = tt.re; bl.im[slot] = tt.im;
+          bl.bit[slot] = tt.lo_bit; bl.need[slot] = tt.lo_need;
+          const int k_src = (PHASE == 0 ? nu : nd) + (tt.lo_need ? -1 : 1);
+          bl.nsrc[slot] = (!is_hi && k_src >= 0 && k_src <= L) ? s_binom[k_src] : 0;
         }
-        nh += __popc(mask);
-        nc += __popc(maskc);
+        nh += __popc(mh);
+        nc += __popc(mc);
       }
-      if (threadIdx.x == 0) {
-        n_hi_blk = min(nh, kMaxBlockTerms);
-        n_cr_blk = min(nc, kMaxBlockTerms);
-      }
+      if (threadIdx.x == 0) { bl.n_hi = nh; bl.n_cr = nc; }
     }
     __syncthreads();
-    const int nhb = n_hi_blk, ncb = n_cr_blk;
-    const int off_u = a.unrank_off[nu], off_d = a.unrank_off[nd];
+    const int nhb = bl.n_hi, ncb = bl.n_cr;
+    const int off_u = s_uoff[nu], off_d = s_uoff[nd];
     const uint32_t magic = (uint32_t)(0xFFFFFFFFull / (uint32_t)nda + 1ull);
-    const double dhi = a.d_hi[ib];
+    const double dhi = (PHASE == 0) ? a.d_hi[ib] : 0.0;
     const double *dlo = a.d_lo + a.d_lo_off[nu * (L + 1) + nd];
     for (int p = threadIdx.x; p < n; p += blockDim.x) {
       const int ra = (nda == 1) ? p : (int)__umulhi((uint32_t)p, magic);
       const int rd = p - ra * nda;
-      const uint32_t ua = a.unrank[off_u + ra], da = a.unrank[off_d + rd];
-      const uint64_t c = chi | (uint64_t)a.spread[ua] | ((uint64_t)a.spread[da] << 1);
-      const T x = xs[p];
-      double dg = dlo[p] + dhi;
-      for (int k = 0; k < a.n_dcross; k++) {
-        const DiagTerm dt = a.d_cross[k];
-        if ((c & dt.cm) == dt.cv) dg += dt.v;
-      }
-      T y = VT<T>::scale(dg, x);
-      // lower-half up hops: rows of the staged block
-      {
-        const int r0 = a.csr_up_ptr[off_u + ra], r1 = a.csr_up_ptr[off_u + ra + 1];
-        for (int e = r0; e < r1; e++) {
-          const uint32_t ent = a.csr_up[e];
-          const int rs = (int)(ent & 0xFFFFu), t = (int)(ent >> 16);
-          const double s = (__popcll(c & a.lo_sm[t]) & 1) ? -1.0 : 1.0;
-          y = VT<T>::add(y, coef_mul<T>(s * a.lo_coef[2 * t], s * a.lo_coef[2 * t + 1], xs[rs * nda + rd]));
+      const uint32_t ua = s_unrank[off_u + ra], da = s_unrank[off_d + rd];
+      const uint32_t c = chi | s_spread[ua] | (s_spread[da] << 1);
+      T x, y;
+      if (PHASE == 0) {
+        x = xs[p];
+        double dg = dlo[p] + dhi;
+        for (int k = 0; k < a.n_dcross; k++) {
+          const DiagTerm dt = a.d_cross[k];
+          if (((uint64_t)c & dt.cm) == dt.cv) dg += dt.v;
         }
-      }
-      // lower-half down hops: columns within the row
-      {
-        const int r0 = a.csr_dn_ptr[off_d + rd], r1 = a.csr_dn_ptr[off_d + rd + 1];
-        const T *row = xs + ra * nda;
-        for (int e = r0; e < r1; e++) {
-          const uint32_t ent = a.csr_dn[e];
-          const int rs = (int)(ent & 0xFFFFu), t = (int)(ent >> 16);
-          const double s = (__popcll(c & a.lo_sm[t]) & 1) ? -1.0 : 1.0;
-          y = VT<T>::add(y, coef_mul<T>(s * a.lo_coef[2 * t], s * a.lo_coef[2 * t + 1], row[rs]));
+        y = VT<T>::scale(dg, x);
+        {  // lower-half up hops: rows of the staged block
+          const int r0 = s_up_ptr[off_u + ra], r1 = s_up_ptr[off_u + ra + 1];
+          for (int e = r0; e < r1; e++) {
+            const uint32_t ent = s_up[e];
+            const int t = (int)(ent >> 16);
+            const double sg = sgn_of(c, s_losm[t]);
+            y = VT<T>::add(y, coef_mul<T>(sg * s_locoef[2 * t], sg * s_locoef[2 * t + 1], xs[(int)(ent & 0xFFFFu) * nda + rd]));
+          }
         }
+        {  // lower-half down hops: columns within the row
+          const int r0 = s_dn_ptr[off_d + rd], r1 = s_dn_ptr[off_d + rd + 1];
+          const T *row = xs + ra * nda;
+          for (int e = r0; e < r1; e++) {
+            const uint32_t ent = s_dn[e];
+            const int t = (int)(ent >> 16);
+            const double sg = sgn_of(c, s_losm[t]);
+            y = VT<T>::add(y, coef_mul<T>(sg * s_locoef[2 * t], sg * s_locoef[2 * t + 1], row[ent & 0xFFFFu]));
+          }
+        }
+      } else {
+        x = v1[jb + p];
+        y = VT<T>::zero();
       }
-      // upper-half hops: same position in another block of the same class
+      // upper-half hops of this phase's spin: the same position in a block of the same class
       for (int k = 0; k < nhb; k++) {
-        const BlockTerm &bt = hi_list[k];
-        if (bt.src < 0) continue;
-        const double s = (__popcll(c & bt.sm) & 1) ? -1.0 : 1.0;
-        y = VT<T>::add(y, coef_mul<T>(s * bt.re, s * bt.im, v1[bt.src + p]));
+        const int64_t src = bl.src[k];
+        if (src < 0) continue;
+        const double sg = sgn_of(c, bl.sm[k]);
+        y = VT<T>::add(y, coef_mul<T>(sg * bl.re[k], sg * bl.im[k], v1[src + p]));
       }
-      // cross hops: one particle moves between the halves
-      for (int k = 0; k < ncb; k++) {
-        const BlockTerm &bt = cr_list[k];
-        const uint32_t own = bt.spin == 0 ? ua : da;
-        if ((int)((own >> bt.lo_bit) & 1u) != bt.lo_need || bt.src < 0) continue;
-        const int r_new = a.rank[own ^ (1u << bt.lo_bit)];
-        const int64_t j = (bt.spin == 0) ? bt.src + (int64_t)r_new * nda + rd
-                                         : bt.src + (int64_t)ra * bt.nsrc + r_new;
-        const double s = (__popcll(c & bt.sm) & 1) ? -1.0 : 1.0;
-        y = VT<T>::add(y, coef_mul<T>(s * bt.re, s * bt.im, v1[j]));
+      // cross hops of this phase's spin
+      const uint32_t own = (PHASE == 0) ? ua : da;
+      for (int q = 0; q < ncb; q++) {
+        const int k = kMaxBlockTerms - 1 - q;
+        if ((int)((own >> bl.bit[k]) & 1u) != bl.need[k]) continue;
+        const int64_t src = bl.src[k];
+        if (src < 0) continue;
+        const int r_new = s_rank[own ^ (1u << bl.bit[k])];
+        const int64_t j = (PHASE == 0) ? src + (int64_t)r_new * nda + rd : src + (int64_t)ra * bl.nsrc[k] + r_new;
+        const double sg = sgn_of(c, bl.sm[k]);
+        y = VT<T>::add(y, coef_mul<T>(sg * bl.re[k], sg * bl.im[k], v1[j]));
       }
       pr[0] += VT<T>::conj_mul_re(x, y);
       pr[1] += VT<T>::conj_mul_im(x, y);
       y = VT<T>::scale(scale, y);
-      v0[jb + p] = (acc == 0.0) ? y : VT<T>::add(VT<T>::scale(acc, v0[jb + p]), y);
+      if (PHASE == 0) v0[jb + p] = (acc == 0.0) ? y : VT<T>::add(VT<T>::scale(acc, v0[jb + p]), y);
+      else v0[jb + p] = VT<T>::add(v0[jb + p], y);
     }
     __syncthreads();
   }
   block_sum<2>(pr);
-  if (threadIdx.x == 0) { part[2 * blockIdx.x] = pr[0]; part[2 * blockIdx.x + 1] = pr[1]; }
+  if (threadIdx.x == 0) {
+    part[2 * (PHASE * gridDim.x + blockIdx.x)] = pr[0];
+    part[2 * (PHASE * gridDim.x + blockIdx.x) + 1] = pr[1];
+  }
 }
 
 // ---- HPhi order <-> native order (per row r of HPhi's list_1)
@@ -250,10 +288,9 @@ __global__ void native_obs_kernel(HubArgs a, const T *__restrict__ v, double *__
   double o[6] = {0, 0, 0, 0, 0, 0};
   const int N = a.N, L = a.L;
   const uint64_t even_mask = 0x5555555555555555ull & ((1ull << N) - 1);
-  for (uint64_t ib = blockIdx.x; ib < a.sdim; ib += gridDim.x) {
-    const uint32_t l22 = a.list_2_2[ib];
-    if (l22 == 0u) continue;
-    const int64_t jb = (int64_t)l22 - 1;
+  for (int bi = blockIdx.x; bi < a.nblocks; bi += gridDim.x) {
+    const uint64_t ib = a.order[0][bi];
+    const int64_t jb = (int64_t)a.list_2_2[ib] - 1;
     const int nu = a.nup - __popcll(ib & even_mask), nd = a.ndn - __popcll(ib & (even_mask << 1));
     const int nda = a.binom[nd], n = a.binom[nu] * nda;
     const int off_u = a.unrank_off[nu], off_d = a.unrank_off[nd];
@@ -297,7 +334,7 @@ int upload(const std::vector<V> &h, V **d, std::string *err) {
 struct HubPlan {
   HubArgs args;
   std::vector<void *> allocs;
-  size_t smem_real = 0, smem_cplx = 0;
+  size_t smem[2][2] = {{0, 0}, {0, 0}};  // [phase][real, complex]
   int grid = 0;
   int n_lo_terms = 0;
 };
@@ -311,24 +348,26 @@ void hub_plan_free(HubPlan *p) {
 int hub_plan_build(Sector *s, std::string *err) {
   const Model &m = s->model;
   s->hub = nullptr;
-  if (m.calc_model != kHubbard || m.nsite % 2 != 0 || m.nsite > 30 || s->gc) return 0;
+  if (m.calc_model != kHubbard || m.nsite % 2 != 0 || m.nsite > 16 || s->gc) return 0;
   const int N = m.nsite, L = N / 2;
   const uint64_t lo_mask = (1ull << N) - 1;
   // classify off-diagonal terms; any term that is not a spin-conserving single hop
   // keeps the general kernel
   struct Hop { uint64_t cm, cv, flip, sm; double re, im; int p, q; };
-  std::vector<Hop> lo_up, lo_dn, hi, cross;
+  std::vector<Hop> lo_up, lo_dn, hi[2], cross[2];
   for (const BitTerm &t : m.offdiag) {
     if (__builtin_popcountll(t.flip) != 2 || t.cm != t.flip) return 0;
     const int p = __builtin_ctzll(t.flip), q = 63 - __builtin_clzll(t.flip);
     if ((p & 1) != (q & 1)) return 0;
     if (t.cv != (1ull << p) && t.cv != (1ull << q)) return 0;
     Hop h{t.cm, t.cv, t.flip, t.sm, t.re, t.im, p, q};
-    if (q < N) ((p & 1) ? lo_dn : lo_up).push_back(h);
-    else if (p >= N) hi.push_back(h);
-    else cross.push_back(h);
+    const int spin = p & 1;
+    if (q < N) (spin ? lo_dn : lo_up).push_back(h);
+    else if (p >= N) hi[spin].push_back(h);
+    else cross[spin].push_back(h);
   }
-  if ((int)(hi.size()) > kMaxBlockTerms || (int)cross.size() > kMaxBlockTerms) return 0;
+  for (int sp = 0; sp < 2; sp++)
+    if ((int)(hi[sp].size() + cross[sp].size()) > kMaxBlockTerms) return 0;
   const int nx = 1 << L;
   // rank / unrank / spread tables for L-bit half-species configurations
   std::vector<uint16_t> rank(nx), unrank(nx);
@@ -351,16 +390,15 @@ int hub_plan_build(Sector *s, std::string *err) {
       if (x >> b & 1) v |= 1u << (2 * b);
     spread[x] = v;
   }
-  if ((uint64_t)binom[L / 2] * (uint64_t)binom[L / 2] >= 65536ull) return 0;  // 16-bit positions
   // lower-half CSR: for species spin (0 up / 1 down), row = (class k, rank r) of that species;
   // entries reference the lower-half hop table lo_coef / lo_sm (ups first, then downs)
   std::vector<double> lo_coef;
-  std::vector<uint64_t> lo_sm;
+  std::vector<uint32_t> lo_sm;
   for (const auto *hops : {&lo_up, &lo_dn})
     for (const Hop &h : *hops) {
       lo_coef.push_back(h.re);
       lo_coef.push_back(h.im);
-      lo_sm.push_back(h.sm);
+      lo_sm.push_back((uint32_t)h.sm);
     }
   auto build_csr = [&](const std::vector<Hop> &hops, int spin, int id0, std::vector<int> *ptr,
                        std::vector<uint32_t> *ent) {
@@ -386,23 +424,25 @@ int hub_plan_build(Sector *s, std::string *err) {
   std::vector<uint32_t> up_ent, dn_ent;
   build_csr(lo_up, 0, 0, &up_ptr, &up_ent);
   build_csr(lo_dn, 1, (int)lo_up.size(), &dn_ptr, &dn_ent);
-  if (lo_coef.size() / 2 >= 65536) return 0;
-  auto to_dev = [&](const std::vector<Hop> &hops, bool is_cross) {
-    std::vector<HubTermDev> out;
-    for (const Hop &h : hops) {
-      HubTermDev d{};
-      d.cm = h.cm; d.cv = h.cv; d.flip = h.flip; d.sm = h.sm; d.re = h.re; d.im = h.im;
-      d.spin = h.p & 1;
-      d.lo_bit = -1; d.lo_need = 0;
-      if (is_cross) {
-        d.lo_bit = h.p >> 1;  // p is the lower-half end (p < N <= q)
-        d.lo_need = (int)((h.cv >> h.p) & 1ull);
+  // upper-half and cross hops per spin: hi first, then cross
+  std::vector<HubTermDev> terms[2];
+  for (int sp = 0; sp < 2; sp++) {
+    for (int pass = 0; pass < 2; pass++)
+      for (const Hop &h : (pass == 0 ? hi[sp] : cross[sp])) {
+        HubTermDev d{};
+        d.cm_hi = (uint32_t)(h.cm >> N);
+        d.cv_hi = (uint32_t)(h.cv >> N);
+        d.flip_hi = (uint32_t)(h.flip >> N);
+        d.sm = (uint32_t)h.sm;
+        d.re = h.re; d.im = h.im;
+        d.lo_bit = -1; d.lo_need = 0;
+        if (pass == 1) {
+          d.lo_bit = h.p >> 1;  // h.p is the lower-half end (p < N <= q)
+          d.lo_need = (int)((h.cv >> h.p) & 1ull);
+        }
+        terms[sp].push_back(d);
       }
-      out.push_back(d);
-    }
-    return out;
-  };
-  std::vector<HubTermDev> hi_dev = to_dev(hi, false), cross_dev = to_dev(cross, true);
+  }
   // diagonal split
   std::vector<DiagTerm> dlo_t, dhi_t, dcross;
   for (const DiagTerm &t : m.diag) {
@@ -434,10 +474,35 @@ int hub_plan_build(Sector *s, std::string *err) {
           dlo.push_back(v);
         }
     }
+  // block processing orders: phase 0 walks the block grid by columns (fixed db),
+  // phase 1 by rows (fixed ub)
+  std::vector<uint32_t> l22(s->sdim);
+  if (cudaMemcpy(l22.data(), s->d_list_2_2, sizeof(uint32_t) * s->sdim, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    *err = "hubbard plan: cannot read list_2_2";
+    return -1;
+  }
+  auto compress = [&](uint32_t x, int shift) {
+    uint32_t v = 0;
+    for (int b = 0; b < L; b++) v |= ((x >> (2 * b + shift)) & 1u) << b;
+    return v;
+  };
+  std::vector<uint32_t> ord0, ord1;
+  for (uint32_t ib = 0; ib < (uint32_t)s->sdim; ib++)
+    if (l22[ib]) ord0.push_back(ib);
+  ord1 = ord0;
+  std::stable_sort(ord0.begin(), ord0.end(), [&](uint32_t x, uint32_t y) {
+    const uint32_t dx = compress(x, 1), dy = compress(y, 1);
+    return dx != dy ? dx < dy : compress(x, 0) < compress(y, 0);
+  });
+  std::stable_sort(ord1.begin(), ord1.end(), [&](uint32_t x, uint32_t y) {
+    const uint32_t ux = compress(x, 0), uy = compress(y, 0);
+    return ux != uy ? ux < uy : compress(x, 1) < compress(y, 1);
+  });
 
   HubPlan *plan = new HubPlan();
   HubArgs &a = plan->args;
-  a.nsite = N; a.L = L; a.N = N; a.nup = m.nup; a.ndn = m.ndown; a.sdim = s->sdim;
+  a.L = L; a.N = N; a.nup = m.nup; a.ndn = m.ndown;
+  a.nblocks = (int)ord0.size();
   a.list_2_2 = s->d_list_2_2;
   auto up = [&](auto &vec, auto **dst) -> int {
     if (upload(vec, dst, err)) return -1;
@@ -446,39 +511,45 @@ int hub_plan_build(Sector *s, std::string *err) {
   };
   uint16_t *d_rank, *d_unrank;
   int *d_uoff, *d_binom, *d_up_ptr, *d_dn_ptr, *d_dlo_off;
-  uint32_t *d_spread, *d_up_ent, *d_dn_ent;
+  uint32_t *d_spread, *d_up_ent, *d_dn_ent, *d_lo_sm, *d_ord0, *d_ord1;
   double *d_lo_coef, *d_dlo, *d_dhi;
-  uint64_t *d_lo_sm;
-  HubTermDev *d_hi, *d_cross;
+  HubTermDev *d_t0, *d_t1;
   DiagTerm *d_dcross;
   if (up(rank, &d_rank) || up(unrank, &d_unrank) || up(unrank_off, &d_uoff) || up(binom, &d_binom) ||
       up(spread, &d_spread) || up(up_ptr, &d_up_ptr) || up(up_ent, &d_up_ent) || up(dn_ptr, &d_dn_ptr) ||
-      up(dn_ent, &d_dn_ent) || up(lo_coef, &d_lo_coef) || up(lo_sm, &d_lo_sm) || up(hi_dev, &d_hi) ||
-      up(cross_dev, &d_cross) || up(dlo, &d_dlo) || up(dlo_off, &d_dlo_off) || up(dhi, &d_dhi) ||
-      up(dcross, &d_dcross)) {
+      up(dn_ent, &d_dn_ent) || up(lo_coef, &d_lo_coef) || up(lo_sm, &d_lo_sm) || up(terms[0], &d_t0) ||
+      up(terms[1], &d_t1) || up(dlo, &d_dlo) || up(dlo_off, &d_dlo_off) || up(dhi, &d_dhi) ||
+      up(dcross, &d_dcross) || up(ord0, &d_ord0) || up(ord1, &d_ord1)) {
     hub_plan_free(plan);
     return -1;
   }
   a.rank = d_rank; a.unrank = d_unrank; a.unrank_off = d_uoff; a.binom = d_binom; a.spread = d_spread;
   a.csr_up_ptr = d_up_ptr; a.csr_up = d_up_ent; a.csr_dn_ptr = d_dn_ptr; a.csr_dn = d_dn_ent;
+  a.n_csr_up = (int)up_ent.size(); a.n_csr_dn = (int)dn_ent.size(); a.n_lo = (int)lo_sm.size();
   a.lo_coef = d_lo_coef; a.lo_sm = d_lo_sm;
-  a.hi_terms = d_hi; a.n_hi = (int)hi_dev.size();
-  a.cross_terms = d_cross; a.n_cross = (int)cross_dev.size();
+  a.terms[0] = d_t0; a.terms[1] = d_t1;
+  for (int sp = 0; sp < 2; sp++) { a.n_hi[sp] = (int)hi[sp].size(); a.n_cross[sp] = (int)cross[sp].size(); }
   a.d_lo = d_dlo; a.d_lo_off = d_dlo_off; a.d_hi = d_dhi; a.d_cross = d_dcross; a.n_dcross = (int)dcross.size();
-  plan->n_lo_terms = (int)lo_coef.size() / 2;
+  a.order[0] = d_ord0; a.order[1] = d_ord1;
+  plan->n_lo_terms = a.n_lo;
   int maxn = 0;
   for (int ku = 0; ku <= L; ku++)
     for (int kd = 0; kd <= L; kd++) maxn = std::max(maxn, binom[ku] * binom[kd]);
-  plan->smem_real = sizeof(double) * (size_t)maxn;
-  plan->smem_cplx = sizeof(cplx) * (size_t)maxn;
-  cudaFuncSetAttribute((const void *)hv_hub_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)plan->smem_real);
-  cudaFuncSetAttribute((const void *)hv_hub_kernel<cplx>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)plan->smem_cplx);
+  // dynamic shared memory: tables (+ lower-half CSR and the staged block in phase 0)
+  const size_t tables = sizeof(uint32_t) * nx + 2 * sizeof(uint16_t) * nx + 2 * sizeof(int) * 32;
+  size_t p0 = tables + 2 * sizeof(int) * (nx + 1) + sizeof(uint32_t) * (up_ent.size() + dn_ent.size() + lo_sm.size());
+  p0 = (p0 + 15) & ~(size_t)15;
+  p0 += sizeof(double) * 2 * lo_sm.size();
+  plan->smem[0][0] = p0 + sizeof(double) * (size_t)maxn;
+  plan->smem[0][1] = p0 + sizeof(cplx) * (size_t)maxn;
+  plan->smem[1][0] = plan->smem[1][1] = tables;
+  if (plan->smem[0][1] > 200 * 1024) { hub_plan_free(plan); return 0; }
+  cudaFuncSetAttribute((const void *)hv_hub_phase<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan->smem[0][0]);
+  cudaFuncSetAttribute((const void *)hv_hub_phase<cplx, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan->smem[0][1]);
   int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hv_hub_kernel<double>, kThreads, plan->smem_real);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hv_hub_phase<double, 0>, kThreads, plan->smem[0][0]);
   plan->grid = std::max(1, per_sm) * s->num_sms;
-  if (plan->grid > s->red_blocks) plan->grid = s->red_blocks;
+  if (2 * plan->grid > 4 * s->red_blocks) plan->grid = 2 * s->red_blocks;
   if (cudaGetLastError() != cudaSuccess) {
     *err = "hubbard plan: kernel configuration failed";
     hub_plan_free(plan);
@@ -496,13 +567,18 @@ int hub_hv_launch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const dou
     set_error("H has complex coefficients: real vectors are not allowed");
     return -1;
   }
-  if (vt == kReal64)
-    hv_hub_kernel<double><<<p->grid, kThreads, p->smem_real, s->stream>>>(p->args, (const double *)d_v1,
-                                                                          (double *)d_v0, d_coef, s->d_red);
-  else
-    hv_hub_kernel<cplx><<<p->grid, kThreads, p->smem_cplx, s->stream>>>(p->args, (const cplx *)d_v1, (cplx *)d_v0,
-                                                                        d_coef, s->d_red);
-  finalize_partials_kernel<2><<<1, 256, 0, s->stream>>>(s->d_red, p->grid, d_out);
+  if (vt == kReal64) {
+    hv_hub_phase<double, 0><<<p->grid, kThreads, p->smem[0][0], s->stream>>>(p->args, (const double *)d_v1,
+                                                                             (double *)d_v0, d_coef, s->d_red);
+    hv_hub_phase<double, 1><<<p->grid, kThreads, p->smem[1][0], s->stream>>>(p->args, (const double *)d_v1,
+                                                                             (double *)d_v0, d_coef, s->d_red);
+  } else {
+    hv_hub_phase<cplx, 0><<<p->grid, kThreads, p->smem[0][1], s->stream>>>(p->args, (const cplx *)d_v1,
+                                                                           (cplx *)d_v0, d_coef, s->d_red);
+    hv_hub_phase<cplx, 1><<<p->grid, kThreads, p->smem[1][1], s->stream>>>(p->args, (const cplx *)d_v1,
+                                                                           (cplx *)d_v0, d_coef, s->d_red);
+  }
+  finalize_partials_kernel<2><<<1, 256, 0, s->stream>>>(s->d_red, 2 * p->grid, d_out);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_error(std::string("hubbard hv launch failed: ") + cudaGetErrorString(e));
