@@ -1,25 +1,35 @@
-// Block kernel for canonical Hubbard Hamiltonians: H*v with every operand access
-// coalesced or conflict-free.
+// Block kernel for canonical Hubbard Hamiltonians.
 //
 // Applies when every off-diagonal term is a spin-conserving single hop c+_{i s} c_{j s}
-// (the Trans terms of a Hubbard model, src/mltplyHubbard.c:174-209 with the element
-// routine CisAjt, src/mltplyHubbardCore.c:305-347) and Nsite is even; diagonal terms
-// of any kind are allowed (src/diagonalcalc.c).  Other inputs use the general kernel.
+// (the Trans terms of a Hubbard model, src/mltplyHubbard.c:174-209, element routine
+// CisAjt src/mltplyHubbardCore.c:305-347) and Nsite is even and at most 16; diagonal
+// terms of any kind are allowed (src/diagonalcalc.c).  Other inputs use hv.cu.
 //
-// Layout ("native" order).  HPhi orders the sector by upper half ib and, inside a
-// block, by increasing lower half ia (src/sz.c:993-1094).  The native order keeps
-// HPhi's block offsets (list_2_2) but stores each block as a dense matrix
+// Native vector order.  HPhi orders the sector by upper half ib and, inside a block,
+// by increasing lower half ia (src/sz.c:993-1094).  The native order keeps HPhi's block
+// offsets (list_2_2) but stores block ib as a dense matrix
 //   pos = rank(ua) * C(L, pop(da)) + rank(da),
-// ua / da = the up / down occupations of the lower half (L = Nsite/2 sites).  The
-// kernel then applies, per output block ib (one CTA at a time, block staged in SMEM):
-//   lower-half up hops    rows of the staged block, warp-uniform CSR rows (conflict-free)
-//   lower-half down hops  columns within a row of the staged block (small CSR per column)
-//   upper-half hops       the same position in block ib ^ flip (coalesced global stream)
-//   cross hops (up)       one row of block ib ^ bit, row rank(ua ^ bit)   (coalesced)
-//   cross hops (down)     one row of block ib ^ bit, columns rank(da ^ bit)
-// Fermion signs are (-1)^popcount(c & sign_mask) on the full configuration c, exactly
-// as in the general kernel (SgnBit, src/bitcalc.c:338-352).  HPhi order is restored by
-// the permutation kernels at the boundary (hv_to_native / hv_from_native).
+// ua / da = up / down occupations of the lower half (L = Nsite/2 sites, ranks among
+// L-bit numbers of equal popcount).  The native basis also orders fermion modes
+// species-first (all up modes, then all down modes) instead of HPhi's interleaved bit
+// order; the two bases differ by a diagonal sign
+//   sigma(c) = (-1)^#{(down at i, up at j) : i < j},
+// applied by the boundary permutation.  In the species-first basis the sign of a hop
+// only counts occupied modes of its own species between its two sites, so every sign
+// is a property of the row (ua or da) or of the block (ub or db) and is folded into
+// precomputed coefficients.
+//
+// H*v runs in two passes over the block grid (ub, db):
+//   pass 0 (blocks ordered by db, then ub): v0 = acc*v0 + scale*(D + H_lower + H_up) v1
+//     lower-half up hops:    rows of the block staged in shared memory
+//     lower-half down hops:  entries within a row of the staged block
+//     upper-half up hops:    the same position in block (ub', db)        (coalesced)
+//     cross up hops:         row rank(ua ^ bit) of block (ub ^ bit, db)   (coalesced)
+//   pass 1 (blocks ordered by ub, then db): v0 += scale * H_down,upper+cross v1
+// Up hops never change db and down hops never change ub, so the source blocks of a
+// pass are the current column (row) of the block grid, a few MB that stay in L2.
+// Blocks are handed out through an atomic counter so the CTAs in flight stay within a
+// compact window of that order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,128 +45,126 @@ namespace hphi {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kMaxBlockTerms = 128;   // per-block hi / cross term lists
+constexpr int kMaxBlockTerms = 96;  // upper-half + cross hops of one spin
 
-struct HubTermDev {       // upper-half or cross hop (pull form on the full configuration)
-  uint32_t cm_hi, cv_hi;  // condition on the upper half (bits of c >> N)
-  uint32_t flip_hi;       // flip of the upper half
-  uint32_t sm;            // sign mask on the full configuration
-  double re, im;
-  int lo_bit;             // cross hops: bit of ua / da that moves (-1 for upper-half hops)
-  int lo_need;            // cross hops: value of that bit in the output configuration
+struct HubTermDev {    // upper-half or cross hop of one spin
+  uint32_t cm_hi, cv_hi, flip_hi;  // condition / flip on the upper half (bits of ib)
+  uint32_t btw_hi;                 // upper-half sites (as bits of ub or db) counted by the sign
+  double re, im;                   // operator coefficient
+  int lo_bit;                      // cross hops: lower-half site (bit of ua / da); -1 otherwise
+  int lo_need;                     // cross hops: occupation of that site in the output
 };
 
 struct HubArgs {
-  int L, N;                        // N = Nsite = bits per half, L = N/2 sites per half
-  int nup, ndn;
-  int nblocks;                     // non-empty blocks
-  const uint32_t *order[2];        // block processing order: [0] by (db, ub), [1] by (ub, db)
-  const uint32_t *list_2_2;        // block offsets + 1 (HPhi's list_2_2), 0 = empty block
-  const uint16_t *rank;            // [2^L] rank of x among L-bit numbers of its popcount
-  const uint16_t *unrank;          // [2^L] grouped by popcount, offsets unrank_off
+  int L, N, nup, ndn;
+  int nblocks;
+  const uint32_t *order[2];        // block processing order of pass 0 / pass 1
+  int *counter;                    // [2] block dispenser of each pass
+  const uint32_t *list_2_2;        // HPhi's list_2_2 (block offsets + 1)
+  const uint16_t *rank;            // [2^L]
+  const uint16_t *unrank;          // [2^L], grouped by popcount (offsets unrank_off)
   const int *unrank_off;           // [L+2]
-  const int *binom;                // [L+1] C(L, k)
-  const uint32_t *spread;          // [2^L] bits of x moved to even positions
-  const int *csr_up_ptr;           // [2^L + 1] rows ordered (k, r) like unrank
-  const uint32_t *csr_up;          // entries: r' | term << 16
-  const int *csr_dn_ptr;
-  const uint32_t *csr_dn;
-  int n_csr_up, n_csr_dn, n_lo;
-  const double *lo_coef;           // [n_lo][2]
-  const uint32_t *lo_sm;           // [n_lo]
-  const HubTermDev *terms[2];      // [0] up-spin upper-half + cross hops, [1] down-spin
-  int n_hi[2], n_cross[2];         // terms[s] = n_hi[s] upper-half hops, then n_cross[s] cross hops
-  const double *d_lo;              // diagonal, lower-half terms, per class pair in native order
-  const int *d_lo_off;             // [(L+1)*(L+1)] offset of class pair (ku, kd)
-  const double *d_hi;              // [2^N] diagonal, upper-half terms
-  const DiagTerm *d_cross;         // diagonal terms spanning both halves
+  const int *binom;                // [L+1]
+  const uint32_t *spread;          // [2^L] site bits -> even bit positions (HPhi layout)
+  const int *csr_ptr[2];           // [2^L + 1] lower-half hops of each spin, rows (k, r)
+  const uint16_t *csr_idx[2];      // source rank
+  const double *csr_val[2];        // signed coefficient (re, im)
+  int n_csr[2];
+  const HubTermDev *terms[2];      // per spin: n_hi upper-half hops, then n_cross cross hops
+  int n_hi[2], n_cross[2];
+  const double *d_lo;              // diagonal (lower-half terms) per class pair, native order
+  const int *d_lo_off;             // [(L+1)^2]
+  const double *d_hi;              // [2^N] diagonal (upper-half terms)
+  const DiagTerm *d_cross;         // diagonal terms spanning both halves (HPhi bit layout)
   int n_dcross;
 };
 
-template <typename T>
-__device__ __forceinline__ T coef_mul(double re, double im, T x);
-template <>
-__device__ __forceinline__ double coef_mul<double>(double re, double, double x) { return re * x; }
-template <>
-__device__ __forceinline__ cplx coef_mul<cplx>(double re, double im, cplx x) {
-  return cplx{re * x.x - im * x.y, re * x.y + im * x.x};
-}
-__device__ __forceinline__ double sgn_of(uint32_t c, uint32_t sm) { return (__popc(c & sm) & 1) ? -1.0 : 1.0; }
-
-// Per-block resolved terms (SoA in shared memory).
-struct BlockTerms {
+struct BlockTerms {  // the current block's upper-half and cross hops, signs resolved
   int64_t src[kMaxBlockTerms];
-  uint32_t sm[kMaxBlockTerms];
   double re[kMaxBlockTerms], im[kMaxBlockTerms];
   int bit[kMaxBlockTerms], need[kMaxBlockTerms], nsrc[kMaxBlockTerms];
-  int n_hi, n_cr;
+  int n_hi, n_cr, bi;
 };
 
-// Phase 0 (up spin) and phase 1 (down spin) of the native-order Hubbard H*v.
-//   phase 0: v0 = acc*v0 + scale*(D + H_lo + H_up,hi + H_up,cross) v1   blocks in (db, ub) order
-//   phase 1: v0 += scale*(H_dn,hi + H_dn,cross) v1                       blocks in (ub, db) order
-// The up-spin hops of a block only reach blocks with the same down part db (and the
-// down-spin hops only blocks with the same ub), so in each phase the source blocks of the
-// CTAs in flight form a few L2-resident columns (rows) of the block grid.
-template <typename T, int PHASE>
-__global__ void __launch_bounds__(kThreads) hv_hub_phase(HubArgs a, const T *__restrict__ v1, T *__restrict__ v0,
-                                                         const double *__restrict__ coef, double *__restrict__ part) {
+template <typename T>
+__device__ __forceinline__ T cfma(double re, double im, T x, T y);
+template <>
+__device__ __forceinline__ double cfma<double>(double re, double, double x, double y) { return fma(re, x, y); }
+template <>
+__device__ __forceinline__ cplx cfma<cplx>(double re, double im, cplx x, cplx y) {
+  return cplx{fma(re, x.x, fma(-im, x.y, y.x)), fma(re, x.y, fma(im, x.x, y.y))};
+}
+
+__host__ __device__ __forceinline__ uint32_t compress_bits(uint32_t x, int shift, int L) {
+  uint32_t v = 0;
+  for (int b = 0; b < L; b++) v |= ((x >> (2 * b + shift)) & 1u) << b;
+  return v;
+}
+
+template <typename T, int PASS>
+__global__ void __launch_bounds__(kThreads) hv_hub_pass(HubArgs a, const T *__restrict__ v1, T *__restrict__ v0,
+                                                        const double *__restrict__ coef, double *__restrict__ part) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ BlockTerms bl;
   const int L = a.L, N = a.N, nx = 1 << L;
-  // shared tables: rank, unrank, spread (+ lower-half CSR in phase 0), then the staged block
+  // shared tables (pass 0 also holds the lower-half CSR of both spins and the staged block)
   unsigned char *sp = smem_raw;
-  uint32_t *s_spread = reinterpret_cast<uint32_t *>(sp); sp += sizeof(uint32_t) * nx;
-  uint16_t *s_rank = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * nx;
-  uint16_t *s_unrank = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * nx;
+  double *s_val[2] = {nullptr, nullptr};
+  int *s_ptr[2] = {nullptr, nullptr};
+  uint16_t *s_idx[2] = {nullptr, nullptr};
+  if (PASS == 0) {
+    s_val[0] = reinterpret_cast<double *>(sp); sp += sizeof(double) * 2 * a.n_csr[0];
+    s_val[1] = reinterpret_cast<double *>(sp); sp += sizeof(double) * 2 * a.n_csr[1];
+    s_ptr[0] = reinterpret_cast<int *>(sp); sp += sizeof(int) * (nx + 1);
+    s_ptr[1] = reinterpret_cast<int *>(sp); sp += sizeof(int) * (nx + 1);
+  }
   int *s_uoff = reinterpret_cast<int *>(sp); sp += sizeof(int) * 32;
   int *s_binom = reinterpret_cast<int *>(sp); sp += sizeof(int) * 32;
-  int *s_up_ptr = nullptr, *s_dn_ptr = nullptr;
-  uint32_t *s_up = nullptr, *s_dn = nullptr, *s_losm = nullptr;
-  double *s_locoef = nullptr;
-  T *xs = nullptr;
-  if (PHASE == 0) {
-    s_up_ptr = reinterpret_cast<int *>(sp); sp += sizeof(int) * (nx + 1);
-    s_dn_ptr = reinterpret_cast<int *>(sp); sp += sizeof(int) * (nx + 1);
-    s_up = reinterpret_cast<uint32_t *>(sp); sp += sizeof(uint32_t) * a.n_csr_up;
-    s_dn = reinterpret_cast<uint32_t *>(sp); sp += sizeof(uint32_t) * a.n_csr_dn;
-    s_losm = reinterpret_cast<uint32_t *>(sp); sp += sizeof(uint32_t) * a.n_lo;
-    sp = smem_raw + (((sp - smem_raw) + 15) & ~(size_t)15);
-    s_locoef = reinterpret_cast<double *>(sp); sp += sizeof(double) * 2 * a.n_lo;
-    xs = reinterpret_cast<T *>(sp);
+  uint16_t *s_rank = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * nx;
+  uint16_t *s_unrank = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * nx;
+  if (PASS == 0) {
+    s_idx[0] = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * a.n_csr[0];
+    s_idx[1] = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * a.n_csr[1];
   }
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-    s_spread[i] = a.spread[i]; s_rank[i] = a.rank[i]; s_unrank[i] = a.unrank[i];
+  sp = smem_raw + (((sp - smem_raw) + 15) & ~(size_t)15);
+  T *xs = reinterpret_cast<T *>(sp);
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) { s_rank[i] = a.rank[i]; s_unrank[i] = a.unrank[i]; }
+  for (int i = threadIdx.x; i < 32; i += blockDim.x) {
+    s_uoff[i] = (i <= L + 1) ? a.unrank_off[i] : 0;
+    s_binom[i] = (i <= L) ? a.binom[i] : 0;
   }
-  for (int i = threadIdx.x; i <= L + 1 && i < 32; i += blockDim.x) {
-    s_uoff[i] = a.unrank_off[i];
-    if (i <= L) s_binom[i] = a.binom[i];
-  }
-  if (PHASE == 0) {
-    for (int i = threadIdx.x; i <= nx; i += blockDim.x) { s_up_ptr[i] = a.csr_up_ptr[i]; s_dn_ptr[i] = a.csr_dn_ptr[i]; }
-    for (int i = threadIdx.x; i < a.n_csr_up; i += blockDim.x) s_up[i] = a.csr_up[i];
-    for (int i = threadIdx.x; i < a.n_csr_dn; i += blockDim.x) s_dn[i] = a.csr_dn[i];
-    for (int i = threadIdx.x; i < a.n_lo; i += blockDim.x) {
-      s_losm[i] = a.lo_sm[i]; s_locoef[2 * i] = a.lo_coef[2 * i]; s_locoef[2 * i + 1] = a.lo_coef[2 * i + 1];
+  if (PASS == 0) {
+    for (int q = 0; q < 2; q++) {
+      for (int i = threadIdx.x; i <= nx; i += blockDim.x) s_ptr[q][i] = a.csr_ptr[q][i];
+      for (int i = threadIdx.x; i < a.n_csr[q]; i += blockDim.x) {
+        s_idx[q][i] = a.csr_idx[q][i];
+        s_val[q][2 * i] = a.csr_val[q][2 * i];
+        s_val[q][2 * i + 1] = a.csr_val[q][2 * i + 1];
+      }
     }
   }
   __syncthreads();
   const double acc = coef[0], scale = coef[1];
-  const uint32_t even_mask = 0x55555555u & ((N >= 32) ? 0xFFFFFFFFu : ((1u << N) - 1u));
-  const HubTermDev *terms = a.terms[PHASE];
-  const int n_hi = a.n_hi[PHASE], n_all = a.n_hi[PHASE] + a.n_cross[PHASE];
+  const uint32_t even_mask = 0x55555555u & ((1u << N) - 1u);
+  const HubTermDev *terms = a.terms[PASS];
+  const int n_hi = a.n_hi[PASS], n_all = a.n_hi[PASS] + a.n_cross[PASS];
   double pr[2] = {0.0, 0.0};
 
-  for (int bi = blockIdx.x; bi < a.nblocks; bi += gridDim.x) {
-    const uint32_t ib = a.order[PHASE][bi];
+  while (true) {
+    if (threadIdx.x == 0) bl.bi = atomicAdd(&a.counter[PASS], 1);
+    __syncthreads();
+    const int bi = bl.bi;
+    if (bi >= a.nblocks) break;
+    const uint32_t ib = a.order[PASS][bi];
     const int64_t jb = (int64_t)a.list_2_2[ib] - 1;
     const int nu = a.nup - __popc(ib & even_mask), nd = a.ndn - __popc(ib & (even_mask << 1));
     const int nua = s_binom[nu], nda = s_binom[nd];
     const int n = nua * nda;
-    const uint32_t chi = ib << N;
-    if (PHASE == 0)
+    if (PASS == 0)
       for (int p = threadIdx.x; p < n; p += blockDim.x) xs[p] = v1[jb + p];
     if (threadIdx.x < 32) {
+      // resolve this block's hops of the pass's spin: source block and block-level sign
+      const uint32_t own_hi = compress_bits(ib, PASS, L);  // ub (pass 0) or db (pass 1)
       int nh = 0, nc = 0;
       for (int base = 0; base < n_all; base += 32) {
         const int t = base + (int)threadIdx.x;
@@ -173,10 +181,13 @@ __global__ void __launch_bounds__(kThreads) hv_hub_phase(HubArgs a, const T *__r
           const uint32_t sl = a.list_2_2[ib ^ tt.flip_hi];
           const int slot = is_hi ? nh + __popc(mh & ((1u << threadIdx.x) - 1))
                                  : kMaxBlockTerms - 1 - (nc + __popc(mc & ((1u << threadIdx.x) - 1)));
+          const double sg = (__popc(own_hi & tt.btw_hi) & 1) ? -1.0 : 1.0;
           bl.src[slot] = (sl == 0u) ? -1 : (int64_t)sl - 1;
-          bl.sm[slot] = tt.sm; bl.re[slot] = tt.re; bl.im[slot] = tt.im;
-          bl.bit[slot] = tt.lo_bit; bl.need[slot] = tt.lo_need;
-          const int k_src = (PHASE == 0 ? nu : nd) + (tt.lo_need ? -1 : 1);
+          bl.re[slot] = sg * tt.re;
+          bl.im[slot] = sg * tt.im;
+          bl.bit[slot] = tt.lo_bit;
+          bl.need[slot] = tt.lo_need;
+          const int k_src = (PASS == 0 ? nu : nd) + (tt.lo_need ? -1 : 1);
           bl.nsrc[slot] = (!is_hi && k_src >= 0 && k_src <= L) ? s_binom[k_src] : 0;
         }
         nh += __popc(mh);
@@ -188,80 +199,80 @@ __global__ void __launch_bounds__(kThreads) hv_hub_phase(HubArgs a, const T *__r
     const int nhb = bl.n_hi, ncb = bl.n_cr;
     const int off_u = s_uoff[nu], off_d = s_uoff[nd];
     const uint32_t magic = (uint32_t)(0xFFFFFFFFull / (uint32_t)nda + 1ull);
-    const double dhi = (PHASE == 0) ? a.d_hi[ib] : 0.0;
+    const double dhi = (PASS == 0) ? a.d_hi[ib] : 0.0;
     const double *dlo = a.d_lo + a.d_lo_off[nu * (L + 1) + nd];
     for (int p = threadIdx.x; p < n; p += blockDim.x) {
       const int ra = (nda == 1) ? p : (int)__umulhi((uint32_t)p, magic);
       const int rd = p - ra * nda;
       const uint32_t ua = s_unrank[off_u + ra], da = s_unrank[off_d + rd];
-      const uint32_t c = chi | s_spread[ua] | (s_spread[da] << 1);
       T x, y;
-      if (PHASE == 0) {
+      if (PASS == 0) {
         x = xs[p];
         double dg = dlo[p] + dhi;
-        for (int k = 0; k < a.n_dcross; k++) {
-          const DiagTerm dt = a.d_cross[k];
-          if (((uint64_t)c & dt.cm) == dt.cv) dg += dt.v;
+        if (a.n_dcross) {
+          const uint64_t c = ((uint64_t)ib << N) | a.spread[ua] | ((uint64_t)a.spread[da] << 1);
+          for (int k = 0; k < a.n_dcross; k++) {
+            const DiagTerm dt = a.d_cross[k];
+            if ((c & dt.cm) == dt.cv) dg += dt.v;
+          }
         }
         y = VT<T>::scale(dg, x);
         {  // lower-half up hops: rows of the staged block
-          const int r0 = s_up_ptr[off_u + ra], r1 = s_up_ptr[off_u + ra + 1];
-          for (int e = r0; e < r1; e++) {
-            const uint32_t ent = s_up[e];
-            const int t = (int)(ent >> 16);
-            const double sg = sgn_of(c, s_losm[t]);
-            y = VT<T>::add(y, coef_mul<T>(sg * s_locoef[2 * t], sg * s_locoef[2 * t + 1], xs[(int)(ent & 0xFFFFu) * nda + rd]));
-          }
+          const int r0 = s_ptr[0][off_u + ra], r1 = s_ptr[0][off_u + ra + 1];
+          for (int e = r0; e < r1; e++)
+            y = cfma<T>(s_val[0][2 * e], s_val[0][2 * e + 1], xs[(int)s_idx[0][e] * nda + rd], y);
         }
-        {  // lower-half down hops: columns within the row
-          const int r0 = s_dn_ptr[off_d + rd], r1 = s_dn_ptr[off_d + rd + 1];
+        {  // lower-half down hops: entries of the row
+          const int r0 = s_ptr[1][off_d + rd], r1 = s_ptr[1][off_d + rd + 1];
           const T *row = xs + ra * nda;
-          for (int e = r0; e < r1; e++) {
-            const uint32_t ent = s_dn[e];
-            const int t = (int)(ent >> 16);
-            const double sg = sgn_of(c, s_losm[t]);
-            y = VT<T>::add(y, coef_mul<T>(sg * s_locoef[2 * t], sg * s_locoef[2 * t + 1], row[ent & 0xFFFFu]));
-          }
+          for (int e = r0; e < r1; e++) y = cfma<T>(s_val[1][2 * e], s_val[1][2 * e + 1], row[s_idx[1][e]], y);
         }
       } else {
         x = v1[jb + p];
         y = VT<T>::zero();
       }
-      // upper-half hops of this phase's spin: the same position in a block of the same class
+      // upper-half hops: the same position in a block of the same class
       for (int k = 0; k < nhb; k++) {
         const int64_t src = bl.src[k];
-        if (src < 0) continue;
-        const double sg = sgn_of(c, bl.sm[k]);
-        y = VT<T>::add(y, coef_mul<T>(sg * bl.re[k], sg * bl.im[k], v1[src + p]));
+        if (src >= 0) y = cfma<T>(bl.re[k], bl.im[k], v1[src + p], y);
       }
-      // cross hops of this phase's spin
-      const uint32_t own = (PHASE == 0) ? ua : da;
+      // cross hops: one particle of this spin changes half
+      const uint32_t own = (PASS == 0) ? ua : da;
       for (int q = 0; q < ncb; q++) {
         const int k = kMaxBlockTerms - 1 - q;
-        if ((int)((own >> bl.bit[k]) & 1u) != bl.need[k]) continue;
-        const int64_t src = bl.src[k];
-        if (src < 0) continue;
-        const int r_new = s_rank[own ^ (1u << bl.bit[k])];
-        const int64_t j = (PHASE == 0) ? src + (int64_t)r_new * nda + rd : src + (int64_t)ra * bl.nsrc[k] + r_new;
-        const double sg = sgn_of(c, bl.sm[k]);
-        y = VT<T>::add(y, coef_mul<T>(sg * bl.re[k], sg * bl.im[k], v1[j]));
+        const int b = bl.bit[k];
+        if ((int)((own >> b) & 1u) != bl.need[k] || bl.src[k] < 0) continue;
+        const int r_new = s_rank[own ^ (1u << b)];
+        const int64_t j = (PASS == 0) ? bl.src[k] + (int64_t)r_new * nda + rd : bl.src[k] + (int64_t)ra * bl.nsrc[k] + r_new;
+        const double sg = (__popc(own >> (b + 1)) & 1) ? -1.0 : 1.0;
+        y = cfma<T>(sg * bl.re[k], sg * bl.im[k], v1[j], y);
       }
       pr[0] += VT<T>::conj_mul_re(x, y);
       pr[1] += VT<T>::conj_mul_im(x, y);
       y = VT<T>::scale(scale, y);
-      if (PHASE == 0) v0[jb + p] = (acc == 0.0) ? y : VT<T>::add(VT<T>::scale(acc, v0[jb + p]), y);
+      if (PASS == 0) v0[jb + p] = (acc == 0.0) ? y : VT<T>::add(VT<T>::scale(acc, v0[jb + p]), y);
       else v0[jb + p] = VT<T>::add(v0[jb + p], y);
     }
     __syncthreads();
   }
   block_sum<2>(pr);
   if (threadIdx.x == 0) {
-    part[2 * (PHASE * gridDim.x + blockIdx.x)] = pr[0];
-    part[2 * (PHASE * gridDim.x + blockIdx.x) + 1] = pr[1];
+    part[2 * (PASS * gridDim.x + blockIdx.x)] = pr[0];
+    part[2 * (PASS * gridDim.x + blockIdx.x) + 1] = pr[1];
   }
 }
 
-// ---- HPhi order <-> native order (per row r of HPhi's list_1)
+// sigma(c) of the species-first basis: (-1)^#{(down at i, up at j) : i < j}.
+__device__ __forceinline__ int species_sign(uint64_t c, int nsite) {
+  int cnt = 0, downs = 0;
+  for (int s = 0; s < nsite; s++) {
+    if ((c >> (2 * s)) & 1ull) cnt += downs;
+    downs += (int)((c >> (2 * s + 1)) & 1ull);
+  }
+  return cnt & 1;
+}
+
+// HPhi order <-> native order, per row r of HPhi's list_1 (sign sigma applied both ways).
 template <typename T, bool TO_NATIVE>
 __global__ void permute_kernel(int64_t dim, int N, int L, const uint64_t *__restrict__ list_1,
                                const uint32_t *__restrict__ list_2_2, const uint16_t *__restrict__ rank,
@@ -269,35 +280,30 @@ __global__ void permute_kernel(int64_t dim, int N, int L, const uint64_t *__rest
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < dim; r += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t c = list_1[r];
     const uint64_t ib = c >> N;
-    const uint64_t ia = c & ((1ull << N) - 1);
-    uint32_t ua = 0, da = 0;
-    for (int s = 0; s < L; s++) {
-      ua |= (uint32_t)((ia >> (2 * s)) & 1ull) << s;
-      da |= (uint32_t)((ia >> (2 * s + 1)) & 1ull) << s;
-    }
-    const int64_t jb = (int64_t)list_2_2[ib] - 1;
-    const int64_t pos = jb + (int64_t)rank[ua] * binom[__popc(da)] + rank[da];
-    if (TO_NATIVE) out[pos] = in[r];
-    else out[r] = in[pos];
+    const uint32_t ia = (uint32_t)(c & ((1ull << N) - 1));
+    const uint32_t ua = compress_bits(ia, 0, L), da = compress_bits(ia, 1, L);
+    const int64_t pos = (int64_t)list_2_2[ib] - 1 + (int64_t)rank[ua] * binom[__popc(da)] + rank[da];
+    const double sg = species_sign(c, N) ? -1.0 : 1.0;
+    if (TO_NATIVE) out[pos] = VT<T>::scale(sg, in[r]);
+    else out[r] = VT<T>::scale(sg, in[pos]);
   }
 }
 
-// Diagonal observables in native order (expec_energy_flct_Hubbard, src/expec_energy_flct.c).
+// Diagonal observables in native order (expec_energy_flct_Hubbard, src/expec_energy_flct.c:259-330).
 template <typename T>
 __global__ void native_obs_kernel(HubArgs a, const T *__restrict__ v, double *__restrict__ part) {
   double o[6] = {0, 0, 0, 0, 0, 0};
-  const int N = a.N, L = a.L;
-  const uint64_t even_mask = 0x5555555555555555ull & ((1ull << N) - 1);
+  const int N = a.N;
+  const uint32_t even_mask = 0x55555555u & ((1u << N) - 1u);
   for (int bi = blockIdx.x; bi < a.nblocks; bi += gridDim.x) {
-    const uint64_t ib = a.order[0][bi];
+    const uint32_t ib = a.order[0][bi];
     const int64_t jb = (int64_t)a.list_2_2[ib] - 1;
-    const int nu = a.nup - __popcll(ib & even_mask), nd = a.ndn - __popcll(ib & (even_mask << 1));
+    const int nu = a.nup - __popc(ib & even_mask), nd = a.ndn - __popc(ib & (even_mask << 1));
     const int nda = a.binom[nd], n = a.binom[nu] * nda;
     const int off_u = a.unrank_off[nu], off_d = a.unrank_off[nd];
-    (void)L;
     for (int p = threadIdx.x; p < n; p += blockDim.x) {
       const int ra = p / nda, rd = p - ra * nda;
-      const uint64_t c = (ib << N) | (uint64_t)a.spread[a.unrank[off_u + ra]] |
+      const uint64_t c = ((uint64_t)ib << N) | (uint64_t)a.spread[a.unrank[off_u + ra]] |
                          ((uint64_t)a.spread[a.unrank[off_d + rd]] << 1);
       const double w = VT<T>::abs2(v[jb + p]);
       const uint64_t ev = 0x5555555555555555ull;
@@ -320,10 +326,13 @@ uint64_t binom_u(int n, int k) {
 
 template <typename V>
 int upload(const std::vector<V> &h, V **d, std::string *err) {
-  if (h.empty()) { *d = nullptr; return 0; }
-  if (cudaMalloc(d, sizeof(V) * h.size()) != cudaSuccess ||
-      cudaMemcpy(*d, h.data(), sizeof(V) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+  const size_t bytes = h.empty() ? 16 : sizeof(V) * h.size();  // empty tables keep a valid pointer
+  if (cudaMalloc(d, bytes) != cudaSuccess) {
     *err = "hubbard plan: device allocation failed";
+    return -1;
+  }
+  if (!h.empty() && cudaMemcpy(*d, h.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+    *err = "hubbard plan: copy failed";
     return -1;
   }
   return 0;
@@ -334,9 +343,8 @@ int upload(const std::vector<V> &h, V **d, std::string *err) {
 struct HubPlan {
   HubArgs args;
   std::vector<void *> allocs;
-  size_t smem[2][2] = {{0, 0}, {0, 0}};  // [phase][real, complex]
+  size_t smem[2][2] = {{0, 0}, {0, 0}};  // [pass][real, complex]
   int grid = 0;
-  int n_lo_terms = 0;
 };
 
 void hub_plan_free(HubPlan *p) {
@@ -351,25 +359,26 @@ int hub_plan_build(Sector *s, std::string *err) {
   if (m.calc_model != kHubbard || m.nsite % 2 != 0 || m.nsite > 16 || s->gc) return 0;
   const int N = m.nsite, L = N / 2;
   const uint64_t lo_mask = (1ull << N) - 1;
-  // classify off-diagonal terms; any term that is not a spin-conserving single hop
-  // keeps the general kernel
-  struct Hop { uint64_t cm, cv, flip, sm; double re, im; int p, q; };
-  std::vector<Hop> lo_up, lo_dn, hi[2], cross[2];
+  // Hops: site i (created) <- site j (annihilated), spin, operator coefficient.  The
+  // compiled term carries HPhi's interleaved-order sign; its operator coefficient is the
+  // amplitude on the configuration holding only the created particle (no modes between).
+  struct Hop { int i, j, spin; double re, im; uint64_t cm, cv, flip; };
+  std::vector<Hop> lo[2], hi[2], cross[2];
   for (const BitTerm &t : m.offdiag) {
     if (__builtin_popcountll(t.flip) != 2 || t.cm != t.flip) return 0;
     const int p = __builtin_ctzll(t.flip), q = 63 - __builtin_clzll(t.flip);
     if ((p & 1) != (q & 1)) return 0;
     if (t.cv != (1ull << p) && t.cv != (1ull << q)) return 0;
-    Hop h{t.cm, t.cv, t.flip, t.sm, t.re, t.im, p, q};
-    const int spin = p & 1;
-    if (q < N) (spin ? lo_dn : lo_up).push_back(h);
-    else if (p >= N) hi[spin].push_back(h);
-    else cross[spin].push_back(h);
+    const int created = __builtin_ctzll(t.cv), annihilated = (created == p) ? q : p;
+    const double sg = (__builtin_popcountll(t.cv & t.sm) & 1) ? -1.0 : 1.0;
+    Hop h{created >> 1, annihilated >> 1, p & 1, sg * t.re, sg * t.im, t.cm, t.cv, t.flip};
+    if (q < N) lo[h.spin].push_back(h);
+    else if (p >= N) hi[h.spin].push_back(h);
+    else cross[h.spin].push_back(h);
   }
   for (int sp = 0; sp < 2; sp++)
     if ((int)(hi[sp].size() + cross[sp].size()) > kMaxBlockTerms) return 0;
   const int nx = 1 << L;
-  // rank / unrank / spread tables for L-bit half-species configurations
   std::vector<uint16_t> rank(nx), unrank(nx);
   std::vector<int> unrank_off(L + 2, 0), binom(L + 1);
   for (int k = 0; k <= L; k++) binom[k] = (int)binom_u(L, k);
@@ -390,41 +399,33 @@ int hub_plan_build(Sector *s, std::string *err) {
       if (x >> b & 1) v |= 1u << (2 * b);
     spread[x] = v;
   }
-  // lower-half CSR: for species spin (0 up / 1 down), row = (class k, rank r) of that species;
-  // entries reference the lower-half hop table lo_coef / lo_sm (ups first, then downs)
-  std::vector<double> lo_coef;
-  std::vector<uint32_t> lo_sm;
-  for (const auto *hops : {&lo_up, &lo_dn})
-    for (const Hop &h : *hops) {
-      lo_coef.push_back(h.re);
-      lo_coef.push_back(h.im);
-      lo_sm.push_back((uint32_t)h.sm);
-    }
-  auto build_csr = [&](const std::vector<Hop> &hops, int spin, int id0, std::vector<int> *ptr,
-                       std::vector<uint32_t> *ent) {
-    ptr->assign(nx + 1, 0);
-    ent->clear();
+  auto between = [](int i, int j) -> uint32_t {  // sites strictly between i and j (as bits)
+    const int lo_ = std::min(i, j), hi_ = std::max(i, j);
+    return (uint32_t)(((1ull << hi_) - 1) ^ ((1ull << (lo_ + 1)) - 1));
+  };
+  // lower-half CSR per spin: row = (class k, rank r) of that spin's lower-half occupation x;
+  // entry = source rank and the signed coefficient (species-first sign: modes of x between i, j)
+  std::vector<int> ptr[2];
+  std::vector<uint16_t> idx[2];
+  std::vector<double> val[2];
+  for (int sp = 0; sp < 2; sp++) {
+    ptr[sp].assign(nx + 1, 0);
     for (int k = 0; k <= L; k++)
       for (int r = 0; r < binom[k]; r++) {
         const int row = unrank_off[k] + r;
         const uint32_t x = unrank[row];
-        const uint64_t cfg = (uint64_t)spread[x] << spin;  // this species' bits in the lower half
-        for (size_t hi_ = 0; hi_ < hops.size(); hi_++) {
-          const Hop &h = hops[hi_];
-          if ((cfg & h.cm) != h.cv) continue;
-          const uint64_t src = cfg ^ h.flip;
-          uint32_t xs = 0;
-          for (int b = 0; b < L; b++) xs |= (uint32_t)((src >> (2 * b + spin)) & 1ull) << b;
-          ent->push_back((uint32_t)rank[xs] | ((uint32_t)(id0 + hi_) << 16));
+        for (const Hop &h : lo[sp]) {
+          if (!((x >> h.i) & 1u) || ((x >> h.j) & 1u)) continue;  // output: i occupied, j empty
+          const uint32_t src = x ^ (1u << h.i) ^ (1u << h.j);
+          const double sg = (__builtin_popcount(x & between(h.i, h.j)) & 1) ? -1.0 : 1.0;
+          idx[sp].push_back(rank[src]);
+          val[sp].push_back(sg * h.re);
+          val[sp].push_back(sg * h.im);
         }
-        (*ptr)[row + 1] = (int)ent->size();
+        ptr[sp][row + 1] = (int)idx[sp].size();
       }
-  };
-  std::vector<int> up_ptr, dn_ptr;
-  std::vector<uint32_t> up_ent, dn_ent;
-  build_csr(lo_up, 0, 0, &up_ptr, &up_ent);
-  build_csr(lo_dn, 1, (int)lo_up.size(), &dn_ptr, &dn_ent);
-  // upper-half and cross hops per spin: hi first, then cross
+  }
+  // upper-half and cross hops per spin (upper-half first, then cross)
   std::vector<HubTermDev> terms[2];
   for (int sp = 0; sp < 2; sp++) {
     for (int pass = 0; pass < 2; pass++)
@@ -433,12 +434,17 @@ int hub_plan_build(Sector *s, std::string *err) {
         d.cm_hi = (uint32_t)(h.cm >> N);
         d.cv_hi = (uint32_t)(h.cv >> N);
         d.flip_hi = (uint32_t)(h.flip >> N);
-        d.sm = (uint32_t)h.sm;
-        d.re = h.re; d.im = h.im;
-        d.lo_bit = -1; d.lo_need = 0;
-        if (pass == 1) {
-          d.lo_bit = h.p >> 1;  // h.p is the lower-half end (p < N <= q)
-          d.lo_need = (int)((h.cv >> h.p) & 1ull);
+        d.re = h.re;
+        d.im = h.im;
+        if (pass == 0) {
+          d.btw_hi = between(h.i - L, h.j - L);
+          d.lo_bit = -1;
+          d.lo_need = 0;
+        } else {
+          const int lo_site = std::min(h.i, h.j), hi_site = std::max(h.i, h.j);
+          d.btw_hi = (uint32_t)((1ull << (hi_site - L)) - 1);  // upper-half sites below hi_site
+          d.lo_bit = lo_site;  // the kernel adds the lower-half sites above lo_site
+          d.lo_need = (lo_site == h.i) ? 1 : 0;
         }
         terms[sp].push_back(d);
       }
@@ -474,29 +480,23 @@ int hub_plan_build(Sector *s, std::string *err) {
           dlo.push_back(v);
         }
     }
-  // block processing orders: phase 0 walks the block grid by columns (fixed db),
-  // phase 1 by rows (fixed ub)
+  // block orders: pass 0 by (db, ub), pass 1 by (ub, db)
   std::vector<uint32_t> l22(s->sdim);
   if (cudaMemcpy(l22.data(), s->d_list_2_2, sizeof(uint32_t) * s->sdim, cudaMemcpyDeviceToHost) != cudaSuccess) {
     *err = "hubbard plan: cannot read list_2_2";
     return -1;
   }
-  auto compress = [&](uint32_t x, int shift) {
-    uint32_t v = 0;
-    for (int b = 0; b < L; b++) v |= ((x >> (2 * b + shift)) & 1u) << b;
-    return v;
-  };
   std::vector<uint32_t> ord0, ord1;
   for (uint32_t ib = 0; ib < (uint32_t)s->sdim; ib++)
     if (l22[ib]) ord0.push_back(ib);
   ord1 = ord0;
   std::stable_sort(ord0.begin(), ord0.end(), [&](uint32_t x, uint32_t y) {
-    const uint32_t dx = compress(x, 1), dy = compress(y, 1);
-    return dx != dy ? dx < dy : compress(x, 0) < compress(y, 0);
+    const uint32_t dx = compress_bits(x, 1, L), dy = compress_bits(y, 1, L);
+    return dx != dy ? dx < dy : compress_bits(x, 0, L) < compress_bits(y, 0, L);
   });
   std::stable_sort(ord1.begin(), ord1.end(), [&](uint32_t x, uint32_t y) {
-    const uint32_t ux = compress(x, 0), uy = compress(y, 0);
-    return ux != uy ? ux < uy : compress(x, 1) < compress(y, 1);
+    const uint32_t ux = compress_bits(x, 0, L), uy = compress_bits(y, 0, L);
+    return ux != uy ? ux < uy : compress_bits(x, 1, L) < compress_bits(y, 1, L);
   });
 
   HubPlan *plan = new HubPlan();
@@ -509,47 +509,51 @@ int hub_plan_build(Sector *s, std::string *err) {
     plan->allocs.push_back((void *)*dst);
     return 0;
   };
-  uint16_t *d_rank, *d_unrank;
-  int *d_uoff, *d_binom, *d_up_ptr, *d_dn_ptr, *d_dlo_off;
-  uint32_t *d_spread, *d_up_ent, *d_dn_ent, *d_lo_sm, *d_ord0, *d_ord1;
-  double *d_lo_coef, *d_dlo, *d_dhi;
+  uint16_t *d_rank, *d_unrank, *d_idx0, *d_idx1;
+  int *d_uoff, *d_binom, *d_ptr0, *d_ptr1, *d_dlo_off;
+  uint32_t *d_spread, *d_ord0, *d_ord1;
+  double *d_val0, *d_val1, *d_dlo, *d_dhi;
   HubTermDev *d_t0, *d_t1;
   DiagTerm *d_dcross;
+  std::vector<int> ctr(2, 0);
+  int *d_ctr;
   if (up(rank, &d_rank) || up(unrank, &d_unrank) || up(unrank_off, &d_uoff) || up(binom, &d_binom) ||
-      up(spread, &d_spread) || up(up_ptr, &d_up_ptr) || up(up_ent, &d_up_ent) || up(dn_ptr, &d_dn_ptr) ||
-      up(dn_ent, &d_dn_ent) || up(lo_coef, &d_lo_coef) || up(lo_sm, &d_lo_sm) || up(terms[0], &d_t0) ||
+      up(spread, &d_spread) || up(ptr[0], &d_ptr0) || up(ptr[1], &d_ptr1) || up(idx[0], &d_idx0) ||
+      up(idx[1], &d_idx1) || up(val[0], &d_val0) || up(val[1], &d_val1) || up(terms[0], &d_t0) ||
       up(terms[1], &d_t1) || up(dlo, &d_dlo) || up(dlo_off, &d_dlo_off) || up(dhi, &d_dhi) ||
-      up(dcross, &d_dcross) || up(ord0, &d_ord0) || up(ord1, &d_ord1)) {
+      up(dcross, &d_dcross) || up(ord0, &d_ord0) || up(ord1, &d_ord1) || up(ctr, &d_ctr)) {
     hub_plan_free(plan);
     return -1;
   }
   a.rank = d_rank; a.unrank = d_unrank; a.unrank_off = d_uoff; a.binom = d_binom; a.spread = d_spread;
-  a.csr_up_ptr = d_up_ptr; a.csr_up = d_up_ent; a.csr_dn_ptr = d_dn_ptr; a.csr_dn = d_dn_ent;
-  a.n_csr_up = (int)up_ent.size(); a.n_csr_dn = (int)dn_ent.size(); a.n_lo = (int)lo_sm.size();
-  a.lo_coef = d_lo_coef; a.lo_sm = d_lo_sm;
+  a.csr_ptr[0] = d_ptr0; a.csr_ptr[1] = d_ptr1; a.csr_idx[0] = d_idx0; a.csr_idx[1] = d_idx1;
+  a.csr_val[0] = d_val0; a.csr_val[1] = d_val1;
+  a.n_csr[0] = (int)idx[0].size(); a.n_csr[1] = (int)idx[1].size();
   a.terms[0] = d_t0; a.terms[1] = d_t1;
   for (int sp = 0; sp < 2; sp++) { a.n_hi[sp] = (int)hi[sp].size(); a.n_cross[sp] = (int)cross[sp].size(); }
   a.d_lo = d_dlo; a.d_lo_off = d_dlo_off; a.d_hi = d_dhi; a.d_cross = d_dcross; a.n_dcross = (int)dcross.size();
   a.order[0] = d_ord0; a.order[1] = d_ord1;
-  plan->n_lo_terms = a.n_lo;
+  a.counter = d_ctr;
   int maxn = 0;
   for (int ku = 0; ku <= L; ku++)
     for (int kd = 0; kd <= L; kd++) maxn = std::max(maxn, binom[ku] * binom[kd]);
-  // dynamic shared memory: tables (+ lower-half CSR and the staged block in phase 0)
-  const size_t tables = sizeof(uint32_t) * nx + 2 * sizeof(uint16_t) * nx + 2 * sizeof(int) * 32;
-  size_t p0 = tables + 2 * sizeof(int) * (nx + 1) + sizeof(uint32_t) * (up_ent.size() + dn_ent.size() + lo_sm.size());
+  // dynamic shared memory of each pass (layout as in hv_hub_pass)
+  const size_t base = sizeof(int) * 64 + 2 * sizeof(uint16_t) * nx;
+  size_t p0 = sizeof(double) * 2 * (idx[0].size() + idx[1].size()) + 2 * sizeof(int) * (nx + 1) + base +
+              sizeof(uint16_t) * (idx[0].size() + idx[1].size());
   p0 = (p0 + 15) & ~(size_t)15;
-  p0 += sizeof(double) * 2 * lo_sm.size();
   plan->smem[0][0] = p0 + sizeof(double) * (size_t)maxn;
   plan->smem[0][1] = p0 + sizeof(cplx) * (size_t)maxn;
-  plan->smem[1][0] = plan->smem[1][1] = tables;
+  plan->smem[1][0] = plan->smem[1][1] = (base + 15) & ~(size_t)15;
   if (plan->smem[0][1] > 200 * 1024) { hub_plan_free(plan); return 0; }
-  cudaFuncSetAttribute((const void *)hv_hub_phase<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan->smem[0][0]);
-  cudaFuncSetAttribute((const void *)hv_hub_phase<cplx, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan->smem[0][1]);
+  cudaFuncSetAttribute((const void *)hv_hub_pass<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)plan->smem[0][0]);
+  cudaFuncSetAttribute((const void *)hv_hub_pass<cplx, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)plan->smem[0][1]);
   int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hv_hub_phase<double, 0>, kThreads, plan->smem[0][0]);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hv_hub_pass<double, 0>, kThreads, plan->smem[0][0]);
   plan->grid = std::max(1, per_sm) * s->num_sms;
-  if (2 * plan->grid > 4 * s->red_blocks) plan->grid = 2 * s->red_blocks;
+  if (plan->grid > 2 * s->red_blocks) plan->grid = 2 * s->red_blocks;  // 2 passes x 2 doubles <= 8 red_blocks
   if (cudaGetLastError() != cudaSuccess) {
     *err = "hubbard plan: kernel configuration failed";
     hub_plan_free(plan);
@@ -567,16 +571,17 @@ int hub_hv_launch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const dou
     set_error("H has complex coefficients: real vectors are not allowed");
     return -1;
   }
+  cudaMemsetAsync(p->args.counter, 0, 2 * sizeof(int), s->stream);
   if (vt == kReal64) {
-    hv_hub_phase<double, 0><<<p->grid, kThreads, p->smem[0][0], s->stream>>>(p->args, (const double *)d_v1,
-                                                                             (double *)d_v0, d_coef, s->d_red);
-    hv_hub_phase<double, 1><<<p->grid, kThreads, p->smem[1][0], s->stream>>>(p->args, (const double *)d_v1,
-                                                                             (double *)d_v0, d_coef, s->d_red);
+    hv_hub_pass<double, 0><<<p->grid, kThreads, p->smem[0][0], s->stream>>>(p->args, (const double *)d_v1,
+                                                                            (double *)d_v0, d_coef, s->d_red);
+    hv_hub_pass<double, 1><<<p->grid, kThreads, p->smem[1][0], s->stream>>>(p->args, (const double *)d_v1,
+                                                                            (double *)d_v0, d_coef, s->d_red);
   } else {
-    hv_hub_phase<cplx, 0><<<p->grid, kThreads, p->smem[0][1], s->stream>>>(p->args, (const cplx *)d_v1,
-                                                                           (cplx *)d_v0, d_coef, s->d_red);
-    hv_hub_phase<cplx, 1><<<p->grid, kThreads, p->smem[1][1], s->stream>>>(p->args, (const cplx *)d_v1,
-                                                                           (cplx *)d_v0, d_coef, s->d_red);
+    hv_hub_pass<cplx, 0><<<p->grid, kThreads, p->smem[0][1], s->stream>>>(p->args, (const cplx *)d_v1, (cplx *)d_v0,
+                                                                          d_coef, s->d_red);
+    hv_hub_pass<cplx, 1><<<p->grid, kThreads, p->smem[1][1], s->stream>>>(p->args, (const cplx *)d_v1, (cplx *)d_v0,
+                                                                          d_coef, s->d_red);
   }
   finalize_partials_kernel<2><<<1, 256, 0, s->stream>>>(s->d_red, 2 * p->grid, d_out);
   const cudaError_t e = cudaGetLastError();
@@ -616,8 +621,10 @@ int hub_permute(Sector *s, VecType vt, const void *in, void *out, bool to_native
 
 int hub_observables(Sector *s, VecType vt, const void *v, double *d_out) {
   HubPlan *p = s->hub;
-  if (vt == kReal64) native_obs_kernel<double><<<s->red_blocks, kThreads, 0, s->stream>>>(p->args, (const double *)v, s->d_red);
-  else native_obs_kernel<cplx><<<s->red_blocks, kThreads, 0, s->stream>>>(p->args, (const cplx *)v, s->d_red);
+  if (vt == kReal64)
+    native_obs_kernel<double><<<s->red_blocks, kThreads, 0, s->stream>>>(p->args, (const double *)v, s->d_red);
+  else
+    native_obs_kernel<cplx><<<s->red_blocks, kThreads, 0, s->stream>>>(p->args, (const cplx *)v, s->d_red);
   finalize_partials_kernel<6><<<1, 256, 0, s->stream>>>(s->d_red, s->red_blocks, d_out);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
