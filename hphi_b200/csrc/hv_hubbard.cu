@@ -46,6 +46,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMaxBlockTerms = 96;  // upper-half + cross hops of one spin
+constexpr int kCols = 3;            // columns per lane: C(L, L/2) <= 96 for L <= 8
 
 struct HubTermDev {    // upper-half or cross hop of one spin
   uint32_t cm_hi, cv_hi, flip_hi;  // condition / flip on the upper half (bits of ib)
@@ -198,67 +199,114 @@ __global__ void __launch_bounds__(kThreads) hv_hub_pass(HubArgs a, const T *__re
     __syncthreads();
     const int nhb = bl.n_hi, ncb = bl.n_cr;
     const int off_u = s_uoff[nu], off_d = s_uoff[nd];
-    const uint32_t magic = (uint32_t)(0xFFFFFFFFull / (uint32_t)nda + 1ull);
     const double dhi = (PASS == 0) ? a.d_hi[ib] : 0.0;
     const double *dlo = a.d_lo + a.d_lo_off[nu * (L + 1) + nd];
-    for (int p = threadIdx.x; p < n; p += blockDim.x) {
-      const int ra = (nda == 1) ? p : (int)__umulhi((uint32_t)p, magic);
-      const int rd = p - ra * nda;
-      const uint32_t ua = s_unrank[off_u + ra], da = s_unrank[off_d + rd];
-      T x, y;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    // per-lane columns rd = lane + 32 r of the block rows
+    uint32_t da[kCols];
+#pragma unroll
+    for (int r = 0; r < kCols; r++) da[r] = (lane + 32 * r < nda) ? s_unrank[off_d + lane + 32 * r] : 0u;
+    // a warp owns a block row ra (ua uniform across the warp)
+    for (int ra = warp; ra < nua; ra += nwarps) {
+      const uint32_t ua = s_unrank[off_u + ra];
+      const int row0 = ra * nda;
+      T x[kCols], y[kCols];
+#pragma unroll
+      for (int r = 0; r < kCols; r++) {
+        const int rd = lane + 32 * r;
+        if (rd < nda) {
+          if (PASS == 0) {
+            x[r] = xs[row0 + rd];
+            double dg = dlo[row0 + rd] + dhi;
+            if (a.n_dcross) {
+              const uint64_t c = ((uint64_t)ib << N) | a.spread[ua] | ((uint64_t)a.spread[da[r]] << 1);
+              for (int k = 0; k < a.n_dcross; k++) {
+                const DiagTerm dt = a.d_cross[k];
+                if ((c & dt.cm) == dt.cv) dg += dt.v;
+              }
+            }
+            y[r] = VT<T>::scale(dg, x[r]);
+          } else {
+            x[r] = v1[jb + row0 + rd];
+            y[r] = VT<T>::zero();
+          }
+        } else {
+          x[r] = VT<T>::zero();
+          y[r] = VT<T>::zero();
+        }
+      }
       if (PASS == 0) {
-        x = xs[p];
-        double dg = dlo[p] + dhi;
-        if (a.n_dcross) {
-          const uint64_t c = ((uint64_t)ib << N) | a.spread[ua] | ((uint64_t)a.spread[da] << 1);
-          for (int k = 0; k < a.n_dcross; k++) {
-            const DiagTerm dt = a.d_cross[k];
-            if ((c & dt.cm) == dt.cv) dg += dt.v;
+        // lower-half up hops: warp-uniform CSR row of ua, source rows of the staged block
+        const int r0 = s_ptr[0][off_u + ra], r1 = s_ptr[0][off_u + ra + 1];
+        for (int e = r0; e < r1; e++) {
+          const double cre = s_val[0][2 * e], cim = s_val[0][2 * e + 1];
+          const T *srow = xs + (int)s_idx[0][e] * nda;
+#pragma unroll
+          for (int r = 0; r < kCols; r++)
+            if (lane + 32 * r < nda) y[r] = cfma<T>(cre, cim, srow[lane + 32 * r], y[r]);
+        }
+        // lower-half down hops: per-column CSR rows within the staged row
+        const T *row = xs + row0;
+#pragma unroll
+        for (int r = 0; r < kCols; r++) {
+          const int rd = lane + 32 * r;
+          if (rd < nda) {
+            const int q0 = s_ptr[1][off_d + rd], q1 = s_ptr[1][off_d + rd + 1];
+            for (int e = q0; e < q1; e++) y[r] = cfma<T>(s_val[1][2 * e], s_val[1][2 * e + 1], row[s_idx[1][e]], y[r]);
           }
         }
-        y = VT<T>::scale(dg, x);
-        {  // lower-half up hops: rows of the staged block
-          const int r0 = s_ptr[0][off_u + ra], r1 = s_ptr[0][off_u + ra + 1];
-          for (int e = r0; e < r1; e++)
-            y = cfma<T>(s_val[0][2 * e], s_val[0][2 * e + 1], xs[(int)s_idx[0][e] * nda + rd], y);
-        }
-        {  // lower-half down hops: entries of the row
-          const int r0 = s_ptr[1][off_d + rd], r1 = s_ptr[1][off_d + rd + 1];
-          const T *row = xs + ra * nda;
-          for (int e = r0; e < r1; e++) y = cfma<T>(s_val[1][2 * e], s_val[1][2 * e + 1], row[s_idx[1][e]], y);
-        }
-      } else {
-        x = v1[jb + p];
-        y = VT<T>::zero();
       }
-      // upper-half hops: the same position in a block of the same class
+      // upper-half hops: the same positions in a block of the same class
       for (int k = 0; k < nhb; k++) {
-        const int64_t src = bl.src[k];
-        if (src >= 0) y = cfma<T>(bl.re[k], bl.im[k], v1[src + p], y);
+        const T *src = v1 + bl.src[k] + row0;
+        const double cre = bl.re[k], cim = bl.im[k];
+#pragma unroll
+        for (int r = 0; r < kCols; r++)
+          if (lane + 32 * r < nda) y[r] = cfma<T>(cre, cim, src[lane + 32 * r], y[r]);
       }
-      // cross hops: one particle of this spin changes half
-      const uint32_t own = (PASS == 0) ? ua : da;
+      // cross hops: one particle of this pass's spin changes half
       for (int q = 0; q < ncb; q++) {
         const int k = kMaxBlockTerms - 1 - q;
-        const int b = bl.bit[k];
-        if ((int)((own >> b) & 1u) != bl.need[k] || bl.src[k] < 0) continue;
-        const int r_new = s_rank[own ^ (1u << b)];
-        const int64_t j = (PASS == 0) ? bl.src[k] + (int64_t)r_new * nda + rd : bl.src[k] + (int64_t)ra * bl.nsrc[k] + r_new;
-        const double sg = (__popc(own >> (b + 1)) & 1) ? -1.0 : 1.0;
-        y = cfma<T>(sg * bl.re[k], sg * bl.im[k], v1[j], y);
+        const int b = bl.bit[k], need = bl.need[k];
+        if (PASS == 0) {
+          // condition, source row and sign depend on ua only: uniform across the warp
+          if ((int)((ua >> b) & 1u) != need) continue;
+          const double sg = (__popc(ua >> (b + 1)) & 1) ? -1.0 : 1.0;
+          const double cre = sg * bl.re[k], cim = sg * bl.im[k];
+          const T *src = v1 + bl.src[k] + (int64_t)s_rank[ua ^ (1u << b)] * nda;
+#pragma unroll
+          for (int r = 0; r < kCols; r++)
+            if (lane + 32 * r < nda) y[r] = cfma<T>(cre, cim, src[lane + 32 * r], y[r]);
+        } else {
+          const T *src = v1 + bl.src[k] + (int64_t)ra * bl.nsrc[k];
+#pragma unroll
+          for (int r = 0; r < kCols; r++) {
+            if (lane + 32 * r < nda && (int)((da[r] >> b) & 1u) == need) {
+              const double sg = (__popc(da[r] >> (b + 1)) & 1) ? -1.0 : 1.0;
+              y[r] = cfma<T>(sg * bl.re[k], sg * bl.im[k], src[s_rank[da[r] ^ (1u << b)]], y[r]);
+            }
+          }
+        }
       }
-      pr[0] += VT<T>::conj_mul_re(x, y);
-      pr[1] += VT<T>::conj_mul_im(x, y);
-      y = VT<T>::scale(scale, y);
-      if (PASS == 0) v0[jb + p] = (acc == 0.0) ? y : VT<T>::add(VT<T>::scale(acc, v0[jb + p]), y);
-      else v0[jb + p] = VT<T>::add(v0[jb + p], y);
+#pragma unroll
+      for (int r = 0; r < kCols; r++) {
+        const int rd = lane + 32 * r;
+        if (rd < nda) {
+          pr[0] += VT<T>::conj_mul_re(x[r], y[r]);
+          pr[1] += VT<T>::conj_mul_im(x[r], y[r]);
+          const T yy = VT<T>::scale(scale, y[r]);
+          T *dst = v0 + jb + row0 + rd;
+          if (PASS == 0) *dst = (acc == 0.0) ? yy : VT<T>::add(VT<T>::scale(acc, *dst), yy);
+          else *dst = VT<T>::add(*dst, yy);
+        }
+      }
     }
     __syncthreads();
   }
   block_sum<2>(pr);
   if (threadIdx.x == 0) {
-    part[2 * (PASS * gridDim.x + blockIdx.x)] = pr[0];
-    part[2 * (PASS * gridDim.x + blockIdx.x) + 1] = pr[1];
+    part[2 * blockIdx.x] = pr[0];
+    part[2 * blockIdx.x + 1] = pr[1];
   }
 }
 
@@ -344,7 +392,7 @@ struct HubPlan {
   HubArgs args;
   std::vector<void *> allocs;
   size_t smem[2][2] = {{0, 0}, {0, 0}};  // [pass][real, complex]
-  int grid = 0;
+  int grid[2] = {0, 0};                  // CTAs of each pass (shared-memory bound differs)
 };
 
 void hub_plan_free(HubPlan *p) {
@@ -489,6 +537,12 @@ int hub_plan_build(Sector *s, std::string *err) {
   std::vector<uint32_t> ord0, ord1;
   for (uint32_t ib = 0; ib < (uint32_t)s->sdim; ib++)
     if (l22[ib]) ord0.push_back(ib);
+  for (int sp = 0; sp < 2; sp++)
+    for (int t = 0; t < (int)hi[sp].size(); t++) {
+      const HubTermDev &d = terms[sp][t];
+      for (uint32_t ib : ord0)
+        if ((ib & d.cm_hi) == d.cv_hi && l22[ib ^ d.flip_hi] == 0) return 0;  // keep the general kernel
+    }
   ord1 = ord0;
   std::stable_sort(ord0.begin(), ord0.end(), [&](uint32_t x, uint32_t y) {
     const uint32_t dx = compress_bits(x, 1, L), dy = compress_bits(y, 1, L);
@@ -550,10 +604,12 @@ int hub_plan_build(Sector *s, std::string *err) {
                        (int)plan->smem[0][0]);
   cudaFuncSetAttribute((const void *)hv_hub_pass<cplx, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)plan->smem[0][1]);
-  int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hv_hub_pass<double, 0>, kThreads, plan->smem[0][0]);
-  plan->grid = std::max(1, per_sm) * s->num_sms;
-  if (plan->grid > 2 * s->red_blocks) plan->grid = 2 * s->red_blocks;  // 2 passes x 2 doubles <= 8 red_blocks
+  int per_sm0 = 1, per_sm1 = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm0, hv_hub_pass<double, 0>, kThreads, plan->smem[0][0]);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, hv_hub_pass<double, 1>, kThreads, plan->smem[1][0]);
+  // partial sums: pass p writes records [p * grid[0] + block]; both fit 4 * red_blocks records
+  plan->grid[0] = std::min(std::max(1, per_sm0) * s->num_sms, 2 * s->red_blocks);
+  plan->grid[1] = std::min(std::max(1, per_sm1) * s->num_sms, 2 * s->red_blocks);
   if (cudaGetLastError() != cudaSuccess) {
     *err = "hubbard plan: kernel configuration failed";
     hub_plan_free(plan);
@@ -573,17 +629,19 @@ int hub_hv_launch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const dou
   }
   cudaMemsetAsync(p->args.counter, 0, 2 * sizeof(int), s->stream);
   if (vt == kReal64) {
-    hv_hub_pass<double, 0><<<p->grid, kThreads, p->smem[0][0], s->stream>>>(p->args, (const double *)d_v1,
-                                                                            (double *)d_v0, d_coef, s->d_red);
-    hv_hub_pass<double, 1><<<p->grid, kThreads, p->smem[1][0], s->stream>>>(p->args, (const double *)d_v1,
-                                                                            (double *)d_v0, d_coef, s->d_red);
+    hv_hub_pass<double, 0><<<p->grid[0], kThreads, p->smem[0][0], s->stream>>>(p->args, (const double *)d_v1,
+                                                                               (double *)d_v0, d_coef, s->d_red);
+    hv_hub_pass<double, 1><<<p->grid[1], kThreads, p->smem[1][0], s->stream>>>(p->args, (const double *)d_v1,
+                                                                               (double *)d_v0, d_coef,
+                                                                               s->d_red + 2 * p->grid[0]);
   } else {
-    hv_hub_pass<cplx, 0><<<p->grid, kThreads, p->smem[0][1], s->stream>>>(p->args, (const cplx *)d_v1, (cplx *)d_v0,
-                                                                          d_coef, s->d_red);
-    hv_hub_pass<cplx, 1><<<p->grid, kThreads, p->smem[1][1], s->stream>>>(p->args, (const cplx *)d_v1, (cplx *)d_v0,
-                                                                          d_coef, s->d_red);
+    hv_hub_pass<cplx, 0><<<p->grid[0], kThreads, p->smem[0][1], s->stream>>>(p->args, (const cplx *)d_v1,
+                                                                             (cplx *)d_v0, d_coef, s->d_red);
+    hv_hub_pass<cplx, 1><<<p->grid[1], kThreads, p->smem[1][1], s->stream>>>(p->args, (const cplx *)d_v1,
+                                                                             (cplx *)d_v0, d_coef,
+                                                                             s->d_red + 2 * p->grid[0]);
   }
-  finalize_partials_kernel<2><<<1, 256, 0, s->stream>>>(s->d_red, 2 * p->grid, d_out);
+  finalize_partials_kernel<2><<<1, 256, 0, s->stream>>>(s->d_red, p->grid[0] + p->grid[1], d_out);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_error(std::string("hubbard hv launch failed: ") + cudaGetErrorString(e));
