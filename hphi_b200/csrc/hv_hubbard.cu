@@ -68,9 +68,11 @@ struct HubArgs {
   const int *binom;                // [L+1]
   const uint32_t *spread;          // [2^L] site bits -> even bit positions (HPhi layout)
   const int *csr_ptr[2];           // [2^L + 1] lower-half hops of each spin, rows (k, r)
-  const uint16_t *csr_idx[2];      // source rank
-  const double *csr_val[2];        // signed coefficient (re, im)
+  const uint16_t *csr[2];          // entry: source rank | hop << 8 | sign << 15
   int n_csr[2];
+  const double *hop_coef[2];       // [n_lo_hops[s]][2] operator coefficients of lower-half hops
+  int n_lo_hops[2];
+  const uint16_t *cross_tab;       // [L][2^L]: rank(x ^ bit) | occupation << 14 | sign << 15
   const HubTermDev *terms[2];      // per spin: n_hi upper-half hops, then n_cross cross hops
   int n_hi[2], n_cross[2];
   const double *d_lo;              // diagonal (lower-half terms) per class pair, native order
@@ -83,7 +85,8 @@ struct HubArgs {
 struct BlockTerms {  // the current block's upper-half and cross hops, signs resolved
   int64_t src[kMaxBlockTerms];
   double re[kMaxBlockTerms], im[kMaxBlockTerms];
-  int bit[kMaxBlockTerms], need[kMaxBlockTerms], nsrc[kMaxBlockTerms];
+  int nsrc[kMaxBlockTerms];
+  unsigned char bit[kMaxBlockTerms], need[kMaxBlockTerms];
   int n_hi, n_cr, bi;
 };
 
@@ -103,19 +106,20 @@ __host__ __device__ __forceinline__ uint32_t compress_bits(uint32_t x, int shift
 }
 
 template <typename T, int PASS>
-__global__ void __launch_bounds__(kThreads) hv_hub_pass(HubArgs a, const T *__restrict__ v1, T *__restrict__ v0,
+__global__ void __launch_bounds__(kThreads, PASS == 0 ? 3 : 4) hv_hub_pass(HubArgs a, const T *__restrict__ v1, T *__restrict__ v0,
                                                         const double *__restrict__ coef, double *__restrict__ part) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ BlockTerms bl;
   const int L = a.L, N = a.N, nx = 1 << L;
   // shared tables (pass 0 also holds the lower-half CSR of both spins and the staged block)
   unsigned char *sp = smem_raw;
-  double *s_val[2] = {nullptr, nullptr};
+  double *s_hop[2] = {nullptr, nullptr};
   int *s_ptr[2] = {nullptr, nullptr};
-  uint16_t *s_idx[2] = {nullptr, nullptr};
+  uint16_t *s_csr[2] = {nullptr, nullptr};
+  uint16_t *s_ctab = nullptr;
   if (PASS == 0) {
-    s_val[0] = reinterpret_cast<double *>(sp); sp += sizeof(double) * 2 * a.n_csr[0];
-    s_val[1] = reinterpret_cast<double *>(sp); sp += sizeof(double) * 2 * a.n_csr[1];
+    s_hop[0] = reinterpret_cast<double *>(sp); sp += sizeof(double) * 2 * a.n_lo_hops[0];
+    s_hop[1] = reinterpret_cast<double *>(sp); sp += sizeof(double) * 2 * a.n_lo_hops[1];
     s_ptr[0] = reinterpret_cast<int *>(sp); sp += sizeof(int) * (nx + 1);
     s_ptr[1] = reinterpret_cast<int *>(sp); sp += sizeof(int) * (nx + 1);
   }
@@ -124,8 +128,10 @@ __global__ void __launch_bounds__(kThreads) hv_hub_pass(HubArgs a, const T *__re
   uint16_t *s_rank = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * nx;
   uint16_t *s_unrank = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * nx;
   if (PASS == 0) {
-    s_idx[0] = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * a.n_csr[0];
-    s_idx[1] = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * a.n_csr[1];
+    s_csr[0] = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * a.n_csr[0];
+    s_csr[1] = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * a.n_csr[1];
+  } else {
+    s_ctab = reinterpret_cast<uint16_t *>(sp); sp += sizeof(uint16_t) * L * nx;
   }
   sp = smem_raw + (((sp - smem_raw) + 15) & ~(size_t)15);
   T *xs = reinterpret_cast<T *>(sp);
@@ -137,12 +143,11 @@ __global__ void __launch_bounds__(kThreads) hv_hub_pass(HubArgs a, const T *__re
   if (PASS == 0) {
     for (int q = 0; q < 2; q++) {
       for (int i = threadIdx.x; i <= nx; i += blockDim.x) s_ptr[q][i] = a.csr_ptr[q][i];
-      for (int i = threadIdx.x; i < a.n_csr[q]; i += blockDim.x) {
-        s_idx[q][i] = a.csr_idx[q][i];
-        s_val[q][2 * i] = a.csr_val[q][2 * i];
-        s_val[q][2 * i + 1] = a.csr_val[q][2 * i + 1];
-      }
+      for (int i = threadIdx.x; i < a.n_csr[q]; i += blockDim.x) s_csr[q][i] = a.csr[q][i];
+      for (int i = threadIdx.x; i < 2 * a.n_lo_hops[q]; i += blockDim.x) s_hop[q][i] = a.hop_coef[q][i];
     }
+  } else {
+    for (int i = threadIdx.x; i < L * nx; i += blockDim.x) s_ctab[i] = a.cross_tab[i];
   }
   __syncthreads();
   const double acc = coef[0], scale = coef[1];
@@ -239,8 +244,11 @@ __global__ void __launch_bounds__(kThreads) hv_hub_pass(HubArgs a, const T *__re
         // lower-half up hops: warp-uniform CSR row of ua, source rows of the staged block
         const int r0 = s_ptr[0][off_u + ra], r1 = s_ptr[0][off_u + ra + 1];
         for (int e = r0; e < r1; e++) {
-          const double cre = s_val[0][2 * e], cim = s_val[0][2 * e + 1];
-          const T *srow = xs + (int)s_idx[0][e] * nda;
+          const uint32_t ent = s_csr[0][e];
+          const int h = (ent >> 8) & 0x7F;
+          const double sg = (ent >> 15) ? -1.0 : 1.0;
+          const double cre = sg * s_hop[0][2 * h], cim = sg * s_hop[0][2 * h + 1];
+          const T *srow = xs + (int)(ent & 0xFF) * nda;
 #pragma unroll
           for (int r = 0; r < kCols; r++)
             if (lane + 32 * r < nda) y[r] = cfma<T>(cre, cim, srow[lane + 32 * r], y[r]);
@@ -252,7 +260,12 @@ __global__ void __launch_bounds__(kThreads) hv_hub_pass(HubArgs a, const T *__re
           const int rd = lane + 32 * r;
           if (rd < nda) {
             const int q0 = s_ptr[1][off_d + rd], q1 = s_ptr[1][off_d + rd + 1];
-            for (int e = q0; e < q1; e++) y[r] = cfma<T>(s_val[1][2 * e], s_val[1][2 * e + 1], row[s_idx[1][e]], y[r]);
+            for (int e = q0; e < q1; e++) {
+              const uint32_t ent = s_csr[1][e];
+              const int h = (ent >> 8) & 0x7F;
+              const double sg = (ent >> 15) ? -1.0 : 1.0;
+              y[r] = cfma<T>(sg * s_hop[1][2 * h], sg * s_hop[1][2 * h + 1], row[ent & 0xFF], y[r]);
+            }
           }
         }
       }
@@ -279,11 +292,14 @@ __global__ void __launch_bounds__(kThreads) hv_hub_pass(HubArgs a, const T *__re
             if (lane + 32 * r < nda) y[r] = cfma<T>(cre, cim, src[lane + 32 * r], y[r]);
         } else {
           const T *src = v1 + bl.src[k] + (int64_t)ra * bl.nsrc[k];
+          const uint16_t *tab = s_ctab + b * nx;
+          const double cre = bl.re[k], cim = bl.im[k];
 #pragma unroll
           for (int r = 0; r < kCols; r++) {
-            if (lane + 32 * r < nda && (int)((da[r] >> b) & 1u) == need) {
-              const double sg = (__popc(da[r] >> (b + 1)) & 1) ? -1.0 : 1.0;
-              y[r] = cfma<T>(sg * bl.re[k], sg * bl.im[k], src[s_rank[da[r] ^ (1u << b)]], y[r]);
+            const uint32_t e = tab[da[r]];
+            if (lane + 32 * r < nda && (int)((e >> 14) & 1u) == need) {
+              const double sg = (e >> 15) ? -1.0 : 1.0;
+              y[r] = cfma<T>(sg * cre, sg * cim, src[e & 0x3FFF], y[r]);
             }
           }
         }
@@ -426,6 +442,7 @@ int hub_plan_build(Sector *s, std::string *err) {
   }
   for (int sp = 0; sp < 2; sp++)
     if ((int)(hi[sp].size() + cross[sp].size()) > kMaxBlockTerms) return 0;
+  if (binom_u(L, L / 2) > 255) return 0;  // ranks fit the 8-bit CSR field
   const int nx = 1 << L;
   std::vector<uint16_t> rank(nx), unrank(nx);
   std::vector<int> unrank_off(L + 2, 0), binom(L + 1);
@@ -452,27 +469,35 @@ int hub_plan_build(Sector *s, std::string *err) {
     return (uint32_t)(((1ull << hi_) - 1) ^ ((1ull << (lo_ + 1)) - 1));
   };
   // lower-half CSR per spin: row = (class k, rank r) of that spin's lower-half occupation x;
-  // entry = source rank and the signed coefficient (species-first sign: modes of x between i, j)
+  // entry = source rank | hop << 8 | sign << 15 (species-first sign: modes of x between i, j)
   std::vector<int> ptr[2];
-  std::vector<uint16_t> idx[2];
-  std::vector<double> val[2];
+  std::vector<uint16_t> csr[2];
+  std::vector<double> hop_coef[2];
   for (int sp = 0; sp < 2; sp++) {
+    if (lo[sp].size() > 127) return 0;
+    for (const Hop &h : lo[sp]) { hop_coef[sp].push_back(h.re); hop_coef[sp].push_back(h.im); }
     ptr[sp].assign(nx + 1, 0);
     for (int k = 0; k <= L; k++)
       for (int r = 0; r < binom[k]; r++) {
         const int row = unrank_off[k] + r;
         const uint32_t x = unrank[row];
-        for (const Hop &h : lo[sp]) {
+        for (size_t hh = 0; hh < lo[sp].size(); hh++) {
+          const Hop &h = lo[sp][hh];
           if (!((x >> h.i) & 1u) || ((x >> h.j) & 1u)) continue;  // output: i occupied, j empty
           const uint32_t src = x ^ (1u << h.i) ^ (1u << h.j);
-          const double sg = (__builtin_popcount(x & between(h.i, h.j)) & 1) ? -1.0 : 1.0;
-          idx[sp].push_back(rank[src]);
-          val[sp].push_back(sg * h.re);
-          val[sp].push_back(sg * h.im);
+          const uint32_t neg = __builtin_popcount(x & between(h.i, h.j)) & 1;
+          csr[sp].push_back((uint16_t)(rank[src] | (hh << 8) | (neg << 15)));
         }
-        ptr[sp][row + 1] = (int)idx[sp].size();
+        ptr[sp][row + 1] = (int)csr[sp].size();
       }
   }
+  // cross-hop table: for site b and occupation x of one spin's lower half
+  std::vector<uint16_t> cross_tab((size_t)L * nx);
+  for (int b = 0; b < L; b++)
+    for (int x = 0; x < nx; x++) {
+      const uint32_t occ = (x >> b) & 1, neg = __builtin_popcount((uint32_t)x >> (b + 1)) & 1;
+      cross_tab[(size_t)b * nx + x] = (uint16_t)(rank[x ^ (1 << b)] | (occ << 14) | (neg << 15));
+    }
   // upper-half and cross hops per spin (upper-half first, then cross)
   std::vector<HubTermDev> terms[2];
   for (int sp = 0; sp < 2; sp++) {
@@ -563,26 +588,29 @@ int hub_plan_build(Sector *s, std::string *err) {
     plan->allocs.push_back((void *)*dst);
     return 0;
   };
-  uint16_t *d_rank, *d_unrank, *d_idx0, *d_idx1;
+  uint16_t *d_rank, *d_unrank, *d_csr0, *d_csr1, *d_ctab;
   int *d_uoff, *d_binom, *d_ptr0, *d_ptr1, *d_dlo_off;
   uint32_t *d_spread, *d_ord0, *d_ord1;
-  double *d_val0, *d_val1, *d_dlo, *d_dhi;
+  double *d_hop0, *d_hop1, *d_dlo, *d_dhi;
   HubTermDev *d_t0, *d_t1;
   DiagTerm *d_dcross;
   std::vector<int> ctr(2, 0);
   int *d_ctr;
   if (up(rank, &d_rank) || up(unrank, &d_unrank) || up(unrank_off, &d_uoff) || up(binom, &d_binom) ||
-      up(spread, &d_spread) || up(ptr[0], &d_ptr0) || up(ptr[1], &d_ptr1) || up(idx[0], &d_idx0) ||
-      up(idx[1], &d_idx1) || up(val[0], &d_val0) || up(val[1], &d_val1) || up(terms[0], &d_t0) ||
+      up(spread, &d_spread) || up(ptr[0], &d_ptr0) || up(ptr[1], &d_ptr1) || up(csr[0], &d_csr0) ||
+      up(csr[1], &d_csr1) || up(hop_coef[0], &d_hop0) || up(hop_coef[1], &d_hop1) || up(cross_tab, &d_ctab) ||
+      up(terms[0], &d_t0) ||
       up(terms[1], &d_t1) || up(dlo, &d_dlo) || up(dlo_off, &d_dlo_off) || up(dhi, &d_dhi) ||
       up(dcross, &d_dcross) || up(ord0, &d_ord0) || up(ord1, &d_ord1) || up(ctr, &d_ctr)) {
     hub_plan_free(plan);
     return -1;
   }
   a.rank = d_rank; a.unrank = d_unrank; a.unrank_off = d_uoff; a.binom = d_binom; a.spread = d_spread;
-  a.csr_ptr[0] = d_ptr0; a.csr_ptr[1] = d_ptr1; a.csr_idx[0] = d_idx0; a.csr_idx[1] = d_idx1;
-  a.csr_val[0] = d_val0; a.csr_val[1] = d_val1;
-  a.n_csr[0] = (int)idx[0].size(); a.n_csr[1] = (int)idx[1].size();
+  a.csr_ptr[0] = d_ptr0; a.csr_ptr[1] = d_ptr1; a.csr[0] = d_csr0; a.csr[1] = d_csr1;
+  a.n_csr[0] = (int)csr[0].size(); a.n_csr[1] = (int)csr[1].size();
+  a.hop_coef[0] = d_hop0; a.hop_coef[1] = d_hop1;
+  a.n_lo_hops[0] = (int)lo[0].size(); a.n_lo_hops[1] = (int)lo[1].size();
+  a.cross_tab = d_ctab;
   a.terms[0] = d_t0; a.terms[1] = d_t1;
   for (int sp = 0; sp < 2; sp++) { a.n_hi[sp] = (int)hi[sp].size(); a.n_cross[sp] = (int)cross[sp].size(); }
   a.d_lo = d_dlo; a.d_lo_off = d_dlo_off; a.d_hi = d_dhi; a.d_cross = d_dcross; a.n_dcross = (int)dcross.size();
@@ -593,12 +621,12 @@ int hub_plan_build(Sector *s, std::string *err) {
     for (int kd = 0; kd <= L; kd++) maxn = std::max(maxn, binom[ku] * binom[kd]);
   // dynamic shared memory of each pass (layout as in hv_hub_pass)
   const size_t base = sizeof(int) * 64 + 2 * sizeof(uint16_t) * nx;
-  size_t p0 = sizeof(double) * 2 * (idx[0].size() + idx[1].size()) + 2 * sizeof(int) * (nx + 1) + base +
-              sizeof(uint16_t) * (idx[0].size() + idx[1].size());
+  size_t p0 = sizeof(double) * 2 * (lo[0].size() + lo[1].size()) + 2 * sizeof(int) * (nx + 1) + base +
+              sizeof(uint16_t) * (csr[0].size() + csr[1].size());
   p0 = (p0 + 15) & ~(size_t)15;
   plan->smem[0][0] = p0 + sizeof(double) * (size_t)maxn;
   plan->smem[0][1] = p0 + sizeof(cplx) * (size_t)maxn;
-  plan->smem[1][0] = plan->smem[1][1] = (base + 15) & ~(size_t)15;
+  plan->smem[1][0] = plan->smem[1][1] = (base + sizeof(uint16_t) * L * nx + 15) & ~(size_t)15;
   if (plan->smem[0][1] > 200 * 1024) { hub_plan_free(plan); return 0; }
   cudaFuncSetAttribute((const void *)hv_hub_pass<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)plan->smem[0][0]);
