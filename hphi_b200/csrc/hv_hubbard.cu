@@ -207,16 +207,10 @@ __global__ void __launch_bounds__(kThreads, PASS == 0 ? 3 : 4) hv_hub_pass(HubAr
     const double dhi = (PASS == 0) ? a.d_hi[ib] : 0.0;
     const double *dlo = a.d_lo + a.d_lo_off[nu * (L + 1) + nd];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int nr = (nda + 31) >> 5;  // column slots in use (warp-uniform)
-    // per-lane columns rd = lane + 32 r; lanes past the row end work on a clamped copy of the
-    // last column and never store, so the inner loops carry no bounds checks
-    int rdc[kCols];
+    // per-lane columns rd = lane + 32 r of the block rows
     uint32_t da[kCols];
 #pragma unroll
-    for (int r = 0; r < kCols; r++) {
-      rdc[r] = min(lane + 32 * r, nda - 1);
-      da[r] = s_unrank[off_d + rdc[r]];
-    }
+    for (int r = 0; r < kCols; r++) da[r] = (lane + 32 * r < nda) ? s_unrank[off_d + lane + 32 * r] : 0u;
     // a warp owns a block row ra (ua uniform across the warp)
     for (int ra = warp; ra < nua; ra += nwarps) {
       const uint32_t ua = s_unrank[off_u + ra];
@@ -224,10 +218,11 @@ __global__ void __launch_bounds__(kThreads, PASS == 0 ? 3 : 4) hv_hub_pass(HubAr
       T x[kCols], y[kCols];
 #pragma unroll
       for (int r = 0; r < kCols; r++) {
-        if (r < nr) {
+        const int rd = lane + 32 * r;
+        if (rd < nda) {
           if (PASS == 0) {
-            x[r] = xs[row0 + rdc[r]];
-            double dg = dlo[row0 + rdc[r]] + dhi;
+            x[r] = xs[row0 + rd];
+            double dg = dlo[row0 + rd] + dhi;
             if (a.n_dcross) {
               const uint64_t c = ((uint64_t)ib << N) | a.spread[ua] | ((uint64_t)a.spread[da[r]] << 1);
               for (int k = 0; k < a.n_dcross; k++) {
@@ -237,7 +232,7 @@ __global__ void __launch_bounds__(kThreads, PASS == 0 ? 3 : 4) hv_hub_pass(HubAr
             }
             y[r] = VT<T>::scale(dg, x[r]);
           } else {
-            x[r] = v1[jb + row0 + rdc[r]];
+            x[r] = v1[jb + row0 + rd];
             y[r] = VT<T>::zero();
           }
         } else {
@@ -256,14 +251,15 @@ __global__ void __launch_bounds__(kThreads, PASS == 0 ? 3 : 4) hv_hub_pass(HubAr
           const T *srow = xs + (int)(ent & 0xFF) * nda;
 #pragma unroll
           for (int r = 0; r < kCols; r++)
-            if (r < nr) y[r] = cfma<T>(cre, cim, srow[rdc[r]], y[r]);
+            if (lane + 32 * r < nda) y[r] = cfma<T>(cre, cim, srow[lane + 32 * r], y[r]);
         }
         // lower-half down hops: per-column CSR rows within the staged row
         const T *row = xs + row0;
 #pragma unroll
         for (int r = 0; r < kCols; r++) {
-          if (r < nr) {
-            const int q0 = s_ptr[1][off_d + rdc[r]], q1 = s_ptr[1][off_d + rdc[r] + 1];
+          const int rd = lane + 32 * r;
+          if (rd < nda) {
+            const int q0 = s_ptr[1][off_d + rd], q1 = s_ptr[1][off_d + rd + 1];
             for (int e = q0; e < q1; e++) {
               const uint32_t ent = s_csr[1][e];
               const int h = (ent >> 8) & 0x7F;
@@ -279,7 +275,7 @@ __global__ void __launch_bounds__(kThreads, PASS == 0 ? 3 : 4) hv_hub_pass(HubAr
         const double cre = bl.re[k], cim = bl.im[k];
 #pragma unroll
         for (int r = 0; r < kCols; r++)
-          if (r < nr) y[r] = cfma<T>(cre, cim, src[rdc[r]], y[r]);
+          if (lane + 32 * r < nda) y[r] = cfma<T>(cre, cim, src[lane + 32 * r], y[r]);
       }
       // cross hops: one particle of this pass's spin changes half
       for (int q = 0; q < ncb; q++) {
@@ -293,19 +289,17 @@ __global__ void __launch_bounds__(kThreads, PASS == 0 ? 3 : 4) hv_hub_pass(HubAr
           const T *src = v1 + bl.src[k] + (int64_t)s_rank[ua ^ (1u << b)] * nda;
 #pragma unroll
           for (int r = 0; r < kCols; r++)
-            if (r < nr) y[r] = cfma<T>(cre, cim, src[rdc[r]], y[r]);
+            if (lane + 32 * r < nda) y[r] = cfma<T>(cre, cim, src[lane + 32 * r], y[r]);
         } else {
           const T *src = v1 + bl.src[k] + (int64_t)ra * bl.nsrc[k];
           const uint16_t *tab = s_ctab + b * nx;
           const double cre = bl.re[k], cim = bl.im[k];
 #pragma unroll
           for (int r = 0; r < kCols; r++) {
-            if (r < nr) {
-              const uint32_t e = tab[da[r]];
-              if ((int)((e >> 14) & 1u) == need) {
-                const double sg = (e >> 15) ? -1.0 : 1.0;
-                y[r] = cfma<T>(sg * cre, sg * cim, src[e & 0x3FFF], y[r]);
-              }
+            const uint32_t e = tab[da[r]];
+            if (lane + 32 * r < nda && (int)((e >> 14) & 1u) == need) {
+              const double sg = (e >> 15) ? -1.0 : 1.0;
+              y[r] = cfma<T>(sg * cre, sg * cim, src[e & 0x3FFF], y[r]);
             }
           }
         }
