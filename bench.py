@@ -300,7 +300,9 @@ def main():
                       "hphi_order_ms_per_step": hphi_order_ms},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak, "peak_kind": peak_kind,
-                        "traffic": profile_traffic("hv", args.workload)},
+                        "traffic": profile_traffic("hv_hub_pass" if H_native else "hv_general", args.workload),
+                        "kernels": "hv_hub_pass<double,0> + hv_hub_pass<double,1> per step" if H_native
+                        else "hv_general_kernel per step"},
            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 2 * args.steps, "clocks": clocks}
     print(json.dumps(out))
     if dist:
