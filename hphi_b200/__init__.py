@@ -39,7 +39,7 @@ EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi
                     "hphi_sz", "hphi_diagonalcalc", "hphi_mltply", "hphi_mltply_device", "hphi_lanczos",
                     "hphi_lanczos_eigenvector", "hphi_tpq", "hphi_run", "hphi_inspect_terms",
                     "hphi_lanczos_tridiagonal", "hphi_mltply_device_async", "hphi_stream",
-                    "hphi_synchronize", "hphi_to_native", "hphi_from_native"]
+                    "hphi_synchronize", "hphi_to_native", "hphi_from_native", "hphi_mltply_device_noalloc"]
 
 
 class HPhiError(RuntimeError):
@@ -82,6 +82,7 @@ def load_library() -> ctypes.CDLL:
     lib.hphi_tpq.argtypes = [P, pd, ctypes.c_char_p, pd, I]
     lib.hphi_run.argtypes = [P, ctypes.c_char_p]
     lib.hphi_mltply_device_async.argtypes = [P, I, VP, VP, VP, VP]
+    lib.hphi_mltply_device_noalloc.argtypes = [P, I, VP, VP, D, D, pd]
     lib.hphi_to_native.argtypes = [P, I, VP, VP]
     lib.hphi_from_native.argtypes = [P, I, VP, VP]
     lib.hphi_stream.argtypes = [P]
@@ -208,6 +209,17 @@ class Hamiltonian:
         _check(load_library().hphi_mltply_device_async(self._h, int(vec_type), ctypes.c_void_p(v0_ptr),
                                                        ctypes.c_void_p(v1_ptr), ctypes.c_void_p(coef_ptr),
                                                        ctypes.c_void_p(prdct_ptr)))
+
+    def mltply_device_noalloc(self, v0_ptr: int, v1_ptr: int, vec_type: int, acc: float = 1.0,
+                              scale: float = 1.0) -> complex:
+        """v0 = acc*v0 + scale*H v1 on native-order device vectors without allocating device
+        memory: the call's scratch is a fixed static device array shared by all calls on the
+        device, so calls must not overlap on the GPU.  Waits for the stream; returns prdct."""
+        pr = np.zeros(2)
+        _check(load_library().hphi_mltply_device_noalloc(self._h, int(vec_type), ctypes.c_void_p(v0_ptr),
+                                                         ctypes.c_void_p(v1_ptr), float(acc), float(scale),
+                                                         _dptr(pr)))
+        return complex(pr[0], pr[1])
 
     def to_native(self, in_ptr: int, out_ptr: int, vec_type: int) -> None:
         """HPhi order -> the engine's native order (0-based device vectors, in != out)."""

@@ -28,10 +28,15 @@ struct hphi_handle {
   void *d_perm1 = nullptr;
 };
 
+namespace hphi {
+// The sector behind a handle (nullptr for an invalid handle); for entry points in other files.
+Sector *handle_sector(hphi_handle *h) { return (h && h->sector) ? h->sector : nullptr; }
+}  // namespace hphi
+
 using namespace hphi;
 
 namespace {
-#define CHECK_HANDLE(h)                        \
+#define CHECK_HANDLE(h)                     \
   do {                                         \
     if (!(h) || !(h)->sector) {                \
       set_error("invalid handle");             \

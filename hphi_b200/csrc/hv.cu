@@ -110,6 +110,55 @@ int hv_launch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double 
   return 0;
 }
 
+int hv_launch_scratch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out,
+                      double *d_part) {
+  if (vt == kReal64 && s->model.complex_terms) {
+    set_error("H has complex coefficients: real vectors are not allowed");
+    return -1;
+  }
+  const int grid = s->red_blocks;
+  const uint64_t lo_mask = s->ihfbit - 1;
+  const bool smem_terms = s->nterms <= kSmemTermMax;
+  const size_t smem = smem_terms ? sizeof(BitTerm) * (size_t)s->nterms : 0;
+#define HPHI_GENERAL_LAUNCH(T, GC)                                                                              \
+  do {                                                                                                          \
+    if (smem_terms)                                                                                             \
+      hv_general_kernel<T, GC, true><<<grid, kHvThreads, smem, s->stream>>>(                                    \
+          s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, s->d_terms, s->nterms,        \
+          s->d_diag, (const T *)d_v1, (T *)d_v0, d_coef, d_part);                                              \
+    else                                                                                                        \
+      hv_general_kernel<T, GC, false><<<grid, kHvThreads, 0, s->stream>>>(                                      \
+          s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, s->d_terms, s->nterms,        \
+          s->d_diag, (const T *)d_v1, (T *)d_v0, d_coef, d_part);                                              \
+  } while (0)
+  if (vt == kReal64) {
+    if (s->gc) HPHI_GENERAL_LAUNCH(double, true);
+    else HPHI_GENERAL_LAUNCH(double, false);
+  } else {
+    if (s->gc) HPHI_GENERAL_LAUNCH(cplx, true);
+    else HPHI_GENERAL_LAUNCH(cplx, false);
+  }
+#undef HPHI_GENERAL_LAUNCH
+  finalize_partials_kernel<2><<<1, 256, 0, s->stream>>>(d_part, grid, d_out);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error(std::string("hv launch failed: ") + cudaGetErrorString(e));
+    return -1;
+  }
+  return 0;
+}
+
+size_t hv_scratch_doubles(const Sector *s) {
+  if (s->hub) return hub_scratch_doubles(s);
+  return 2 * (size_t)s->red_blocks;
+}
+
+int hv_native_scratch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out,
+                      double *d_part, int *d_counter) {
+  if (s->hub) return hub_hv_launch_scratch(s, vt, d_v1, d_v0, d_coef, d_out, d_part, d_counter);
+  return hv_launch_scratch(s, vt, d_v1, d_v0, d_coef, d_out, d_part);
+}
+
 bool has_native_order(const Sector *s) { return s->hub != nullptr; }
 
 int hv_native(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out,

@@ -678,6 +678,43 @@ int hub_hv_launch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const dou
   return 0;
 }
 
+size_t hub_scratch_doubles(const Sector *s) { return 2 * (size_t)(s->hub->grid[0] + s->hub->grid[1]); }
+
+int hub_hv_launch_scratch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out,
+                          double *d_part, int *d_counter) {
+  HubPlan *p = s->hub;
+  if (vt == kReal64 && s->model.complex_terms) {
+    set_error("H has complex coefficients: real vectors are not allowed");
+    return -1;
+  }
+  HubArgs args = p->args;
+  args.counter = d_counter;
+  if (cudaMemsetAsync(d_counter, 0, 2 * sizeof(int), s->stream) != cudaSuccess) {
+    set_error("hubbard hv: clearing the block counters failed");
+    return -1;
+  }
+  if (vt == kReal64) {
+    hv_hub_pass<double, 0><<<p->grid[0], kThreads, p->smem[0][0], s->stream>>>(args, (const double *)d_v1,
+                                                                               (double *)d_v0, d_coef, d_part);
+    hv_hub_pass<double, 1><<<p->grid[1], kThreads, p->smem[1][0], s->stream>>>(args, (const double *)d_v1,
+                                                                               (double *)d_v0, d_coef,
+                                                                               d_part + 2 * p->grid[0]);
+  } else {
+    hv_hub_pass<cplx, 0><<<p->grid[0], kThreads, p->smem[0][1], s->stream>>>(args, (const cplx *)d_v1,
+                                                                             (cplx *)d_v0, d_coef, d_part);
+    hv_hub_pass<cplx, 1><<<p->grid[1], kThreads, p->smem[1][1], s->stream>>>(args, (const cplx *)d_v1,
+                                                                             (cplx *)d_v0, d_coef,
+                                                                             d_part + 2 * p->grid[0]);
+  }
+  finalize_partials_kernel<2><<<1, 256, 0, s->stream>>>(d_part, p->grid[0] + p->grid[1], d_out);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error(std::string("hubbard hv launch failed: ") + cudaGetErrorString(e));
+    return -1;
+  }
+  return 0;
+}
+
 int hub_permute(Sector *s, VecType vt, const void *in, void *out, bool to_native) {
   HubPlan *p = s->hub;
   const HubArgs &a = p->args;

@@ -14,6 +14,10 @@ void hub_plan_free(HubPlan *p);
 int hub_hv_launch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out,
                   bool acc_read);
 int hub_permute(Sector *s, VecType vt, const void *in, void *out, bool to_native);
+// Same as hub_hv_launch with caller-provided partial sums and block counters (2 ints).
+int hub_hv_launch_scratch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out,
+                          double *d_part, int *d_counter);
+size_t hub_scratch_doubles(const Sector *s);
 int hub_observables(Sector *s, VecType vt, const void *v, double *d_out);
 
 }  // namespace hphi

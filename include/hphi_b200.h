@@ -116,6 +116,23 @@ int hphi_mltply_device_async(hphi_handle *h, int vec_type, void *d_v0, const voi
                              double *d_prdct);
 
 /*
+ * The H*v of hphi_mltply_device_async for callers that may not allocate device memory
+ * when they call it: code whose device memory belongs to another allocator's budget, or a
+ * latency-bound loop that cannot take cudaMalloc's device-wide synchronisation.  Same
+ * vectors (native order, d_v0 = acc * d_v0 + scale * (H d_v1), acc == 0 never reads d_v0),
+ * but the coefficients, the block counters and the partial sums of prdct live in one fixed
+ * static device array of 128 KiB that every GPU loading the library keeps until exit; no
+ * cudaMalloc or cudaFree is called.  prdct (host, 2 doubles) = sum conj(d_v1) (H d_v1);
+ * the call waits for the handle's stream.  A sector whose kernel needs more partial sums
+ * than the array holds is refused with an error (-1).  Every call shares the array: calls
+ * that overlap on the GPU (other threads, streams or handles on the same device) race.
+ * The first call on a device looks up the array's address; make it before any stream
+ * capture.  No counterpart in the reference (HPhi allocates its work vectors itself).
+ */
+int hphi_mltply_device_noalloc(hphi_handle *h, int vec_type, void *d_v0, const void *d_v1, double acc,
+                               double scale, double *prdct);
+
+/*
  * Native vector order.  For canonical Hubbard inputs the engine stores each block of
  * HPhi's sector (rows sharing the upper half of the configuration, src/sz.c:993-1094)
  * as an (up, down) product matrix; otherwise the native order is HPhi's order.  These

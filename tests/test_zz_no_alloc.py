@@ -1,0 +1,70 @@
+"""hphi_mltply_device_noalloc, the H*v entry point for callers that may not allocate device
+memory (code under another allocator's memory budget, loops that cannot take cudaMalloc's
+synchronisation), against hphi_mltply_device_async on the same native-order vectors.
+
+Its scratch is one static device array shared by every call, so each case makes two calls in
+a row with different inputs: the second must not see the first one's counters or partial
+sums.  This file is named to be collected last; it passes alone and after the other tests."""
+import pytest
+
+import hphi_b200
+from hphi_b200 import expert
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _complex_hubbard_chain(L):
+    m = expert.hubbard(L, expert.chain_bonds(L), 1.0, 3.0, L // 2, L // 2)
+    m.trans = []
+    for i, j in expert.chain_bonds(L):
+        for s in (0, 1):
+            m.trans += [(i, s, j, s, 0.8, 0.3), (j, s, i, s, 0.8, -0.3)]
+    return m
+
+
+CASES = {
+    # Hubbard block kernel (native order differs from HPhi's order)
+    "hubbard3x4": (lambda: expert.hubbard(12, expert.square_bonds(3, 4), 1.0, 8.0, 6, 6), False, 1),
+    "hubbard_chain10_complex": (lambda: _complex_hubbard_chain(10), True, 1),
+    # general kernel (native order is HPhi's order)
+    "heisenberg_chain16": (lambda: expert.heisenberg(16, expert.chain_bonds(16), 1.0), False, 0),
+}
+
+
+def _async_hv(H, v1, v0, vt, acc, scale):
+    out = v0.clone()
+    coef = torch.tensor([acc, scale], dtype=torch.float64, device="cuda")
+    pr = torch.zeros(2, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    H.mltply_device_async(out.data_ptr(), v1.data_ptr(), vt, coef.data_ptr(), pr.data_ptr())
+    H.synchronize()
+    return out, complex(pr[0].item(), pr[1].item())
+
+
+def _noalloc_hv(H, v1, v0, vt, acc, scale):
+    out = v0.clone()
+    torch.cuda.synchronize()
+    pr = H.mltply_device_noalloc(out.data_ptr(), v1.data_ptr(), vt, acc=acc, scale=scale)
+    return out, pr
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_noalloc_matches_async_on_two_calls(name, tmp_path):
+    make, cplx, native = CASES[name]
+    H = hphi_b200.Hamiltonian(make().write(str(tmp_path)))
+    try:
+        assert H.info["native_order"] == native
+        dt = torch.complex128 if cplx else torch.float64
+        vt = hphi_b200.COMPLEX128 if cplx else hphi_b200.REAL64
+        g = torch.Generator(device="cuda").manual_seed(17)
+        for acc, scale in ((0.7, -1.3), (0.0, 1.0)):
+            v1 = torch.randn(H.dim, dtype=dt, device="cuda", generator=g)
+            v0 = torch.randn(H.dim, dtype=dt, device="cuda", generator=g)
+            ya, pa = _async_hv(H, v1, v0, vt, acc, scale)
+            yn, pn = _noalloc_hv(H, v1, v0, vt, acc, scale)
+            err = (yn - ya).abs().max().item() / ya.abs().max().item()
+            assert err < 1e-12, (acc, scale, err)
+            assert abs(pn - pa) <= 1e-10 * abs(pa), (pn, pa)
+    finally:
+        H.close()
