@@ -27,7 +27,7 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-__all__ = ["Hamiltonian", "HPhiError", "inspect_terms", "load_library", "library_path", "REAL64", "COMPLEX128",
+__all__ = ["Hamiltonian", "Batch", "Server", "HPhiError", "inspect_terms", "load_library", "library_path", "REAL64", "COMPLEX128",
            "INFO_FIELDS", "EXPORTED_SYMBOLS"]
 
 REAL64 = 0
@@ -39,7 +39,16 @@ EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi
                     "hphi_sz", "hphi_diagonalcalc", "hphi_mltply", "hphi_mltply_device", "hphi_lanczos",
                     "hphi_lanczos_eigenvector", "hphi_tpq", "hphi_run", "hphi_inspect_terms",
                     "hphi_lanczos_tridiagonal", "hphi_mltply_device_async", "hphi_stream",
-                    "hphi_synchronize", "hphi_to_native", "hphi_from_native", "hphi_mltply_device_noalloc"]
+                    "hphi_synchronize", "hphi_to_native", "hphi_from_native", "hphi_mltply_device_noalloc",
+                    "hphi_lanczos_steps", "hphi_batch_create", "hphi_batch_lanczos", "hphi_batch_tuning",
+                    "hphi_batch_free", "hphi_server_create", "hphi_server_submit", "hphi_server_step",
+                    "hphi_server_poll", "hphi_server_clock", "hphi_server_free"]
+FP64 = 0
+FP32 = 1
+BATCH_GRAPH = 1
+BATCH_REFINE = 2
+BATCH_RESULT_FIELDS = 5
+SERVE_RESULT_FIELDS = 8
 
 
 class HPhiError(RuntimeError):
@@ -90,8 +99,23 @@ def load_library() -> ctypes.CDLL:
     lib.hphi_synchronize.argtypes = [P]
     lib.hphi_lanczos_tridiagonal.argtypes = [P, pd, pd, I, ctypes.POINTER(I)]
     lib.hphi_inspect_terms.argtypes = [ctypes.c_char_p, pu64, pd, I, pu64, pd, I, pi64]
+    lib.hphi_lanczos_steps.argtypes = [P, I, ctypes.c_uint64, pd, I]
+    lib.hphi_batch_create.argtypes = [ctypes.POINTER(P), I, I, ctypes.POINTER(P)]
+    lib.hphi_batch_lanczos.argtypes = [P, I, ctypes.c_uint64, I, D, pd, pd]
+    lib.hphi_batch_tuning.argtypes = [P, I, ctypes.POINTER(I)]
+    lib.hphi_batch_free.argtypes = [P]
+    lib.hphi_batch_free.restype = None
+    lib.hphi_server_create.argtypes = [I, I, ctypes.c_int64, I, I, ctypes.POINTER(P)]
+    lib.hphi_server_submit.argtypes = [P, ctypes.c_char_p, ctypes.c_uint64, D, pi64]
+    lib.hphi_server_step.argtypes = [P, pi64]
+    lib.hphi_server_poll.argtypes = [P, pi64, pd]
+    lib.hphi_server_clock.argtypes = []
+    lib.hphi_server_clock.restype = D
+    lib.hphi_server_free.argtypes = [P]
+    lib.hphi_server_free.restype = None
     for name in EXPORTED_SYMBOLS:
-        if name not in ("hphi_version", "hphi_last_error", "hphi_close", "hphi_stream"):
+        if name not in ("hphi_version", "hphi_last_error", "hphi_close", "hphi_stream", "hphi_batch_free",
+                        "hphi_server_clock", "hphi_server_free"):
             getattr(lib, name).restype = I
     _lib = lib
     return lib
@@ -286,3 +310,135 @@ class Hamiltonian:
 
     def run(self, output_dir: str = "output") -> None:
         _check(load_library().hphi_run(self._h, os.fsencode(output_dir)))
+
+    def lanczos_steps(self, steps: int, seed: int = 1, nev: int = 4) -> np.ndarray:
+        """Fixed-length Lanczos (exactly `steps` steps, convergence test off) from the hashed
+        start vector of `seed`; returns the nev lowest tridiagonal eigenvalues."""
+        e = np.zeros(max(nev, 1))
+        _check(load_library().hphi_lanczos_steps(self._h, int(steps), ctypes.c_uint64(seed), _dptr(e), nev))
+        return e[:nev]
+
+
+class Batch:
+    """Many open Hamiltonians advanced together by the batched Lanczos engine.
+
+    precision FP64 or FP32 (vector storage; sums, dots and scalars stay FP64).  The
+    Hamiltonians must stay open while the batch lives."""
+
+    def __init__(self, hamiltonians: Sequence[Hamiltonian], precision: int = FP64):
+        lib = load_library()
+        self._members = list(hamiltonians)
+        arr = (ctypes.c_void_p * len(self._members))(*[h.handle.value for h in self._members])
+        b = ctypes.c_void_p()
+        _check(lib.hphi_batch_create(arr, len(self._members), int(precision), ctypes.byref(b)))
+        self._b = b
+        self.precision = precision
+
+    def __len__(self):
+        return len(self._members)
+
+    def lanczos(self, steps: int, seed: int = 1, graph: bool = True, refine: bool = False,
+                replay_tol: float = 1e-6) -> dict:
+        """`steps` Lanczos steps for every instance (instance i starts from the hashed vector
+        of seed + 1000003*i).  With refine, the ground state is rebuilt (replay truncated where
+        the rest of the Ritz vector is below replay_tol) and refined in FP64.  Returns arrays
+        e_lanczos, e_refined, residual, steps, replay_steps and the phase timings in ms."""
+        n = len(self._members)
+        res = np.zeros(n * BATCH_RESULT_FIELDS)
+        tim = np.zeros(4)
+        flags = (BATCH_GRAPH if graph else 0) | (BATCH_REFINE if refine else 0)
+        _check(load_library().hphi_batch_lanczos(self._b, int(steps), ctypes.c_uint64(seed), flags,
+                                                 float(replay_tol), _dptr(res), _dptr(tim)))
+        r = res.reshape(n, BATCH_RESULT_FIELDS)
+        return {"e_lanczos": r[:, 0].copy(), "e_refined": r[:, 1].copy(), "residual": r[:, 2].copy(),
+                "steps": r[:, 3].astype(int), "replay_steps": r[:, 4].astype(int),
+                "forward_ms": float(tim[0]), "replay_ms": float(tim[1]), "refine_ms": float(tim[2]),
+                "tuned_hv_ms": float(tim[3])}
+
+    def tuning(self, retune: bool = False) -> dict:
+        shape = (ctypes.c_int * 3)()
+        _check(load_library().hphi_batch_tuning(self._b, 1 if retune else 0, shape))
+        return {"threads": shape[0], "rows_per_thread": shape[1], "ctas_per_sm": shape[2]}
+
+    def close(self) -> None:
+        if getattr(self, "_b", None) is not None and self._b.value:
+            load_library().hphi_batch_free(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching Lanczos request server on one device (see hphi_server_create)."""
+
+    FIELDS = ["status", "energy", "e_lanczos", "residual", "steps", "dim", "wait_s", "latency_s"]
+
+    def __init__(self, device: int = 0, precision: int = FP64, hbm_budget: int = 0, max_active: int = 64,
+                 steps_per_iteration: int = 16):
+        lib = load_library()
+        s = ctypes.c_void_p()
+        _check(lib.hphi_server_create(int(device), int(precision), int(hbm_budget), int(max_active),
+                                      int(steps_per_iteration), ctypes.byref(s)))
+        self._s = s
+
+    @staticmethod
+    def clock() -> float:
+        return float(load_library().hphi_server_clock())
+
+    def submit(self, namelist_def: str, seed: int = 1, arrival: float = -1.0) -> int:
+        rid = ctypes.c_int64()
+        _check(load_library().hphi_server_submit(self._s, os.fsencode(namelist_def), ctypes.c_uint64(seed),
+                                                 float(arrival), ctypes.byref(rid)))
+        return rid.value
+
+    def step(self) -> dict:
+        c = (ctypes.c_int64 * 3)()
+        _check(load_library().hphi_server_step(self._s, c))
+        return {"active": c[0], "queued": c[1], "finished": c[2]}
+
+    def poll(self) -> list:
+        """All finished requests as (request_id, dict) pairs."""
+        out = []
+        lib = load_library()
+        while True:
+            rid = ctypes.c_int64()
+            res = np.zeros(SERVE_RESULT_FIELDS)
+            rc = lib.hphi_server_poll(self._s, ctypes.byref(rid), _dptr(res))
+            if rc < 0:
+                raise HPhiError(lib.hphi_last_error().decode())
+            if rc == 0:
+                return out
+            d = {k: float(res[i]) for i, k in enumerate(self.FIELDS)}
+            d["status"] = int(res[0])
+            d["steps"] = int(res[4])
+            d["dim"] = int(res[5])
+            if d["status"] < 0:
+                d["error"] = lib.hphi_last_error().decode()
+            out.append((rid.value, d))
+
+    def close(self) -> None:
+        if getattr(self, "_s", None) is not None and self._s.value:
+            load_library().hphi_server_free(self._s)
+            self._s = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

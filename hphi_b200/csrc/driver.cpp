@@ -26,16 +26,16 @@
 #include <sys/stat.h>
 #include <vector>
 
+#include "batch.hpp"
 #include "driver.hpp"
 #include "engine.hpp"
 
 namespace hphi {
-namespace {
 
 // ---------------------------------------------------------------- tridiagonal
 // Number of eigenvalues of the symmetric tridiagonal (a[0..n), b[0..n-1)) below x
 // (Sturm sequence of the LDL^T factorisation of T - x).
-int sturm_count(const double *a, const double *b, int n, double x) {
+static int sturm_count(const double *a, const double *b, int n, double x) {
   int cnt = 0;
   double d = a[0] - x;
   const double tiny = 1e-300;
@@ -121,6 +121,8 @@ void tridiag_eigenvector(const double *a, const double *b, int n, double lam, st
   *out = x;
 }
 
+namespace {
+
 // ---------------------------------------------------------------- helpers
 struct DevBuf {
   void *p = nullptr;
@@ -205,6 +207,30 @@ void random_start(const Sector &s, uint64_t seed, bool complex_vec, std::vector<
   for (uint64_t i = 1; i <= dim; i++) { (*v)[2 * i] /= nrm; (*v)[2 * i + 1] /= nrm; }
 }
 
+// Hashed start (start_value of batch.hpp) in HPhi's 1-based complex128 layout, normalised.
+int hashed_start(const Sector &s, uint64_t seed, bool complex_vec, std::vector<double> *v) {
+  const uint64_t dim = (uint64_t)s.dim;
+  std::vector<uint64_t> cfg;
+  if (!s.gc) {
+    cfg.resize(dim);
+    if (cuda_ok(cudaMemcpy(cfg.data(), s.d_list_1, sizeof(uint64_t) * dim, cudaMemcpyDeviceToHost), "read list_1"))
+      return -1;
+  }
+  v->assign(2 * (dim + 1), 0.0);
+  double nrm = 0.0;
+  for (uint64_t i = 0; i < dim; i++) {
+    const uint64_t c = s.gc ? i : cfg[i];
+    const double re = start_value(seed, c, 0);
+    const double im = complex_vec ? start_value(seed, c, 1) : 0.0;
+    (*v)[2 * (i + 1)] = re;
+    (*v)[2 * (i + 1) + 1] = im;
+    nrm += re * re + im * im;
+  }
+  nrm = std::sqrt(nrm);
+  for (uint64_t i = 1; i <= dim; i++) { (*v)[2 * i] /= nrm; (*v)[2 * i + 1] /= nrm; }
+  return 0;
+}
+
 // ------------------------------------------------------------------- Lanczos
 int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOptions &opt, LanczosResult *res) {
   const Model &m = s->model;
@@ -215,9 +241,10 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   RET(cuda_ok(cudaMalloc(&P.p, esz * dim), "alloc P"));
   RET(cuda_ok(cudaMalloc(&Q.p, esz * dim), "alloc Q"));
   RET(cuda_ok(cudaMalloc(&ST.p, sizeof(double) * 32), "alloc scalars"));  // slots used: [0, 19)
-  int max_steps = m.lanczos_max;
+  const bool fixed = opt.fixed_steps > 0;
+  int max_steps = fixed ? opt.fixed_steps : m.lanczos_max;
   if ((int64_t)max_steps > dim) max_steps = (int)dim;
-  if (dim < m.lanczos_target) max_steps = (int)dim;
+  if (!fixed && dim < m.lanczos_target) max_steps = (int)dim;
   RET(cuda_ok(cudaMalloc(&AL.p, sizeof(double) * (max_steps + 2)), "alloc alpha"));
   RET(cuda_ok(cudaMalloc(&BE.p, sizeof(double) * (max_steps + 2)), "alloc beta"));
   // start vector: HPhi order on the host -> native order on the device
@@ -249,7 +276,7 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   res->lines.clear();
   res->converged = false;
   res->steps = 0;
-  const int batch = opt.batch > 0 ? opt.batch : (dim >= (1 << 20) ? 1 : 16);
+  const int batch = opt.batch > 0 ? opt.batch : (fixed ? 32 : (dim >= (1 << 20) ? 1 : 16));
   int done = 0;       // steps executed on the device
   int checked = 1;    // steps examined on the host
   double ebefor = 0.0;
@@ -275,6 +302,15 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
       checked = stp;
       const double *a = alpha.data() + 1;
       const double *b = beta.data() + 1;
+      if (fixed) {  // no step lines, no convergence test: stop at max_steps or on a breakdown
+        if (std::fabs(beta[stp]) < 1e-14 || stp == max_steps) {
+          res->converged = true;
+          res->steps = stp;
+          res->e_target = tridiag_eigenvalue(a, b, stp, std::min(target, stp - 1));
+          break;
+        }
+        continue;
+      }
       if (stp == 2) {
         E[1] = tridiag_eigenvalue(a, b, 2, 0);
         E[2] = tridiag_eigenvalue(a, b, 2, 1);

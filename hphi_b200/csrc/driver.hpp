@@ -11,6 +11,7 @@ struct LanczosOptions {
   bool eigenvector = false;       // replay the recurrence for the k_exct-th eigenvector
   bool copy_eigenvector = false;  // copy it back to the host (HPhi layout)
   int batch = 0;                  // steps between host convergence checks (0: automatic)
+  int fixed_steps = 0;            // > 0: exactly this many steps, convergence test off
 };
 
 struct LanczosResult {
@@ -29,9 +30,16 @@ struct TpqResult {
   std::vector<double> inv_temp, energy;
 };
 
+// k-th smallest eigenvalue (0-based) of the symmetric tridiagonal matrix with diagonal
+// a[0..n) and off-diagonal b[0..n-1), by Sturm bisection; its eigenvector by inverse iteration.
+double tridiag_eigenvalue(const double *a, const double *b, int n, int k);
+void tridiag_eigenvector(const double *a, const double *b, int n, double lam, std::vector<double> *out);
+
 VecType default_vec_type(const Sector &s);
 bool single_element_start(const Sector &s, std::vector<double> *v);
 void random_start(const Sector &s, uint64_t seed, bool complex_vec, std::vector<double> *v);
+// start_value (batch.hpp) per configuration, normalised, in HPhi's 1-based complex128 layout.
+int hashed_start(const Sector &s, uint64_t seed, bool complex_vec, std::vector<double> *v);
 
 // h_init: normalised start vector in HPhi's 1-based complex128 layout.
 int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOptions &opt, LanczosResult *res);

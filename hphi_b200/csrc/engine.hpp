@@ -53,7 +53,11 @@ struct Sector {
   HubPlan *hub = nullptr;
 };
 
-int sector_build(const Model &m, int device, Sector **out, std::string *err);
+// specialise = false skips the specialised kernel plans (the batched engine uses the
+// general row kernel only).
+int sector_build(const Model &m, int device, Sector **out, std::string *err, bool specialise = true);
+// idim_max of the model's sector, computed on the host (src/check.c:51-209).
+int64_t sector_dim(const Model &m);
 void sector_free(Sector *s);
 
 // v0 = acc * v0 + s * (H v1) with (acc, s) = d_coef[0..1] read on the device, and the raw

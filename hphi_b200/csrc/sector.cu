@@ -175,7 +175,14 @@ uint64_t binom_host(int n, int k) {
 
 }  // namespace
 
-int sector_build(const Model &m, int device, Sector **out, std::string *err) {
+int64_t sector_dim(const Model &m) {
+  if (m.is_gc()) return (int64_t)(1ull << m.nbits);
+  if (m.calc_model == kHubbard) return (int64_t)(binom_host(m.nsite, m.nup) * binom_host(m.nsite, m.ndown));
+  if (m.calc_model == kHubbardNConserved) return (int64_t)binom_host(2 * m.nsite, m.ne);
+  return (int64_t)binom_host(m.nsite, m.ne);
+}
+
+int sector_build(const Model &m, int device, Sector **out, std::string *err, bool specialise) {
   CK(cudaSetDevice(device));
   Sector *s = new Sector();
   s->model = m;
@@ -301,7 +308,7 @@ int sector_build(const Model &m, int device, Sector **out, std::string *err) {
   CK(cudaStreamSynchronize(s->stream));
   // Specialised kernels (HPHI_B200_KERNEL=general keeps the general kernel).
   const char *kern = getenv("HPHI_B200_KERNEL");
-  if (!(kern && std::string(kern) == "general")) {
+  if (specialise && !(kern && std::string(kern) == "general")) {
     if (hub_plan_build(s, err) != 0) return -1;
   }
   *out = s;

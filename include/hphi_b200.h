@@ -190,6 +190,86 @@ int hphi_tpq(hphi_handle *h, const double *v_init, const char *output_dir, doubl
  */
 int hphi_run(hphi_handle *h, const char *output_dir);
 
+/*
+ * Fixed-length Lanczos through the same driver as hphi_lanczos: exactly `steps` steps
+ * (fewer only on a breakdown, beta < 1e-14) with the convergence test off, from the
+ * hashed start vector of `seed` (element of configuration c: uniform in [-0.5, 0.5)
+ * keyed by (seed, c), imaginary part too for complex vectors; the same vector
+ * hphi_batch_lanczos uses).  energies[0 .. nev) receives the lowest eigenvalues of the
+ * tridiagonal matrix.  This is CalcByLanczos (src/CalcByLanczos.c:55-276) with
+ * Lanczos_max = steps and the LanczosEps test of src/Lanczos_EigenValue.c:262-275 off.
+ */
+int hphi_lanczos_steps(hphi_handle *h, int steps, uint64_t seed, double *energies, int nev);
+
+/*
+ * Batched Lanczos over many open Hamiltonians (same device).  No counterpart in the
+ * reference, which solves one Hamiltonian per run; each instance follows the recurrence
+ * of Lanczos_EigenValue (src/Lanczos_EigenValue.c:50-310).  precision HPHI_FP32 stores
+ * the Lanczos vectors in float (FP64 sums, dots and scalars); with HPHI_BATCH_REFINE the
+ * ground state of every instance is rebuilt in FP64 by replaying the recurrence
+ * (as Lanczos_EigenVector, src/Lanczos_EigenVector.c:46-208) and its FP64 Rayleigh
+ * quotient and residual are reported.  The handles must stay open while the batch lives.
+ */
+typedef struct hphi_batch hphi_batch;
+#define HPHI_FP64 0
+#define HPHI_FP32 1
+#define HPHI_BATCH_GRAPH 1   /* capture the iterations in CUDA graphs */
+#define HPHI_BATCH_REFINE 2  /* rebuild the ground state and refine its energy in FP64 */
+#define HPHI_BATCH_RESULT_FIELDS 5
+int hphi_batch_create(hphi_handle *const *handles, int n, int precision, hphi_batch **out);
+/*
+ * `steps` Lanczos steps for every instance from the hashed start vector of seed + 1000003*i
+ * (instance i).  With HPHI_BATCH_REFINE the replay stops where the rest of the Ritz vector
+ * has norm below replay_tol (<= 0: 1e-6).  result (n x HPHI_BATCH_RESULT_FIELDS, may be
+ * NULL): [0] lowest eigenvalue of the tridiagonal matrix, [1] refined energy, [2] residual
+ * |Hx - Ex|/|x|, [3] steps used, [4] steps replayed ([1]-[2],[4] zero without
+ * HPHI_BATCH_REFINE).  timing (4, may be NULL): forward, replay and refinement
+ * milliseconds, and the tuned hv-phase milliseconds.
+ */
+int hphi_batch_lanczos(hphi_batch *b, int steps, uint64_t seed, int flags, double replay_tol, double *result,
+                       double *timing);
+/* Launch shape (threads, rows per thread, CTAs per SM) chosen by the autotuner; retune != 0
+ * times the candidates again. */
+int hphi_batch_tuning(hphi_batch *b, int retune, int *shape);
+void hphi_batch_free(hphi_batch *b);
+
+/*
+ * Request server: continuous batching of Lanczos ground-state requests (expert-mode
+ * inputs of any model and sector size, CalcType 0) on one device.  No counterpart in the
+ * reference; each request follows Lanczos_EigenValue (src/Lanczos_EigenValue.c:50-310)
+ * with its own Lanczos_max, LanczosEps and LanczosTarget, tested every
+ * steps_per_iteration steps.  Requests are admitted first come first served while a slot
+ * (max_active) and the HBM budget (bytes; <= 0: 80% of the free memory) allow; every
+ * admitted request keeps its sector and Lanczos state on the device and advances in the
+ * same launches as the others; finished ones free their memory at once.  With HPHI_FP32
+ * each ground state is rebuilt and refined in FP64 as in hphi_batch_lanczos.  An
+ * instance's arithmetic does not depend on the other members, so a request gives the
+ * same result alone and in a mix.
+ */
+typedef struct hphi_server hphi_server;
+#define HPHI_SERVE_RESULT_FIELDS 8
+int hphi_server_create(int device, int precision, int64_t hbm_budget, int max_active, int steps_per_iteration,
+                       hphi_server **out);
+/* Queues a request (the input is parsed now); arrival is its arrival time on
+ * hphi_server_clock() (< 0: now), from which its latency is counted. */
+int hphi_server_submit(hphi_server *s, const char *namelist_def, uint64_t seed, double arrival,
+                       int64_t *request_id);
+/* Admits, runs one iteration, retires finished requests.  counts (3, may be NULL):
+ * active, queued, finished but not yet polled. */
+int hphi_server_step(hphi_server *s, int64_t *counts);
+/*
+ * Pops one finished request: returns 1 and fills result (HPHI_SERVE_RESULT_FIELDS):
+ * [0] status (0 converged, 1 stopped at Lanczos_max, -1 failed: message in
+ * hphi_last_error), [1] energy (FP64-refined with HPHI_FP32), [2] lowest tridiagonal
+ * eigenvalue, [3] residual of the refined vector (0 for HPHI_FP64), [4] Lanczos steps,
+ * [5] dimension, [6] seconds waiting for admission, [7] seconds from arrival to result.
+ * Returns 0 when nothing has finished.
+ */
+int hphi_server_poll(hphi_server *s, int64_t *request_id, double *result);
+/* Seconds on the server's monotonic clock. */
+double hphi_server_clock(void);
+void hphi_server_free(hphi_server *s);
+
 #ifdef __cplusplus
 }
 #endif
