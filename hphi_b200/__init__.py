@@ -34,7 +34,7 @@ REAL64 = 0
 COMPLEX128 = 1
 _HERE = os.path.dirname(os.path.abspath(__file__))
 INFO_FIELDS = ["dim", "nsite", "calc_model", "calc_type", "size_list_2_1", "size_list_2_2", "is_gc",
-               "vec_type", "n_offdiag", "n_diag", "lanczos_max", "num_ave", "native_order"]
+               "vec_type", "n_offdiag", "n_diag", "lanczos_max", "num_ave", "native_order", "exct"]
 EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi_close", "hphi_info",
                     "hphi_sz", "hphi_diagonalcalc", "hphi_mltply", "hphi_mltply_device", "hphi_lanczos",
                     "hphi_lanczos_eigenvector", "hphi_tpq", "hphi_run", "hphi_inspect_terms",
@@ -42,7 +42,7 @@ EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi
                     "hphi_synchronize", "hphi_to_native", "hphi_from_native", "hphi_mltply_device_noalloc",
                     "hphi_lanczos_steps", "hphi_batch_create", "hphi_batch_lanczos", "hphi_batch_tuning",
                     "hphi_batch_free", "hphi_server_create", "hphi_server_submit", "hphi_server_step",
-                    "hphi_server_poll", "hphi_server_clock", "hphi_server_free"]
+                    "hphi_server_poll", "hphi_server_clock", "hphi_server_free", "hphi_lobpcg"]
 FP64 = 0
 FP32 = 1
 BATCH_GRAPH = 1
@@ -100,6 +100,7 @@ def load_library() -> ctypes.CDLL:
     lib.hphi_lanczos_tridiagonal.argtypes = [P, pd, pd, I, ctypes.POINTER(I)]
     lib.hphi_inspect_terms.argtypes = [ctypes.c_char_p, pu64, pd, I, pu64, pd, I, pi64]
     lib.hphi_lanczos_steps.argtypes = [P, I, ctypes.c_uint64, pd, I]
+    lib.hphi_lobpcg.argtypes = [P, pd, ctypes.c_char_p, pd, I]
     lib.hphi_batch_create.argtypes = [ctypes.POINTER(P), I, I, ctypes.POINTER(P)]
     lib.hphi_batch_lanczos.argtypes = [P, I, ctypes.c_uint64, I, D, pd, pd]
     lib.hphi_batch_tuning.argtypes = [P, I, ctypes.POINTER(I)]
@@ -308,6 +309,27 @@ class Hamiltonian:
                                        None if output_dir is None else os.fsencode(output_dir), _dptr(res), n))
         return res
 
+    def calc_by_lobpcg(self, v_init: Optional[Sequence[np.ndarray]] = None,
+                       output_dir: Optional[str] = None) -> dict:
+        """Block LOBPCG for the exct lowest states (CalcByLOBPCG).  v_init: exct start vectors
+        in HPhi layout (dim+1 complex128 each).  Returns converged, steps, residual and per-state
+        energy, var (<Hx|Hx>), doublon, sz arrays; raises if not converged."""
+        k = max(1, self.info["exct"])
+        buf = None
+        if v_init is not None:
+            buf = np.ascontiguousarray(np.stack([_as_hphi_vector(v, self.dim) for v in v_init]))
+        n = 3 + 4 * 4
+        res = np.zeros(n)
+        rc = load_library().hphi_lobpcg(self._h, None if buf is None else _dptr(buf.view(np.float64)),
+                                        None if output_dir is None else os.fsencode(output_dir), _dptr(res), n)
+        out = {"converged": bool(res[0]), "steps": int(res[1]), "residual": float(res[2])}
+        per = res[3:].reshape(4, 4)
+        for j, key in enumerate(["energy", "var", "doublon", "sz"]):
+            out[key] = per[:k, j].copy()
+        if rc != 0:
+            raise HPhiError(load_library().hphi_last_error().decode())
+        return out
+
     def run(self, output_dir: str = "output") -> None:
         _check(load_library().hphi_run(self._h, os.fsencode(output_dir)))
 
@@ -338,7 +360,7 @@ class Batch:
         return len(self._members)
 
     def lanczos(self, steps: int, seed: int = 1, graph: bool = True, refine: bool = False,
-                replay_tol: float = 1e-6) -> dict:
+                replay_tol: float = 1e-9) -> dict:
         """`steps` Lanczos steps for every instance (instance i starts from the hashed vector
         of seed + 1000003*i).  With refine, the ground state is rebuilt (replay truncated where
         the rest of the Ritz vector is below replay_tol) and refined in FP64.  Returns arrays

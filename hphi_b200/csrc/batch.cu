@@ -964,7 +964,7 @@ struct Server {
   int device = 0;
   int64_t budget = 0, used = 0;
   int max_active = 0, K = 16;
-  double replay_tol = 1e-6;
+  double replay_tol = 1e-9;
   int64_t next_id = 1;
   std::deque<Request> queue;
   std::vector<Request> active;
@@ -1255,7 +1255,7 @@ int hphi_batch_lanczos(hphi_batch *hb, int steps, uint64_t seed, int flags, doub
   cudaGetLastError();
   BatchResult r;
   if (batch_lanczos(hb->b, steps, seed, (flags & HPHI_BATCH_GRAPH) != 0, (flags & HPHI_BATCH_REFINE) != 0,
-                    replay_tol > 0.0 ? replay_tol : 1e-6, &r) != 0)
+                    replay_tol > 0.0 ? replay_tol : 1e-9, &r) != 0)
     return -1;
   const int n = (int)r.e_lanczos.size();
   if (result)

@@ -1,6 +1,8 @@
 // extern "C" entry points (include/hphi_b200.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -136,6 +138,7 @@ int hphi_info(const hphi_handle *h, int64_t *info, int n) {
   v[HPHI_INFO_LANCZOS_MAX] = s.model.lanczos_max;
   v[HPHI_INFO_NUM_AVE] = s.model.num_ave;
   v[HPHI_INFO_NATIVE_ORDER] = has_native_order(&s) ? 1 : 0;
+  v[HPHI_INFO_EXCT] = s.model.k_exct;
   for (int i = 0; i < n && i < HPHI_INFO_COUNT; i++) info[i] = v[i];
   return 0;
 }
@@ -350,14 +353,53 @@ int hphi_tpq(hphi_handle *h, const double *v_init, const char *output_dir, doubl
   return 0;
 }
 
+int hphi_lobpcg(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult) {
+  CHECK_HANDLE(h);
+  Sector *s = h->sector;
+  const VecType vt = default_vec_type(*s);
+  const int k = std::max(1, s->model.k_exct);
+  std::vector<double> start;
+  if (!v_init) {
+    if (!lobpcg_single_element_start(*s, &start)) {
+      std::vector<double> one;
+      start.clear();
+      for (int i = 0; i < k; i++) {
+        random_start(*s, 123432ull + (uint64_t)std::abs(s->model.initial_iv) + 7919ull * (uint64_t)i,
+                     vt == kComplex128, &one);
+        start.insert(start.end(), one.begin(), one.end());
+      }
+    }
+    v_init = start.data();
+  }
+  LobpcgResult r;
+  const int rc = lobpcg_run(s, vt, v_init, &r);
+  if (result && nresult > 0) {
+    std::vector<double> v = {r.converged ? 1.0 : 0.0, (double)r.steps, r.residual};
+    for (int i = 0; i < k; i++) {
+      v.push_back(r.energy.size() > (size_t)i ? r.energy[i] : 0.0);
+      v.push_back(r.var.size() > (size_t)i ? r.var[i] : 0.0);
+      v.push_back(r.doublon.size() > (size_t)i ? r.doublon[i] : 0.0);
+      v.push_back(r.sz.size() > (size_t)i ? r.sz[i] : 0.0);
+    }
+    for (int i = 0; i < nresult && i < (int)v.size(); i++) result[i] = v[i];
+  }
+  if (output_dir) {
+    const std::string err = get_error();
+    if (write_lobpcg_outputs(*s, r, output_dir) != 0) return -1;
+    if (rc != 0) set_error(err);
+  }
+  return rc;
+}
+
 int hphi_run(hphi_handle *h, const char *output_dir) {
   CHECK_HANDLE(h);
   const std::string out = output_dir ? output_dir : "output";
   switch (h->sector->model.calc_type) {
     case kLanczos: return hphi_lanczos(h, nullptr, out.c_str(), nullptr, 0);
     case kTPQ: return hphi_tpq(h, nullptr, out.c_str(), nullptr, 0);
+    case kCG: return hphi_lobpcg(h, nullptr, out.c_str(), nullptr, 0);
     default:
-      set_error("CalcType not supported by this engine (Lanczos = 0 and TPQ = 1 are)");
+      set_error("CalcType not supported by this engine (Lanczos = 0, TPQ = 1 and LOBPCG = 3 are)");
       return -1;
   }
 }

@@ -26,6 +26,17 @@ struct LanczosResult {
   std::vector<double> eigenvector;   // 1-based complex128 (HPhi layout) when requested
 };
 
+struct LobpcgResult {
+  bool converged = false;
+  bool copy_vectors = false;         // copy the eigenvectors back (HPhi layout, exct blocks)
+  int steps = 0;                     // X->Large.itr
+  double residual = 0.0;             // largest residual 2-norm of the last step
+  std::vector<double> eig;           // LOBPCG eigenvalue estimates of the last step
+  std::vector<double> energy, var, doublon, sz;  // phys() of each converged vector
+  std::vector<std::string> lines;    // zvo_Lanczos_Step.dat
+  std::vector<double> eigenvectors;  // exct x (dim + 1) complex128 when copy_vectors
+};
+
 struct TpqResult {
   std::vector<double> inv_temp, energy;
 };
@@ -46,5 +57,10 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
 int write_lanczos_outputs(const Sector &s, const LanczosResult &r, const std::string &outdir);
 // h_init: start vector (any norm) of sample rand_i; writes SS/Norm/Flct_rand<rand_i>.dat.
 int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::string &outdir, TpqResult *res);
+// Block LOBPCG for the exct lowest states (CalcType 3).  h_init: exct start vectors in
+// HPhi's 1-based complex128 layout, back to back (any norm).
+bool lobpcg_single_element_start(const Sector &s, std::vector<double> *v);
+int lobpcg_run(Sector *s, VecType vt, const double *h_init, LobpcgResult *res);
+int write_lobpcg_outputs(const Sector &s, const LobpcgResult &r, const std::string &outdir);
 
 }  // namespace hphi

@@ -298,9 +298,10 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       else if (k == "numave") m->num_ave = (int)v;
       else if (k == "expecinterval") m->expec_interval = (int)v;
       else if (k == "calchs") m->read_hacker = (int)v;
+      else if (k == "precg") m->pre_cg = (int)v;
       else if (k == "timeslice" || k == "expandcoef" || k == "outputinterval" || k == "tinit" ||
                k == "omegamax" || k == "omegamin" || k == "omegaim" || k == "omegaorg" || k == "nomega" ||
-               k == "targettpqrand" || k == "precg") {
+               k == "targettpqrand") {
         // accepted and ignored: parameters of modes outside this engine
       } else {
         *err = "modpara.def: unknown keyword " + kw;

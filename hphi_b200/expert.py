@@ -60,6 +60,7 @@ class ExpertModel:
     initial_vec_type: int = 1
     output_eigenvec: int = 0
     restart: int = 0
+    pre_cg: int = 0
     trans: List[Tuple] = field(default_factory=list)
     coulombintra: List[Tuple] = field(default_factory=list)
     coulombinter: List[Tuple] = field(default_factory=list)
@@ -134,6 +135,8 @@ class ExpertModel:
                   f"exct           {self.exct}", f"LanczosEps     {self.lanczos_eps}",
                   f"LanczosTarget  {self.lanczos_target}", f"LargeValue     {self.large_value}",
                   f"NumAve         {self.num_ave}", f"ExpecInterval  {self.expec_interval}"]
+        if self.pre_cg:
+            lines.append(f"PreCG          {self.pre_cg}")
         with open(path, "w") as f:
             f.write("\n".join(lines) + "\n")
 

@@ -39,7 +39,8 @@ typedef struct hphi_handle hphi_handle;
 #define HPHI_INFO_LANCZOS_MAX 10
 #define HPHI_INFO_NUM_AVE 11
 #define HPHI_INFO_NATIVE_ORDER 12 /* 1 if the engine's native vector order differs from HPhi's */
-#define HPHI_INFO_COUNT 13
+#define HPHI_INFO_EXCT 13         /* exct: states of LOBPCG / the Lanczos eigenvector index */
+#define HPHI_INFO_COUNT 14
 
 /* Library version string. */
 const char *hphi_version(void);
@@ -184,8 +185,20 @@ int hphi_lanczos_eigenvector(hphi_handle *h, double *v);
 int hphi_tpq(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult);
 
 /*
- * The whole expert-mode run of `HPhi -e namelist.def` for CalcType 0 (Lanczos) and
- * 1 (TPQ), writing HPhi's output files into output_dir ("output" when NULL).
+ * Block LOBPCG for the exct lowest states (CalcType 3, "CG"; preconditioned when PreCG = 1).
+ * v_init: exct start vectors in HPhi's layout, back to back (any norm), or NULL for the
+ * reference's single-element starts (initial_iv > 0 on canonical models) or seeded random
+ * ones.  Writes zvo_Lanczos_Step.dat and, when converged, zvo_energy.dat into output_dir
+ * (NULL: no files).  result (may be NULL, nresult values at most): [0] converged (1/0),
+ * [1] steps, [2] last residual 2-norm, then per state [3 + 4i] energy, [4 + 4i] <Hx|Hx>,
+ * [5 + 4i] doublon, [6 + 4i] Sz.  exct <= 4.
+ * Replaces: CalcByLOBPCG / LOBPCG_Main (src/CalcByLOBPCG.c:328-776) with phys (src/phys.c:48).
+ */
+int hphi_lobpcg(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult);
+
+/*
+ * The whole expert-mode run of `HPhi -e namelist.def` for CalcType 0 (Lanczos),
+ * 1 (TPQ) and 3 (LOBPCG), writing HPhi's output files into output_dir ("output" when NULL).
  * Replaces: main (src/HPhiMain.c:178-358) for those modes.
  */
 int hphi_run(hphi_handle *h, const char *output_dir);
@@ -220,7 +233,7 @@ int hphi_batch_create(hphi_handle *const *handles, int n, int precision, hphi_ba
 /*
  * `steps` Lanczos steps for every instance from the hashed start vector of seed + 1000003*i
  * (instance i).  With HPHI_BATCH_REFINE the replay stops where the rest of the Ritz vector
- * has norm below replay_tol (<= 0: 1e-6).  result (n x HPHI_BATCH_RESULT_FIELDS, may be
+ * has norm below replay_tol (<= 0: 1e-9).  result (n x HPHI_BATCH_RESULT_FIELDS, may be
  * NULL): [0] lowest eigenvalue of the tridiagonal matrix, [1] refined energy, [2] residual
  * |Hx - Ex|/|x|, [3] steps used, [4] steps replayed ([1]-[2],[4] zero without
  * HPHI_BATCH_REFINE).  timing (4, may be NULL): forward, replay and refinement

@@ -44,6 +44,7 @@ class Def:
     lanczos_target: int = 2
     large_value: float = 0.0
     num_ave: int = 1
+    pre_cg: int = 0
     trans: List[Tuple[int, int, int, int, complex]] = field(default_factory=list)   # off-diagonal, Hermitian pairs
     chemi: List[Tuple[int, int, float]] = field(default_factory=list)                # (site, spin, mu): -mu n
     coulomb_intra: List[Tuple[int, float]] = field(default_factory=list)
@@ -99,6 +100,7 @@ def read_expert(namelist: str) -> Def:
         elif k == "lanczos_max": d.lanczos_max = int(v)
         elif k == "initial_iv": d.initial_iv = int(v)
         elif k == "exct": d.k_exct = int(v)
+        elif k == "precg": d.pre_cg = int(v)
         elif k == "lanczoseps": d.lanczos_eps = int(v)
         elif k == "lanczostarget": d.lanczos_target = int(v)
         elif k == "largevalue": d.large_value = v
@@ -467,3 +469,74 @@ def dense_hamiltonian(d: Def, lists, diag) -> np.ndarray:
         col, _ = mltply(d, lists, diag, np.zeros_like(e), e)
         H[:, j] = col[1:]
     return H
+
+
+# ----------------------------------------------------------------------------- LOBPCG
+def _lowdin_eigen(hsub: np.ndarray, ovlp: np.ndarray):
+    """diag_ovrp (src/CalcByLOBPCG.c:43-123): Lowdin-orthogonalised H v = mu O v, overlap
+    eigenvalues <= 1e-10 dropped.  Returns (mu ascending, vectors as columns)."""
+    oe, ov = np.linalg.eigh(ovlp)
+    keep = oe > 1.0e-10
+    S = ov[:, keep] / np.sqrt(oe[keep])
+    mu, phi = np.linalg.eigh(S.conj().T @ hsub @ S)
+    return mu, S @ phi
+
+
+def _preshift(eig: float, res: float, eps: float) -> float:
+    """calc_preshift (src/CalcByLOBPCG.c:129-148)."""
+    if res >= 1.0:
+        return 0.0
+    k = np.trunc(np.log10(abs(eig)))
+    i = np.ceil(np.log10(eps)) if eps > res else np.ceil(np.log10(res))
+    return float(np.trunc(eig / 10.0 ** (k + i)) * 10.0 ** (k + i))
+
+
+def lobpcg(d: Def, lists, diag, x_init: np.ndarray):
+    """LOBPCG_Main (src/CalcByLOBPCG.c:328-632) on a dense H: x_init is (exct, dim+1).
+    Returns (step rows [step, max residual, threshold, eig...], final x (exct, dim))."""
+    H = dense_hamiltonian(d, lists, diag)
+    dg = diag[1:]
+    k = x_init.shape[0]
+    x = np.array(x_init[:, 1:], dtype=np.complex128)
+    x /= np.linalg.norm(x, axis=1)[:, None]
+    hx = x @ H.T
+    p = np.zeros_like(x)
+    hp = np.zeros_like(x)
+    eig = np.real(np.sum(x.conj() * hx, axis=1))
+    shift0 = d.large_value * d.nsite
+    rows = []
+    for stp in range(1, d.lanczos_max + 1):
+        eps = 10.0 ** (-0.5 * d.lanczos_eps)
+        if np.max(np.abs(eig)) > 1.0:
+            eps *= np.max(np.abs(eig))
+        w = hx - eig[:, None] * x
+        dmax = 0.0
+        for i in range(k):
+            dn = np.linalg.norm(w[i])
+            dmax = max(dmax, dn)
+            if stp != 1:
+                if d.pre_cg == 1:
+                    sh = _preshift(eig[i] + shift0, dn, eps) - shift0
+                    pc = dg - sh
+                    m = np.abs(pc) > eps
+                    w[i, m] /= pc[m]
+                w[i] /= np.linalg.norm(w[i])
+        rows.append([stp, dmax, eps] + list(eig))
+        if dmax < eps:
+            break
+        hw = w @ H.T
+        B = np.concatenate([w, x, p])
+        HB = np.concatenate([hw, hx, hp])
+        hsub = B.conj() @ HB.T
+        ovlp = B.conj() @ B.T
+        eig = np.real(np.diag(hsub)[k:2 * k]).copy()
+        mu, V = _lowdin_eigen(hsub, ovlp)
+        eig = 0.5 * (eig + mu[:k])
+        C = V[:, :k]
+        Cp = C.copy()
+        Cp[k:2 * k] = 0.0
+        x, hx, p, hp = C.T @ B, C.T @ HB, Cp.T @ B, Cp.T @ HB
+        nx = np.linalg.norm(x, axis=1)[:, None]
+        np_ = np.linalg.norm(p, axis=1)[:, None]
+        x, hx, p, hp = x / nx, hx / nx, p / np_, hp / np_
+    return np.array(rows), x

@@ -92,3 +92,35 @@ def tpq_table(workdir: str, rand_i: int = 0) -> np.ndarray:
                 continue
             rows.append([float(x) for x in line.split()])
     return np.array(rows)
+
+
+def lobpcg_steps(workdir: str) -> np.ndarray:
+    """zvo_Lanczos_Step.dat of a LOBPCG run (src/CalcByLOBPCG.c:445-453): rows of
+    (step, largest residual 2-norm, threshold, eigenvalue estimates...)."""
+    rows = []
+    with open(os.path.join(workdir, "output", "zvo_Lanczos_Step.dat")) as f:
+        for line in f:
+            p = line.split()
+            if not p or not p[0].isdigit():
+                continue
+            rows.append([float(x) for x in p])
+    return np.array(rows)
+
+
+def energy_states(workdir: str) -> np.ndarray:
+    """zvo_energy.dat of a LOBPCG run (src/CalcByLOBPCG.c:736-745): rows (energy, doublon, Sz)."""
+    rows, cur = [], {}
+    with open(os.path.join(workdir, "output", "zvo_energy.dat")) as f:
+        for line in f:
+            p = line.split()
+            if not p:
+                continue
+            if p[0] == "State":
+                if cur:
+                    rows.append([cur["Energy"], cur["Doublon"], cur["Sz"]])
+                cur = {}
+            elif p[0] in ("Energy", "Doublon", "Sz"):
+                cur[p[0]] = float(p[1])
+    if cur:
+        rows.append([cur["Energy"], cur["Doublon"], cur["Sz"]])
+    return np.array(rows)

@@ -30,6 +30,10 @@ def golden_cases(kind=None):
             continue
         if kind == "tpq" and (large or "tpq" not in z.files):
             continue
+        if kind == "lobpcg" and (large or "lobpcg_steps" not in z.files):
+            continue
+        if kind == "lanczos_or_tpq" and (large or ("steps" not in z.files and "tpq" not in z.files)):
+            continue
         out.append(name)
     return out
 

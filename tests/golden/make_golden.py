@@ -8,6 +8,7 @@ of oracle/ref_hooks.c:
   hv0_v1, hv0_v0a, hv0_pr        the first mltply call (v0 = 0 before: the start vector in v1)
   hv3_v1, hv3_v0b, hv3_v0a, hv3_pr  the 4th mltply call (accumulates into a non-zero v0)
   steps, step_vals               zvo_Lanczos_Step.dat (Lanczos cases)
+  lobpcg_steps, lobpcg_states    zvo_Lanczos_Step.dat rows and zvo_energy.dat states (LOBPCG cases)
   tpq                            SS_rand0.dat rows (TPQ cases)
 Large cases store only SHA-256 digests of the lists (sha_list_1 ...).
 
@@ -96,6 +97,17 @@ def _cases():
                        large_value=6.0)
     m.initial_vec_type = 0
     c["tpq_hub6"] = m
+    # LOBPCG (CalcType 3): single-element starts (initial_iv > 0), with and without PreCG,
+    # two states; a grand-canonical case with the reference's random start (its first
+    # mltply input is dumped and injected).
+    c["lobpcg_chain12"] = expert.heisenberg(12, expert.chain_bonds(12), calc_type="CG", initial_iv=1,
+                                            lanczos_max=400)
+    m = expert.hubbard(6, expert.chain_bonds(6), 1.0, 4.0, 3, 3, calc_type="CG", initial_iv=2, exct=2,
+                       lanczos_max=400, pre_cg=1)
+    c["lobpcg_hub6_k2"] = m
+    m = expert.kitaev_heisenberg(2, 2, -1.0, 0.2, calc_type="CG", lanczos_max=400, lanczos_eps=12)
+    m.initial_vec_type = 0
+    c["lobpcg_kitaev2x2"] = m
     return c
 
 
@@ -138,7 +150,10 @@ def make_case(name: str, m, large: bool = False) -> None:
         data["diag"] = run_ref.read_diag(tmp)
         v1, v0b, v0a, pr = run_ref.read_hv(tmp)
         data.update(hv0_v1=v1, hv0_v0a=v0a, hv0_pr=np.array(pr))
-        if m.calc_type == "Lanczos":
+        if m.calc_type == "CG":
+            data["lobpcg_steps"] = run_ref.lobpcg_steps(tmp)
+            data["lobpcg_states"] = run_ref.energy_states(tmp)
+        elif m.calc_type == "Lanczos":
             steps = run_ref.lanczos_steps(tmp)
             data["steps"] = np.array([s for s, _ in steps])
             data["step_vals"] = np.array([[np.nan if v is None else v for v in (vals + [None] * 6)[:6]]

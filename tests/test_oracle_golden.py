@@ -79,3 +79,34 @@ def test_oracle_tpq_energies(name):
     ref = g["tpq"]
     e = O.tpq_energies(d, lists, diag, g["hv0_v1"], ref.shape[0])
     np.testing.assert_allclose(e, ref[:, 1], rtol=1e-10, atol=1e-12)
+
+
+def lobpcg_start(d, g):
+    """The reference's start vectors: single-element ones for initial_iv > 0 on canonical
+    models (Initialize_wave, src/CalcByLOBPCG.c:220-251), else its dumped first mltply input."""
+    dim = g["diag"].size - 1
+    k = d.k_exct
+    if "list_1" not in g or d.initial_iv <= 0:
+        return g["hv0_v1"][None, :]
+    x0 = np.zeros((k, dim + 1), complex)
+    for ie in range(k):
+        iv = (dim // 2 + d.initial_iv + ie) % dim + 1
+        if iv < dim:
+            x0[ie, iv + 1] = 1.0 if d.initial_vec_type == 1 else (1 + 1j) / np.sqrt(2)
+    return x0
+
+
+@pytest.mark.parametrize("name", golden_cases("lobpcg"))
+def test_oracle_lobpcg_matches_reference(name):
+    g = load_golden(name)
+    d = O.read_expert(case_dir(name) + "/namelist.def")
+    lists = O.sz(d) if "list_1" in g else None
+    diag = O.diagonalcalc(d, lists)
+    rows, x = O.lobpcg(d, lists, diag, lobpcg_start(d, g))
+    ref = g["lobpcg_steps"]
+    assert rows.shape[0] == ref.shape[0]
+    # the step file prints 6 significant digits
+    np.testing.assert_allclose(rows[:, 1:], ref[:, 1:], rtol=1e-5, atol=0)
+    H = O.dense_hamiltonian(d, lists, diag)
+    e = np.real(np.sum(x.conj() * (x @ H.T), axis=1))
+    np.testing.assert_allclose(e, g["lobpcg_states"][:, 0], rtol=0, atol=1e-12)
