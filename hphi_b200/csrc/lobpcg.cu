@@ -107,6 +107,16 @@ __global__ void precondition_kernel(int64_t dim, const double *__restrict__ diag
   }
 }
 
+__global__ void fill_kernel(int64_t dim, double v, double *__restrict__ x) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < dim; r += (int64_t)gridDim.x * blockDim.x)
+    x[r] = v;
+}
+
+__global__ void mul_kernel(int64_t dim, const double *__restrict__ a, double *__restrict__ x) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < dim; r += (int64_t)gridDim.x * blockDim.x)
+    x[r] *= a[r];
+}
+
 int cuda_ok(cudaError_t e, const char *what) {
   if (e != cudaSuccess) {
     set_error(std::string("lobpcg: ") + what + ": " + cudaGetErrorString(e));
@@ -355,11 +365,22 @@ int lobpcg_run(Sector *s, VecType vt, const double *h_init, LobpcgResult *res) {
                                                     2 * kMaxIn * kMaxOut + 8)), "alloc scratch"));
   Ops ops{s, vt, (double *)AUX.p, (double *)AUX.p + 2 * kMaxPairs * s->red_blocks,
           (double *)AUX.p + 2 * kMaxPairs * s->red_blocks + 2 * kMaxPairs};
-  // diagonal in the native order for the preconditioner
+  // diagonal in the native order for the preconditioner.  The native order may carry a
+  // per-configuration sign s(c) = +-1 (fermion reordering); the diagonal is a function of
+  // the configuration, so undo it: to_native(diag) * to_native(1) = s^2 diag = diag.
   LRET(cuda_ok(cudaMalloc(&DIAG.p, sizeof(double) * dim), "alloc diagonal"));
-  LRET(to_native(s, kReal64, s->d_diag, DIAG.p));
-  // start vectors (HPhi layout, normalised here) -> native order
   LRET(cuda_ok(cudaMalloc(&HOST_TMP.p, vbytes), "alloc staging"));
+  LRET(to_native(s, kReal64, s->d_diag, DIAG.p));
+  if (has_native_order(s)) {
+    DevMem ONES;
+    LRET(cuda_ok(cudaMalloc(&ONES.p, sizeof(double) * dim), "alloc signs"));
+    fill_kernel<<<s->red_blocks, kThreads, 0, s->stream>>>(dim, 1.0, (double *)HOST_TMP.p);
+    LRET(to_native(s, kReal64, HOST_TMP.p, ONES.p));
+    mul_kernel<<<s->red_blocks, kThreads, 0, s->stream>>>(dim, (const double *)ONES.p, (double *)DIAG.p);
+    LRET(cuda_ok(cudaGetLastError(), "diagonal signs"));
+    LRET(cuda_ok(cudaStreamSynchronize(s->stream), "diagonal signs"));
+  }
+  // start vectors (HPhi layout, normalised here) -> native order
   for (int i = 0; i < k; i++) {
     LRET(vec_from_host_c128(s, vt, h_init + (size_t)i * 2 * (dim + 1), HOST_TMP.p));
     LRET(to_native(s, vt, HOST_TMP.p, vec(1, i)));
