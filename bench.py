@@ -13,6 +13,19 @@ timed region (B_alg = 3 * dim * 16 for complex vectors).
 --impl reference: the reference HPhi's own OpenMP mltply (oracle/_ref/HPhi_ref, built
 from the reference sources) on the same sector, timed per call on the host cores.
 
+--mode batch | precision | serve print one JSON line each for the other workloads of the
+metric (solves/s and latency against the plain FP64 GPU path):
+  batch      256 J1-J2 chains (L from {18,20,22,24}, J2 in [0,1], seeded), 300 Lanczos steps
+             each through the batched engine, FP64 and FP32 storage (FP64 refinement),
+             against the plain single-instance FP64 driver (hphi_lanczos_steps) on the same
+             start vectors.
+  precision  4x8 periodic Heisenberg, Sz=0 (dim 601,080,390): FP32-storage Lanczos with FP64
+             refinement against the plain FP64 GPU driver, |dE| stated.
+  serve      Poisson request stream (seeded, mean 50 req/s) of Heisenberg chains L=16..26,
+             half-filled Hubbard chains L=10..14 (U in [2,10]) and 24-site Kitaev-Heisenberg
+             honeycomb (SpinGC, complex) through the continuous-batching server: solves/s,
+             p50/p99 latency, |dE| against each request solved alone by the plain driver.
+
 Multi-GPU (--gpus N under torchrun): the path does not shard for this workload, so
 N independent replicas run (one per GPU); value = total bytes / max-over-ranks time.
 """
@@ -162,8 +175,207 @@ def run_reference_arm(args):
     print(json.dumps(out))
 
 
+def _clock_start():
+    try:
+        import torch
+        idx = torch.cuda.current_device()
+    except Exception:
+        idx = 0
+    c = ClockSampler(idx)
+    c.start()
+    return c
+
+
+def j1j2_batch_models(n: int, seed: int = 2024):
+    from hphi_b200 import expert
+    rng = np.random.default_rng(seed)
+    Ls = rng.choice([18, 20, 22, 24], size=n)
+    J2 = rng.uniform(0.0, 1.0, size=n)
+    return [(int(L), float(j2), expert.j1j2_chain(int(L), 1.0, float(j2))) for L, j2 in zip(Ls, J2)]
+
+
+def run_batch_mode(args):
+    """Batched Lanczos (256 J1-J2 chains, 300 steps) vs the plain FP64 driver."""
+    import hphi_b200
+    n, steps, seed = args.batch_size, args.batch_steps, 7
+    tmp = tempfile.mkdtemp()
+    hams = []
+    for i, (L, j2, m) in enumerate(j1j2_batch_models(n)):
+        d = os.path.join(tmp, f"i{i}")
+        os.makedirs(d)
+        m.initial_vec_type = 1
+        hams.append(hphi_b200.Hamiltonian(m.write(d)))
+    dims = [h.dim for h in hams]
+    res = {}
+    clocks = _clock_start()
+    for prec, name in ((hphi_b200.FP64, "fp64"), (hphi_b200.FP32, "fp32")):
+        with hphi_b200.Batch(hams, prec) as b:
+            tune = b.tuning()
+            b.lanczos(steps, seed=seed, refine=(prec == hphi_b200.FP32))   # warm-up (graphs, allocations)
+            t0 = time.perf_counter()
+            r = b.lanczos(steps, seed=seed, refine=(prec == hphi_b200.FP32))
+            wall = time.perf_counter() - t0
+        res[name] = dict(r=r, wall=wall, tune=tune)
+    # plain FP64 GPU path: each instance alone through the Lanczos driver, same start vector
+    nplain = min(n, args.plain_sample)
+    e_plain = []
+    hams[0].lanczos_steps(steps, seed=seed, nev=1)  # warm-up
+    t0 = time.perf_counter()
+    for i in range(nplain):
+        e_plain.append(hams[i].lanczos_steps(steps, seed=seed + 1000003 * i, nev=1)[0])
+    t_plain = time.perf_counter() - t0
+    cl = clocks.stop()
+    for h in hams:
+        h.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    e64 = res["fp64"]["r"]["e_lanczos"]
+    e32 = res["fp32"]["r"]["e_refined"]
+    plain_rate = nplain / t_plain
+    rate64 = n / res["fp64"]["wall"]
+    rate32 = n / res["fp32"]["wall"]
+    out = {"metric": METRIC, "mode": "batch", "value": rate32, "unit": "solves/s", "n_gpus": 1,
+           "higher_is_better": True, "dtype": "f32 storage, f64 sums/scalars/refinement", "data": "synthetic",
+           "config": {"workload": f"{n} J1-J2 chains, L in {{18,20,22,24}}, J2 in [0,1], {steps} Lanczos steps",
+                      "sum_dim": int(sum(dims)), "min_dim": int(min(dims)), "max_dim": int(max(dims)),
+                      "graph": True, "launch_shape_fp64": res["fp64"]["tune"], "launch_shape_fp32": res["fp32"]["tune"]},
+           "fp64_batched_solves_per_s": rate64, "fp32_batched_refined_solves_per_s": rate32,
+           "plain_fp64_solves_per_s": plain_rate, "plain_sample": nplain,
+           "speedup_fp32_vs_plain": rate32 / plain_rate, "speedup_fp64_batched_vs_plain": rate64 / plain_rate,
+           "max_abs_dE_fp32_refined_vs_fp64": float(np.max(np.abs(e32 - e64))),
+           "max_abs_dE_fp32_unrefined_vs_fp64": float(np.max(np.abs(res["fp32"]["r"]["e_lanczos"] - e64))),
+           "max_abs_dE_batched_fp64_vs_plain": float(np.max(np.abs(np.array(e_plain) - e64[:nplain]))),
+           "fp32_phase_ms": {"forward": res["fp32"]["r"]["forward_ms"], "replay": res["fp32"]["r"]["replay_ms"],
+                             "refine": res["fp32"]["r"]["refine_ms"]},
+           "fp64_forward_ms": res["fp64"]["r"]["forward_ms"], "clocks": cl}
+    print(json.dumps(out))
+
+
+def run_precision_mode(args):
+    """FP32-storage Lanczos on the 4x8 Heisenberg sector vs the plain FP64 GPU driver."""
+    import hphi_b200
+    from hphi_b200 import expert
+    steps, seed = args.precision_steps, 11
+    tmp = tempfile.mkdtemp()
+    m = expert.heisenberg(32, expert.square_bonds(4, 8), 1.0)
+    m.initial_vec_type = 1
+    H = hphi_b200.Hamiltonian(m.write(tmp))
+    clocks = _clock_start()
+    t0 = time.perf_counter()
+    e64 = H.lanczos_steps(steps, seed=seed, nev=1)[0]
+    t64 = time.perf_counter() - t0
+    with hphi_b200.Batch([H], hphi_b200.FP32) as b:
+        t0 = time.perf_counter()
+        r = b.lanczos(steps, seed=seed, refine=True)
+        t32 = time.perf_counter() - t0
+    cl = clocks.stop()
+    dim = H.dim
+    H.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    out = {"metric": METRIC, "mode": "precision", "value": 1.0 / t32, "unit": "solves/s", "n_gpus": 1,
+           "higher_is_better": True, "dtype": "f32 storage, f64 sums/scalars/refinement", "data": "synthetic",
+           "config": {"workload": "Heisenberg 4x8 periodic, J=1, Sz=0", "dim": dim, "steps": steps},
+           "e_fp64_plain": e64, "e_fp32_refined": float(r["e_refined"][0]), "e_fp32_unrefined": float(r["e_lanczos"][0]),
+           "abs_dE_refined": abs(float(r["e_refined"][0]) - e64),
+           "abs_dE_unrefined": abs(float(r["e_lanczos"][0]) - e64),
+           "residual_refined": float(r["residual"][0]), "replay_steps": int(r["replay_steps"][0]),
+           "plain_fp64_s": t64, "fp32_s": t32, "speedup_vs_plain": t64 / t32,
+           "fp32_phase_ms": {"forward": r["forward_ms"], "replay": r["replay_ms"], "refine": r["refine_ms"]},
+           "clocks": cl}
+    print(json.dumps(out))
+
+
+def serve_requests(n: int, seed: int = 50):
+    from hphi_b200 import expert
+    rng = np.random.default_rng(seed)
+    kw = dict(lanczos_max=1000, lanczos_eps=12, lanczos_target=1)
+    out = []
+    for i in range(n):
+        kind = int(rng.integers(0, 3))
+        if kind == 0:
+            L = int(rng.choice([16, 18, 20, 22, 24, 26]))
+            out.append((f"heis{L}", expert.heisenberg(L, expert.chain_bonds(L), 1.0, **kw)))
+        elif kind == 1:
+            L = int(rng.choice([10, 12, 14]))
+            U = float(rng.uniform(2.0, 10.0))
+            out.append((f"hub{L}", expert.hubbard(L, expert.chain_bonds(L), 1.0, U, L // 2, L // 2, **kw)))
+        else:
+            J = float(rng.uniform(0.0, 0.3))
+            out.append(("kh24", expert.kitaev_heisenberg(3, 4, -1.0, J, initial_vec_type=0, **kw)))
+    arrivals = np.cumsum(rng.exponential(1.0 / 50.0, size=n))
+    return out, arrivals
+
+
+def run_serve_mode(args):
+    """Continuous-batching server on a Poisson stream vs the plain FP64 driver per request."""
+    import hphi_b200
+    n = args.serve_requests
+    reqs, arr = serve_requests(n)
+    tmp = tempfile.mkdtemp()
+    paths = []
+    for i, (name, m) in enumerate(reqs):
+        d = os.path.join(tmp, f"r{i}")
+        os.makedirs(d)
+        paths.append(m.write(d))
+    result = {}
+    clocks = _clock_start()
+    for prec, pname in ((hphi_b200.FP64, "fp64"), (hphi_b200.FP32, "fp32")):
+        srv = hphi_b200.Server(precision=prec, max_active=args.serve_slots, steps_per_iteration=16)
+        t0 = srv.clock()
+        ids, res, nxt = {}, {}, 0
+        while len(res) < n:
+            now = srv.clock() - t0
+            while nxt < n and arr[nxt] <= now:
+                ids[srv.submit(paths[nxt], seed=nxt + 1, arrival=t0 + arr[nxt])] = nxt
+                nxt += 1
+            c = srv.step()
+            for rid, d in srv.poll():
+                res[ids[rid]] = d
+            if c["active"] == 0 and c["queued"] == 0 and nxt < n:
+                time.sleep(max(0.0, arr[nxt] - (srv.clock() - t0)))
+        wall = srv.clock() - t0
+        srv.close()
+        lat = np.array([res[i]["latency_s"] for i in range(n)])
+        result[pname] = dict(res=res, wall=wall, lat=lat)
+    # plain FP64 GPU path: a sample of the same requests, one at a time, open + Lanczos each
+    nplain = min(n, args.plain_sample)
+    e_plain, t_plain = [], 0.0
+    for i in range(nplain):
+        t0 = time.perf_counter()
+        with hphi_b200.Hamiltonian(paths[i]) as H:
+            r = H.calc_by_lanczos()
+        t_plain += time.perf_counter() - t0
+        e_plain.append(r["e1"])
+    cl = clocks.stop()
+    shutil.rmtree(tmp, ignore_errors=True)
+    plain_rate = nplain / t_plain
+    out = {"metric": METRIC, "mode": "serve", "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
+           "data": "synthetic", "dtype": "f64 (fp64 server) / f32 storage + f64 refinement (fp32 server)",
+           "config": {"workload": f"{n} Poisson requests at mean 50/s: Heisenberg chains L=16..26, half-filled "
+                                  "Hubbard chains L=10..14 (U in [2,10]), Kitaev-Heisenberg 24-site honeycomb "
+                                  "(SpinGC dim 2^24, complex)", "max_active": args.serve_slots,
+                      "steps_per_iteration": 16, "convergence": "LanczosEps=12 on E[LanczosTarget=1]"},
+           "plain_fp64_solves_per_s": plain_rate, "plain_sample": nplain, "clocks": cl}
+    for pname in ("fp64", "fp32"):
+        r = result[pname]
+        e = np.array([r["res"][i]["energy"] for i in range(nplain)])
+        out[pname] = {"solves_per_s": n / r["wall"], "p50_latency_s": float(np.percentile(r["lat"], 50)),
+                      "p99_latency_s": float(np.percentile(r["lat"], 99)), "wall_s": r["wall"],
+                      "status_codes": sorted({int(r["res"][i]["status"]) for i in range(n)}),
+                      "max_abs_dE_vs_plain": float(np.max(np.abs(e - np.array(e_plain)))),
+                      "speedup_vs_plain": (n / r["wall"]) / plain_rate}
+    out["value"] = out["fp32"]["solves_per_s"]
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--mode", default="hv", choices=["hv", "batch", "precision", "serve"])
+    ap.add_argument("--batch-size", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=300)
+    ap.add_argument("--precision-steps", type=int, default=300)
+    ap.add_argument("--serve-requests", type=int, default=100)
+    ap.add_argument("--serve-slots", type=int, default=64)
+    ap.add_argument("--plain-sample", type=int, default=256)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
@@ -176,6 +388,13 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference_arm(args)
+        return
+    if args.mode != "hv":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        {"batch": run_batch_mode, "precision": run_precision_mode, "serve": run_serve_mode}[args.mode](args)
         return
 
     import torch

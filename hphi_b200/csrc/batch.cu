@@ -701,16 +701,30 @@ void tridiag_of(const std::vector<double> &scal, int cap, int k, int64_t dim, in
   *e_out = tridiag_eigenvalue(al, be, m, 0);
 }
 
-// Replay length and coefficients of the ground state of T_m: the dropped tail of the Ritz
-// vector has norm below replay_tol, which moves the Rayleigh quotient by about
-// replay_tol^2 times the spectral width.
-int replay_plan(const std::vector<double> &scal, int cap, int m, double e, double replay_tol,
-                std::vector<double> *coef) {
+// Replay length and coefficients of the ground state.  Without reorthogonalisation the
+// recurrence keeps going after the ground state has converged and produces ghost copies of
+// it; a Ritz vector of the full T_m then mixes the copies and loses accuracy.  So the vector
+// is taken from T_mc, mc the first step (checked every 4) whose Ritz residual estimate
+// beta_k |s_k| (s_k the last component of the lowest eigenvector of T_k) is below
+// 1e-7 max(1, |E_k|), as the reference's driver stops at convergence before building its
+// eigenvector.  The dropped tail of that Ritz vector has norm below replay_tol, which moves
+// the Rayleigh quotient by about replay_tol^2 times the spectral width.
+int replay_plan(const std::vector<double> &scal, int cap, int m, double replay_tol, std::vector<double> *coef) {
   const size_t stride = (size_t)cap + 2;
   const double *al = scal.data() + kStSlots + 1;
   const double *be = scal.data() + kStSlots + stride + 1;
   std::vector<double> c;
-  tridiag_eigenvector(al, be, m, e, &c);
+  int mc = m;
+  for (int k = 8; k < m; k += 4) {
+    const double ek = tridiag_eigenvalue(al, be, k, 0);
+    tridiag_eigenvector(al, be, k, ek, &c);
+    if (std::fabs(be[k - 1] * c[k - 1]) <= 1e-7 * std::max(1.0, std::fabs(ek))) {
+      mc = k;
+      break;
+    }
+  }
+  m = mc;
+  tridiag_eigenvector(al, be, m, tridiag_eigenvalue(al, be, m, 0), &c);
   const double tol2 = replay_tol * replay_tol;
   int K = m;
   double tail = 0.0;
@@ -903,7 +917,7 @@ int batch_lanczos(Batch *b, int steps, uint64_t seed, bool use_graph, bool refin
     sl.inst.mode = kIdle;
     if (refine) {
       std::vector<double> coef;
-      const int K = replay_plan(scal[j], sl.cap, res->steps[j], res->e_lanczos[j], replay_tol, &coef);
+      const int K = replay_plan(scal[j], sl.cap, res->steps[j], replay_tol, &coef);
       BRET(cuda_ok(cudaMemcpyAsync(sl.inst.coef, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice,
                                    b->stream), "upload coefficients"));
       sl.inst.mode = kReplayInit;
@@ -1160,7 +1174,7 @@ int server_step(Server *sv, int64_t counts[3]) {
           r.status = (conv || breakdown) ? 0 : 1;
           if (sv->prec == kFP32) {
             std::vector<double> coef;
-            const int Kr = replay_plan(scal[j], sl.cap, mstep, e0, sv->replay_tol, &coef);
+            const int Kr = replay_plan(scal[j], sl.cap, mstep, sv->replay_tol, &coef);
             BRET(cuda_ok(cudaMemcpyAsync(sl.inst.coef, coef.data(), sizeof(double) * coef.size(),
                                          cudaMemcpyHostToDevice, b->stream), "upload coefficients"));
             sl.inst.mode = kReplayInit;
