@@ -25,6 +25,7 @@
 #include "batch.hpp"
 #include "device_util.cuh"
 #include "driver.hpp"
+#include "split.cuh"
 
 namespace hphi {
 namespace {
@@ -43,7 +44,8 @@ struct BInst {
   const uint64_t *list_1;
   const uint32_t *l21, *l22;
   const double *diag;
-  const BitTerm *terms;
+  const BitTerm *terms;         // generic-path terms (the split plan holds the others)
+  SplitView split;
   int64_t dim;
   uint64_t lo_mask;
   uint64_t seed;
@@ -187,6 +189,8 @@ __device__ __forceinline__ void hv_rows(const BInst &I, const BitTerm *terms, in
     const uint64_t c = GC ? (uint64_t)r : __ldg(list_1 + r);
     const A x = St::ldg(v1, r);
     A y = VT<A>::scale(__ldg(diag + r), x);
+    if (I.split.lo_ptr)
+      y = split_terms<A, GC>(I.split, c, r, lo_bits, lo_mask, l22, [&](int64_t jj) { return St::ldg(v1, jj); }, y);
     for (int k = 0; k < nterms; k++) {
       const BitTerm t = terms[k];
       if ((c & t.cm) != t.cv) continue;
@@ -492,10 +496,11 @@ int engine_add(Batch *b, Sector *s, bool owned, uint64_t seed, int cap, int *slo
   I.l21 = s->d_list_2_1;
   I.l22 = s->d_list_2_2;
   I.diag = s->d_diag;
-  I.terms = s->d_terms;
+  I.terms = s->split.gen;
+  I.split = split_view(s->split);
   I.dim = s->dim;
   I.lo_mask = s->ihfbit - 1;
-  I.nterms = s->nterms;
+  I.nterms = s->split.ngen;
   I.lo_bits = s->lo_bits;
   I.gc = s->gc ? 1 : 0;
   I.cplx = (default_vec_type(*s) == kComplex128) ? 1 : 0;

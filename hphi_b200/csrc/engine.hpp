@@ -23,6 +23,25 @@ struct cplx { double x, y; };
 
 enum VecType : int { kReal64 = 0, kComplex128 = 1 };
 
+// Upper-half entry of the split-term plan: source row = row + delta (grand-canonical
+// models: row ^ delta) with coefficient index k.
+struct HiEnt {
+  int64_t delta;
+  uint32_t k, pad;
+};
+
+// Split-term plan of the general kernels (split.cuh): per lower half the applicable
+// lower-half terms, per upper half the applicable upper-half terms, the rest generic.
+// Device pointers; lo_ptr == nullptr means no plan (every term generic).
+struct SplitPlan {
+  uint32_t *lo_ptr = nullptr, *lo_ent = nullptr, *hi_ptr = nullptr;
+  HiEnt *hi_ent = nullptr;
+  double *coef = nullptr;
+  BitTerm *gen = nullptr;  // terms left to the generic path
+  int ngen = 0;
+  int64_t n_lo_ent = 0, n_hi_ent = 0;
+};
+
 struct Sector {
   Model model;
   int device = 0;
@@ -51,6 +70,7 @@ struct Sector {
   // Optional specialised plan (canonical Hubbard).  When present, the drivers keep
   // vectors in the plan's native order; see hv_native / to_native.
   HubPlan *hub = nullptr;
+  SplitPlan split;
 };
 
 // specialise = false skips the specialised kernel plans (the batched engine uses the

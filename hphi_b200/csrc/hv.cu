@@ -16,6 +16,7 @@
 #include "device_util.cuh"
 #include "engine.hpp"
 #include "hv_hubbard.hpp"
+#include "split.cuh"
 
 namespace hphi {
 namespace {
@@ -26,9 +27,9 @@ constexpr int kSmemTermMax = 1024;  // 48 KiB of BitTerm
 template <typename T, bool GC, bool SMEM>
 __global__ void __launch_bounds__(kHvThreads) hv_general_kernel(
     int64_t dim, const uint64_t *__restrict__ list_1, const uint32_t *__restrict__ l21,
-    const uint32_t *__restrict__ l22, int lo_bits, uint64_t lo_mask, const BitTerm *__restrict__ gterms,
-    int nterms, const double *__restrict__ diag, const T *__restrict__ v1, T *__restrict__ v0,
-    const double *__restrict__ coef, double *__restrict__ part) {
+    const uint32_t *__restrict__ l22, int lo_bits, uint64_t lo_mask, SplitView split,
+    const BitTerm *__restrict__ gterms, int nterms, const double *__restrict__ diag, const T *__restrict__ v1,
+    T *__restrict__ v0, const double *__restrict__ coef, double *__restrict__ part) {
   const double acc = coef[0], scale = coef[1];
   extern __shared__ BitTerm sterms[];
   const BitTerm *terms = gterms;
@@ -42,6 +43,7 @@ __global__ void __launch_bounds__(kHvThreads) hv_general_kernel(
     const uint64_t c = GC ? (uint64_t)r : list_1[r];
     const T x = v1[r];
     T y = VT<T>::scale(diag[r], x);
+    if (split.lo_ptr) y = split_terms<T, GC>(split, c, r, lo_bits, lo_mask, l22, [&](int64_t j) { return v1[j]; }, y);
     for (int k = 0; k < nterms; k++) {
       const BitTerm t = terms[k];
       if ((c & t.cm) != t.cv) continue;
@@ -75,15 +77,16 @@ template <typename T, bool GC>
 void launch_general(Sector *s, const T *v1, T *v0, const double *coef) {
   const int grid = s->red_blocks;
   const uint64_t lo_mask = s->ihfbit - 1;
-  if (s->nterms <= kSmemTermMax) {
-    const size_t smem = sizeof(BitTerm) * (size_t)s->nterms;
+  const SplitView sv = split_view(s->split);
+  if (s->split.ngen <= kSmemTermMax) {
+    const size_t smem = sizeof(BitTerm) * (size_t)s->split.ngen;
     hv_general_kernel<T, GC, true><<<grid, kHvThreads, smem, s->stream>>>(
-        s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, s->d_terms, s->nterms, s->d_diag,
-        v1, v0, coef, s->d_red);
+        s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, sv, s->split.gen, s->split.ngen,
+        s->d_diag, v1, v0, coef, s->d_red);
   } else {
     hv_general_kernel<T, GC, false><<<grid, kHvThreads, 0, s->stream>>>(
-        s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, s->d_terms, s->nterms, s->d_diag,
-        v1, v0, coef, s->d_red);
+        s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, sv, s->split.gen, s->split.ngen,
+        s->d_diag, v1, v0, coef, s->d_red);
   }
 }
 
@@ -118,18 +121,19 @@ int hv_launch_scratch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const
   }
   const int grid = s->red_blocks;
   const uint64_t lo_mask = s->ihfbit - 1;
-  const bool smem_terms = s->nterms <= kSmemTermMax;
-  const size_t smem = smem_terms ? sizeof(BitTerm) * (size_t)s->nterms : 0;
+  const bool smem_terms = s->split.ngen <= kSmemTermMax;
+  const size_t smem = smem_terms ? sizeof(BitTerm) * (size_t)s->split.ngen : 0;
+  const SplitView sv = split_view(s->split);
 #define HPHI_GENERAL_LAUNCH(T, GC)                                                                              \
   do {                                                                                                          \
     if (smem_terms)                                                                                             \
       hv_general_kernel<T, GC, true><<<grid, kHvThreads, smem, s->stream>>>(                                    \
-          s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, s->d_terms, s->nterms,        \
-          s->d_diag, (const T *)d_v1, (T *)d_v0, d_coef, d_part);                                              \
+          s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, sv, s->split.gen,             \
+          s->split.ngen, s->d_diag, (const T *)d_v1, (T *)d_v0, d_coef, d_part);                               \
     else                                                                                                        \
       hv_general_kernel<T, GC, false><<<grid, kHvThreads, 0, s->stream>>>(                                      \
-          s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, s->d_terms, s->nterms,        \
-          s->d_diag, (const T *)d_v1, (T *)d_v0, d_coef, d_part);                                              \
+          s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, sv, s->split.gen,             \
+          s->split.ngen, s->d_diag, (const T *)d_v1, (T *)d_v0, d_coef, d_part);                               \
   } while (0)
   if (vt == kReal64) {
     if (s->gc) HPHI_GENERAL_LAUNCH(double, true);

@@ -20,6 +20,7 @@
 
 #include "engine.hpp"
 #include "hv_hubbard.hpp"
+#include "split.cuh"
 
 namespace hphi {
 namespace {
@@ -175,6 +176,114 @@ uint64_t binom_host(int n, int k) {
 
 }  // namespace
 
+// Split-term plan (split.cuh): classifies the compiled terms by which half of the
+// configuration their masks touch and tabulates the lower-half and upper-half ones.
+// Skipped (every term generic) when a half has more than 18 bits or the entry fields
+// would overflow.
+static int split_plan_build(Sector *s, std::string *err) {
+  SplitPlan &P = s->split;
+  const std::vector<BitTerm> &T = s->model.offdiag;
+  const uint64_t lo_mask = s->ihfbit - 1;
+  std::vector<int> lo_t, hi_t, gen_t;
+  for (int q = 0; q < (int)T.size(); q++) {
+    const uint64_t all = T[q].cm | T[q].flip | T[q].sm;
+    if ((all & ~lo_mask) == 0) lo_t.push_back(q);
+    else if ((all & lo_mask) == 0) hi_t.push_back(q);
+    else gen_t.push_back(q);
+  }
+  const bool usable = s->lo_bits <= 18 && s->hi_bits <= 18 && 2 * (lo_t.size() + hi_t.size()) < 4096 &&
+                      (s->gc || s->dim < (int64_t)(1ll << 40));
+  if (!usable) {
+    lo_t.clear();
+    hi_t.clear();
+    gen_t.clear();
+    for (int q = 0; q < (int)T.size(); q++) gen_t.push_back(q);
+  }
+  std::vector<BitTerm> gen;
+  for (int q : gen_t) gen.push_back(T[q]);
+  P.ngen = (int)gen.size();
+  if (P.ngen) {
+    CK(cudaMalloc(&P.gen, sizeof(BitTerm) * gen.size()));
+    CK(cudaMemcpy(P.gen, gen.data(), sizeof(BitTerm) * gen.size(), cudaMemcpyHostToDevice));
+  }
+  if (!usable) return 0;
+  // coefficient table: index 2i / 2i+1 = +/- coefficient of the i-th tabulated term
+  std::vector<int> tab;
+  for (int q : lo_t) tab.push_back(q);
+  for (int q : hi_t) tab.push_back(q);
+  std::vector<double> coef(4 * tab.size() + 2, 0.0);
+  for (size_t i = 0; i < tab.size(); i++) {
+    coef[4 * i] = T[tab[i]].re;
+    coef[4 * i + 1] = T[tab[i]].im;
+    coef[4 * i + 2] = -T[tab[i]].re;
+    coef[4 * i + 3] = -T[tab[i]].im;
+  }
+  std::vector<uint32_t> l21, l22;
+  if (!s->gc) {
+    l21.resize(s->ihfbit);
+    l22.resize(s->sdim);
+    CK(cudaMemcpy(l21.data(), s->d_list_2_1, sizeof(uint32_t) * s->ihfbit, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(l22.data(), s->d_list_2_2, sizeof(uint32_t) * s->sdim, cudaMemcpyDeviceToHost));
+  }
+  const uint64_t nlo = s->ihfbit, nhi = s->sdim;
+  std::vector<uint32_t> lo_ptr(nlo + 1, 0), lo_ent;
+  for (uint64_t ia = 0; ia < nlo; ia++) {
+    lo_ptr[ia] = (uint32_t)lo_ent.size();
+    if (!s->gc && l21[ia] == 0) continue;
+    for (size_t i = 0; i < lo_t.size(); i++) {
+      const BitTerm &t = T[lo_t[i]];
+      if ((ia & t.cm) != t.cv) continue;
+      const uint64_t src = ia ^ t.flip;
+      const uint64_t val = s->gc ? src : l21[src];
+      if (!s->gc && val == 0) continue;
+      if (val >= (1ull << kSplitTargetBits)) {
+        *err = "split plan: lower-half value out of range";
+        return -1;
+      }
+      const uint32_t k = 2 * (uint32_t)i + (uint32_t)(__builtin_popcountll(ia & t.sm) & 1);
+      lo_ent.push_back((uint32_t)val | (k << kSplitTargetBits));
+    }
+    if (lo_ent.size() > 0xFFFFFFF0ull) { *err = "split plan: too many entries"; return -1; }
+  }
+  lo_ptr[nlo] = (uint32_t)lo_ent.size();
+  std::vector<uint32_t> hi_ptr(nhi + 1, 0);
+  std::vector<HiEnt> hi_ent;
+  for (uint64_t ib = 0; ib < nhi; ib++) {
+    hi_ptr[ib] = (uint32_t)hi_ent.size();
+    if (!s->gc && l22[ib] == 0) continue;
+    const uint64_t cfg = ib << s->lo_bits;
+    for (size_t i = 0; i < hi_t.size(); i++) {
+      const BitTerm &t = T[hi_t[i]];
+      if ((cfg & t.cm) != t.cv) continue;
+      HiEnt h{};
+      if (s->gc) {
+        h.delta = (int64_t)t.flip;
+      } else {
+        const uint64_t src = (cfg ^ t.flip) >> s->lo_bits;
+        if (l22[src] == 0) continue;
+        h.delta = (int64_t)l22[src] - (int64_t)l22[ib];
+      }
+      h.k = 2 * (uint32_t)(lo_t.size() + i) + (uint32_t)(__builtin_popcountll(cfg & t.sm) & 1);
+      hi_ent.push_back(h);
+    }
+    if (hi_ent.size() > 0xFFFFFFF0ull) { *err = "split plan: too many entries"; return -1; }
+  }
+  hi_ptr[nhi] = (uint32_t)hi_ent.size();
+  P.n_lo_ent = (int64_t)lo_ent.size();
+  P.n_hi_ent = (int64_t)hi_ent.size();
+  CK(cudaMalloc(&P.lo_ptr, sizeof(uint32_t) * lo_ptr.size()));
+  CK(cudaMalloc(&P.lo_ent, sizeof(uint32_t) * std::max<size_t>(1, lo_ent.size())));
+  CK(cudaMalloc(&P.hi_ptr, sizeof(uint32_t) * hi_ptr.size()));
+  CK(cudaMalloc(&P.hi_ent, sizeof(HiEnt) * std::max<size_t>(1, hi_ent.size())));
+  CK(cudaMalloc(&P.coef, sizeof(double) * coef.size()));
+  CK(cudaMemcpy(P.lo_ptr, lo_ptr.data(), sizeof(uint32_t) * lo_ptr.size(), cudaMemcpyHostToDevice));
+  if (!lo_ent.empty()) CK(cudaMemcpy(P.lo_ent, lo_ent.data(), sizeof(uint32_t) * lo_ent.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(P.hi_ptr, hi_ptr.data(), sizeof(uint32_t) * hi_ptr.size(), cudaMemcpyHostToDevice));
+  if (!hi_ent.empty()) CK(cudaMemcpy(P.hi_ent, hi_ent.data(), sizeof(HiEnt) * hi_ent.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(P.coef, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice));
+  return 0;
+}
+
 int64_t sector_dim(const Model &m) {
   if (m.is_gc()) return (int64_t)(1ull << m.nbits);
   if (m.calc_model == kHubbard) return (int64_t)(binom_host(m.nsite, m.nup) * binom_host(m.nsite, m.ndown));
@@ -302,6 +411,7 @@ int sector_build(const Model &m, int device, Sector **out, std::string *err, boo
     CK(cudaMalloc(&s->d_dterms, sizeof(DiagTerm) * s->ndterms));
     CK(cudaMemcpyAsync(s->d_dterms, m.diag.data(), sizeof(DiagTerm) * s->ndterms, cudaMemcpyHostToDevice, s->stream));
   }
+  if (split_plan_build(s, err) != 0) return -1;
   CK(cudaMalloc(&s->d_diag, sizeof(double) * (size_t)s->dim));
   diag_kernel<<<nsm * 8, 256, 0, s->stream>>>(s->dim, s->gc ? 1 : 0, s->d_list_1, s->d_dterms, s->ndterms, s->d_diag);
   CK(cudaGetLastError());
@@ -321,6 +431,8 @@ void sector_free(Sector *s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   cudaFree(s->d_list_1); cudaFree(s->d_list_2_1); cudaFree(s->d_list_2_2); cudaFree(s->d_diag);
   cudaFree(s->d_terms); cudaFree(s->d_dterms); cudaFree(s->d_red); cudaFree(s->d_scal);
+  cudaFree(s->split.lo_ptr); cudaFree(s->split.lo_ent); cudaFree(s->split.hi_ptr); cudaFree(s->split.hi_ent);
+  cudaFree(s->split.coef); cudaFree(s->split.gen);
   hub_plan_free(s->hub);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
