@@ -56,6 +56,9 @@ def workload_model(name: str):
         return m, "Hubbard 4x4 periodic, t=1, U=8, Nup=Ndown=8 (dim 165,636,900)"
     if name == "chain16":
         return expert.heisenberg(16, expert.chain_bonds(16)), "Heisenberg chain L=16, Sz=0 (dim 12,870)"
+    if name == "hubbard4x4_6e":
+        m = expert.hubbard(16, expert.square_bonds(4, 4), 1.0, 8.0, 6, 6, lanczos_max=2000)
+        return m, "Hubbard 4x4 periodic, t=1, U=8, Nup=Ndown=6 (dim 64,128,064; profiling case)"
     if name == "hubbard3x4":
         m = expert.hubbard(12, expert.square_bonds(3, 4), 1.0, 8.0, 6, 6)
         return m, "Hubbard 3x4 periodic, t=1, U=8, half filling (dim 853,776)"
@@ -153,7 +156,8 @@ def run_reference_arm(args):
     if rank != 0:
         return
     model, desc = workload_model(args.workload)
-    dim = {"hubbard4x4": 165636900, "chain16": 12870, "hubbard3x4": 853776}[args.workload]
+    dim = {"hubbard4x4": 165636900, "chain16": 12870, "hubbard3x4": 853776,
+           "hubbard4x4_6e": 64128064}[args.workload]
     threads = os.cpu_count()
     times, note = reference_mltply_times(model, args.warmup + args.steps, threads)
     if times is None:
@@ -382,7 +386,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="hubbard4x4")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=3, help="0 skips the end-to-end leg")
+    ap.add_argument("--no-hphi-order", action="store_true", help="skip the HPhi-order device leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -420,6 +425,10 @@ def main():
         pass
     dim = H.dim
     H_native = bool(H.info.get("native_order"))
+    kind = H.info.get("kernel", 0)
+    kname, kdesc = {2: ("prod_hv_kernel", "prod_hv_kernel<double> + finalize_partials_kernel<2> per step"),
+                    1: ("hv_hub_pass", "hv_hub_pass<double,0> + hv_hub_pass<double,1> + finalize per step")}.get(
+        kind, ("hv_general", "hv_general_kernel + finalize per step"))
     vt = hphi_b200.REAL64
     gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
     v1 = torch.rand(dim, dtype=torch.float64, device="cuda", generator=gen) - 0.5
@@ -461,7 +470,7 @@ def main():
 
     # ---- the same H*v on HPhi-ordered device vectors (permutations to / from the native order included)
     hphi_order_ms = None
-    if H.info.get("native_order"):
+    if H.info.get("native_order") and not args.no_hphi_order:
         H.mltply_device(v0.data_ptr(), v1.data_ptr(), vt)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -471,6 +480,16 @@ def main():
 
     # ---- e2e through the reference-facing host mltply (complex128, pinned host buffers)
     e2e = None
+    if args.e2e_steps > 0:
+        e2e = run_e2e(H, v1, dim, world, dist, args)
+    H.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    finish(args, H_native, kind, kname, kdesc, desc, dim, balg, value, t_max, achieved, hphi_order_ms, e2e, clocks,
+           world, rank, dist)
+
+
+def run_e2e(H, v1, dim, world, dist, args):
+    import torch
     hv0 = torch.zeros(2 * (dim + 1), dtype=torch.float64).pin_memory()
     hv1 = torch.zeros(2 * (dim + 1), dtype=torch.float64).pin_memory()
     hv1[2::2] = v1.cpu()
@@ -485,13 +504,14 @@ def main():
         tt = torch.tensor([te], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         te = float(tt.item())
-    e2e = {"value": world * 3.0 * dim * 16 / te / 1e9, "unit": "GB/s",
-           "h2d_bytes_per_step": 2 * 16 * (dim + 1), "d2h_bytes_per_step": 16 * (dim + 1),
-           "steps": args.e2e_steps, "vector": "complex128 HPhi layout (dim+1), pinned host memory",
-           "ms_per_step": te * 1e3}
-    H.close()
-    shutil.rmtree(tmp, ignore_errors=True)
+    return {"value": world * 3.0 * dim * 16 / te / 1e9, "unit": "GB/s",
+            "h2d_bytes_per_step": 2 * 16 * (dim + 1), "d2h_bytes_per_step": 16 * (dim + 1),
+            "steps": args.e2e_steps, "vector": "complex128 HPhi layout (dim+1), pinned host memory",
+            "ms_per_step": te * 1e3}
 
+
+def finish(args, H_native, kind, kname, kdesc, desc, dim, balg, value, t_max, achieved, hphi_order_ms, e2e, clocks,
+           world, rank, dist):
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -515,14 +535,14 @@ def main():
                       "step": "one v0 += H v1 (mltply)", "b_alg_bytes": balg,
                       "l2": "inputs larger than L2 (1.3 GB vectors), no flush",
                       "parallelism": "replicas" if world > 1 else "single",
-                      "vector_order": "native (per-block up x down product order)" if H_native else "HPhi",
+                      "vector_order": {2: "native (up-rank x down-rank product matrix)",
+                                       1: "native (per-block up x down product order)"}.get(kind, "HPhi"),
                       "hphi_order_ms_per_step": hphi_order_ms},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak, "peak_kind": peak_kind,
-                        "traffic": profile_traffic("hv_hub_pass" if H_native else "hv_general", args.workload),
-                        "kernels": "hv_hub_pass<double,0> + hv_hub_pass<double,1> per step" if H_native
-                        else "hv_general_kernel per step"},
-           "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 2 * args.steps, "clocks": clocks}
+                        "traffic": profile_traffic(kname, args.workload),
+                        "kernels": kdesc},
+           "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": (2 if kind == 2 else 3) * args.steps, "clocks": clocks}
     print(json.dumps(out))
     if dist:
         dist.destroy_process_group()

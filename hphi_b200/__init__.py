@@ -34,7 +34,7 @@ REAL64 = 0
 COMPLEX128 = 1
 _HERE = os.path.dirname(os.path.abspath(__file__))
 INFO_FIELDS = ["dim", "nsite", "calc_model", "calc_type", "size_list_2_1", "size_list_2_2", "is_gc",
-               "vec_type", "n_offdiag", "n_diag", "lanczos_max", "num_ave", "native_order", "exct"]
+               "vec_type", "n_offdiag", "n_diag", "lanczos_max", "num_ave", "native_order", "exct", "kernel"]
 EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi_close", "hphi_info",
                     "hphi_sz", "hphi_diagonalcalc", "hphi_mltply", "hphi_mltply_device", "hphi_lanczos",
                     "hphi_lanczos_eigenvector", "hphi_tpq", "hphi_run", "hphi_inspect_terms",

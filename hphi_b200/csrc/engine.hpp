@@ -17,6 +17,7 @@
 namespace hphi {
 
 struct HubPlan;
+struct ProdPlan;
 
 // Real or complex double scalar for host/device code.
 struct cplx { double x, y; };
@@ -70,6 +71,8 @@ struct Sector {
   // Optional specialised plan (canonical Hubbard).  When present, the drivers keep
   // vectors in the plan's native order; see hv_native / to_native.
   HubPlan *hub = nullptr;
+  // Product-layout plan (canonical Hubbard); preferred over the block plan when both apply.
+  ProdPlan *prod = nullptr;
   SplitPlan split;
 };
 

@@ -16,6 +16,7 @@
 #include "device_util.cuh"
 #include "engine.hpp"
 #include "hv_hubbard.hpp"
+#include "hv_product.hpp"
 #include "split.cuh"
 
 namespace hphi {
@@ -153,25 +154,29 @@ int hv_launch_scratch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const
 }
 
 size_t hv_scratch_doubles(const Sector *s) {
+  if (s->prod) return prod_scratch_doubles(s);
   if (s->hub) return hub_scratch_doubles(s);
   return 2 * (size_t)s->red_blocks;
 }
 
 int hv_native_scratch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out,
                       double *d_part, int *d_counter) {
+  if (s->prod) return prod_hv_launch_scratch(s, vt, d_v1, d_v0, d_coef, d_out, d_part, d_counter);
   if (s->hub) return hub_hv_launch_scratch(s, vt, d_v1, d_v0, d_coef, d_out, d_part, d_counter);
   return hv_launch_scratch(s, vt, d_v1, d_v0, d_coef, d_out, d_part);
 }
 
-bool has_native_order(const Sector *s) { return s->hub != nullptr; }
+bool has_native_order(const Sector *s) { return s->hub != nullptr || s->prod != nullptr; }
 
 int hv_native(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out,
               bool acc_read) {
+  if (s->prod) return prod_hv_launch(s, vt, d_v1, d_v0, d_coef, d_out);
   if (s->hub) return hub_hv_launch(s, vt, d_v1, d_v0, d_coef, d_out, acc_read);
   return hv_launch(s, vt, d_v1, d_v0, d_coef, d_out);
 }
 
 int to_native(Sector *s, VecType vt, const void *in, void *out) {
+  if (s->prod) return prod_permute(s, vt, in, out, true);
   if (s->hub) return hub_permute(s, vt, in, out, true);
   const size_t esz = (vt == kReal64) ? sizeof(double) : sizeof(cplx);
   if (in != out && cudaMemcpyAsync(out, in, esz * (size_t)s->dim, cudaMemcpyDeviceToDevice, s->stream) != cudaSuccess) {
@@ -182,6 +187,7 @@ int to_native(Sector *s, VecType vt, const void *in, void *out) {
 }
 
 int from_native(Sector *s, VecType vt, const void *in, void *out) {
+  if (s->prod) return prod_permute(s, vt, in, out, false);
   if (s->hub) return hub_permute(s, vt, in, out, false);
   const size_t esz = (vt == kReal64) ? sizeof(double) : sizeof(cplx);
   if (in != out && cudaMemcpyAsync(out, in, esz * (size_t)s->dim, cudaMemcpyDeviceToDevice, s->stream) != cudaSuccess) {
@@ -192,6 +198,7 @@ int from_native(Sector *s, VecType vt, const void *in, void *out) {
 }
 
 int native_observables(Sector *s, VecType vt, const void *v, double *d_out) {
+  if (s->prod) return prod_observables(s, vt, v, d_out);
   if (s->hub) return hub_observables(s, vt, v, d_out);
   return vec_diag_observables(s, vt, v, d_out);
 }

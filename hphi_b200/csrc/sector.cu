@@ -20,6 +20,7 @@
 
 #include "engine.hpp"
 #include "hv_hubbard.hpp"
+#include "hv_product.hpp"
 #include "split.cuh"
 
 namespace hphi {
@@ -418,7 +419,13 @@ int sector_build(const Model &m, int device, Sector **out, std::string *err, boo
   CK(cudaStreamSynchronize(s->stream));
   // Specialised kernels (HPHI_B200_KERNEL=general keeps the general kernel).
   const char *kern = getenv("HPHI_B200_KERNEL");
-  if (specialise && !(kern && std::string(kern) == "general")) {
+  // HPHI_B200_KERNEL=general keeps the general kernel, =block the block plan; by default the
+  // product-layout plan is used where it applies, else the block plan.
+  const std::string kname = kern ? kern : "";
+  if (specialise && kname != "general" && kname != "block") {
+    if (prod_plan_build(s, err) != 0) return -1;
+  }
+  if (specialise && kname != "general" && !s->prod) {
     if (hub_plan_build(s, err) != 0) return -1;
   }
   *out = s;
@@ -434,6 +441,7 @@ void sector_free(Sector *s) {
   cudaFree(s->split.lo_ptr); cudaFree(s->split.lo_ent); cudaFree(s->split.hi_ptr); cudaFree(s->split.hi_ent);
   cudaFree(s->split.coef); cudaFree(s->split.gen);
   hub_plan_free(s->hub);
+  prod_plan_free(s->prod);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }

@@ -13,10 +13,13 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 
-def _open(path, general=False):
+def _open(path, general=False, kernel=None):
+    """kernel: None (default plan: product layout where it applies), "block" or "general"."""
     old = os.environ.get("HPHI_B200_KERNEL")
     if general:
-        os.environ["HPHI_B200_KERNEL"] = "general"
+        kernel = "general"
+    if kernel:
+        os.environ["HPHI_B200_KERNEL"] = kernel
     else:
         os.environ.pop("HPHI_B200_KERNEL", None)
     try:
@@ -59,10 +62,13 @@ def _with_inter():
     return m
 
 
+@pytest.mark.parametrize("kernel", [None, "block"])
 @pytest.mark.parametrize("name", list(MODELS))
-def test_block_kernel_matches_general_kernel(name, tmp_path):
+def test_block_kernel_matches_general_kernel(name, kernel, tmp_path):
+    """Native-order kernels (product layout by default, the block plan on request) against
+    the general kernel."""
     path = MODELS[name]().write(str(tmp_path))
-    Hf = _open(path)
+    Hf = _open(path, kernel=kernel)
     Hg = _open(path, general=True)
     try:
         assert Hf.info["native_order"] == 1, "block kernel should apply to this input"
@@ -108,6 +114,25 @@ def test_block_kernel_lanczos_energy(tmp_path):
     assert rf["converged"] and rg["converged"]
     assert abs(rf["e1"] - rg["e1"]) < 1e-10
     assert abs(rf["e1"] - (-5.8334842575)) < 1e-9   # reference HPhi, 3x4 U=8 half filling
+
+
+def test_product_and_block_plans_agree_full_size_4x4(tmp_path):
+    """Half-filled 4x4 Hubbard: product-layout and block plans give the same H*v (1e-12)
+    after conversion to HPhi order, and the same <v|H|v>."""
+    path = expert.hubbard(16, expert.square_bonds(4, 4), 1.0, 8.0, 8, 8).write(str(tmp_path))
+    g = torch.Generator(device="cuda").manual_seed(21)
+    out = []
+    for kernel in (None, "block"):
+        H = _open(path, kernel=kernel)
+        if not out:
+            v = torch.rand(H.dim, dtype=torch.float64, device="cuda", generator=g) - 0.5
+            zero = torch.zeros_like(v)
+        y, pr = _hv_device(H, v, zero, hphi_b200.REAL64, acc=0.0)
+        out.append((y, pr))
+        H.close()
+    err = (out[0][0] - out[1][0]).abs().max().item() / out[1][0].abs().max().item()
+    assert err < 1e-12
+    assert abs(out[0][1] - out[1][1]) < 1e-11 * abs(out[1][1])
 
 
 def test_full_size_hubbard4x4_block_vs_general(tmp_path):
