@@ -54,6 +54,8 @@ struct ProdArgs {
   const uint32_t *ell_dn;      // [wd][Dc]: source rank | coefficient index << 16
   const uint32_t *ell_up;      // [Uc][wu]
   const uint8_t *cnt_dn;       // [Dc] valid entries of each ELL column
+  const uint8_t *wmax_dn;      // [ceil(Dc / 32)] largest count in each aligned block of 32 columns
+  const double *utab;          // [17] u0 * k for k = 0..16 (cross_mode 0)
   const double2 *cf_dn, *cf_up;
   const double *du, *dd;       // diagonal terms of one species, by rank
   const double *usite;         // on-site U per site (cross_mode 1)
@@ -127,65 +129,73 @@ __global__ void __launch_bounds__(kProdThreads, 2) prod_hv_kernel(ProdArgs a, co
     const double du = a.du[ua];
     double pr[2] = {0.0, 0.0};
     T *dst = v0 + (int64_t)ua * Dc;
-    constexpr int kU = (sizeof(T) == 8) ? 8 : 4;  // up-hop loads in flight per thread
-    // Every lane of a warp runs the same iterations (blockDim.x is a multiple of 32) and the
-    // hop loops have warp-uniform trip counts, so the warp never splits.
-    for (int base = 0; base < Dc; base += blockDim.x) {
-      const int da0 = base + threadIdx.x;
-      const bool ok = da0 < Dc;
-      const int da = ok ? da0 : Dc - 1;
-      // first block of up-hop source loads goes out before the in-row work
-      T up[kU];
+    constexpr int CPT = 2;  // columns per thread per iteration
+    for (int base = 0; base < Dc; base += CPT * (int)blockDim.x) {
+      int da[CPT];
+      bool ok[CPT];
+      T y[CPT], x[CPT];
+      int cnt[CPT], wmax = 0;
 #pragma unroll
-      for (int k = 0; k < kU; k++)
-        up[k] = (k < nu) ? ldg_v<T>(v1 + (int64_t)s_src[k] * Dc + da) : VT<T>::zero();
-      const T x = row[da];
-      double D;
-      if (a.cross_mode == 2) {
-        D = __ldg(a.dfull + (int64_t)ua * Dc + da);
-      } else {
-        D = du + __ldg(a.dd + da);
-        const uint32_t ud = u & (uint32_t)__ldg(a.unrank_dn + da);
-        if (a.cross_mode == 0) {
-          D += a.u0 * (double)__popc(ud);
+      for (int c = 0; c < CPT; c++) {
+        const int d0 = base + c * (int)blockDim.x + (int)threadIdx.x;
+        ok[c] = d0 < Dc;
+        da[c] = ok[c] ? d0 : Dc - 1;
+        x[c] = row[da[c]];
+        double D;
+        if (a.cross_mode == 2) {
+          D = __ldg(a.dfull + (int64_t)ua * Dc + da[c]);
         } else {
-          for (uint32_t m = ud; m; m &= m - 1) D += __ldg(a.usite + (__ffs(m) - 1));
+          D = du + __ldg(a.dd + da[c]);
+          const uint32_t ud = u & (uint32_t)__ldg(a.unrank_dn + da[c]);
+          if (a.cross_mode == 0) D += __ldg(a.utab + __popc(ud));
+          else for (uint32_t m = ud; m; m &= m - 1) D += __ldg(a.usite + (__ffs(m) - 1));
         }
+        y[c] = VT<T>::scale(D, x[c]);
+        cnt[c] = __ldg(a.cnt_dn + da[c]);
+        // a warp's columns are the aligned block [base + c*blockDim + 32w, ... + 32)
+        wmax = max(wmax, (int)__ldg(a.wmax_dn + ((base + c * (int)blockDim.x + (int)(threadIdx.x & ~31u)) >> 5)));
       }
-      T y = VT<T>::scale(D, x);
-      // down hops: gathers inside the staged row, 4 ELL entries in flight, up to the
-      // warp's largest count
-      const int cnt = __ldg(a.cnt_dn + da);
-      const int wmax = __reduce_max_sync(0xffffffffu, cnt);
       for (int s = 0; s < wmax; s += 4) {
-        uint32_t e[4];
+        uint32_t e[CPT][4];
 #pragma unroll
-        for (int k = 0; k < 4; k++) e[k] = (s + k < cnt) ? __ldg(a.ell_dn + (int64_t)(s + k) * Dc + da) : kEllNone;
+        for (int c = 0; c < CPT; c++)
 #pragma unroll
-        for (int k = 0; k < 4; k++)
-          if (e[k] != kEllNone) {
-            const double2 c = __ldg(a.cf_dn + (e[k] >> 16));
-            y = VT<T>::add(y, VT<T>::cmul_re_im(c.x, c.y, row[e[k] & 0xFFFFu]));
+          for (int k = 0; k < 4; k++)
+            e[c][k] = (s + k < cnt[c]) ? __ldg(a.ell_dn + (int64_t)(s + k) * Dc + da[c]) : kEllNone;
+#pragma unroll
+        for (int c = 0; c < CPT; c++)
+#pragma unroll
+          for (int k = 0; k < 4; k++)
+            if (e[c][k] != kEllNone) {
+              const double2 cf = __ldg(a.cf_dn + (e[c][k] >> 16));
+              y[c] = VT<T>::add(y[c], VT<T>::cmul_re_im(cf.x, cf.y, row[e[c][k] & 0xFFFFu]));
+            }
+      }
+      constexpr int kS = (sizeof(T) > 8) ? 2 : 4;  // up hops per batch (registers: complex holds twice as much)
+      for (int s = 0; s < nu; s += kS) {
+        T v[kS][CPT];
+#pragma unroll
+        for (int k = 0; k < kS; k++) {
+          const T *p = v1 + (int64_t)s_src[(s + k < nu) ? s + k : s] * Dc;
+#pragma unroll
+          for (int c = 0; c < CPT; c++) v[k][c] = (s + k < nu) ? ldg_v<T>(p + da[c]) : VT<T>::zero();
+        }
+#pragma unroll
+        for (int k = 0; k < kS; k++)
+          if (s + k < nu) {
+            const double2 cf = s_cf[s + k];
+#pragma unroll
+            for (int c = 0; c < CPT; c++) y[c] = VT<T>::add(y[c], VT<T>::cmul_re_im(cf.x, cf.y, v[k][c]));
           }
       }
-      // up hops: whole source rows, kU loads in flight
 #pragma unroll
-      for (int k = 0; k < kU; k++)
-        if (k < nu) y = VT<T>::add(y, VT<T>::cmul_re_im(s_cf[k].x, s_cf[k].y, up[k]));
-      for (int s = kU; s < nu; s += kU) {
-#pragma unroll
-        for (int k = 0; k < kU; k++)
-          up[k] = (s + k < nu) ? ldg_v<T>(v1 + (int64_t)s_src[s + k] * Dc + da) : VT<T>::zero();
-#pragma unroll
-        for (int k = 0; k < kU; k++)
-          if (s + k < nu) y = VT<T>::add(y, VT<T>::cmul_re_im(s_cf[s + k].x, s_cf[s + k].y, up[k]));
-      }
-      if (ok) {
-        pr[0] += VT<T>::conj_mul_re(x, y);
-        pr[1] += VT<T>::conj_mul_im(x, y);
-        y = VT<T>::scale(scale, y);
-        dst[da] = (acc == 0.0) ? y : VT<T>::add(VT<T>::scale(acc, dst[da]), y);
-      }
+      for (int c = 0; c < CPT; c++)
+        if (ok[c]) {
+          pr[0] += VT<T>::conj_mul_re(x[c], y[c]);
+          pr[1] += VT<T>::conj_mul_im(x[c], y[c]);
+          const T yy = VT<T>::scale(scale, y[c]);
+          dst[da[c]] = (acc == 0.0) ? yy : VT<T>::add(VT<T>::scale(acc, dst[da[c]]), yy);
+        }
     }
     block_sum<2>(pr);
     if (threadIdx.x == 0) {
@@ -376,10 +386,11 @@ int prod_plan_build(Sector *s, std::string *err) {
   build_ell(hops[0], unrank_up, rank, &rows_up, &wu);
   if (wu > kMaxUpWidth || wd > 255) return 0;
   std::vector<uint32_t> ell_dn((size_t)std::max(wd, 1) * Dc, kEllNone), ell_up((size_t)Uc * std::max(wu, 1), kEllNone);
-  std::vector<uint8_t> cnt_dn(Dc);
+  std::vector<uint8_t> cnt_dn(Dc), wmax_dn((Dc + 31) / 32, 0);
   for (int r = 0; r < Dc; r++) {
     for (size_t k = 0; k < rows_dn[r].size(); k++) ell_dn[k * (size_t)Dc + r] = rows_dn[r][k];
     cnt_dn[r] = (uint8_t)rows_dn[r].size();
+    wmax_dn[r >> 5] = std::max<uint8_t>(wmax_dn[r >> 5], cnt_dn[r]);
   }
   for (int r = 0; r < Uc; r++)
     for (size_t k = 0; k < rows_up[r].size(); k++) ell_up[(size_t)r * std::max(wu, 1) + k] = rows_up[r][k];
@@ -451,12 +462,15 @@ int prod_plan_build(Sector *s, std::string *err) {
   for (int i = 1; i < N; i++) uniform = uniform && (usite[i] == usite[0]);
   a.cross_mode = general_cross ? 2 : (uniform ? 0 : 1);
   a.u0 = usite[0];
+  std::vector<double> utab(17);
+  for (int k = 0; k <= 16; k++) utab[k] = a.u0 * (double)k;
   auto fail = [&]() { prod_plan_free(p); return -1; };
   if (upload(p, rank, &a.rank, err) || upload(p, unrank_up, &a.unrank_up, err) ||
       upload(p, unrank_dn, &a.unrank_dn, err) || upload(p, ell_dn, &a.ell_dn, err) ||
       upload(p, ell_up, &a.ell_up, err) || upload(p, coef_table(hops[1]), &a.cf_dn, err) ||
       upload(p, coef_table(hops[0]), &a.cf_up, err) || upload(p, du, &a.du, err) || upload(p, dd, &a.dd, err) ||
-      upload(p, usite, &a.usite, err) || upload(p, order, &a.order, err) || upload(p, cnt_dn, &a.cnt_dn, err))
+      upload(p, usite, &a.usite, err) || upload(p, order, &a.order, err) || upload(p, cnt_dn, &a.cnt_dn, err) ||
+      upload(p, wmax_dn, &a.wmax_dn, err) || upload(p, utab, &a.utab, err))
     return fail();
   if (a.cross_mode == 2) {
     void *q = nullptr;
