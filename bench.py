@@ -198,46 +198,77 @@ def j1j2_batch_models(n: int, seed: int = 2024):
     return [(int(L), float(j2), expert.j1j2_chain(int(L), 1.0, float(j2))) for L, j2 in zip(Ls, J2)]
 
 
+def _dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world == 1:
+        return None, 0, 1
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return dist, dist.get_rank(), world
+
+
 def run_batch_mode(args):
-    """Batched Lanczos (256 J1-J2 chains, 300 steps) vs the plain FP64 driver."""
+    """Batched Lanczos (256 J1-J2 chains, 300 steps) vs the plain FP64 driver.  Under
+    torchrun the instances are split across ranks (hphi_b200.shard: no exchange during the
+    solves), the time is the max over ranks and the energies are gathered."""
     import hphi_b200
+    from hphi_b200 import expert, shard
+    dist, rank, world = _dist_init()
     n, steps, seed = args.batch_size, args.batch_steps, 7
+    models = j1j2_batch_models(n)
+    dims_all = [expert.sector_dim_estimate(m) for _, _, m in models]
+    mine = shard.partition(dims_all, world)[rank]
     tmp = tempfile.mkdtemp()
     hams = []
-    for i, (L, j2, m) in enumerate(j1j2_batch_models(n)):
+    for i in mine:
+        m = models[i][2]
         d = os.path.join(tmp, f"i{i}")
         os.makedirs(d)
         m.initial_vec_type = 1
         hams.append(hphi_b200.Hamiltonian(m.write(d)))
-    dims = [h.dim for h in hams]
+    dims = dims_all
     res = {}
     clocks = _clock_start()
     for prec, name in ((hphi_b200.FP64, "fp64"), (hphi_b200.FP32, "fp32")):
         with hphi_b200.Batch(hams, prec) as b:
             tune = b.tuning()
             b.lanczos(steps, seed=seed, refine=(prec == hphi_b200.FP32))   # warm-up (graphs, allocations)
+            if dist:
+                dist.barrier()
             t0 = time.perf_counter()
             r = b.lanczos(steps, seed=seed, refine=(prec == hphi_b200.FP32))
-            wall = time.perf_counter() - t0
+            wall = shard.max_over_ranks(time.perf_counter() - t0, dist)
+        cols = np.stack([r["e_lanczos"], r["e_refined"]], axis=1)
+        full = shard.gather(cols, mine, n, dist)
+        r = dict(r, e_lanczos=full[:, 0], e_refined=full[:, 1])
         res[name] = dict(r=r, wall=wall, tune=tune)
     # plain FP64 GPU path: each instance alone through the Lanczos driver, same start vector
-    nplain = min(n, args.plain_sample)
+    # (rank 0's instances; instance j of a batch starts from seed + 1000003 * j)
+    nplain = min(len(hams), args.plain_sample)
     e_plain = []
-    hams[0].lanczos_steps(steps, seed=seed, nev=1)  # warm-up
-    t0 = time.perf_counter()
-    for i in range(nplain):
-        e_plain.append(hams[i].lanczos_steps(steps, seed=seed + 1000003 * i, nev=1)[0])
-    t_plain = time.perf_counter() - t0
+    if rank == 0:
+        hams[0].lanczos_steps(steps, seed=seed, nev=1)  # warm-up
+        t0 = time.perf_counter()
+        for j in range(nplain):
+            e_plain.append(hams[j].lanczos_steps(steps, seed=seed + 1000003 * j, nev=1)[0])
+        t_plain = time.perf_counter() - t0
     cl = clocks.stop()
     for h in hams:
         h.close()
     shutil.rmtree(tmp, ignore_errors=True)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
     e64 = res["fp64"]["r"]["e_lanczos"]
     e32 = res["fp32"]["r"]["e_refined"]
+    plain_idx = mine[:nplain]
     plain_rate = nplain / t_plain
     rate64 = n / res["fp64"]["wall"]
     rate32 = n / res["fp32"]["wall"]
-    out = {"metric": METRIC, "mode": "batch", "value": rate32, "unit": "solves/s", "n_gpus": 1,
+    out = {"metric": METRIC, "mode": "batch", "value": rate32, "unit": "solves/s", "n_gpus": world,
+           "scaling": "strong" if world > 1 else None,
            "higher_is_better": True, "dtype": "f32 storage, f64 sums/scalars/refinement", "data": "synthetic",
            "config": {"workload": f"{n} J1-J2 chains, L in {{18,20,22,24}}, J2 in [0,1], {steps} Lanczos steps",
                       "sum_dim": int(sum(dims)), "min_dim": int(min(dims)), "max_dim": int(max(dims)),
@@ -247,11 +278,13 @@ def run_batch_mode(args):
            "speedup_fp32_vs_plain": rate32 / plain_rate, "speedup_fp64_batched_vs_plain": rate64 / plain_rate,
            "max_abs_dE_fp32_refined_vs_fp64": float(np.max(np.abs(e32 - e64))),
            "max_abs_dE_fp32_unrefined_vs_fp64": float(np.max(np.abs(res["fp32"]["r"]["e_lanczos"] - e64))),
-           "max_abs_dE_batched_fp64_vs_plain": float(np.max(np.abs(np.array(e_plain) - e64[:nplain]))),
+           "max_abs_dE_batched_fp64_vs_plain": float(np.max(np.abs(np.array(e_plain) - e64[plain_idx]))),
            "fp32_phase_ms": {"forward": res["fp32"]["r"]["forward_ms"], "replay": res["fp32"]["r"]["replay_ms"],
                              "refine": res["fp32"]["r"]["refine_ms"]},
            "fp64_forward_ms": res["fp64"]["r"]["forward_ms"], "clocks": cl}
     print(json.dumps(out))
+    if dist:
+        dist.destroy_process_group()
 
 
 def run_precision_mode(args):
@@ -395,7 +428,7 @@ def main():
         run_reference_arm(args)
         return
     if args.mode != "hv":
-        if int(os.environ.get("RANK", "0")) != 0:
+        if args.mode != "batch" and int(os.environ.get("RANK", "0")) != 0:
             return
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))

@@ -247,3 +247,20 @@ def random_interall_spin(nsite: int, nterms: int, seed: int) -> List[Tuple]:
             out.append((i, s1, i, s2, k, s3, k, s4, v.real, v.imag))
             out.append((k, s4, k, s3, i, s2, i, s1, v.real, -v.imag))
     return out
+
+
+def sector_dim_estimate(m: ExpertModel) -> int:
+    """Dimension of the model's sector (idim_max) without building it."""
+    from math import comb
+    if m.model.endswith("GC"):
+        return 2 ** (m.nsite if m.model == "SpinGC" else 2 * m.nsite)
+    if m.model == "Spin":
+        nup = (m.nsite + (m.two_sz or 0)) // 2
+        return comb(m.nsite, nup)
+    if m.nup is not None and m.ndown is not None:
+        return comb(m.nsite, m.nup) * comb(m.nsite, m.ndown)
+    ne = m.ncond
+    if m.two_sz is None:
+        return comb(2 * m.nsite, ne)
+    nup = (ne + m.two_sz) // 2
+    return comb(m.nsite, nup) * comb(m.nsite, ne - nup)
