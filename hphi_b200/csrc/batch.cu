@@ -1000,7 +1000,7 @@ namespace {
 // Device bytes a request holds while active: lists, diagonal, tables, vectors, scalars.
 int64_t footprint_of(const Model &m, int64_t dim, Precision prec) {
   const bool cplx = m.complex_terms || m.initial_vec_type != 1;
-  const int64_t lists = m.is_gc() ? 0 : 8 * dim + 4 * ((1ll << ((m.nbits + 1) / 2)) + (1ll << (m.nbits / 2)));
+  const int64_t lists = m.rows_are_configs() ? 0 : 8 * dim + 4 * ((1ll << ((m.nbits + 1) / 2)) + (1ll << (m.nbits / 2)));
   const int64_t vecs = 3 * (int64_t)storage_elem(prec, cplx) * dim + (prec == kFP32 ? 2 * (cplx ? 16 : 8) * dim : 0);
   return lists + 8 * dim + vecs + (int64_t)sizeof(BitTerm) * (int64_t)m.offdiag.size() + (1 << 20);
 }

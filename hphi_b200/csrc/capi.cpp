@@ -131,7 +131,7 @@ int hphi_info(const hphi_handle *h, int64_t *info, int n) {
   v[HPHI_INFO_CALC_TYPE] = s.model.calc_type;
   v[HPHI_INFO_SIZE_LIST_2_1] = s.size_list_2_1;
   v[HPHI_INFO_SIZE_LIST_2_2] = s.size_list_2_2;
-  v[HPHI_INFO_IS_GC] = s.gc ? 1 : 0;
+  v[HPHI_INFO_IS_GC] = s.model.is_gc() ? 1 : 0;
   v[HPHI_INFO_VEC_TYPE] = default_vec_type(s);
   v[HPHI_INFO_N_OFFDIAG] = s.nterms;
   v[HPHI_INFO_N_DIAG] = s.ndterms;

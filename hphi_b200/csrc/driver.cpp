@@ -167,7 +167,7 @@ VecType default_vec_type(const Sector &s) {
 // 1-based complex128 layout.  Returns false when the reference would use a random vector.
 bool single_element_start(const Sector &s, std::vector<double> *v) {
   const Model &m = s.model;
-  if (s.gc || m.initial_iv <= 0) return false;
+  if (m.is_gc() || m.initial_iv <= 0) return false;
   const uint64_t dim = (uint64_t)s.dim;
   const uint64_t iv = (dim / 2 + (uint64_t)m.initial_iv) % dim + 1;
   v->assign(2 * (dim + 1), 0.0);

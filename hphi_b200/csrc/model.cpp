@@ -382,8 +382,14 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
   if (m->lanczos_target < m->k_exct) m->lanczos_target = m->k_exct;
   if (m->k_exct < 1 || m->k_exct > m->nvec) { *err = "modpara.def: exct out of range"; return -1; }
   if (m->calc_model == kKondo || m->calc_model == kKondoGC) {
-    *err = "Kondo models are not supported by this engine yet";
-    return -1;
+    // Local spins are S = 1/2 sites held singly occupied by the sector (src/sz.c:1110-1220,
+    // 1342-1420).  An odd number of sites splits one site across the two halves of the
+    // configuration; the engine supports even Nsite.
+    if (m->nsite % 2 != 0) { *err = "Kondo models with an odd number of sites are not supported by this engine"; return -1; }
+    for (int i = 0; i < m->nsite; i++)
+      if (m->locspn[i] != 0 && m->locspn[i] != 1) {
+        *err = "locspn.def: Kondo local spins must be S=1/2 (2S=1)"; return -1;
+      }
   }
   const bool spin = m->is_spin();
   m->nbits = spin ? m->nsite : 2 * m->nsite;
@@ -409,6 +415,9 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       }
       if (m->calc_model == kSpin && i != j) { *err = files["trans"] + ": Spin needs site-diagonal transfers"; return -1; }
       if (m->calc_model == kSpinGC && i != j) { *err = files["trans"] + ": SpinGC needs site-diagonal transfers"; return -1; }
+      if ((m->calc_model == kKondo || m->calc_model == kKondoGC) && i != j && (m->locspn[i] != 0 || m->locspn[j] != 0)) {
+        *err = files["trans"] + ": Kondo transfers touching a local spin must be site-diagonal"; return -1;
+      }
       auto key = std::make_tuple(i, s1, j, s2);
       if (!tr.count(key)) order.push_back(key);
       tr[key] += std::complex<double>(r[4], r[5]);
@@ -547,6 +556,12 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       for (int q = 0; q < 4; q++)
         if (!check_site(s[q]) || g[q] < 0 || g[q] > 1) { *err = files["interall"] + ": bad index"; return -1; }
       const std::complex<double> V(r[8], r[9]);
+      if (m->calc_model == kKondo || m->calc_model == kKondoGC) {  // CheckFormatForKondoInt (src/readdef.c:2665-2684)
+        if (((m->locspn[s[0]] != 0 || m->locspn[s[1]] != 0) && s[0] != s[1]) ||
+            ((m->locspn[s[2]] != 0 || m->locspn[s[3]] != 0) && s[2] != s[3])) {
+          *err = files["interall"] + ": Kondo InterAll on a local spin must pair operators of the same site"; return -1;
+        }
+      }
       if (spin) {
         if (s[0] != s[1] || s[2] != s[3]) {
           *err = files["interall"] + ": spin InterAll needs i==j and k==l"; return -1;

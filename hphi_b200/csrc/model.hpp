@@ -70,6 +70,10 @@ struct Model {
     return calc_model == kHubbardGC || calc_model == kSpinGC || calc_model == kKondoGC;
   }
   bool is_spin() const { return calc_model == kSpin || calc_model == kSpinGC; }
+  // Grand-canonical models whose basis is every configuration (row index == configuration);
+  // KondoGC keeps lists because its local spins must stay singly occupied.
+  bool rows_are_configs() const { return calc_model == kHubbardGC || calc_model == kSpinGC; }
+  bool is_kondo() const { return calc_model == kKondo || calc_model == kKondoGC; }
 };
 
 // Reads namelist.def and every file it names (expert mode).  Returns 0 on success,

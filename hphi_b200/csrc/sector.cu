@@ -286,6 +286,17 @@ static int split_plan_build(Sector *s, std::string *err) {
 }
 
 int64_t sector_dim(const Model &m) {
+  if (m.calc_model == kKondoGC) {  // 4^Ncond * 2^NLocSpn (src/check.c:160-168)
+    const int nloc = m.nlocspn, ncond = m.nsite - m.nlocspn;
+    return (int64_t)1 << (2 * ncond + nloc);
+  }
+  if (m.calc_model == kKondo) {  // src/check.c:134-158
+    const int nloc = m.nlocspn, ncond = m.nsite - m.nlocspn;
+    uint64_t sum = 0;
+    for (int ul = 0; ul <= m.nup; ul++)
+      sum += binom_host(nloc, ul) * binom_host(ncond, m.nup - ul) * binom_host(ncond, m.ndown + ul - nloc);
+    return (int64_t)sum;
+  }
   if (m.is_gc()) return (int64_t)(1ull << m.nbits);
   if (m.calc_model == kHubbard) return (int64_t)(binom_host(m.nsite, m.nup) * binom_host(m.nsite, m.ndown));
   if (m.calc_model == kHubbardNConserved) return (int64_t)binom_host(2 * m.nsite, m.ne);
@@ -306,7 +317,7 @@ int sector_build(const Model &m, int device, Sector **out, std::string *err, boo
   CK(cudaMalloc(&s->d_scal, sizeof(double) * 64));
 
   const int nbits = m.nbits;
-  s->gc = m.is_gc();
+  s->gc = m.rows_are_configs();
   // GetSplitBit (src/bitcalc.c:45-62): ihfbit = 2^((Nbits+1)/2).
   s->lo_bits = (nbits + 1) / 2;
   s->hi_bits = nbits - s->lo_bits;
@@ -318,6 +329,64 @@ int sector_build(const Model &m, int device, Sector **out, std::string *err, boo
 
   if (s->gc) {
     s->dim = (int64_t)(1ull << nbits);
+  } else if (m.is_kondo()) {
+    // Kondo / KondoGC (src/sz.c:541-635, 1110-1220, 1342-1420): a half is admissible when
+    // its local spins are singly occupied; blocks by increasing upper half ib, inside a block
+    // the admissible lower halves ia of the needed (up, down) counts (KondoGC: all of them)
+    // in increasing order; list_2_1[ia] = rank + 2, list_2_2[ib] = block offset + 1.
+    const int N = m.nsite, half = N / 2;
+    const uint64_t nh = 1ull << N;
+    if (s->lo_bits != N || s->hi_bits != N) { *err = "Kondo sector: unexpected half split"; return -1; }
+    auto admissible = [&](uint64_t x, int site0) {
+      for (int j = 0; j < half; j++)
+        if (m.locspn[site0 + j] != 0 && ((x >> (2 * j)) & 1ull) == ((x >> (2 * j + 1)) & 1ull)) return false;
+      return true;
+    };
+    const uint64_t even = 0x5555555555555555ull;
+    const bool gck = (m.calc_model == kKondoGC);
+    std::vector<std::vector<uint32_t>> members((half + 1) * (half + 1));
+    std::vector<uint32_t> l21(nh, 0), l22(nh, 0);
+    std::vector<char> used(members.size(), 0);
+    for (uint64_t ia = 0; ia < nh; ia++) {
+      if (!admissible(ia, 0)) continue;
+      const int key = gck ? 0 : __builtin_popcountll(ia & even) * (half + 1) + __builtin_popcountll(ia & ~even);
+      members[key].push_back((uint32_t)ia);
+    }
+    std::vector<uint64_t> l1;
+    uint64_t jb = 0;
+    for (uint64_t ib = 0; ib < nh; ib++) {
+      if (!admissible(ib, half)) continue;
+      int key = 0;
+      if (!gck) {
+        const int nu = m.nup - __builtin_popcountll(ib & even), nd = m.ndown - __builtin_popcountll(ib & ~even);
+        if (nu < 0 || nd < 0 || nu > half || nd > half) continue;
+        key = nu * (half + 1) + nd;
+      }
+      const std::vector<uint32_t> &mem = members[key];
+      if (mem.empty()) continue;
+      used[key] = 1;
+      l22[ib] = (uint32_t)(jb + 1);
+      for (uint32_t ia : mem) l1.push_back((uint64_t)ia | (ib << N));
+      jb += mem.size();
+    }
+    // list_2_1 holds a rank only for lower halves some block uses (the reference writes it
+    // while filling the blocks)
+    for (size_t key = 0; key < members.size(); key++)
+      if (used[key])
+        for (size_t r = 0; r < members[key].size(); r++) l21[members[key][r]] = (uint32_t)r + 2u;
+    const int64_t expect = sector_dim(m);
+    if ((int64_t)jb != expect || jb == 0) {
+      *err = "Kondo sector size mismatch: enumerated " + std::to_string(jb) + ", expected " + std::to_string(expect);
+      return -1;
+    }
+    if (jb > 0xFFFFFFF0ull) { *err = "sector too large for 32-bit list_2 tables"; return -1; }
+    s->dim = (int64_t)jb;
+    CK(cudaMalloc(&s->d_list_2_1, sizeof(uint32_t) * nh));
+    CK(cudaMalloc(&s->d_list_2_2, sizeof(uint32_t) * nh));
+    CK(cudaMalloc(&s->d_list_1, sizeof(uint64_t) * jb));
+    CK(cudaMemcpy(s->d_list_2_1, l21.data(), sizeof(uint32_t) * nh, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->d_list_2_2, l22.data(), sizeof(uint32_t) * nh, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->d_list_1, l1.data(), sizeof(uint64_t) * jb, cudaMemcpyHostToDevice));
   } else {
     const int hubbard = (m.calc_model == kHubbard) ? 1 : 0;
     // Targets and class geometry.

@@ -264,3 +264,30 @@ def sector_dim_estimate(m: ExpertModel) -> int:
         return comb(2 * m.nsite, ne)
     nup = (ne + m.two_sz) // 2
     return comb(m.nsite, nup) * comb(m.nsite, ne - nup)
+
+
+def kondo_chain(cells: int, t: float, J: float, U: float = 0.0, ncond: Optional[int] = None, two_sz: int = 0,
+                gc: bool = False, **kw) -> ExpertModel:
+    """1D Kondo lattice: conduction site 2c (hopping t around the ring of cells, on-site U)
+    and local spin 2c+1 per cell, coupled by J S_loc . s_cond written as InterAll terms:
+    J/4 sum n n (sign by spins) + J/2 (c+_{l up} c_{l dn} c+_{c dn} c_{c up} + h.c.)."""
+    n = 2 * cells
+    m = ExpertModel(model="KondoGC" if gc else "Kondo", nsite=n, two_sz=None if gc else two_sz,
+                    ncond=None if gc else (cells if ncond is None else ncond),
+                    locspin=[(i % 2) for i in range(n)], **kw)
+    for c in range(cells):
+        a, b = 2 * c, 2 * ((c + 1) % cells)
+        if cells > 1 and a != b:
+            for s in (0, 1):
+                m.trans += [(a, s, b, s, t, 0.0), (b, s, a, s, t, 0.0)]
+    if U:
+        m.coulombintra = [(2 * c, U) for c in range(cells)]
+    for c in range(cells):
+        l, e = 2 * c + 1, 2 * c
+        for s1 in (0, 1):
+            for s2 in (0, 1):
+                sg = (1 if s1 == 0 else -1) * (1 if s2 == 0 else -1)
+                m.interall.append((l, s1, l, s1, e, s2, e, s2, 0.25 * J * sg, 0.0))
+        m.interall.append((l, 0, l, 1, e, 1, e, 0, 0.5 * J, 0.0))
+        m.interall.append((l, 1, l, 0, e, 0, e, 1, 0.5 * J, 0.0))
+    return m

@@ -45,6 +45,7 @@ class Def:
     large_value: float = 0.0
     num_ave: int = 1
     pre_cg: int = 0
+    locspn: List[int] = field(default_factory=list)   # 0 itinerant, 1 local spin (Kondo)
     trans: List[Tuple[int, int, int, int, complex]] = field(default_factory=list)   # off-diagonal, Hermitian pairs
     chemi: List[Tuple[int, int, float]] = field(default_factory=list)                # (site, spin, mu): -mu n
     coulomb_intra: List[Tuple[int, float]] = field(default_factory=list)
@@ -105,8 +106,14 @@ def read_expert(namelist: str) -> Def:
         elif k == "lanczostarget": d.lanczos_target = int(v)
         elif k == "largevalue": d.large_value = v
         elif k == "numave": d.num_ave = int(v)
-    d.nlocspn = int(open(files["locspin"]).read().splitlines()[1].split()[1])
-    if d.calc_model in (SPIN, HUBBARD):
+    loc_lines = open(files["locspin"]).read().splitlines()
+    d.nlocspn = int(loc_lines[1].split()[1])
+    d.locspn = [0] * d.nsite
+    for l in loc_lines[5:]:
+        p = l.split()
+        if len(p) >= 2 and 0 <= int(p[0]) < d.nsite:
+            d.locspn[int(p[0])] = int(p[1])
+    if d.calc_model in (SPIN, HUBBARD, KONDO):
         if read_ncond:
             if sz_cons:
                 d.nup = (d.nlocspn + d.ncond + d.total_2sz) // 2
@@ -171,6 +178,12 @@ def _is_gc(d: Def) -> bool:
     return d.calc_model in (HUBBARDGC, SPINGC, KONDOGC)
 
 
+def _rows_are_configs(d: Def) -> bool:
+    """Grand-canonical models without lists (KondoGC keeps lists: its local spins stay
+    singly occupied, src/sz.c:1342-1420)."""
+    return d.calc_model in (HUBBARDGC, SPINGC)
+
+
 def nbits(d: Def) -> int:
     return d.nsite if _is_spin(d) else 2 * d.nsite
 
@@ -211,8 +224,10 @@ def sz(d: Def):
     """sz (src/sz.c:62-832), hacker enumeration omp_sz_hacker (:993-1094) /
     omp_sz_spin_hacker (:1495-1546): blocks by upper half ib ascending, each block the
     ascending lower halves ia whose particle numbers complete the sector."""
-    if _is_gc(d):
+    if _rows_are_configs(d):
         raise ValueError("grand-canonical models have no lists")
+    if d.calc_model in (KONDO, KONDOGC):
+        return _sz_kondo(d)
     ihfbit, irght, ilft = split_bits(d)
     sd = sdim(d)
     lo = (nbits(d) + 1) // 2
@@ -251,9 +266,53 @@ def sz(d: Def):
     return list_1, list_2_1, list_2_2
 
 
+def _sz_kondo(d: Def):
+    """omp_sz_Kondo / omp_sz_KondoGC (src/sz.c:1110-1220, 1342-1420) for even Nsite: a half
+    is admissible when its local spins are singly occupied; blocks by ascending upper half,
+    each block the ascending admissible lower halves with the missing (up, down) counts
+    (KondoGC: all admissible lower halves)."""
+    if d.nsite % 2:
+        raise ValueError("odd Nsite Kondo is not restated")
+    N, half = d.nsite, d.nsite // 2
+    nh = 1 << N
+    x = np.arange(nh, dtype=np.uint64)
+
+    def admissible(site0):
+        ok = np.ones(nh, dtype=bool)
+        for j in range(half):
+            if d.locspn[site0 + j]:
+                u = (x >> np.uint64(2 * j)) & np.uint64(1)
+                dn = (x >> np.uint64(2 * j + 1)) & np.uint64(1)
+                ok &= (u != dn)
+        return ok
+
+    even = np.uint64(0x5555555555555555)
+    up, dn = _popcount(x & even), _popcount(x & ~even)
+    lo_ok, hi_ok = admissible(0), admissible(half)
+    list_2_1 = np.zeros(nh + 2, dtype=np.uint64)
+    list_2_2 = np.zeros(nh + 2, dtype=np.uint64)
+    gc = d.calc_model == KONDOGC
+    blocks, jb = [], 0
+    for ib in range(nh):
+        if not hi_ok[ib]:
+            continue
+        if gc:
+            sel = np.nonzero(lo_ok)[0]
+        else:
+            nu, nd = d.nup - int(up[ib]), d.ndown - int(dn[ib])
+            sel = np.nonzero(lo_ok & (up == nu) & (dn == nd))[0]
+        if sel.size:
+            blocks.append(sel.astype(np.uint64) + np.uint64(ib << N))
+            list_2_1[sel] = np.arange(sel.size, dtype=np.uint64) + np.uint64(2)
+            list_2_2[ib] = jb + 1
+            jb += sel.size
+    list_1 = np.concatenate([np.zeros(1, dtype=np.uint64)] + blocks)
+    return list_1, list_2_1, list_2_2
+
+
 def configs(d: Def, lists) -> np.ndarray:
     """Configuration of every row (1-based arrays: element 0 unused)."""
-    if _is_gc(d):
+    if _rows_are_configs(d):
         n = 1 << nbits(d)
         return np.concatenate([np.zeros(1, np.uint64), np.arange(n, dtype=np.uint64)])
     return lists[0]
@@ -261,7 +320,7 @@ def configs(d: Def, lists) -> np.ndarray:
 
 def get_off(d: Def, lists, c: np.ndarray) -> np.ndarray:
     """GetOffComp (src/bitcalc.c:195-223): 1-based row of configuration c, 0 if absent."""
-    if _is_gc(d):
+    if _rows_are_configs(d):
         return c.astype(np.int64) + 1
     ihfbit, irght, ilft = split_bits(d)
     lo = (nbits(d) + 1) // 2

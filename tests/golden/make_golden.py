@@ -108,6 +108,15 @@ def _cases():
     m = expert.kitaev_heisenberg(2, 2, -1.0, 0.2, calc_type="CG", lanczos_max=400, lanczos_eps=12)
     m.initial_vec_type = 0
     c["lobpcg_kitaev2x2"] = m
+    # Kondo lattices (itinerant ring + one local spin per cell, J S.s as InterAll): canonical
+    # with real and complex vectors, and the grand-canonical KondoGC sector.
+    c["kondo_chain4"] = expert.kondo_chain(4, 1.0, 1.5, lanczos_max=300)
+    m = expert.kondo_chain(4, 1.0, 1.2, U=2.0, two_sz=2, lanczos_max=300)
+    m.initial_vec_type = 0
+    c["kondo_chain4_u"] = m
+    m = expert.kondo_chain(2, 1.0, 0.8, gc=True, lanczos_max=200)
+    m.initial_vec_type = 0
+    c["kondogc_chain2"] = m
     return c
 
 
@@ -118,6 +127,7 @@ def _large_cases():
     c["hub4x4_lists"] = m
     m = expert.heisenberg(24, expert.chain_bonds(24), lanczos_max=1)
     c["chain24_lists"] = m
+    c["kondo_chain8_lists"] = expert.kondo_chain(8, 1.0, 1.0, lanczos_max=1)
     return c
 
 
