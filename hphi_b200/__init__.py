@@ -271,15 +271,18 @@ class Hamiltonian:
         _check(load_library().hphi_synchronize(self._h))
 
     def calc_by_lanczos(self, v_init: Optional[np.ndarray] = None, output_dir: Optional[str] = None) -> dict:
-        res = np.zeros(11)
+        res = np.zeros(17)
         vi = None if v_init is None else _as_hphi_vector(v_init, self.dim)
         _check(load_library().hphi_lanczos(self._h, None if vi is None else _dptr(vi.view(np.float64)),
                                            None if output_dir is None else os.fsencode(output_dir),
                                            _dptr(res), len(res)))
-        keys = ["converged", "steps", "e_target", "e1", "e2", "e3", "e4", "energy", "var", "doublon", "sz"]
+        keys = ["converged", "steps", "e_target", "e1", "e2", "e3", "e4", "energy", "var", "doublon", "sz",
+                "check_diff", "check_var", "cg_rounds", "cg_iterations", "cg_diff", "cg_var"]
         out = {k: float(res[i]) for i, k in enumerate(keys)}
         out["converged"] = bool(res[0])
         out["steps"] = int(res[1])
+        out["cg_rounds"] = int(res[13])
+        out["cg_iterations"] = int(res[14])
         return out
 
     def lanczos_tridiagonal(self):

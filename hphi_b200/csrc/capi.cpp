@@ -302,9 +302,10 @@ int hphi_lanczos(hphi_handle *h, const double *v_init, const char *output_dir, d
   r = LanczosResult();
   const int rc = lanczos_run(s, vt, v_init, opt, &r);
   if (result && nresult > 0) {
-    double v[11] = {r.converged ? 1.0 : 0.0, (double)r.steps, r.e_target, 0, 0, 0, 0, r.energy, r.var, r.doublon, r.sz};
+    double v[17] = {r.converged ? 1.0 : 0.0, (double)r.steps, r.e_target, 0, 0, 0, 0, r.energy, r.var, r.doublon, r.sz,
+                    r.check_diff, r.check_var, (double)r.cg_rounds, (double)r.cg_iterations, r.cg_diff, r.cg_var};
     for (int q = 0; q < 4 && q < (int)r.energies.size(); q++) v[3 + q] = r.energies[q];
-    for (int i = 0; i < nresult && i < 11; i++) result[i] = v[i];
+    for (int i = 0; i < nresult && i < 17; i++) result[i] = v[i];
   }
   if (rc != 0) return -1;
   if (output_dir && write_lanczos_outputs(*s, r, output_dir) != 0) return -1;

@@ -27,6 +27,7 @@ template <> struct VT<double> {
   static __device__ __forceinline__ double scale(double a, double x) { return a * x; }
   static __device__ __forceinline__ double add(double a, double b) { return a + b; }
   static __device__ __forceinline__ double sub(double a, double b) { return a - b; }
+  static __device__ __forceinline__ double add_re(double x, double a) { return x + a; }
 };
 template <> struct VT<cplx> {
   static __device__ __forceinline__ cplx zero() { return cplx{0.0, 0.0}; }
@@ -40,6 +41,7 @@ template <> struct VT<cplx> {
   static __device__ __forceinline__ cplx scale(double a, cplx x) { return cplx{a * x.x, a * x.y}; }
   static __device__ __forceinline__ cplx add(cplx a, cplx b) { return a + b; }
   static __device__ __forceinline__ cplx sub(cplx a, cplx b) { return a - b; }
+  static __device__ __forceinline__ cplx add_re(cplx x, double a) { return cplx{x.x + a, x.y}; }
 };
 
 // Sum of NV doubles over the block; thread 0 gets the result.  Fixed order, so

@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <sys/stat.h>
@@ -231,6 +232,81 @@ int hashed_start(const Sector &s, uint64_t seed, bool complex_vec, std::vector<d
   return 0;
 }
 
+// ------------------------------------------------------- CG eigenvector refinement
+namespace {
+constexpr double kEpsEnergy = 1e-12;  // eps_Energy (src/readdef.c:2703,2707)
+constexpr double kEpsCG = 1e-8;       // eps and eps_CG (src/readdef.c:2701-2706)
+
+// Inverse iteration with conjugate-gradient solves of (H - Eig + eps_CG) x = b
+// (src/CG_EigenVector.c:30-255).  vg holds the normalised Lanczos vector on entry and the
+// refined, normalised vector on return (native order).  b gets vg plus random components
+// of amplitude 1e-3 (the reference draws them from per-thread dSFMT streams seeded
+// 123432 + |iv| + thread; here they are start_value(seed, configuration), so the result
+// does not depend on thread counts or the vector order), normalised.  Each round runs CG
+// from x = 0 until |r| < eps |b| (at most 500 iterations), normalises x and stops when
+// ||<x|b>| - 1| < eps, else restarts from b = x (at most 51 rounds).  The CG scalars are
+// real: for a Hermitian H, <p|(H - Eig) p> has no imaginary part.
+int cg_eigenvector(Sector *s, VecType vt, double eig, uint64_t seed, void *vg, void *b, void *r, void *p, void *hp,
+                   double *st, LanczosResult *res) {
+  const int64_t dim = s->dim;
+  const size_t esz = (vt == kReal64) ? sizeof(double) : sizeof(cplx);
+  const double shift = -eig + kEpsCG;
+  auto read = [&](const double *d, double *h, int n) -> int {
+    RET(cuda_ok(cudaMemcpyAsync(h, d, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream), "read"));
+    return cuda_ok(cudaStreamSynchronize(s->stream), "sync");
+  };
+  auto copy = [&](void *dst, const void *src) {
+    return cuda_ok(cudaMemcpyAsync(dst, src, esz * dim, cudaMemcpyDeviceToDevice, s->stream), "copy");
+  };
+  // b = vg + random components, in HPhi order so the components follow the configurations
+  RET(from_native(s, vt, vg, hp));
+  RET(vec_add_hashed(s, vt, seed, 0.002, hp));
+  RET(to_native(s, vt, hp, b));
+  double h[2];
+  RET(vec_norm2(s, vt, b, st + 20));
+  RET(read(st + 20, h, 1));
+  RET(vec_scale(s, vt, 1.0 / std::sqrt(h[0]), b));
+  const double coef[2] = {0.0, 1.0};  // hp = H p
+  RET(cuda_ok(cudaMemcpyAsync(st + 22, coef, sizeof(coef), cudaMemcpyHostToDevice, s->stream), "coef"));
+  res->cg_rounds = 0;
+  res->cg_iterations = 0;
+  for (int round = 0; round <= 50; round++) {
+    res->cg_rounds = round + 1;
+    RET(vec_norm2(s, vt, b, st + 20));
+    RET(read(st + 20, h, 1));
+    const double bnorm = h[0];
+    RET(copy(r, b));
+    RET(copy(p, b));
+    RET(cuda_ok(cudaMemsetAsync(vg, 0, esz * dim, s->stream), "zero x"));
+    double rnorm = bnorm;  // |r|^2 of the current residual
+    for (int itr = 1; itr <= 500; itr++) {
+      RET(hv_native(s, vt, p, hp, st + 22, st + 24, false));
+      RET(vec_dot(s, vt, p, hp, st + 26));
+      RET(vec_norm2(s, vt, p, st + 28));
+      double d[3];
+      RET(read(st + 26, d, 3));
+      const double yp = d[0] + shift * d[2];  // <p|(H - Eig + eps_CG) p>
+      const double alpha = rnorm / yp;
+      RET(vec_cg_sweep(s, vt, alpha, shift, p, hp, vg, r, st + 20));
+      RET(read(st + 20, h, 1));
+      const double rnorm2 = h[0];
+      RET(vec_axpby(s, vt, 1.0, r, rnorm2 / rnorm, p));  // p = r + beta p
+      rnorm = rnorm2;
+      res->cg_iterations++;
+      if (std::sqrt(rnorm2) < kEpsCG * std::sqrt(bnorm)) break;
+    }
+    RET(vec_norm2(s, vt, vg, st + 20));
+    RET(read(st + 20, h, 1));
+    RET(vec_scale(s, vt, 1.0 / std::sqrt(h[0]), vg));
+    RET(vec_dot(s, vt, vg, b, st + 20));
+    RET(read(st + 20, h, 2));
+    if (std::fabs(std::hypot(h[0], h[1]) - 1.0) < kEpsCG) break;
+    RET(copy(b, vg));
+  }
+  return 0;
+}
+}  // namespace
+
 // ------------------------------------------------------------------- Lanczos
 int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOptions &opt, LanczosResult *res) {
   const Model &m = s->model;
@@ -240,7 +316,7 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   DevBuf P, Q, V0, ST, AL, BE;
   RET(cuda_ok(cudaMalloc(&P.p, esz * dim), "alloc P"));
   RET(cuda_ok(cudaMalloc(&Q.p, esz * dim), "alloc Q"));
-  RET(cuda_ok(cudaMalloc(&ST.p, sizeof(double) * 32), "alloc scalars"));  // slots used: [0, 19)
+  RET(cuda_ok(cudaMalloc(&ST.p, sizeof(double) * 32), "alloc scalars"));  // slots used: [0, 29)
   const bool fixed = opt.fixed_steps > 0;
   int max_steps = fixed ? opt.fixed_steps : m.lanczos_max;
   if ((int64_t)max_steps > dim) max_steps = (int)dim;
@@ -397,18 +473,38 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
   RET(vec_scale(s, vt, 1.0 / std::sqrt(nrm2), VG.p));
   // expec_energy_flct: H vg -> E = <vg|H vg>, var = <H vg|H vg>
-  const double coef1[2] = {0.0, 1.0};
-  RET(cuda_ok(cudaMemcpyAsync(st + 8, coef1, sizeof(coef1), cudaMemcpyHostToDevice, s->stream), "coef"));
-  RET(hv_native(s, vt, VG.p, pp, st + 8, st + 10));
-  RET(vec_norm2(s, vt, pp, st + 12));
-  RET(native_observables(s, vt, VG.p, st + 13));
-  double sc[10];
-  RET(cuda_ok(cudaMemcpyAsync(sc, st + 10, sizeof(double) * 9, cudaMemcpyDeviceToHost, s->stream), "read"));
-  RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
-  res->energy = sc[0];
-  res->var = sc[2];
-  res->doublon = sc[3];
-  res->sz = sc[7];
+  auto expec = [&]() -> int {
+    const double coef1[2] = {0.0, 1.0};
+    RET(cuda_ok(cudaMemcpyAsync(st + 8, coef1, sizeof(coef1), cudaMemcpyHostToDevice, s->stream), "coef"));
+    RET(hv_native(s, vt, VG.p, pp, st + 8, st + 10));
+    RET(vec_norm2(s, vt, pp, st + 12));
+    RET(native_observables(s, vt, VG.p, st + 13));
+    double sc[10];
+    RET(cuda_ok(cudaMemcpyAsync(sc, st + 10, sizeof(double) * 9, cudaMemcpyDeviceToHost, s->stream), "read"));
+    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+    res->energy = sc[0];
+    res->var = sc[2];
+    res->doublon = sc[3];
+    res->sz = sc[7];
+    return 0;
+  };
+  RET(expec());
+  // accuracy check (src/CalcByLanczos.c:120-128), eps_Energy = 1e-12 (src/readdef.c:2701-2707)
+  auto rel_var = [&]() { return std::fabs(res->var - res->energy * res->energy) / std::fabs(res->var); };
+  auto rel_diff = [&]() { return std::fabs(lam - res->energy) / std::fabs(lam); };
+  res->check_var = rel_var();
+  res->check_diff = rel_diff();
+  if (!(res->check_diff < kEpsEnergy && res->check_var < kEpsEnergy) && m.calc_eigenvec == 0) {
+    DevBuf B, HP;
+    RET(cuda_ok(cudaMalloc(&B.p, esz * dim), "alloc CG b"));
+    RET(cuda_ok(cudaMalloc(&HP.p, esz * dim), "alloc CG hp"));
+    // V0 (the start vector) is no longer needed: it holds the CG search direction
+    RET(cg_eigenvector(s, vt, lam, (uint64_t)(123432 + std::abs((long)m.initial_iv)), VG.p, B.p, pp, V0.p, HP.p, st, res));
+    RET(expec());
+    res->cg_ran = true;
+    res->cg_var = rel_var();
+    res->cg_diff = rel_diff();
+  }
   res->eigenvector.assign(2 * (dim + 1), 0.0);
   if (opt.copy_eigenvector) {
     RET(from_native(s, vt, VG.p, pp));

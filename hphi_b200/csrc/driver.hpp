@@ -23,6 +23,12 @@ struct LanczosResult {
   std::vector<double> energies;      // lowest eigenvalues of the final tridiagonal matrix
   std::vector<std::string> lines;    // zvo_Lanczos_Step.dat
   double energy = 0.0, var = 0.0, doublon = 0.0, sz = 0.0;
+  // accuracy check of the Lanczos vector (src/CalcByLanczos.c:120-121) and, when it fails
+  // with CalcEigenVec 0, the CG refinement (src/CG_EigenVector.c): relative variance and
+  // energy difference before / after, inverse-iteration rounds and total CG iterations
+  double check_var = 0.0, check_diff = 0.0, cg_var = 0.0, cg_diff = 0.0;
+  bool cg_ran = false;
+  int cg_rounds = 0, cg_iterations = 0;
   std::vector<double> eigenvector;   // 1-based complex128 (HPhi layout) when requested
 };
 

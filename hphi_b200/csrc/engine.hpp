@@ -128,6 +128,12 @@ int vec_replay_sweep(Sector *s, VecType vt, double a_sq, double c_over_b, void *
 // v = cv*v - ch*h and d_out[0] = |v|^2 (TPQ step before normalisation)
 int vec_tpq_sweep(Sector *s, VecType vt, double cv, double ch, void *v, const void *h, double *d_out);
 
+// CG sweep (eigenvector refinement): x += a*p; r -= a*(hp + shift*p); d_out[0] = |r|^2.
+int vec_cg_sweep(Sector *s, VecType vt, double a, double shift, const void *p, const void *hp, void *x, void *r,
+                 double *d_out);
+// x[i] += amp * start_value(seed, configuration of row i, 0) on the real part (HPhi order).
+int vec_add_hashed(Sector *s, VecType vt, uint64_t seed, double amp, void *d_x);
+
 // Copies between HPhi's 1-based complex128 host layout and a device vector.
 int vec_from_host_c128(Sector *s, VecType vt, const double *h_v_1based, void *d_v);
 int vec_to_host_c128(Sector *s, VecType vt, const void *d_v, double *h_v_1based);

@@ -8,6 +8,7 @@
 
 #include <string>
 
+#include "batch.hpp"
 #include "device_util.cuh"
 #include "engine.hpp"
 
@@ -258,6 +259,36 @@ __global__ void tpq_sweep_kernel(int64_t n, double cv, double ch, T *__restrict_
   if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
 }
 
+// CG sweep of the eigenvector refinement (src/CG_EigenVector.c:143-185) with the shifted
+// product y = hp + shift*p formed on the fly: x += a*p; r -= a*y; |r|^2 into part.
+template <typename T>
+__global__ void cg_sweep_kernel(int64_t n, double a, double shift, const T *__restrict__ p,
+                                const T *__restrict__ hp, T *__restrict__ x, T *__restrict__ r,
+                                double *__restrict__ part) {
+  double acc[1] = {0.0};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T pi = p[i];
+    const T yi = VT<T>::add(hp[i], VT<T>::scale(shift, pi));
+    x[i] = VT<T>::add(x[i], VT<T>::scale(a, pi));
+    const T w = VT<T>::sub(r[i], VT<T>::scale(a, yi));
+    r[i] = w;
+    acc[0] += VT<T>::abs2(w);
+  }
+  block_sum<1>(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
+}
+
+// Adds amp * start_value(seed, configuration, 0) to the real part of an HPhi-order vector
+// (the random components of src/CG_EigenVector.c:84-99, keyed by configuration).
+template <typename T>
+__global__ void add_hashed_kernel(int64_t n, uint64_t seed, double amp, const uint64_t *__restrict__ list_1,
+                                  T *__restrict__ x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = list_1 ? list_1[i] : (uint64_t)i;
+    x[i] = VT<T>::add_re(x[i], amp * start_value(seed, c, 0));
+  }
+}
+
 }  // namespace
 
 int lanczos_scalars(Sector *s, int phase, int k, double *st, double *alpha, double *beta) {
@@ -284,6 +315,31 @@ int vec_tpq_sweep(Sector *s, VecType vt, double cv, double ch, void *v, const vo
                                                                       s->d_red);
   finalize_partials_kernel<1><<<1, 256, 0, s->stream>>>(s->d_red, s->red_blocks, out);
   return check_launch("vec_tpq_sweep");
+}
+
+}  // namespace hphi
+
+namespace hphi {
+
+int vec_cg_sweep(Sector *s, VecType vt, double a, double shift, const void *p, const void *hp, void *x, void *r,
+                 double *out) {
+  if (vt == kReal64)
+    cg_sweep_kernel<double><<<s->red_blocks, kThreads, 0, s->stream>>>(
+        s->dim, a, shift, (const double *)p, (const double *)hp, (double *)x, (double *)r, s->d_red);
+  else
+    cg_sweep_kernel<cplx><<<s->red_blocks, kThreads, 0, s->stream>>>(s->dim, a, shift, (const cplx *)p,
+                                                                     (const cplx *)hp, (cplx *)x, (cplx *)r, s->d_red);
+  finalize_partials_kernel<1><<<1, 256, 0, s->stream>>>(s->d_red, s->red_blocks, out);
+  return check_launch("vec_cg_sweep");
+}
+
+int vec_add_hashed(Sector *s, VecType vt, uint64_t seed, double amp, void *x) {
+  const uint64_t *l1 = s->gc ? nullptr : s->d_list_1;
+  if (vt == kReal64)
+    add_hashed_kernel<double><<<s->red_blocks, kThreads, 0, s->stream>>>(s->dim, seed, amp, l1, (double *)x);
+  else
+    add_hashed_kernel<cplx><<<s->red_blocks, kThreads, 0, s->stream>>>(s->dim, seed, amp, l1, (cplx *)x);
+  return check_launch("vec_add_hashed");
 }
 
 }  // namespace hphi

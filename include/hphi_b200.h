@@ -156,8 +156,15 @@ int hphi_synchronize(hphi_handle *h);
  * eigenvector) into output_dir when it is not NULL.  result (may be NULL) receives
  *   [0] converged (1/0)  [1] steps  [2] E_target  [3] E[1]  [4] E[2]  [5] E[3]  [6] E[4]
  *   [7] energy <v|H|v>   [8] <Hv|Hv>  [9] doublon  [10] Sz
+ *   [11] diff_ene and [12] var of the accuracy check of the Lanczos vector
+ *   [13] CG rounds (0: the check passed or CalcEigenVec is 1)  [14] CG iterations
+ *   [15] diff_ene and [16] var after the CG refinement
+ * With CalcEigenVec 0 and a failed accuracy check (relative variance or energy difference
+ * not below 1e-12) the vector is refined by inverse iteration with CG solves before the
+ * energy, doublon and Sz are taken.
  * Replaces: CalcByLanczos (src/CalcByLanczos.c:55-276) with Lanczos_EigenValue
- * (src/Lanczos_EigenValue.c:50) and Lanczos_EigenVector (src/Lanczos_EigenVector.c:46).
+ * (src/Lanczos_EigenValue.c:50), Lanczos_EigenVector (src/Lanczos_EigenVector.c:46) and
+ * CG_EigenVector (src/CG_EigenVector.c:30).
  */
 int hphi_lanczos(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult);
 

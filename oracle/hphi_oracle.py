@@ -500,6 +500,82 @@ def lanczos_eigenvalues(d: Def, lists, diag, v_init: np.ndarray, max_steps: int 
     raise RuntimeError("Lanczos did not converge")
 
 
+def lanczos_eigenvector(d: Def, lists, diag, v_init: np.ndarray, alpha, beta, k: int = 0) -> np.ndarray:
+    """Lanczos_EigenVector (src/Lanczos_EigenVector.c:46-195): the k-th eigenvector c of the
+    tridiagonal matrix, then the recurrence replayed from the start vector with the stored
+    alpha / beta, accumulating vg = sum_j c_j q_j; returned normalised (1-based)."""
+    n = len(alpha)
+    T = np.diag(alpha) + np.diag(beta[:n - 1], 1) + np.diag(beta[:n - 1], -1)
+    c = np.linalg.eigh(T)[1][:, k]
+    v1 = v_init.astype(np.complex128).copy()
+    vg = c[0] * v1
+    v0, _ = mltply(d, lists, diag, np.zeros_like(v1), v1)
+    for stp in range(1, n):
+        a1, b1 = alpha[stp - 1], beta[stp - 1]
+        tmp = v1.copy()
+        v1[1:] = (v0[1:] - a1 * v1[1:]) / b1
+        v0[1:] = -b1 * tmp[1:]
+        v0, _ = mltply(d, lists, diag, v0, v1)
+        vg[1:] += c[stp] * v1[1:]
+    vg[1:] /= np.sqrt(np.sum(np.abs(vg[1:]) ** 2))
+    return vg
+
+
+def expec_energy(d: Def, lists, diag, v: np.ndarray):
+    """expec_energy_flct (src/expec_energy_flct.c:60-180) for a normalised vector: energy
+    <v|H|v>, var <Hv|Hv>, doublon sum |v|^2 D and Sz sum |v|^2 (N_up - N_dn)/2 (Hubbard bit
+    2i + s; spin bit i = up)."""
+    hv, _ = mltply(d, lists, diag, np.zeros_like(v), v)
+    energy = float(np.vdot(v[1:], hv[1:]).real)
+    var = float(np.sum(np.abs(hv[1:]) ** 2))
+    w = np.abs(v[1:]) ** 2
+    c = configs(d, lists)[1:].astype(np.uint64)
+    if _is_spin(d):
+        doublon = 0.0
+        sz = float(np.sum(w * 0.5 * (2 * _popcount(c) - d.nsite)))
+    else:
+        even = np.uint64(0x5555555555555555)
+        up, dn = _popcount(c & even), _popcount(c & ~even)
+        doublon = float(np.sum(w * _popcount(c & (c >> np.uint64(1)) & even)))
+        sz = float(np.sum(w * 0.5 * (up - dn)))
+    return energy, var, doublon, sz
+
+
+def cg_eigenvector(d: Def, lists, diag, v: np.ndarray, eig: float, noise: np.ndarray,
+                   eps: float = 1e-8, eps_cg: float = 1e-8):
+    """CG_EigenVector (src/CG_EigenVector.c:30-255): inverse iteration with conjugate-gradient
+    solves of (H - eig + eps_cg) x = b.  b = v + noise, normalised (the reference draws the
+    noise, amplitude 1e-3, from per-thread dSFMT streams); each round runs CG from x = 0
+    until |r| < eps |b| (at most 500 iterations), normalises x and stops when
+    ||<x|b>| - 1| < eps, else restarts from b = x (at most 51 rounds).
+    Returns (x normalised, rounds, total CG iterations)."""
+    b = v.astype(np.complex128).copy()
+    b[1:] += noise
+    b[1:] /= np.sqrt(np.sum(np.abs(b[1:]) ** 2))
+    total = 0
+    for rnd in range(51):
+        bnorm = float(np.sum(np.abs(b[1:]) ** 2))
+        r, p, x = b.copy(), b.copy(), np.zeros_like(b)
+        for _ in range(500):
+            y = (-eig + eps_cg) * p
+            y, _ = mltply(d, lists, diag, y, p)
+            rp = float(np.sum(np.abs(r[1:]) ** 2))
+            alpha = rp / np.sum(y[1:] * np.conj(p[1:]))
+            x[1:] += alpha * p[1:]
+            r[1:] -= alpha * y[1:]
+            rnorm2 = float(np.sum(np.abs(r[1:]) ** 2))
+            p[1:] = r[1:] + (rnorm2 / rp) * p[1:]
+            total += 1
+            if np.sqrt(rnorm2) < eps * np.sqrt(bnorm):
+                break
+        x[1:] /= np.sqrt(np.sum(np.abs(x[1:]) ** 2))
+        xb = np.vdot(x[1:], b[1:])
+        if abs(abs(xb) - 1.0) < eps:
+            return x, rnd + 1, total
+        b = x
+    return x, 51, total
+
+
 def tpq_energies(d: Def, lists, diag, v_start: np.ndarray, nsteps: int):
     """CalcByTPQ (src/CalcByTPQ.c:52-294) for one sample: returns the energies of the
     SS_rand lines for steps 0 .. nsteps-1 (step 0 = the start vector itself)."""

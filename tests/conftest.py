@@ -34,6 +34,8 @@ def golden_cases(kind=None):
             continue
         if kind == "lanczos_or_tpq" and (large or ("steps" not in z.files and "tpq" not in z.files)):
             continue
+        if kind == "eigenvector" and (large or "energy_state" not in z.files):
+            continue
         out.append(name)
     return out
 

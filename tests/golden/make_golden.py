@@ -9,6 +9,8 @@ of oracle/ref_hooks.c:
   hv3_v1, hv3_v0b, hv3_v0a, hv3_pr  the 4th mltply call (accumulates into a non-zero v0)
   steps, step_vals               zvo_Lanczos_Step.dat (Lanczos cases)
   lobpcg_steps, lobpcg_states    zvo_Lanczos_Step.dat rows and zvo_energy.dat states (LOBPCG cases)
+  energy_state, cg_ran           zvo_energy.dat of a Lanczos case with CalcEigenVec != -1, and
+                                 whether the reference refined the vector by CG
   tpq                            SS_rand0.dat rows (TPQ cases)
 Large cases store only SHA-256 digests of the lists (sha_list_1 ...).
 
@@ -117,6 +119,12 @@ def _cases():
     m = expert.kondo_chain(2, 1.0, 0.8, gc=True, lanczos_max=200)
     m.initial_vec_type = 0
     c["kondogc_chain2"] = m
+    # Lanczos stopped early (LanczosEps 5) with CalcEigenVec 0: the reference's accuracy
+    # check fails and CG_EigenVector refines the vector before zvo_energy.dat is written.
+    c["lanczos_cg_chain12"] = expert.heisenberg(12, expert.chain_bonds(12), lanczos_eps=5, calc_eigenvec=0)
+    m = expert.hubbard(6, expert.chain_bonds(6), 1.0, 4.0, 3, 3, lanczos_eps=3, calc_eigenvec=0)
+    m.initial_vec_type = 0
+    c["lanczos_cg_hub6"] = m
     return c
 
 
@@ -168,6 +176,10 @@ def make_case(name: str, m, large: bool = False) -> None:
             data["steps"] = np.array([s for s, _ in steps])
             data["step_vals"] = np.array([[np.nan if v is None else v for v in (vals + [None] * 6)[:6]]
                                           for _, vals in steps])
+            if m.calc_eigenvec != -1:
+                # zvo_energy.dat (Energy, Doublon, Sz) and whether the CG refinement ran
+                data["energy_state"] = run_ref.energy_states(tmp)[0]
+                data["cg_ran"] = np.array("Accuracy of Lanczos vectors is NOT enough" in p.stdout)
         else:
             data["tpq"] = run_ref.tpq_table(tmp, 0)
     with tempfile.TemporaryDirectory() as tmp:

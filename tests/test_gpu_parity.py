@@ -116,6 +116,28 @@ def test_lanczos_eigenvector_energy_and_variance(name, tmp_path):
         assert re.match(r"Energy  -?\d+\.\d{16} \nDoublon  -?\d+\.\d{16} \nSz  -?\d+\.\d{16} \n", text)
 
 
+@pytest.mark.parametrize("name", golden_cases("eigenvector"))
+def test_lanczos_cg_refinement_matches_reference(name, tmp_path):
+    """CalcEigenVec 0 with a Lanczos run stopped early: the accuracy check fails as in the
+    reference and the CG refinement gives the reference's Energy / Doublon / Sz."""
+    g = load_golden(name)
+    ref = g["energy_state"]
+    with open_case(name) as H:
+        r = H.calc_by_lanczos(v_init=g["hv0_v1"], output_dir=str(tmp_path))
+        assert r["converged"]
+        assert (r["cg_rounds"] > 0) == bool(g["cg_ran"])
+        if g["cg_ran"]:
+            assert r["check_var"] >= 1e-12 or r["check_diff"] >= 1e-12
+            assert r["cg_var"] < 1e-12 and r["cg_iterations"] >= r["cg_rounds"]
+        assert abs(r["energy"] - ref[0]) < E_TOL * max(1.0, abs(ref[0]))
+        assert abs(r["doublon"] - ref[1]) < 1e-9
+        assert abs(r["sz"] - ref[2]) < 1e-9
+        v = H.lanczos_eigenvector()
+        assert abs(np.vdot(v[1:], v[1:]).real - 1.0) < 1e-12
+    vals = [float(l.split()[1]) for l in open(tmp_path / "zvo_energy.dat")]
+    np.testing.assert_allclose(vals, ref, rtol=0, atol=1e-9)
+
+
 @pytest.mark.parametrize("name", golden_cases("tpq"))
 def test_tpq_energies_match_reference(name, tmp_path):
     g = load_golden(name)

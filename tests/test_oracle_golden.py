@@ -70,6 +70,39 @@ def test_oracle_lanczos_eigenvalue(name):
     check_lanczos_against_reference(g, E[0], alpha, beta)
 
 
+def tridiag_lowest(alpha, beta, k):
+    n = len(alpha)
+    T = np.diag(alpha) + np.diag(beta[:n - 1], 1) + np.diag(beta[:n - 1], -1)
+    return float(np.linalg.eigvalsh(T)[k])
+
+
+@pytest.mark.parametrize("name", golden_cases("eigenvector"))
+def test_oracle_eigenvector_and_cg_refinement(name):
+    """Lanczos eigenvector, the accuracy check of CalcByLanczos (eps_Energy 1e-12) and the
+    CG refinement against the reference's zvo_energy.dat.  The refined vector does not
+    depend on the random components added to b (the reference's come from dSFMT)."""
+    g = load_golden(name)
+    d = O.read_expert(case_dir(name) + "/namelist.def")
+    lists = O.sz(d) if "list_1" in g else None
+    diag = O.diagonalcalc(d, lists)
+    _, _, _, alpha, beta = O.lanczos_eigenvalues(d, lists, diag, g["hv0_v1"])
+    lam = tridiag_lowest(alpha, beta, d.k_exct - 1)
+    v = O.lanczos_eigenvector(d, lists, diag, g["hv0_v1"], alpha, beta, d.k_exct - 1)
+    e, var, dbl, sz = O.expec_energy(d, lists, diag, v)
+    accurate = abs(lam - e) / abs(lam) < 1e-12 and abs(var - e * e) / abs(var) < 1e-12
+    assert accurate == (not bool(g["cg_ran"]))
+    if not accurate and d.calc_eigenvec == 0:
+        noise = 0.002 * (np.random.default_rng(5).random(v.size - 1) - 0.5)
+        x, rounds, iters = O.cg_eigenvector(d, lists, diag, v, lam, noise)
+        assert 1 <= rounds <= 51 and iters >= 1
+        e, var, dbl, sz = O.expec_energy(d, lists, diag, x)
+        assert abs(var - e * e) / abs(var) < 1e-12
+    ref = g["energy_state"]
+    assert abs(e - ref[0]) < 1e-10 * max(1.0, abs(ref[0]))
+    assert abs(dbl - ref[1]) < 1e-9
+    assert abs(sz - ref[2]) < 1e-9
+
+
 @pytest.mark.parametrize("name", golden_cases("tpq"))
 def test_oracle_tpq_energies(name):
     g = load_golden(name)
