@@ -459,7 +459,9 @@ def main():
     dim = H.dim
     H_native = bool(H.info.get("native_order"))
     kind = H.info.get("kernel", 0)
-    kname, kdesc = {2: ("prod_hv_kernel", "prod_hv_kernel<double> + finalize_partials_kernel<2> per step"),
+    kname, kdesc = {3: ("prod_two_pass", "prod_down_kernel (row pass) + prod_up_kernel<true> (column pass) + "
+                                         "finalize_partials_kernel<2> per step; achieved = B_alg / time of all three"),
+                    2: ("prod_hv_kernel", "prod_hv_kernel<double> + finalize_partials_kernel<2> per step"),
                     1: ("hv_hub_pass", "hv_hub_pass<double,0> + hv_hub_pass<double,1> + finalize per step")}.get(
         kind, ("hv_general", "hv_general_kernel + finalize per step"))
     vt = hphi_b200.REAL64
@@ -568,7 +570,8 @@ def finish(args, H_native, kind, kname, kdesc, desc, dim, balg, value, t_max, ac
                       "step": "one v0 += H v1 (mltply)", "b_alg_bytes": balg,
                       "l2": "inputs larger than L2 (1.3 GB vectors), no flush",
                       "parallelism": "replicas" if world > 1 else "single",
-                      "vector_order": {2: "native (up-rank x down-rank product matrix)",
+                      "vector_order": {3: "native (up-rank x down-rank product matrix)",
+                                       2: "native (up-rank x down-rank product matrix)",
                                        1: "native (per-block up x down product order)"}.get(kind, "HPhi"),
                       "hphi_order_ms_per_step": hphi_order_ms},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -26,10 +26,24 @@
 // rebuilt from per-species tables plus U * popcount(u & d) (or read when it has other
 // cross-species terms).  Each row's <v1|H v1> contribution is reduced in the CTA and summed
 // over rows in a fixed order afterwards, so results do not depend on scheduling.
+//
+// Two-pass form (real vectors, down hops of one magnitude |t|; the default there).  H v is
+// split into a row pass (diagonal + down hops: every row is a gather inside itself) and a
+// column pass (up hops: whole source rows).  The row pass stages two rows per CTA in shared
+// memory and reads them through an edge-coloured gather table: within each slot of a warp,
+// the 16 lanes of a half-warp hit 16 different shared-memory bank pairs, so every 8-byte
+// gather takes the minimum two wavefronts; entries are 16-bit word indices with the hop's
+// sign in bit 15, eight per lane in one 16-byte load issued a column block ahead, and empty
+// slots point at zero words placed one per bank.  The column pass walks
+// the matrix in column chunks (all rows of chunk 0, then chunk 1, ...) so the source rows of
+// the chunk being processed stay in L2 while every row gathers its ~N/2 up-hop sources.
+// Both passes take their work by static striding (no dispenser) and keep per-CTA partial
+// sums of <v1|H v1>, so the result is reproducible.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdlib>
 #include <string>
 #include <vector>
@@ -206,6 +220,249 @@ __global__ void __launch_bounds__(kProdThreads, 2) prod_hv_kernel(ProdArgs a, co
   retire(counter);
 }
 
+constexpr int kDownThreads = 1024;            // row pass: one CTA per SM, two rows at a time
+constexpr int kRow2Bytes = 103168;            // shared-memory offset of the second row (>= (12870 + 16) * 8)
+constexpr int kUpThreads = 256;               // column pass
+constexpr int kUpChunk = 2 * kUpThreads;      // columns per column-pass task (two per thread)
+
+struct TwoPassArgs {
+  int npad;                    // Dc rounded up to a multiple of 32
+  int groups;                  // slot groups of 8 stored per warp (max over warps)
+  const uint4 *gat;            // [npad / 32][groups][32 lanes] 8 entries: word | sign << 15
+  const uint8_t *wslots;       // [npad / 32] slots of each warp's 32 columns
+  double t_dn;                 // magnitude of every down hop
+  double t_up;                 // magnitude of every up hop (up_uniform)
+  int up_uniform;              // usrc carries the sign in bit 31 and ucf is unused
+  const int *usrc;             // [Uc][wu] up-hop source rank
+  const double *ucf;           // [Uc][wu] up-hop coefficient
+  const uint8_t *nus;          // [Uc] up hops of each row
+};
+
+__device__ __forceinline__ double flip_sign(double x, uint32_t sg) {
+  return __hiloint2double(__double2hiint(x) ^ (int)sg, __double2loint(x));
+}
+
+// Row pass: v0[u, :] = acc * v0[u, :] + scale * (D + down hops) v1[u, :] for two rows at a time;
+// part[blockIdx] = sum over the CTA's rows of v1 . (D + down) v1.
+__global__ void __launch_bounds__(kDownThreads, 1) prod_down_kernel(ProdArgs a, TwoPassArgs b,
+                                                                   const double *__restrict__ v1,
+                                                                   double *__restrict__ v0,
+                                                                   const double *__restrict__ coef,
+                                                                   double *__restrict__ part) {
+  extern __shared__ double rows[];  // row 0 at 0, row 1 at kRow2Bytes; each Dc + 16 words
+  double *row1 = rows + kRow2Bytes / 8;
+  const double acc = coef[0], scale = coef[1];
+  const int Dc = a.Dc, Uc = a.Uc;
+  const char *rb = reinterpret_cast<const char *>(rows);
+  double pr = 0.0;
+  // rows are copied with cp.async: 16-byte pieces when the rows start on 16-byte boundaries
+  const bool v16 = (Dc % 2 == 0) && ((uintptr_t)v1 % 16 == 0);
+  const uint32_t sm0 = (uint32_t)__cvta_generic_to_shared(rows), sm1 = sm0 + kRow2Bytes;
+  for (int u0 = 2 * blockIdx.x; u0 < Uc; u0 += 2 * gridDim.x) {
+    const bool two = u0 + 1 < Uc;
+    __syncthreads();  // the previous rows are no longer read
+    const double *s0 = v1 + (int64_t)u0 * Dc;
+    const double *s1 = two ? s0 + Dc : s0;
+    if (v16) {
+      for (int i = threadIdx.x; i < Dc / 2; i += kDownThreads) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sm0 + 16 * i), "l"(s0 + 2 * i) : "memory");
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sm1 + 16 * i), "l"(s1 + 2 * i) : "memory");
+      }
+    } else {
+      for (int i = threadIdx.x; i < Dc; i += kDownThreads) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sm0 + 8 * i), "l"(s0 + i) : "memory");
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sm1 + 8 * i), "l"(s1 + i) : "memory");
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    if (threadIdx.x < 16) {
+      rows[Dc + threadIdx.x] = 0.0;
+      row1[Dc + threadIdx.x] = 0.0;
+    }
+    // the next pair's rows toward L2 while this pair is processed (a hint, no completion)
+    const int un = u0 + 2 * gridDim.x;
+    if (v16 && threadIdx.x < 2 && un + (int)threadIdx.x < Uc) {
+      const double *pf = v1 + (int64_t)(un + threadIdx.x) * Dc;
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(pf), "r"((uint32_t)(Dc * 8)) : "memory");
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+    const int ua1 = two ? u0 + 1 : u0;
+    const uint32_t uc0 = a.unrank_up[u0], uc1 = a.unrank_up[ua1];
+    const double du0 = a.du[u0], du1 = a.du[ua1];
+    const int lane = threadIdx.x & 31;
+    // entries of the first four slot groups of the next column block, loaded one block ahead
+    uint4 q[4];
+    auto load_block = [&](int pp, uint4 (&dst)[4]) {
+      const int w = pp >> 5, ng = (b.wslots[w] + 7) >> 3;
+      const uint4 *base = b.gat + ((int64_t)w * b.groups) * 32 + lane;
+#pragma unroll
+      for (int g = 0; g < 4; g++) dst[g] = (g < ng) ? __ldg(base + g * 32) : make_uint4(0, 0, 0, 0);
+    };
+    if ((int)threadIdx.x < b.npad) load_block(threadIdx.x, q);
+    for (int p = threadIdx.x; p < b.npad; p += kDownThreads) {
+      const int w = p >> 5, ns = b.wslots[w];  // the same for the warp's 32 columns
+      uint4 cur[4] = {q[0], q[1], q[2], q[3]};
+      if (p + kDownThreads < b.npad) load_block(p + kDownThreads, q);
+      // per-column diagonal parts, loaded before the gathers
+      const int pc = (p < Dc) ? p : Dc - 1;
+      const double ddp = (a.cross_mode == 2) ? 0.0 : __ldg(a.dd + pc);
+      const uint32_t cdp = __ldg(a.unrank_dn + pc);
+      double *o0 = v0 + (int64_t)u0 * Dc + pc;
+      const double y0old = (acc != 0.0) ? *o0 : 0.0;
+      const double y1old = (acc != 0.0 && two) ? o0[Dc] : 0.0;
+      double g0 = 0.0, g1 = 0.0;
+      auto gather2 = [&](uint32_t r, int slot) {
+        // two 16-bit entries: word index (15 bits) | sign << 15; every slot at or beyond the
+        // warp's count holds a zero word, so only whole words are skipped
+        if (slot < ns) {
+          const uint32_t o0 = (r << 3) & 0x3FFF8u, s0 = (r << 16) & 0x80000000u;
+          const uint32_t o1 = (r >> 13) & 0x3FFF8u, s1 = r & 0x80000000u;
+          g0 += flip_sign(*reinterpret_cast<const double *>(rb + o0), s0);
+          g1 += flip_sign(*reinterpret_cast<const double *>(rb + kRow2Bytes + o0), s0);
+          g0 += flip_sign(*reinterpret_cast<const double *>(rb + o1), s1);
+          g1 += flip_sign(*reinterpret_cast<const double *>(rb + kRow2Bytes + o1), s1);
+        }
+      };
+#pragma unroll
+      for (int g = 0; g < 4; g++) {
+        if (8 * g >= ns) break;
+        gather2(cur[g].x, 8 * g);
+        gather2(cur[g].y, 8 * g + 2);
+        gather2(cur[g].z, 8 * g + 4);
+        gather2(cur[g].w, 8 * g + 6);
+      }
+      for (int g = 4; 8 * g < ns; g++) {  // more than 32 slots: remaining groups loaded here
+        const uint4 e = __ldg(b.gat + ((int64_t)w * b.groups + g) * 32 + lane);
+        gather2(e.x, 8 * g);
+        gather2(e.y, 8 * g + 2);
+        gather2(e.z, 8 * g + 4);
+        gather2(e.w, 8 * g + 6);
+      }
+      if (p < Dc) {
+        auto diag = [&](int ua, uint32_t uc, double du) -> double {
+          if (a.cross_mode == 2) return __ldg(a.dfull + (int64_t)ua * Dc + p);
+          double D = du + ddp;
+          const uint32_t ud = uc & cdp;
+          if (a.cross_mode == 0) D += a.u0 * (double)__popc(ud);
+          else for (uint32_t m = ud; m; m &= m - 1) D += __ldg(a.usite + (__ffs(m) - 1));
+          return D;
+        };
+        const double x0 = rows[p], y0 = diag(u0, uc0, du0) * x0 + b.t_dn * g0;
+        *o0 = (acc == 0.0) ? scale * y0 : acc * y0old + scale * y0;
+        pr += x0 * y0;
+        if (two) {
+          const double x1 = row1[p], y1 = diag(ua1, uc1, du1) * x1 + b.t_dn * g1;
+          o0[Dc] = (acc == 0.0) ? scale * y1 : acc * y1old + scale * y1;
+          pr += x1 * y1;
+        }
+      }
+    }
+  }
+  double v[2] = {pr, 0.0};
+  block_sum<2>(v);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = v[0];
+    part[2 * blockIdx.x + 1] = 0.0;
+  }
+}
+
+// Column pass: v0[u, chunk] += scale * sum_up c * v1[u', chunk], chunk-major tasks by static
+// striding; part[blockIdx] = sum of v1 . (up hops) v1 over the CTA's tasks.  VEC2: Dc is even,
+// so a thread's two columns are one aligned 16-byte load.
+template <bool VEC2, bool UNIFORM>
+__global__ void __launch_bounds__(kUpThreads, 8) prod_up_kernel(ProdArgs a, TwoPassArgs b, const double *__restrict__ v1,
+                                                             double *__restrict__ v0, const double *__restrict__ coef,
+                                                             double *__restrict__ part) {
+  __shared__ int s_src[kMaxUpWidth];
+  __shared__ double s_cf[UNIFORM ? 1 : kMaxUpWidth];
+  const double scale = coef[1];
+  const int Dc = a.Dc, Uc = a.Uc, wu = a.wu;
+  const int nchunk = (Dc + kUpChunk - 1) / kUpChunk;
+  const int64_t ntask = (int64_t)nchunk * Uc;
+  double pr = 0.0;
+  for (int64_t task = blockIdx.x; task < ntask; task += gridDim.x) {
+    const int c = (int)(task / Uc), u = (int)(task - (int64_t)c * Uc);
+    const int nu = b.nus[u];
+    __syncthreads();
+    for (int k = threadIdx.x; k < nu; k += kUpThreads) {
+      s_src[k] = b.usrc[(int64_t)u * wu + k];
+      if (!UNIFORM) s_cf[k] = b.ucf[(int64_t)u * wu + k];
+    }
+    __syncthreads();
+    const int d = c * kUpChunk + 2 * (int)threadIdx.x;
+    if (d >= Dc) continue;
+    const bool pair = VEC2 || d + 1 < Dc;
+    double h0 = 0.0, h1 = 0.0;
+    int k = 0;
+    for (; k + 4 <= nu; k += 4) {
+      double w0[4], w1[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const double *sp = v1 + (int64_t)(s_src[k + q] & 0x7FFFFFFF) * Dc + d;
+        if (VEC2) {
+          const double2 sv = __ldg(reinterpret_cast<const double2 *>(sp));
+          w0[q] = sv.x; w1[q] = sv.y;
+        } else {
+          w0[q] = __ldg(sp);
+          w1[q] = pair ? __ldg(sp + 1) : 0.0;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        if (UNIFORM) {
+          const uint32_t sg = (uint32_t)s_src[k + q] & 0x80000000u;
+          h0 += flip_sign(w0[q], sg);
+          h1 += flip_sign(w1[q], sg);
+        } else {
+          h0 += s_cf[k + q] * w0[q];
+          h1 += s_cf[k + q] * w1[q];
+        }
+      }
+    }
+    for (; k < nu; k++) {
+      const double *sp = v1 + (int64_t)(s_src[k] & 0x7FFFFFFF) * Dc + d;
+      if (UNIFORM) {
+        const uint32_t sg = (uint32_t)s_src[k] & 0x80000000u;
+        h0 += flip_sign(__ldg(sp), sg);
+        if (pair) h1 += flip_sign(__ldg(sp + 1), sg);
+      } else {
+        h0 += s_cf[k] * __ldg(sp);
+        if (pair) h1 += s_cf[k] * __ldg(sp + 1);
+      }
+    }
+    if (UNIFORM) {
+      h0 *= b.t_up;
+      h1 *= b.t_up;
+    }
+    const double *xp = v1 + (int64_t)u * Dc + d;
+    double *yp = v0 + (int64_t)u * Dc + d;
+    double x0, x1 = 0.0, y0, y1 = 0.0;
+    if (VEC2) {
+      const double2 xv = __ldg(reinterpret_cast<const double2 *>(xp));
+      const double2 yv = *reinterpret_cast<const double2 *>(yp);
+      x0 = xv.x; x1 = xv.y; y0 = yv.x; y1 = yv.y;
+    } else {
+      x0 = __ldg(xp);
+      y0 = *yp;
+      if (pair) { x1 = __ldg(xp + 1); y1 = yp[1]; }
+    }
+    pr += x0 * h0 + x1 * h1;
+    if (VEC2) {
+      *reinterpret_cast<double2 *>(yp) = make_double2(y0 + scale * h0, y1 + scale * h1);
+    } else {
+      *yp = y0 + scale * h0;
+      if (pair) yp[1] = y1 + scale * h1;
+    }
+  }
+  double v[2] = {pr, 0.0};
+  block_sum<2>(v);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = v[0];
+    part[2 * blockIdx.x + 1] = 0.0;
+  }
+}
+
 __device__ __forceinline__ uint32_t compress_species(uint64_t c, int s, int N) {
   uint32_t x = 0;
   for (int i = 0; i < N; i++) x |= (uint32_t)((c >> (2 * i + s)) & 1ull) << i;
@@ -276,8 +533,12 @@ struct ProdPlan {
   std::vector<void *> allocs;
   int grid = 0;
   size_t smem[2] = {0, 0};  // real, complex
-  double *part = nullptr;   // 2 * Uc row partial sums
+  double *part = nullptr;   // partial sums: 2 * max(Uc, grid_dn + grid_up)
   int *counter = nullptr;
+  bool two_pass = false;    // real vectors take the two-pass kernels
+  TwoPassArgs tp{};
+  int grid_dn = 0, grid_up = 0;
+  size_t smem_dn = 0;
 };
 
 void prod_plan_free(ProdPlan *p) {
@@ -345,6 +606,104 @@ uint64_t spread_species(uint32_t x, int s, int N) {
   for (int i = 0; i < N; i++)
     if ((x >> i) & 1u) c |= 1ull << (2 * i + s);
   return c;
+}
+
+// Gather table of the row pass.  Column p belongs to warp p / 32 and half-warp (p / 16) % 2;
+// the entries of the 16 columns of a half-warp form a bipartite multigraph between lanes and
+// shared-memory bank pairs (source word mod 16).  A proper edge colouring with Delta colours
+// (Delta = its largest degree; Konig's theorem, built by swapping alternating paths) gives
+// slots in which every lane and every bank pair carries at most one entry.  Lanes left
+// without an entry in a slot read a zero word of a bank pair that slot leaves free (words
+// Dc .. Dc+15, one per bank pair).  Stored packed: per warp and group of 8 slots, each lane's
+// 8 entries (16 bits: word | sign << 15) are one 16-byte load.
+void build_gather(const std::vector<std::vector<uint32_t>> &rows_dn, const std::vector<SpeciesHop> &hops, int Dc,
+                  int npad, std::vector<uint32_t> *gat, std::vector<uint8_t> *wslots, int *nslots, int *groups) {
+  const int nwarp = npad / 32;
+  auto zero_word = [&](int bank) { return (uint32_t)(Dc + (((bank - Dc) % 16) + 16) % 16); };
+  std::vector<std::vector<uint32_t>> lane_slots(npad);  // per column: entry of each slot of its half
+  wslots->assign(nwarp, 0);
+  *nslots = 0;
+  for (int w = 0; w < nwarp; w++) {
+    int wmax = 0;
+    for (int hw = 0; hw < 2; hw++) {
+      std::vector<int> el, eb;
+      std::vector<uint32_t> ev;
+      for (int l = 0; l < 16; l++) {
+        const int col = 32 * w + 16 * hw + l;
+        if (col >= Dc) continue;
+        for (uint32_t e : rows_dn[col]) {
+          const uint32_t word = e & 0xFFFFu, h = (e >> 16) >> 1, sign = (e >> 16) & 1u;
+          const bool neg = ((hops[h].re < 0) != (sign != 0));
+          el.push_back(l);
+          eb.push_back((int)(word % 16));
+          ev.push_back((word * 8u) | (neg ? 0x80000000u : 0u));
+        }
+      }
+      int ldeg[16] = {0}, bdeg[16] = {0};
+      for (size_t i = 0; i < el.size(); i++) { ldeg[el[i]]++; bdeg[eb[i]]++; }
+      int D = 0;
+      for (int i = 0; i < 16; i++) D = std::max(D, std::max(ldeg[i], bdeg[i]));
+      std::vector<int> L(16 * std::max(D, 1), -1), B(16 * std::max(D, 1), -1), colr(el.size(), -1);
+      for (size_t i = 0; i < el.size(); i++) {
+        const int l = el[i], bk = eb[i];
+        int a = 0, c = 0;
+        while (L[l * D + a] >= 0) a++;
+        while (B[bk * D + c] >= 0) c++;
+        if (B[bk * D + a] >= 0) {
+          // alternating a/c path from bank bk; swapping it frees a at bk
+          std::vector<int> path;
+          int node = bk, want = a;
+          bool at_bank = true;
+          for (;;) {
+            const int ed = at_bank ? B[node * D + want] : L[node * D + want];
+            if (ed < 0) break;
+            path.push_back(ed);
+            node = at_bank ? el[ed] : eb[ed];
+            at_bank = !at_bank;
+            want = (want == a) ? c : a;
+          }
+          for (int ed : path) { L[el[ed] * D + colr[ed]] = -1; B[eb[ed] * D + colr[ed]] = -1; }
+          for (int ed : path) colr[ed] = (colr[ed] == a) ? c : a;
+          for (int ed : path) { L[el[ed] * D + colr[ed]] = ed; B[eb[ed] * D + colr[ed]] = ed; }
+        }
+        colr[i] = a;
+        L[l * D + a] = (int)i;
+        B[bk * D + a] = (int)i;
+      }
+      for (int l = 0; l < 16; l++) lane_slots[32 * w + 16 * hw + l].assign(D, 0u);
+      for (int c = 0; c < D; c++) {
+        std::vector<int> free_banks;
+        for (int bk = 0; bk < 16; bk++)
+          if (B[bk * D + c] < 0) free_banks.push_back(bk);
+        size_t f = 0;
+        for (int l = 0; l < 16; l++) {
+          const int ed = L[l * D + c];
+          lane_slots[32 * w + 16 * hw + l][c] = (ed >= 0) ? ev[ed] : zero_word(free_banks[f++]) * 8u;
+        }
+      }
+      wmax = std::max(wmax, D);
+    }
+    (*wslots)[w] = (uint8_t)wmax;
+    *nslots = std::max(*nslots, wmax);
+  }
+  // packed: per warp and slot group g, 32 lanes x 8 entries of 16 bits (word | sign << 15)
+  *groups = std::max(1, (*nslots + 7) / 8);
+  gat->assign((size_t)nwarp * *groups * 32 * 4, 0u);
+  for (int p = 0; p < npad; p++) {
+    const int w = p / 32, lane = p % 32, l = p % 16;
+    for (int sl = 0; sl < 8 * *groups; sl++) {
+      uint32_t word, neg = 0;
+      if (sl < (int)lane_slots[p].size()) {
+        word = (lane_slots[p][sl] & 0x7FFFFFFFu) / 8u;
+        neg = lane_slots[p][sl] >> 31;
+      } else {
+        word = zero_word(l);
+      }
+      const uint32_t e16 = word | (neg << 15);
+      const size_t q = (((size_t)w * *groups + sl / 8) * 32 + lane) * 4 + (sl % 8) / 2;
+      (*gat)[q] |= (sl % 2) ? (e16 << 16) : e16;
+    }
+  }
 }
 
 }  // namespace
@@ -511,11 +870,97 @@ int prod_plan_build(Sector *s, std::string *err) {
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, prod_hv_kernel<double>, kProdThreads, smem_r);
   p->grid = std::max(1, std::min(Uc, std::max(1, per_sm) * s->num_sms));
+  // Two-pass kernels (real vectors): every down hop of one magnitude, real up hops, the
+  // second staged row at its fixed offset.  HPHI_B200_PROD=single keeps the one-pass kernel.
+  {
+    const char *pe = getenv("HPHI_B200_PROD");
+    bool ok = !(pe && std::string(pe) == "single") && !hops[1].empty() && (size_t)(Dc + 16) * 8 <= (size_t)kRow2Bytes &&
+              wd <= 255;
+    const double tmag = hops[1].empty() ? 0.0 : std::fabs(hops[1][0].re);
+    for (const SpeciesHop &h : hops[1]) ok = ok && h.im == 0.0 && std::fabs(h.re) == tmag && tmag > 0.0;
+    for (const SpeciesHop &h : hops[0]) ok = ok && h.im == 0.0;
+    if (ok) {
+      TwoPassArgs &b = p->tp;
+      b.npad = (Dc + 31) / 32 * 32;
+      b.t_dn = tmag;
+      std::vector<uint32_t> gat;
+      std::vector<uint8_t> wslots;
+      int nslots = 0;
+      build_gather(rows_dn, hops[1], Dc, b.npad, &gat, &wslots, &nslots, &b.groups);
+      std::vector<uint4> gat4(gat.size() / 4);
+      for (size_t i = 0; i < gat4.size(); i++) gat4[i] = make_uint4(gat[4 * i], gat[4 * i + 1], gat[4 * i + 2], gat[4 * i + 3]);
+      b.t_up = hops[0].empty() ? 0.0 : std::fabs(hops[0][0].re);
+      b.up_uniform = b.t_up > 0.0 ? 1 : 0;
+      for (const SpeciesHop &h : hops[0]) b.up_uniform = b.up_uniform && std::fabs(h.re) == b.t_up;
+      const int wuu = std::max(wu, 1);
+      std::vector<int> usrc((size_t)Uc * wuu, 0);
+      std::vector<double> ucf((size_t)Uc * wuu, 0.0);
+      std::vector<uint8_t> nus(Uc, 0);
+      for (int r = 0; r < Uc; r++) {
+        for (size_t k = 0; k < rows_up[r].size(); k++) {
+          const uint32_t e = rows_up[r][k], h = (e >> 16) >> 1, sign = (e >> 16) & 1u;
+          const double cf = sign ? -hops[0][h].re : hops[0][h].re;
+          usrc[(size_t)r * wuu + k] = (int)(e & 0xFFFFu) | ((b.up_uniform && cf < 0) ? (int)0x80000000 : 0);
+          ucf[(size_t)r * wuu + k] = cf;
+        }
+        nus[r] = (uint8_t)rows_up[r].size();
+      }
+      if (upload(p, gat4, &b.gat, err) || upload(p, wslots, &b.wslots, err) || upload(p, usrc, &b.usrc, err) ||
+          upload(p, ucf, &b.ucf, err) || upload(p, nus, &b.nus, err))
+        return fail();
+      p->smem_dn = (size_t)kRow2Bytes + (size_t)(Dc + 16) * 8;
+      if (cudaFuncSetAttribute(prod_down_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_dn) !=
+          cudaSuccess) {
+        *err = "product plan: shared-memory attribute rejected (row pass)";
+        return fail();
+      }
+      int up_per_sm = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&up_per_sm, prod_up_kernel<true, true>, kUpThreads, 0);
+      p->grid_dn = std::max(1, std::min((Uc + 1) / 2, s->num_sms));
+      p->grid_up = std::max(1, std::max(1, up_per_sm) * s->num_sms);
+      p->two_pass = true;
+      if (2 * (p->grid_dn + p->grid_up) > 2 * Uc) {
+        cudaFree(p->part);
+        p->allocs.erase(std::find(p->allocs.begin(), p->allocs.end(), (void *)p->part));
+        p->part = nullptr;
+        if (cudaMalloc(&p->part, sizeof(double) * 2 * (size_t)(p->grid_dn + p->grid_up)) != cudaSuccess) {
+          *err = "product plan: device allocation failed";
+          return fail();
+        }
+        p->allocs.push_back(p->part);
+      }
+    }
+  }
   s->prod = p;
   return 0;
 }
 
-size_t prod_scratch_doubles(const Sector *s) { return 2 * (size_t)s->prod->args.Uc; }
+bool prod_two_pass(const Sector *s) { return s->prod && s->prod->two_pass; }
+
+size_t prod_scratch_doubles(const Sector *s) {
+  const ProdPlan *p = s->prod;
+  return 2 * std::max((size_t)p->args.Uc, (size_t)(p->grid_dn + p->grid_up));
+}
+
+namespace {
+// Row pass then column pass; partial sums at d_part (grid_dn + grid_up records of 2).
+void two_pass_launch(Sector *s, const double *v1, double *v0, const double *d_coef, double *d_out, double *d_part) {
+  ProdPlan *p = s->prod;
+  prod_down_kernel<<<p->grid_dn, kDownThreads, p->smem_dn, s->stream>>>(p->args, p->tp, v1, v0, d_coef, d_part);
+  const bool vec2 = (p->args.Dc % 2 == 0) && ((((uintptr_t)v1) | ((uintptr_t)v0)) % 16 == 0);
+  double *pu = d_part + 2 * p->grid_dn;
+  const int g = p->grid_up;
+  if (vec2 && p->tp.up_uniform)
+    prod_up_kernel<true, true><<<g, kUpThreads, 0, s->stream>>>(p->args, p->tp, v1, v0, d_coef, pu);
+  else if (vec2)
+    prod_up_kernel<true, false><<<g, kUpThreads, 0, s->stream>>>(p->args, p->tp, v1, v0, d_coef, pu);
+  else if (p->tp.up_uniform)
+    prod_up_kernel<false, true><<<g, kUpThreads, 0, s->stream>>>(p->args, p->tp, v1, v0, d_coef, pu);
+  else
+    prod_up_kernel<false, false><<<g, kUpThreads, 0, s->stream>>>(p->args, p->tp, v1, v0, d_coef, pu);
+  finalize_partials_kernel<2><<<1, 256, 0, s->stream>>>(d_part, p->grid_dn + p->grid_up, d_out);
+}
+}  // namespace
 
 int prod_hv_launch_scratch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out,
                            double *d_part, int *d_counter) {
@@ -523,6 +968,10 @@ int prod_hv_launch_scratch(Sector *s, VecType vt, const void *d_v1, void *d_v0, 
   if (vt == kReal64 && s->model.complex_terms) {
     set_error("H has complex coefficients: real vectors are not allowed");
     return -1;
+  }
+  if (vt == kReal64 && p->two_pass) {
+    two_pass_launch(s, (const double *)d_v1, (double *)d_v0, d_coef, d_out, d_part);
+    return cuda_ok(cudaGetLastError(), "launch");
   }
   if (cudaMemsetAsync(d_counter, 0, 2 * sizeof(int), s->stream) != cudaSuccess) {
     set_error("product kernel: clearing the row counter failed");
@@ -543,6 +992,10 @@ int prod_hv_launch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const do
   if (vt == kReal64 && s->model.complex_terms) {
     set_error("H has complex coefficients: real vectors are not allowed");
     return -1;
+  }
+  if (vt == kReal64 && p->two_pass) {
+    two_pass_launch(s, (const double *)d_v1, (double *)d_v0, d_coef, d_out, p->part);
+    return cuda_ok(cudaGetLastError(), "launch");
   }
   if (vt == kReal64)
     prod_hv_kernel<double><<<p->grid, kProdThreads, p->smem[0], s->stream>>>(

@@ -14,21 +14,25 @@ torch = pytest.importorskip("torch")
 
 
 def _open(path, general=False, kernel=None):
-    """kernel: None (default plan: product layout where it applies), "block" or "general"."""
-    old = os.environ.get("HPHI_B200_KERNEL")
+    """kernel: None (default plan: product layout where it applies, two-pass kernels for real
+    vectors), "single" (product layout, one-pass kernel), "block" or "general"."""
+    saved = {k: os.environ.get(k) for k in ("HPHI_B200_KERNEL", "HPHI_B200_PROD")}
     if general:
         kernel = "general"
-    if kernel:
+    os.environ.pop("HPHI_B200_KERNEL", None)
+    os.environ.pop("HPHI_B200_PROD", None)
+    if kernel == "single":
+        os.environ["HPHI_B200_PROD"] = "single"
+    elif kernel:
         os.environ["HPHI_B200_KERNEL"] = kernel
-    else:
-        os.environ.pop("HPHI_B200_KERNEL", None)
     try:
         return hphi_b200.Hamiltonian(path)
     finally:
-        if old is None:
-            os.environ.pop("HPHI_B200_KERNEL", None)
-        else:
-            os.environ["HPHI_B200_KERNEL"] = old
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
 
 
 def _hv_device(H, v1, v0, vt, acc=1.0, scale=1.0):
@@ -62,11 +66,11 @@ def _with_inter():
     return m
 
 
-@pytest.mark.parametrize("kernel", [None, "block"])
+@pytest.mark.parametrize("kernel", [None, "single", "block"])
 @pytest.mark.parametrize("name", list(MODELS))
 def test_block_kernel_matches_general_kernel(name, kernel, tmp_path):
-    """Native-order kernels (product layout by default, the block plan on request) against
-    the general kernel."""
+    """Native-order kernels (product layout by default, two-pass for real vectors; the
+    one-pass product kernel and the block plan on request) against the general kernel."""
     path = MODELS[name]().write(str(tmp_path))
     Hf = _open(path, kernel=kernel)
     Hg = _open(path, general=True)
@@ -80,12 +84,28 @@ def test_block_kernel_matches_general_kernel(name, kernel, tmp_path):
         vt = hphi_b200.COMPLEX128 if cplx else hphi_b200.REAL64
         v1 = torch.randn(dim, dtype=dt, device="cuda", generator=g)
         v0 = torch.randn(dim, dtype=dt, device="cuda", generator=g)
+        # two-pass kernels need real vectors and down hops of one magnitude (a periodic
+        # direction of width 2 doubles its hoppings, so only hub3x4 is sure to qualify)
+        if kernel is None:
+            assert Hf.info["kernel"] in ((3,) if name == "hub3x4" else (2, 3))
+        else:
+            assert Hf.info["kernel"] == {"single": 2, "block": 1}[kernel]
         for acc, scale in ((1.0, 1.0), (0.0, 1.0), (-0.75, 1.3)):
             yf, pf = _hv_device(Hf, v1, v0, vt, acc, scale)
             yg, pg = _hv_device(Hg, v1, v0, vt, acc, scale)
             err = (yf - yg).abs().max().item() / yg.abs().max().item()
             assert err < 1e-12, (acc, scale, err)
             assert abs(pf - pg) < 1e-10 * abs(pg)
+        # vectors that start 8 bytes past a 16-byte boundary (no paired 16-byte loads)
+        b1 = torch.empty(dim + 1, dtype=dt, device="cuda")
+        b0 = torch.empty(dim + 1, dtype=dt, device="cuda")
+        o1, o0 = b1[1:], b0[1:]
+        o1.copy_(v1)
+        o0.copy_(v0)
+        pf = Hf.mltply_device(o0.data_ptr(), o1.data_ptr(), vt, acc=0.5, scale=1.0)
+        yg, pg = _hv_device(Hg, v1, v0, vt, 0.5, 1.0)
+        assert (o0 - yg).abs().max().item() < 1e-12 * yg.abs().max().item()
+        assert abs(pf - pg) < 1e-10 * abs(pg)
         # native order round trip
         nat = torch.empty_like(v1)
         back = torch.empty_like(v1)
@@ -122,7 +142,7 @@ def test_product_and_block_plans_agree_full_size_4x4(tmp_path):
     path = expert.hubbard(16, expert.square_bonds(4, 4), 1.0, 8.0, 8, 8).write(str(tmp_path))
     g = torch.Generator(device="cuda").manual_seed(21)
     out = []
-    for kernel in (None, "block"):
+    for kernel in (None, "single", "block"):
         H = _open(path, kernel=kernel)
         if not out:
             v = torch.rand(H.dim, dtype=torch.float64, device="cuda", generator=g) - 0.5
@@ -130,9 +150,11 @@ def test_product_and_block_plans_agree_full_size_4x4(tmp_path):
         y, pr = _hv_device(H, v, zero, hphi_b200.REAL64, acc=0.0)
         out.append((y, pr))
         H.close()
-    err = (out[0][0] - out[1][0]).abs().max().item() / out[1][0].abs().max().item()
-    assert err < 1e-12
-    assert abs(out[0][1] - out[1][1]) < 1e-11 * abs(out[1][1])
+    ref_y, ref_pr = out[-1]   # block plan
+    for y, pr in out[:-1]:
+        err = (y - ref_y).abs().max().item() / ref_y.abs().max().item()
+        assert err < 1e-12
+        assert abs(pr - ref_pr) < 1e-11 * abs(ref_pr)
 
 
 def test_full_size_hubbard4x4_block_vs_general(tmp_path):
