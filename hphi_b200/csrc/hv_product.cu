@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(kProdThreads, 2) prod_hv_kernel(ProdArgs a, co
 
 constexpr int kDownThreads = 1024;            // row pass: one CTA per SM, two rows at a time
 constexpr int kRow2Bytes = 103168;            // shared-memory offset of the second row (>= (12870 + 16) * 8)
-constexpr int kUpThreads = 256;               // column pass
+constexpr int kUpThreads = 128;               // column pass
 constexpr int kUpChunk = 2 * kUpThreads;      // columns per column-pass task (two per thread)
 
 struct TwoPassArgs {
@@ -309,8 +309,8 @@ __global__ void __launch_bounds__(kDownThreads, 1) prod_down_kernel(ProdArgs a, 
       const double ddp = (a.cross_mode == 2) ? 0.0 : __ldg(a.dd + pc);
       const uint32_t cdp = __ldg(a.unrank_dn + pc);
       double *o0 = v0 + (int64_t)u0 * Dc + pc;
-      const double y0old = (acc != 0.0) ? *o0 : 0.0;
-      const double y1old = (acc != 0.0 && two) ? o0[Dc] : 0.0;
+      const double y0old = (acc != 0.0) ? __ldcs(o0) : 0.0;
+      const double y1old = (acc != 0.0 && two) ? __ldcs(o0 + Dc) : 0.0;
       double g0 = 0.0, g1 = 0.0;
       auto gather2 = [&](uint32_t r, int slot) {
         // two 16-bit entries: word index (15 bits) | sign << 15; every slot at or beyond the
@@ -349,11 +349,11 @@ __global__ void __launch_bounds__(kDownThreads, 1) prod_down_kernel(ProdArgs a, 
           return D;
         };
         const double x0 = rows[p], y0 = diag(u0, uc0, du0) * x0 + b.t_dn * g0;
-        *o0 = (acc == 0.0) ? scale * y0 : acc * y0old + scale * y0;
+        __stcs(o0, (acc == 0.0) ? scale * y0 : acc * y0old + scale * y0);
         pr += x0 * y0;
         if (two) {
           const double x1 = row1[p], y1 = diag(ua1, uc1, du1) * x1 + b.t_dn * g1;
-          o0[Dc] = (acc == 0.0) ? scale * y1 : acc * y1old + scale * y1;
+          __stcs(o0 + Dc, (acc == 0.0) ? scale * y1 : acc * y1old + scale * y1);
           pr += x1 * y1;
         }
       }
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(kDownThreads, 1) prod_down_kernel(ProdArgs a, 
 // striding; part[blockIdx] = sum of v1 . (up hops) v1 over the CTA's tasks.  VEC2: Dc is even,
 // so a thread's two columns are one aligned 16-byte load.
 template <bool VEC2, bool UNIFORM>
-__global__ void __launch_bounds__(kUpThreads, 8) prod_up_kernel(ProdArgs a, TwoPassArgs b, const double *__restrict__ v1,
+__global__ void __launch_bounds__(kUpThreads, 2048 / kUpThreads) prod_up_kernel(ProdArgs a, TwoPassArgs b, const double *__restrict__ v1,
                                                              double *__restrict__ v0, const double *__restrict__ coef,
                                                              double *__restrict__ part) {
   __shared__ int s_src[kMaxUpWidth];
@@ -438,21 +438,23 @@ __global__ void __launch_bounds__(kUpThreads, 8) prod_up_kernel(ProdArgs a, TwoP
     const double *xp = v1 + (int64_t)u * Dc + d;
     double *yp = v0 + (int64_t)u * Dc + d;
     double x0, x1 = 0.0, y0, y1 = 0.0;
+    // v0 is streamed (read and written once): evict-first, so it does not push the chunk of
+    // v1 that the following rows gather from out of L2
     if (VEC2) {
       const double2 xv = __ldg(reinterpret_cast<const double2 *>(xp));
-      const double2 yv = *reinterpret_cast<const double2 *>(yp);
+      const double2 yv = __ldcs(reinterpret_cast<const double2 *>(yp));
       x0 = xv.x; x1 = xv.y; y0 = yv.x; y1 = yv.y;
     } else {
       x0 = __ldg(xp);
-      y0 = *yp;
-      if (pair) { x1 = __ldg(xp + 1); y1 = yp[1]; }
+      y0 = __ldcs(yp);
+      if (pair) { x1 = __ldg(xp + 1); y1 = __ldcs(yp + 1); }
     }
     pr += x0 * h0 + x1 * h1;
     if (VEC2) {
-      *reinterpret_cast<double2 *>(yp) = make_double2(y0 + scale * h0, y1 + scale * h1);
+      __stcs(reinterpret_cast<double2 *>(yp), make_double2(y0 + scale * h0, y1 + scale * h1));
     } else {
-      *yp = y0 + scale * h0;
-      if (pair) yp[1] = y1 + scale * h1;
+      __stcs(yp, y0 + scale * h0);
+      if (pair) __stcs(yp + 1, y1 + scale * h1);
     }
   }
   double v[2] = {pr, 0.0};
