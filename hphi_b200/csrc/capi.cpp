@@ -148,7 +148,16 @@ int hphi_info(const hphi_handle *h, int64_t *info, int n) {
 int hphi_sz(const hphi_handle *h, uint64_t *list_1, uint64_t *list_2_1, uint64_t *list_2_2) {
   CHECK_HANDLE(h);
   const Sector &s = *h->sector;
-  if (s.gc) { set_error("grand-canonical models have no sector lists"); return -1; }
+  if (s.model.is_gc()) { set_error("grand-canonical models have no sector lists"); return -1; }
+  if (s.model.general_spin) {  // HPhi's mixed-radix lists, kept on the host
+    if (list_1) {
+      list_1[0] = 0;
+      std::memcpy(list_1 + 1, s.gs_list_1.data() + 1, sizeof(uint64_t) * s.dim);
+    }
+    if (list_2_1) std::memcpy(list_2_1, s.gs_list_2_1.data(), sizeof(uint64_t) * s.size_list_2_1);
+    if (list_2_2) std::memcpy(list_2_2, s.gs_list_2_2.data(), sizeof(uint64_t) * s.size_list_2_2);
+    return 0;
+  }
   cudaSetDevice(s.device);
   if (list_1) {
     list_1[0] = 0;

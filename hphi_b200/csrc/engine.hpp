@@ -74,6 +74,9 @@ struct Sector {
   // Product-layout plan (canonical Hubbard); preferred over the block plan when both apply.
   ProdPlan *prod = nullptr;
   SplitPlan split;
+  // General spin: the device tables above are indexed by packed digit codes; HPhi's own
+  // mixed-radix lists (src/sz.c:795-830, 1564-1590) are kept here for export.
+  std::vector<uint64_t> gs_list_1, gs_list_2_1, gs_list_2_2;
 };
 
 // specialise = false skips the specialised kernel plans (the batched engine uses the

@@ -117,18 +117,30 @@ bool compile_fermion(const std::vector<FermionOp> &ops, uint64_t *req_mask, uint
   return true;
 }
 
-bool compile_spin(const std::vector<SpinOp> &ops, uint64_t *req_mask, uint64_t *req_val, uint64_t *flip) {
-  uint64_t rm = 0, rv = 0, fl = 0;
+// Spin strings on packed digit fields (site_bits bits per site; 1 for S = 1/2): each
+// |to><from| requires the site's current digit to be `from` and sets it to `to`.  Push form:
+// a source s with (s & req_mask) == req_val maps to s ^ flip (the fields it touches go from
+// their required values to their final values).
+bool compile_spin(const std::vector<SpinOp> &ops, int site_bits, uint64_t *req_mask, uint64_t *req_val,
+                  uint64_t *flip) {
+  uint64_t rm = 0, rv = 0;
+  std::map<int, int> cur;  // current digit of each touched site
   for (int k = (int)ops.size() - 1; k >= 0; k--) {
-    const uint64_t b = 1ull << ops[k].site;
-    const int need_orig = ops[k].from ^ ((fl & b) ? 1 : 0);
-    if (rm & b) {
-      if ((int)((rv & b) ? 1 : 0) != need_orig) return false;
+    const int sh = site_bits * ops[k].site;
+    const uint64_t fm = ((1ull << site_bits) - 1) << sh;
+    auto it = cur.find(ops[k].site);
+    if (it != cur.end()) {
+      if (it->second != ops[k].from) return false;
     } else {
-      rm |= b;
-      if (need_orig) rv |= b;
+      rm |= fm;
+      rv |= (uint64_t)ops[k].from << sh;
     }
-    if (ops[k].to != ops[k].from) fl ^= b;
+    cur[ops[k].site] = ops[k].to;
+  }
+  uint64_t fl = 0;
+  for (const auto &kv : cur) {
+    const int sh = site_bits * kv.first;
+    fl |= (((rv >> sh) ^ (uint64_t)kv.second) & ((1ull << site_bits) - 1)) << sh;
   }
   *req_mask = rm; *req_val = rv; *flip = fl;
   return true;
@@ -159,7 +171,7 @@ bool add_fermion_string(Model *m, const std::vector<FermionOp> &ops, std::comple
 
 bool add_spin_string(Model *m, const std::vector<SpinOp> &ops, std::complex<double> coef) {
   uint64_t rm, rv, fl;
-  if (!compile_spin(ops, &rm, &rv, &fl)) return false;
+  if (!compile_spin(ops, m->site_bits, &rm, &rv, &fl)) return false;
   push_term(m, rm, rv, fl, 0, 0, coef);
   return true;
 }
@@ -335,10 +347,13 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
     for (int i = 0; i < m->nsite; i++)
       if (m->locspn[i] < 0) { *err = "locspn.def: missing site"; return -1; }
     for (int i = 0; i < m->nsite; i++) {
-      if (m->is_spin() && m->locspn[i] != 1) {
-        *err = "locspn.def: only S=1/2 spins (2S=1) are supported by this engine";
+      // CheckLocSpin (src/readdef.c:2725-2765): spin sites have 2S >= 1; 2S > 1 anywhere
+      // makes the model a general-spin one
+      if (m->is_spin() && m->locspn[i] < 1) {
+        *err = "locspn.def: spin sites need 2S >= 1";
         return -1;
       }
+      if (m->is_spin() && m->locspn[i] > 1) m->general_spin = true;
       if ((m->calc_model == kHubbard || m->calc_model == kHubbardGC) && m->locspn[i] != 0) {
         *err = "locspn.def: Hubbard models need itinerant sites (0)";
         return -1;
@@ -392,8 +407,16 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       }
   }
   const bool spin = m->is_spin();
-  m->nbits = spin ? m->nsite : 2 * m->nsite;
+  if (m->general_spin) {
+    int maxs = 1;
+    for (int i = 0; i < m->nsite; i++) maxs = std::max(maxs, m->locspn[i]);
+    m->site_bits = 1;
+    while ((1 << m->site_bits) < maxs + 1) m->site_bits++;
+  }
+  m->nbits = spin ? m->site_bits * m->nsite : 2 * m->nsite;
   if (m->nbits > 64) { *err = "too many sites for 64-bit configurations"; return -1; }
+  // two-spin-state index range of a site (0 .. 2S_i; 0 .. 1 for fermions)
+  auto sigma_ok = [&](int site, int g) { return g >= 0 && g <= (spin ? m->locspn[site] : 1); };
 
   auto fbit = [&](int site, int s) { return 2 * site + s; };
   auto check_site = [&](int i) { return i >= 0 && i < m->nsite; };
@@ -407,8 +430,11 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
     std::vector<std::tuple<int, int, int, int>> order;
     for (const auto &r : rows) {
       const int i = (int)r[0], s1 = (int)r[1], j = (int)r[2], s2 = (int)r[3];
-      if (!check_site(i) || !check_site(j) || s1 < 0 || s1 > 1 || s2 < 0 || s2 > 1) {
+      if (!check_site(i) || !check_site(j) || !sigma_ok(i, s1) || !sigma_ok(j, s2)) {
         *err = files["trans"] + ": bad site or spin index"; return -1;
+      }
+      if (m->general_spin && m->calc_model == kSpin && s1 != s2) {
+        *err = files["trans"] + ": a canonical general-spin model only takes diagonal transfers"; return -1;
       }
       if (i == j && s1 == s2 && std::fabs(r[5]) > 1e-12) {
         *err = files["trans"] + ": diagonal transfer with an imaginary part"; return -1;
@@ -440,6 +466,10 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
     }
     m->n_trans = (int)rows.size();
   }
+  // General spin takes its interactions as InterAll only (src/readdef.c:2027-2044).
+  if (m->general_spin)
+    for (const char *k : {"coulombintra", "coulombinter", "hund", "pairhop", "exchange", "ising", "pairlift"})
+      if (files.count(k)) { *err = std::string(k) + ": general spin takes interactions as InterAll only"; return -1; }
   // ---- CoulombIntra
   if (files.count("coulombintra")) {
     if (!read_table(*m, files["coulombintra"], &rows, 2, err)) return -1;
@@ -554,7 +584,10 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       int s[4], g[4];
       for (int q = 0; q < 4; q++) { s[q] = (int)r[2 * q]; g[q] = (int)r[2 * q + 1]; }
       for (int q = 0; q < 4; q++)
-        if (!check_site(s[q]) || g[q] < 0 || g[q] > 1) { *err = files["interall"] + ": bad index"; return -1; }
+        if (!check_site(s[q]) || !sigma_ok(s[q], g[q])) { *err = files["interall"] + ": bad index"; return -1; }
+      if (m->general_spin && m->calc_model == kSpin && (g[0] - g[1]) + (g[2] - g[3]) != 0) {
+        *err = files["interall"] + ": a canonical general-spin InterAll term must conserve Sz"; return -1;
+      }
       const std::complex<double> V(r[8], r[9]);
       if (m->calc_model == kKondo || m->calc_model == kKondoGC) {  // CheckFormatForKondoInt (src/readdef.c:2665-2684)
         if (((m->locspn[s[0]] != 0 || m->locspn[s[1]] != 0) && s[0] != s[1]) ||

@@ -61,6 +61,12 @@ struct Model {
   std::vector<DiagTerm> diag;
   bool complex_terms = false;   // any off-diagonal coefficient with a non-zero imaginary part
   int nbits = 0;                // configuration bits: 2*Nsite (Hubbard/Kondo) or Nsite (spin)
+  // General spin (some site with 2S > 1, src/readdef.c:2735-2760): site i holds a digit
+  // 0 .. 2S_i (2Sz_i = 2*digit - 2S_i, GetLocal2Sz src/bitcalc.c:447-461) in a field of
+  // site_bits bits at bit site_bits * i, so configurations are packed digit strings whose
+  // numeric order is HPhi's mixed-radix order.  Spin-1/2 models have site_bits = 1.
+  bool general_spin = false;
+  int site_bits = 1;
   // Raw term counts as read (for logs).
   int n_trans = 0, n_coulomb_intra = 0, n_coulomb_inter = 0, n_hund = 0, n_exchange = 0;
   int n_ising = 0, n_pairhop = 0, n_pairlift = 0, n_interall = 0;
@@ -72,7 +78,7 @@ struct Model {
   bool is_spin() const { return calc_model == kSpin || calc_model == kSpinGC; }
   // Grand-canonical models whose basis is every configuration (row index == configuration);
   // KondoGC keeps lists because its local spins must stay singly occupied.
-  bool rows_are_configs() const { return calc_model == kHubbardGC || calc_model == kSpinGC; }
+  bool rows_are_configs() const { return calc_model == kHubbardGC || (calc_model == kSpinGC && !general_spin); }
   bool is_kondo() const { return calc_model == kKondo || calc_model == kKondoGC; }
 };
 

@@ -15,8 +15,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <map>
 
 #include "engine.hpp"
 #include "hv_hubbard.hpp"
@@ -297,6 +299,24 @@ int64_t sector_dim(const Model &m) {
       sum += binom_host(nloc, ul) * binom_host(ncond, m.nup - ul) * binom_host(ncond, m.ndown + ul - nloc);
     return (int64_t)sum;
   }
+  if (m.general_spin) {
+    // check.c:171-200 / 102-111: configurations of the mixed-radix space with total 2Sz
+    // (every configuration in the grand-canonical case), counted by a sum over sites
+    std::map<int, uint64_t> cnt{{0, 1}};
+    for (int i = 0; i < m.nsite; i++) {
+      std::map<int, uint64_t> nx;
+      for (const auto &kv : cnt)
+        for (int d = 0; d <= m.locspn[i]; d++) nx[kv.first + 2 * d - m.locspn[i]] += kv.second;
+      cnt.swap(nx);
+    }
+    if (m.is_gc()) {
+      uint64_t t = 0;
+      for (const auto &kv : cnt) t += kv.second;
+      return (int64_t)t;
+    }
+    auto it = cnt.find(m.total_2sz);
+    return it == cnt.end() ? 0 : (int64_t)it->second;
+  }
   if (m.is_gc()) return (int64_t)(1ull << m.nbits);
   if (m.calc_model == kHubbard) return (int64_t)(binom_host(m.nsite, m.nup) * binom_host(m.nsite, m.ndown));
   if (m.calc_model == kHubbardNConserved) return (int64_t)binom_host(2 * m.nsite, m.ne);
@@ -329,6 +349,94 @@ int sector_build(const Model &m, int device, Sector **out, std::string *err, boo
 
   if (s->gc) {
     s->dim = (int64_t)(1ull << nbits);
+  } else if (m.general_spin) {
+    // General spin (src/sz.c:795-830, 1564-1590; GetSplitBitForGeneralSpin src/bitcalc.c:
+    // 124-150).  HPhi splits the mixed-radix configuration at the first prefix of sites whose
+    // product ihfbit reaches floor(sqrt(total)); blocks by increasing upper index ib, inside a
+    // block the lower indices ia whose 2Sz completes Total2Sz (every ia when grand-canonical),
+    // list_2_1[ia] = rank within its 2Sz class + 2, list_2_2[ib] = block offset + 1.  The
+    // engine's configurations are packed digit codes split at the same site; its device tables
+    // hold HPhi's values at the packed codes (0 for codes with an out-of-range digit).
+    const int N = m.nsite, b = m.site_bits;
+    const bool gcs = m.is_gc();
+    std::vector<uint64_t> radix(N), tpow(N + 1, 1);
+    for (int i = 0; i < N; i++) { radix[i] = (uint64_t)m.locspn[i] + 1; tpow[i + 1] = tpow[i] * radix[i]; }
+    const uint64_t total = tpow[N];
+    const int64_t isq = (int64_t)std::sqrt((double)(int64_t)total);
+    int k = 0;
+    uint64_t hf = 1;
+    for (int i = 0; i < N; i++) {
+      hf *= radix[i];
+      k = i + 1;
+      if ((int64_t)hf >= isq) break;
+    }
+    const uint64_t nlo = hf, nhi = total / hf;
+    s->lo_bits = b * k;
+    s->hi_bits = nbits - s->lo_bits;
+    if (s->lo_bits > 26 || s->hi_bits > 26) { *err = "general-spin sector too large for the packed tables"; return -1; }
+    s->ihfbit = 1ull << s->lo_bits;
+    s->sdim = 1ull << s->hi_bits;
+    s->size_list_2_1 = (int64_t)nlo + 2;     // GetlistSize (src/xsetmem.c:305-310)
+    s->size_list_2_2 = (int64_t)nhi + 2;
+    auto digits_sz = [&](uint64_t x, int site0, int nsites, uint64_t *packed) {
+      int sz = 0;
+      uint64_t pk = 0;
+      for (int j = 0; j < nsites; j++) {
+        const int d = (int)(x % radix[site0 + j]);
+        x /= radix[site0 + j];
+        sz += 2 * d - m.locspn[site0 + j];
+        pk |= (uint64_t)d << (b * j);
+      }
+      *packed = pk;
+      return sz;
+    };
+    std::vector<int> sz_lo(nlo), sz_hi(nhi);
+    std::vector<uint64_t> pk_lo(nlo), pk_hi(nhi);
+    for (uint64_t ia = 0; ia < nlo; ia++) sz_lo[ia] = digits_sz(ia, 0, k, &pk_lo[ia]);
+    for (uint64_t ib = 0; ib < nhi; ib++) sz_hi[ib] = digits_sz(ib, k, N - k, &pk_hi[ib]);
+    std::map<int, std::vector<uint64_t>> cls;  // 2Sz of the lower part -> its ia, increasing
+    for (uint64_t ia = 0; ia < nlo; ia++) cls[gcs ? 0 : sz_lo[ia]].push_back(ia);
+    std::vector<uint64_t> h21(nlo + 2, 0), h22(nhi + 2, 0), h1(1, 0), l1;
+    std::vector<uint32_t> d21(s->ihfbit, 0), d22(s->sdim, 0);
+    std::map<int, bool> used;
+    uint64_t jb = 0;
+    for (uint64_t ib = 0; ib < nhi; ib++) {
+      auto it = cls.find(gcs ? 0 : m.total_2sz - sz_hi[ib]);
+      if (it == cls.end()) continue;
+      used[it->first] = true;
+      h22[ib] = jb + 1;
+      d22[pk_hi[ib]] = (uint32_t)(jb + 1);
+      for (uint64_t ia : it->second) {
+        h1.push_back(ia + ib * nlo);
+        l1.push_back(pk_lo[ia] | (pk_hi[ib] << s->lo_bits));
+      }
+      jb += it->second.size();
+    }
+    for (const auto &kv : cls)
+      if (used.count(kv.first))
+        for (size_t r = 0; r < kv.second.size(); r++) {
+          h21[kv.second[r]] = r + 2;
+          d21[pk_lo[kv.second[r]]] = (uint32_t)(r + 2);
+        }
+    const int64_t expect = sector_dim(m);
+    if ((int64_t)jb != expect || jb == 0) {
+      *err = "general-spin sector size mismatch: enumerated " + std::to_string(jb) + ", expected " +
+             std::to_string(expect);
+      return -1;
+    }
+    if (jb > 0xFFFFFFF0ull) { *err = "sector too large for 32-bit list_2 tables"; return -1; }
+    s->dim = (int64_t)jb;
+    if (!gcs) {
+      s->gs_list_1.swap(h1);
+      s->gs_list_2_1.swap(h21);
+      s->gs_list_2_2.swap(h22);
+    }
+    CK(cudaMalloc(&s->d_list_2_1, sizeof(uint32_t) * s->ihfbit));
+    CK(cudaMalloc(&s->d_list_2_2, sizeof(uint32_t) * s->sdim));
+    CK(cudaMalloc(&s->d_list_1, sizeof(uint64_t) * jb));
+    CK(cudaMemcpy(s->d_list_2_1, d21.data(), sizeof(uint32_t) * s->ihfbit, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->d_list_2_2, d22.data(), sizeof(uint32_t) * s->sdim, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->d_list_1, l1.data(), sizeof(uint64_t) * jb, cudaMemcpyHostToDevice));
   } else if (m.is_kondo()) {
     // Kondo / KondoGC (src/sz.c:541-635, 1110-1220, 1342-1420): a half is admissible when
     // its local spins are singly occupied; blocks by increasing upper half ib, inside a block

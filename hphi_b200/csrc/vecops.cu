@@ -67,16 +67,27 @@ __global__ void lanczos_sweep_kernel(int64_t n, const double *__restrict__ coef,
 // Occupation statistics of a configuration, as expec_energy_flct_Hubbard /
 // _HalfSpinGC (src/expec_energy_flct.c:186-666): out = <D>, <D^2>, <N>, <N^2>, <Sz>, <Sz^2>
 // with D = doubly occupied sites, Sz = (N_up - N_dn)/2 (Hubbard bit 2i+s; spin bit i = up).
+// General spin (site_bits > 0): site i's digit is bits [site_bits*i, site_bits*(i+1)) and
+// Sz = sum of digits - sum of S_i (expec_energy_flct_GeneralSpin[GC], src/expec_energy_flct.c:
+// 501-540, 618-660).
 template <typename T>
-__global__ void diag_obs_kernel(int64_t n, int gc, int spin, int nsite, const uint64_t *__restrict__ list_1,
-                                const T *__restrict__ x, double *__restrict__ part) {
+__global__ void diag_obs_kernel(int64_t n, int gc, int spin, int nsite, int site_bits, int sum2s,
+                                const uint64_t *__restrict__ list_1, const T *__restrict__ x,
+                                double *__restrict__ part) {
   double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   const uint64_t even = 0x5555555555555555ull;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t c = gc ? (uint64_t)i : list_1[i];
     const double w = VT<T>::abs2(x[i]);
     double D, N, Sz;
-    if (spin) {
+    if (spin && site_bits > 0) {
+      int dsum = 0;
+      const uint64_t fm = (1ull << site_bits) - 1;
+      for (int q = 0; q < nsite; q++) dsum += (int)((c >> (site_bits * q)) & fm);
+      D = 0.0;
+      N = (double)nsite;
+      Sz = 0.5 * (double)(2 * dsum - sum2s);
+    } else if (spin) {
       D = 0.0;
       N = (double)nsite;
       Sz = 0.5 * (double)(2 * __popcll(c) - nsite);
@@ -158,13 +169,17 @@ int vec_lanczos_sweep(Sector *s, VecType vt, const double *coef, void *p, const 
 }
 
 int vec_diag_observables(Sector *s, VecType vt, const void *x, double *out) {
-  const int spin = s->model.is_spin() ? 1 : 0;
+  const Model &m = s->model;
+  const int spin = m.is_spin() ? 1 : 0;
+  const int gbits = m.general_spin ? m.site_bits : 0;
+  int sum2s = 0;
+  for (int q = 0; q < m.nsite && m.general_spin; q++) sum2s += m.locspn[q];
   if (vt == kReal64)
-    diag_obs_kernel<double><<<s->red_blocks, kThreads, 0, s->stream>>>(s->dim, s->gc ? 1 : 0, spin, s->model.nsite,
-                                                                       s->d_list_1, (const double *)x, s->d_red);
+    diag_obs_kernel<double><<<s->red_blocks, kThreads, 0, s->stream>>>(
+        s->dim, s->gc ? 1 : 0, spin, m.nsite, gbits, sum2s, s->d_list_1, (const double *)x, s->d_red);
   else
-    diag_obs_kernel<cplx><<<s->red_blocks, kThreads, 0, s->stream>>>(s->dim, s->gc ? 1 : 0, spin, s->model.nsite,
-                                                                     s->d_list_1, (const cplx *)x, s->d_red);
+    diag_obs_kernel<cplx><<<s->red_blocks, kThreads, 0, s->stream>>>(
+        s->dim, s->gc ? 1 : 0, spin, m.nsite, gbits, sum2s, s->d_list_1, (const cplx *)x, s->d_red);
   finalize_partials_kernel<6><<<1, 256, 0, s->stream>>>(s->d_red, s->red_blocks, out);
   return check_launch("vec_diag_observables");
 }

@@ -197,6 +197,53 @@ def heisenberg(nsite: int, bonds: Sequence[Tuple[int, int]], J: float | Sequence
     return m
 
 
+def _spin_raise(two_s: int, d: int) -> float:
+    """<d+1| S+ |d> for spin S = two_s/2, digit d <-> m = d - S."""
+    S, m = 0.5 * two_s, d - 0.5 * two_s
+    return (S * (S + 1) - m * (m + 1)) ** 0.5
+
+
+def general_heisenberg(two_s: Sequence[int], bonds: Sequence[Tuple[int, int]], J: float | Sequence[float] = 1.0,
+                       two_sz: Optional[int] = 0, D: float = 0.0, hx: float = 0.0, **kw) -> ExpertModel:
+    """Spin-S Heisenberg model with site spins two_s[i]/2 (general spin: InterAll only),
+    H = sum J S_i.S_j + D sum (Sz_i)^2 - hx sum Sx_i.  A site's state is its digit
+    d = 0 .. 2S (2Sz = 2d - 2S); InterAll (i a i b j c j d V) is V |a><b|_i |c><d|_j, listed
+    with its Hermitian partner (j d j c i b i a V*).  hx needs two_sz=None (SpinGC); it is
+    written as site-diagonal Trans rows (H += -t |a><b|)."""
+    n = len(two_s)
+    Js = [J] * len(bonds) if isinstance(J, (int, float)) else list(J)
+    m = ExpertModel(model="Spin" if two_sz is not None else "SpinGC", nsite=n, two_sz=two_sz,
+                    locspin=list(two_s), **kw)
+    rows = []
+    for (i, j), c in zip(bonds, Js):
+        for a in range(two_s[i] + 1):
+            for b in range(two_s[j] + 1):
+                v = c * (a - 0.5 * two_s[i]) * (b - 0.5 * two_s[j])
+                if v != 0.0:
+                    rows.append((i, a, i, a, j, b, j, b, v, 0.0))
+        for a in range(two_s[i]):
+            for b in range(1, two_s[j] + 1):
+                v = 0.5 * c * _spin_raise(two_s[i], a) * _spin_raise(two_s[j], b - 1)
+                rows.append((i, a + 1, i, a, j, b - 1, j, b, v, 0.0))
+                rows.append((j, b, j, b - 1, i, a, i, a + 1, v, 0.0))
+    if D != 0.0:
+        for i in range(n):
+            for a in range(two_s[i] + 1):
+                mz = a - 0.5 * two_s[i]
+                if mz != 0.0:
+                    # (Sz_i)^2 = sum_a mz^2 |a><a|_i, written as |a><a|_i |a><a|_i
+                    rows.append((i, a, i, a, i, a, i, a, D * mz * mz, 0.0))
+    m.interall = rows
+    if hx != 0.0:
+        if two_sz is not None:
+            raise ValueError("a transverse field needs the grand-canonical SpinGC model (two_sz=None)")
+        for i in range(n):
+            for a in range(two_s[i]):
+                t = 0.5 * hx * _spin_raise(two_s[i], a)   # -hx Sx = -(hx/2)(S+ + S-): Trans t = hx/2 * <|S+|>
+                m.trans += [(i, a + 1, i, a, t, 0.0), (i, a, i, a + 1, t, 0.0)]
+    return m
+
+
 def j1j2_chain(L: int, J1: float, J2: float, **kw) -> ExpertModel:
     bonds = chain_bonds(L, 1) + chain_bonds(L, 2)
     return heisenberg(L, bonds, [J1] * L + [J2] * L, **kw)

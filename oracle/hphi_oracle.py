@@ -184,6 +184,37 @@ def _rows_are_configs(d: Def) -> bool:
     return d.calc_model in (HUBBARDGC, SPINGC)
 
 
+def _general(d: Def) -> bool:
+    """General spin: a spin model with some site 2S > 1 (CheckLocSpin, src/readdef.c:2735-2760)."""
+    return _is_spin(d) and any(x > 1 for x in d.locspn)
+
+
+def _tpow(d: Def) -> List[int]:
+    """Mixed-radix place values (check, src/check.c:171-178): Tpow[i] = prod_{j<i} (2S_j + 1)."""
+    t = [1]
+    for x in d.locspn:
+        t.append(t[-1] * (x + 1))
+    return t
+
+
+def _digit(d: Def, c: np.ndarray, site: int) -> np.ndarray:
+    """GetBitGeneral (src/bitcalc.c:421-432): digit of `site` in mixed-radix configurations."""
+    t = _tpow(d)
+    return ((c // np.uint64(t[site])) % np.uint64(d.locspn[site] + 1)).astype(np.int64)
+
+
+def _general_split(d: Def) -> Tuple[int, int]:
+    """GetSplitBitForGeneralSpin (src/bitcalc.c:124-150): (ihfbit, number of lower sites)."""
+    total = _tpow(d)[-1]
+    isq = int(np.sqrt(float(total)))
+    t = 1
+    for i, x in enumerate(d.locspn):
+        t *= x + 1
+        if t >= isq:
+            return t, i + 1
+    return t, d.nsite
+
+
 def nbits(d: Def) -> int:
     return d.nsite if _is_spin(d) else 2 * d.nsite
 
@@ -228,6 +259,8 @@ def sz(d: Def):
         raise ValueError("grand-canonical models have no lists")
     if d.calc_model in (KONDO, KONDOGC):
         return _sz_kondo(d)
+    if _general(d):
+        return _sz_general(d)
     ihfbit, irght, ilft = split_bits(d)
     sd = sdim(d)
     lo = (nbits(d) + 1) // 2
@@ -259,6 +292,36 @@ def sz(d: Def):
         sel = cache[key]
         if sel.size:
             blocks.append(sel + np.uint64(ib) * np.uint64(ihfbit))
+            list_2_1[sel] = np.arange(sel.size, dtype=np.uint64) + np.uint64(2)
+            list_2_2[ib] = jb + 1
+            jb += sel.size
+    list_1 = np.concatenate([np.zeros(1, dtype=np.uint64)] + blocks)
+    return list_1, list_2_1, list_2_2
+
+
+def _sz_general(d: Def):
+    """General spin (src/sz.c:795-830 with omp_sz_GeneralSpin :1564-1590): 2Sz of every lower
+    index ia < ihfbit and upper index ib; blocks by ib ascending, each the ascending ia whose
+    2Sz completes Total2Sz; list_2_1[ia] = rank in its 2Sz class + 2 (classes some block
+    uses), list_2_2[ib] = block offset + 1; list_1 holds mixed-radix configurations."""
+    ihfbit, k = _general_split(d)
+    total = _tpow(d)[-1]
+    nhi = total // ihfbit
+    ia = np.arange(ihfbit, dtype=np.uint64)
+    sz_lo = np.zeros(ihfbit, dtype=np.int64)
+    for site in range(k):
+        sz_lo += 2 * _digit(d, ia, site) - d.locspn[site]
+    ib_cfg = np.arange(nhi, dtype=np.uint64) * np.uint64(ihfbit)
+    sz_hi = np.zeros(nhi, dtype=np.int64)
+    for site in range(k, d.nsite):
+        sz_hi += 2 * _digit(d, ib_cfg, site) - d.locspn[site]
+    list_2_1 = np.zeros(ihfbit + 2, dtype=np.uint64)
+    list_2_2 = np.zeros(nhi + 2, dtype=np.uint64)
+    blocks, jb = [], 0
+    for ib in range(nhi):
+        sel = np.nonzero(sz_lo == d.total_2sz - sz_hi[ib])[0].astype(np.uint64)
+        if sel.size:
+            blocks.append(sel + np.uint64(ib * ihfbit))
             list_2_1[sel] = np.arange(sel.size, dtype=np.uint64) + np.uint64(2)
             list_2_2[ib] = jb + 1
             jb += sel.size
@@ -313,7 +376,7 @@ def _sz_kondo(d: Def):
 def configs(d: Def, lists) -> np.ndarray:
     """Configuration of every row (1-based arrays: element 0 unused)."""
     if _rows_are_configs(d):
-        n = 1 << nbits(d)
+        n = _tpow(d)[-1] if _general(d) else 1 << nbits(d)
         return np.concatenate([np.zeros(1, np.uint64), np.arange(n, dtype=np.uint64)])
     return lists[0]
 
@@ -322,6 +385,11 @@ def get_off(d: Def, lists, c: np.ndarray) -> np.ndarray:
     """GetOffComp (src/bitcalc.c:195-223): 1-based row of configuration c, 0 if absent."""
     if _rows_are_configs(d):
         return c.astype(np.int64) + 1
+    if _general(d):   # ConvertToList1GeneralSpin (src/bitcalc.c:285-300)
+        ihfbit = np.uint64(_general_split(d)[0])
+        a = lists[1][(c % ihfbit).astype(np.int64)].astype(np.int64)
+        b = lists[2][(c // ihfbit).astype(np.int64)].astype(np.int64)
+        return np.where((a == 0) | (b == 0), 0, a + b - 2)
     ihfbit, irght, ilft = split_bits(d)
     lo = (nbits(d) + 1) // 2
     a = lists[1][(c & np.uint64(irght)).astype(np.int64)].astype(np.int64)
@@ -335,6 +403,15 @@ def diagonalcalc(d: Def, lists) -> np.ndarray:
     CoulombIntra, Chemi, CoulombInter, Hund, InterAll-diagonal."""
     c = configs(d, lists)
     diag = np.zeros(c.size)
+    if _general(d):
+        # general spin: Chemi -mu [digit_i == s] (:425-433), InterAll-diagonal
+        # V [digit_i == s1][digit_k == s3] (:1180-1202)
+        for i, s_, mu in d.chemi:
+            diag += -mu * (_digit(d, c, i) == s_)
+        for i, s1, k, s3, V in d.interall_diag:
+            diag += V * ((_digit(d, c, i) == s1) & (_digit(d, c, k) == s3))
+        diag[0] = 0.0
+        return diag
     bit = lambda pos: ((c >> np.uint64(pos)) & np.uint64(1)).astype(np.int64)
     spin = _is_spin(d)
     for i, U in d.coulomb_intra:   # SetDiagonalCoulombIntra :260-355 (zero for spin)
@@ -412,7 +489,25 @@ def mltply(d: Def, lists, diag: np.ndarray, v0: np.ndarray, v1: np.ndarray):
         np.add.at(v0, off[ok], dmv)
         prdct += np.sum(np.conj(v1[off[ok]]) * dmv)
 
-    if spin:
+    if spin and _general(d):
+        tp = _tpow(d)
+
+        def dflip(cc, site, to, frm):
+            """GetOffCompGeneralSpin (src/bitcalc.c:243-275): digit frm -> to."""
+            ok = _digit(d, cc, site) == frm
+            return ok, (cc.astype(np.int64) + (to - frm) * tp[site]).astype(np.uint64)
+        # Trans (GC, |s1><s2| with -t; mltplyGeneralSpinGC src/mltplySpin.c:738-770)
+        for (i, s1, j, s2, t) in d.trans:
+            ok, t1 = dflip(cj, i, s1, s2)
+            scatter(ok, np.where(ok, t1, cj), np.full(cj.size, -t))
+        # InterAll (mltplyGeneralSpin src/mltplySpin.c:351-381): site k first, then site i
+        for (i, s1, j, s2, k, s3, l, s4, V) in d.interall_off:
+            ok2, t2 = dflip(cj, k, s3, s4)
+            t2 = np.where(ok2, t2, cj)
+            ok1, t1 = dflip(t2, i, s1, s2)
+            ok = ok1 & ok2
+            scatter(ok, np.where(ok, t1, cj), np.full(cj.size, V))
+    elif spin:
         # InterAll off-diagonal (general_int_spin :1020-1051 / GC_general_int_spin :1058-1112)
         for (i, s1, j, s2, k, s3, l, s4, V) in d.interall_off:
             ok2, t2 = _spin_flip(cj, k, s3, s4)
@@ -530,7 +625,11 @@ def expec_energy(d: Def, lists, diag, v: np.ndarray):
     var = float(np.sum(np.abs(hv[1:]) ** 2))
     w = np.abs(v[1:]) ** 2
     c = configs(d, lists)[1:].astype(np.uint64)
-    if _is_spin(d):
+    if _general(d):
+        doublon = 0.0
+        two_sz = sum(2 * _digit(d, c, i) - d.locspn[i] for i in range(d.nsite))
+        sz = float(np.sum(w * 0.5 * two_sz))
+    elif _is_spin(d):
         doublon = 0.0
         sz = float(np.sum(w * 0.5 * (2 * _popcount(c) - d.nsite)))
     else:

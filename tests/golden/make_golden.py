@@ -125,6 +125,16 @@ def _cases():
     m = expert.hubbard(6, expert.chain_bonds(6), 1.0, 4.0, 3, 3, lanczos_eps=3, calc_eigenvec=0)
     m.initial_vec_type = 0
     c["lanczos_cg_hub6"] = m
+    # General spin (some 2S > 1; InterAll only): spin-1 chain, mixed spin-1/2 / spin-1 chain
+    # with a single-ion term, spin-3/2 chain, and a grand-canonical spin-1 chain in a
+    # transverse field (off-diagonal Trans), complex vectors.
+    c["gspin1_chain8"] = expert.general_heisenberg([2] * 8, expert.chain_bonds(8), lanczos_max=300)
+    c["gspin_mixed6"] = expert.general_heisenberg([1, 2, 1, 2, 1, 2], expert.chain_bonds(6), two_sz=1, D=0.3,
+                                                  lanczos_max=300)
+    c["gspin32_chain6"] = expert.general_heisenberg([3] * 6, expert.chain_bonds(6), two_sz=2, lanczos_max=300)
+    m = expert.general_heisenberg([2] * 5, expert.chain_bonds(5), two_sz=None, D=0.2, hx=0.4, lanczos_max=300)
+    m.initial_vec_type = 0
+    c["gspingc_field5"] = m
     return c
 
 
@@ -136,6 +146,7 @@ def _large_cases():
     m = expert.heisenberg(24, expert.chain_bonds(24), lanczos_max=1)
     c["chain24_lists"] = m
     c["kondo_chain8_lists"] = expert.kondo_chain(8, 1.0, 1.0, lanczos_max=1)
+    c["gspin1_chain14_lists"] = expert.general_heisenberg([2] * 14, expert.chain_bonds(14), lanczos_max=1)
     return c
 
 

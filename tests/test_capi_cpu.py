@@ -60,11 +60,41 @@ def _popcount(x):
     return c
 
 
+def _general_spins(name):
+    """2S of every site when the case is a general-spin one (some 2S > 1), else None."""
+    lines = open(os.path.join(case_dir(name), "locspn.def")).read().splitlines()[5:]
+    two_s = [int(l.split()[1]) for l in lines if len(l.split()) >= 2]
+    calc = open(os.path.join(case_dir(name), "calcmod.def")).read()
+    spin = any(l.split()[:2] in (["CalcModel", "1"], ["CalcModel", "4"]) for l in calc.splitlines())
+    return two_s if spin and any(x > 1 for x in two_s) else None
+
+
+def _packed(mixed, two_s):
+    """Mixed-radix configurations -> the engine's packed digit codes (fixed-width fields)."""
+    bits = max(1, int(np.ceil(np.log2(max(two_s) + 1))))
+    x = mixed.astype(np.uint64).copy()
+    out = np.zeros(x.size, dtype=np.uint64)
+    for i, t in enumerate(two_s):
+        out |= (x % np.uint64(t + 1)) << np.uint64(bits * i)
+        x //= np.uint64(t + 1)
+    return out
+
+
 def emulate_hv(name, v1_1based):
     """H v1 from the compiled terms with the device kernel's gather rule."""
     g = load_golden(name)
     masks, coefs, dmasks, dcoefs = hphi_b200.inspect_terms(os.path.join(case_dir(name), "namelist.def"))
-    if "list_1" in g:
+    two_s = _general_spins(name)
+    if two_s is not None:
+        # packed codes in row order (ascending, as the mixed-radix configurations)
+        mixed = g["list_1"][1:] if "list_1" in g else np.arange(v1_1based.size - 1, dtype=np.uint64)
+        conf = _packed(mixed, two_s)
+
+        def row(s):
+            idx = np.searchsorted(conf, s)
+            hit = (idx < conf.size) & (conf[np.minimum(idx, conf.size - 1)] == s)
+            return np.where(hit, idx, -1)
+    elif "list_1" in g:
         conf = g["list_1"][1:]
         l21, l22 = g["list_2_1"], g["list_2_2"]
         nb = int(np.log2(l22.size - 2)) if l22.size > 2 else 0
