@@ -148,7 +148,11 @@ int hphi_info(const hphi_handle *h, int64_t *info, int n) {
 int hphi_sz(const hphi_handle *h, uint64_t *list_1, uint64_t *list_2_1, uint64_t *list_2_2) {
   CHECK_HANDLE(h);
   const Sector &s = *h->sector;
-  if (s.model.is_gc()) { set_error("grand-canonical models have no sector lists"); return -1; }
+  // HubbardGC and SpinGC (any spin) have no lists: the row is the configuration index
+  if (s.model.calc_model == kHubbardGC || s.model.calc_model == kSpinGC) {
+    set_error("grand-canonical models have no sector lists");
+    return -1;
+  }
   if (s.model.general_spin) {  // HPhi's mixed-radix lists, kept on the host
     if (list_1) {
       list_1[0] = 0;
