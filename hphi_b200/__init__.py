@@ -42,7 +42,8 @@ EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi
                     "hphi_synchronize", "hphi_to_native", "hphi_from_native", "hphi_mltply_device_noalloc",
                     "hphi_lanczos_steps", "hphi_batch_create", "hphi_batch_lanczos", "hphi_batch_tuning",
                     "hphi_batch_free", "hphi_server_create", "hphi_server_submit", "hphi_server_step",
-                    "hphi_server_poll", "hphi_server_clock", "hphi_server_free", "hphi_lobpcg"]
+                    "hphi_server_poll", "hphi_server_clock", "hphi_server_free", "hphi_lobpcg",
+                    "hphi_reference_start"]
 FP64 = 0
 FP32 = 1
 BATCH_GRAPH = 1
@@ -114,6 +115,7 @@ def load_library() -> ctypes.CDLL:
     lib.hphi_server_clock.restype = D
     lib.hphi_server_free.argtypes = [P]
     lib.hphi_server_free.restype = None
+    lib.hphi_reference_start.argtypes = [ctypes.c_int64, I, I, I, I, I, I, pd]
     for name in EXPORTED_SYMBOLS:
         if name not in ("hphi_version", "hphi_last_error", "hphi_close", "hphi_stream", "hphi_batch_free",
                         "hphi_server_clock", "hphi_server_free"):
@@ -135,6 +137,20 @@ def _as_hphi_vector(v: np.ndarray, dim: int) -> np.ndarray:
     v = np.ascontiguousarray(v, dtype=np.complex128)
     if v.shape != (dim + 1,):
         raise ValueError(f"expected an HPhi vector of length dim+1 = {dim + 1}, got {v.shape}")
+    return v
+
+
+REF_LANCZOS, REF_TPQ, REF_LOBPCG = 0, 1, 2
+
+
+def reference_start(dim: int, kind: int = REF_LANCZOS, initial_iv: int = -1, sample: int = 0, vec_type: int = 1,
+                    threads: int = 1, count: int = 1) -> np.ndarray:
+    """The reference's random start vector(s) drawn with `threads` OpenMP threads (dSFMT-19937
+    per thread, static-schedule rows): an array (count, dim + 1) of complex128 in HPhi's layout
+    (element 0 unused); Lanczos / LOBPCG vectors are normalised, TPQ ones are not."""
+    v = np.zeros((max(count, 1), dim + 1), dtype=np.complex128)
+    _check(load_library().hphi_reference_start(int(dim), int(kind), int(initial_iv), int(sample), int(vec_type),
+                                               int(threads), int(count), _dptr(v.view(np.float64))))
     return v
 
 

@@ -11,6 +11,7 @@
 #include "driver.hpp"
 #include "engine.hpp"
 #include "hv_product.hpp"
+#include "refrand.hpp"
 #include "model.hpp"
 
 namespace hphi {
@@ -299,6 +300,18 @@ int hphi_lanczos_steps(hphi_handle *h, int steps, uint64_t seed, double *energie
   return 0;
 }
 
+namespace {
+// OpenMP thread count whose random start vectors HPhi would draw: HPHI_B200_REF_THREADS,
+// else OMP_NUM_THREADS, else 1.
+int reference_threads() {
+  for (const char *k : {"HPHI_B200_REF_THREADS", "OMP_NUM_THREADS"}) {
+    const char *v = getenv(k);
+    if (v && atoi(v) > 0) return atoi(v);
+  }
+  return 1;
+}
+}  // namespace
+
 int hphi_lanczos(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult) {
   CHECK_HANDLE(h);
   Sector *s = h->sector;
@@ -306,7 +319,8 @@ int hphi_lanczos(hphi_handle *h, const double *v_init, const char *output_dir, d
   std::vector<double> start;
   if (!v_init) {
     if (!single_element_start(*s, &start))
-      random_start(*s, 123432ull + (uint64_t)std::abs(s->model.initial_iv), vt == kComplex128, &start);
+      reference_random_start(s->dim, kRefLanczos, s->model.initial_iv, 0, s->model.initial_vec_type,
+                             reference_threads(), 1, &start);
     v_init = start.data();
   }
   LanczosOptions opt;
@@ -358,8 +372,8 @@ int hphi_tpq(hphi_handle *h, const double *v_init, const char *output_dir, doubl
     if (v_init) {
       v = v_init + stride * rand_i;
     } else {
-      random_start(*s, 123432ull + (uint64_t)(rand_i + 1) * (uint64_t)std::abs(s->model.initial_iv),
-                   vt == kComplex128, &start);
+      reference_random_start(s->dim, kRefTPQ, s->model.initial_iv, rand_i, s->model.initial_vec_type,
+                             reference_threads(), 1, &start);
       v = start.data();
     }
     if (tpq_run(s, vt, v, rand_i, out, &r) != 0) return -1;
@@ -376,15 +390,9 @@ int hphi_lobpcg(hphi_handle *h, const double *v_init, const char *output_dir, do
   const int k = std::max(1, s->model.k_exct);
   std::vector<double> start;
   if (!v_init) {
-    if (!lobpcg_single_element_start(*s, &start)) {
-      std::vector<double> one;
-      start.clear();
-      for (int i = 0; i < k; i++) {
-        random_start(*s, 123432ull + (uint64_t)std::abs(s->model.initial_iv) + 7919ull * (uint64_t)i,
-                     vt == kComplex128, &one);
-        start.insert(start.end(), one.begin(), one.end());
-      }
-    }
+    if (!lobpcg_single_element_start(*s, &start))
+      reference_random_start(s->dim, kRefLOBPCG, s->model.initial_iv, 0, s->model.initial_vec_type,
+                             reference_threads(), k, &start);
     v_init = start.data();
   }
   LobpcgResult r;
@@ -418,6 +426,18 @@ int hphi_run(hphi_handle *h, const char *output_dir) {
       set_error("CalcType not supported by this engine (Lanczos = 0, TPQ = 1 and LOBPCG = 3 are)");
       return -1;
   }
+}
+
+int hphi_reference_start(int64_t dim, int kind, int initial_iv, int sample, int vec_type, int threads, int count,
+                         double *v) {
+  if (dim < 1 || kind < 0 || kind > 2 || !v) {
+    set_error("hphi_reference_start: bad arguments");
+    return -1;
+  }
+  std::vector<double> out;
+  reference_random_start(dim, (RefStartKind)kind, initial_iv, sample, vec_type, threads, count, &out);
+  std::memcpy(v, out.data(), sizeof(double) * out.size());
+  return 0;
 }
 
 }  // extern "C"

@@ -168,7 +168,8 @@ VecType default_vec_type(const Sector &s) {
 // 1-based complex128 layout.  Returns false when the reference would use a random vector.
 bool single_element_start(const Sector &s, std::vector<double> *v) {
   const Model &m = s.model;
-  if (m.is_gc() || m.initial_iv <= 0) return false;
+  // random for grand-canonical and general-spin models (src/CalcByLanczos.c:66-93)
+  if (m.is_gc() || m.general_spin || m.initial_iv <= 0) return false;
   const uint64_t dim = (uint64_t)s.dim;
   const uint64_t iv = (dim / 2 + (uint64_t)m.initial_iv) % dim + 1;
   v->assign(2 * (dim + 1), 0.0);

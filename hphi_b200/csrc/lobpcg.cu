@@ -323,7 +323,7 @@ int ensure_dir(const std::string &dir) {
 // iv = (dim/2 + initial_iv + ie) % dim + 1 (no element when iv == dim).
 bool lobpcg_single_element_start(const Sector &s, std::vector<double> *v) {
   const Model &m = s.model;
-  if (m.is_gc() || m.initial_iv <= 0) return false;
+  if (m.is_gc() || m.general_spin || m.initial_iv <= 0) return false;
   const uint64_t dim = (uint64_t)s.dim;
   const int k = std::max(1, m.k_exct);
   v->assign((size_t)k * 2 * (dim + 1), 0.0);

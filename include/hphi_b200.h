@@ -291,6 +291,21 @@ int hphi_server_poll(hphi_server *s, int64_t *request_id, double *result);
 double hphi_server_clock(void);
 void hphi_server_free(hphi_server *s);
 
+/*
+ * The reference's random start vector(s) for a sector of `dim` rows, as HPhi draws them
+ * with `threads` OpenMP threads (each thread seeds its own dSFMT-19937 generator and fills
+ * its static-schedule share of the rows): kind 0 Lanczos (SetInitialVector,
+ * src/Lanczos_EigenValue.c:552-610; normalised), 1 TPQ sample `sample` (MakeIniVec,
+ * src/MakeIniVec.c:41-117; not normalised, its norm is the first TPQ norm), 2 LOBPCG
+ * (Initialize_wave, src/CalcByLOBPCG.c:252-290; `count` normalised vectors).  vec_type is
+ * InitialVecType (0 complex, 1 real, -1 Gaussian complex for TPQ).  v receives
+ * count * (dim + 1) complex128 in HPhi's layout.  Host only.  hphi_lanczos, hphi_tpq and
+ * hphi_lobpcg use these vectors when called without one (HPHI_B200_REF_THREADS, else
+ * OMP_NUM_THREADS, else 1 thread).
+ */
+int hphi_reference_start(int64_t dim, int kind, int initial_iv, int sample, int vec_type, int threads, int count,
+                         double *v);
+
 #ifdef __cplusplus
 }
 #endif

@@ -12,6 +12,8 @@ of oracle/ref_hooks.c:
   energy_state, cg_ran           zvo_energy.dat of a Lanczos case with CalcEigenVec != -1, and
                                  whether the reference refined the vector by CG
   tpq                            SS_rand0.dat rows (TPQ cases)
+refstart_* directories hold start.npz: the first mltply input of a golden case's input rerun
+with several OpenMP threads (the reference's per-thread random start vectors).
 Large cases store only SHA-256 digests of the lists (sha_list_1 ...).
 
 Run in a container that has the reference sources and oracle/_ref/HPhi_ref
@@ -205,15 +207,39 @@ def make_case(name: str, m, large: bool = False) -> None:
     np.savez_compressed(os.path.join(out, "golden.npz"), **data)
 
 
+def _start_cases():
+    """Reference start vectors drawn with several OpenMP threads (the inputs of golden cases,
+    rerun with `threads` threads): only the first mltply input is kept."""
+    return {"refstart_chain16_t3": ("chain16", 3), "refstart_kitaev2x2_t4": ("kitaev2x2", 4),
+            "refstart_tpq_hub6_t3": ("tpq_hub6", 3)}
+
+
+def make_start_case(name: str, src: str, threads: int) -> None:
+    out = os.path.join(HERE, name)
+    shutil.rmtree(out, ignore_errors=True)
+    os.makedirs(out)
+    with tempfile.TemporaryDirectory() as tmp:
+        for f in os.listdir(os.path.join(HERE, src)):
+            if f.endswith(".def"):
+                shutil.copy(os.path.join(HERE, src, f), tmp)
+        p = run_ref.run(tmp, threads=threads, dump_call=0)
+        if p.returncode != 0:
+            raise RuntimeError(f"{name}: reference failed")
+        v1, _, _, _ = run_ref.read_hv(tmp)
+    np.savez_compressed(os.path.join(out, "start.npz"), source=np.array(src), threads=np.array(threads), v1=v1)
+
+
 def main(argv) -> None:
     if not run_ref.available():
         raise SystemExit("oracle/_ref/HPhi_ref is missing: run `make -C oracle` first")
-    small, large = _cases(), _large_cases()
-    names = argv or list(small) + list(large)
+    small, large, starts = _cases(), _large_cases(), _start_cases()
+    names = argv or list(small) + list(large) + list(starts)
     for n in names:
         print("case", n, flush=True)
         if n in small:
             make_case(n, small[n])
+        elif n in starts:
+            make_start_case(n, *starts[n])
         else:
             make_case(n, large[n], large=True)
 

@@ -96,6 +96,29 @@ def test_lanczos_matches_reference(name, tmp_path):
         assert len(lines) - 1 == r["steps"] - 1
 
 
+@pytest.mark.parametrize("name", ["chain16", "hubchain8_complex", "kitaev2x2", "gspin1_chain8", "hubgc4"])
+def test_lanczos_default_start_matches_reference(name, tmp_path, monkeypatch):
+    """Without an injected vector the driver draws the reference's own random start (one
+    OpenMP thread, as the fixtures were made), so the run reproduces the reference's."""
+    monkeypatch.setenv("HPHI_B200_REF_THREADS", "1")
+    g = load_golden(name)
+    with open_case(name) as H:
+        r = H.calc_by_lanczos(output_dir=str(tmp_path))
+        assert r["converged"]
+        alpha, beta = H.lanczos_tridiagonal()
+        check_lanczos_against_reference(g, r["e1"], alpha, beta)
+
+
+@pytest.mark.parametrize("name", golden_cases("tpq"))
+def test_tpq_default_start_matches_reference(name, tmp_path, monkeypatch):
+    monkeypatch.setenv("HPHI_B200_REF_THREADS", "1")
+    g = load_golden(name)
+    ref = g["tpq"]
+    with open_case(name) as H:
+        e = H.calc_by_tpq(output_dir=str(tmp_path), nresult=ref.shape[0])
+    np.testing.assert_allclose(e, ref[:, 1], rtol=E_TOL, atol=1e-12)
+
+
 @pytest.mark.parametrize("name", ["chain16", "hub2x4", "kitaev2x2", "hub6_allterms"])
 def test_lanczos_eigenvector_energy_and_variance(name, tmp_path):
     g = load_golden(name)
