@@ -337,12 +337,12 @@ class Hamiltonian:
         buf = None
         if v_init is not None:
             buf = np.ascontiguousarray(np.stack([_as_hphi_vector(v, self.dim) for v in v_init]))
-        n = 3 + 4 * 4
+        n = 3 + 4 * k
         res = np.zeros(n)
         rc = load_library().hphi_lobpcg(self._h, None if buf is None else _dptr(buf.view(np.float64)),
                                         None if output_dir is None else os.fsencode(output_dir), _dptr(res), n)
         out = {"converged": bool(res[0]), "steps": int(res[1]), "residual": float(res[2])}
-        per = res[3:].reshape(4, 4)
+        per = res[3:].reshape(k, 4)
         for j, key in enumerate(["energy", "var", "doublon", "sz"]):
             out[key] = per[:k, j].copy()
         if rc != 0:

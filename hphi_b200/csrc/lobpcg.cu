@@ -69,10 +69,12 @@ struct LinComb {
   const void *in[kMaxIn];
   void *out[kMaxOut];
   int nin, nout;
+  int accumulate;  // add to the outputs (a later chunk of inputs)
 };
 
-// out_o[r] = sum_j coef[j][o] in_j[r] (coef complex, row-major nin x nout; real vectors use
-// the real parts).  Outputs never alias inputs.
+// out_o[r] (+)= sum_j coef[j][o] in_j[r] (coef complex, row-major nin x nout; real vectors
+// use the real parts).  Outputs never alias inputs.  Larger combinations run as chunks of at
+// most kMaxIn inputs and kMaxOut outputs.
 template <typename T>
 __global__ void lincomb_kernel(int64_t dim, LinComb L, const double *__restrict__ coef) {
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < dim; r += (int64_t)gridDim.x * blockDim.x) {
@@ -83,7 +85,7 @@ __global__ void lincomb_kernel(int64_t dim, LinComb L, const double *__restrict_
 #pragma unroll
     for (int o = 0; o < kMaxOut; o++) {
       if (o < L.nout) {
-        T y = VT<T>::zero();
+        T y = L.accumulate ? ((const T *)L.out[o])[r] : VT<T>::zero();
 #pragma unroll
         for (int j = 0; j < kMaxIn; j++)
           if (j < L.nin) {
@@ -268,30 +270,34 @@ struct Ops {
     return 0;
   }
 
-  // out[o] = sum_j c[j][o] in[j]
+  // out[o] = sum_j c[j][o] in[j], in chunks of kMaxOut outputs x kMaxIn inputs (later input
+  // chunks accumulate into the outputs)
   int lincomb(const std::vector<const void *> &in, const std::vector<void *> &out, const std::vector<zc> &c) {
-    LinComb L{};
-    L.nin = (int)in.size();
-    L.nout = (int)out.size();
-    if (L.nin > kMaxIn || L.nout > kMaxOut) {
-      set_error("lobpcg: exct larger than this engine's block limit (4)");
-      return -1;
-    }
-    std::vector<double> hc(2 * L.nin * L.nout);
-    for (int j = 0; j < L.nin; j++)
-      for (int o = 0; o < L.nout; o++) {
-        hc[2 * (j * L.nout + o)] = c[j * L.nout + o].real();
-        hc[2 * (j * L.nout + o) + 1] = c[j * L.nout + o].imag();
+    const int nin = (int)in.size(), nout = (int)out.size();
+    for (int o0 = 0; o0 < nout; o0 += kMaxOut)
+      for (int j0 = 0; j0 < nin; j0 += kMaxIn) {
+        LinComb L{};
+        L.nin = std::min(kMaxIn, nin - j0);
+        L.nout = std::min(kMaxOut, nout - o0);
+        L.accumulate = j0 > 0;
+        std::vector<double> hc(2 * L.nin * L.nout);
+        for (int j = 0; j < L.nin; j++)
+          for (int o = 0; o < L.nout; o++) {
+            const zc cc = c[(j0 + j) * nout + (o0 + o)];
+            hc[2 * (j * L.nout + o)] = cc.real();
+            hc[2 * (j * L.nout + o) + 1] = cc.imag();
+          }
+        for (int j = 0; j < L.nin; j++) L.in[j] = in[j0 + j];
+        for (int o = 0; o < L.nout; o++) L.out[o] = out[o0 + o];
+        LRET(cuda_ok(cudaMemcpyAsync(d_coef, hc.data(), sizeof(double) * hc.size(), cudaMemcpyHostToDevice,
+                                     s->stream), "coefficients"));
+        if (vt == kReal64) lincomb_kernel<double><<<s->red_blocks, kThreads, 0, s->stream>>>(s->dim, L, d_coef);
+        else lincomb_kernel<cplx><<<s->red_blocks, kThreads, 0, s->stream>>>(s->dim, L, d_coef);
+        LRET(cuda_ok(cudaGetLastError(), "lincomb launch"));
+        // the coefficient buffer is reused by the next call: wait for this one
+        LRET(cuda_ok(cudaStreamSynchronize(s->stream), "lincomb"));
       }
-    for (int j = 0; j < L.nin; j++) L.in[j] = in[j];
-    for (int o = 0; o < L.nout; o++) L.out[o] = out[o];
-    LRET(cuda_ok(cudaMemcpyAsync(d_coef, hc.data(), sizeof(double) * hc.size(), cudaMemcpyHostToDevice, s->stream),
-                 "coefficients"));
-    if (vt == kReal64) lincomb_kernel<double><<<s->red_blocks, kThreads, 0, s->stream>>>(s->dim, L, d_coef);
-    else lincomb_kernel<cplx><<<s->red_blocks, kThreads, 0, s->stream>>>(s->dim, L, d_coef);
-    LRET(cuda_ok(cudaGetLastError(), "lincomb launch"));
-    // the coefficient buffer is reused by the next call: wait for this one
-    return cuda_ok(cudaStreamSynchronize(s->stream), "lincomb");
+    return 0;
   }
 
   // H v into out (out = H v, acc = 0)
@@ -345,10 +351,6 @@ int lobpcg_run(Sector *s, VecType vt, const double *h_init, LobpcgResult *res) {
   const Model &m = s->model;
   const int k = std::max(1, m.k_exct);
   const int64_t dim = s->dim;
-  if (k > kMaxOut || 3 * k > kMaxIn) {
-    set_error("lobpcg: exct > 4 is not supported by this engine");
-    return -1;
-  }
   if (dim < 3 * k) {
     set_error("lobpcg: sector dimension smaller than the LOBPCG subspace (3 * exct)");
     return -1;

@@ -195,11 +195,11 @@ int hphi_tpq(hphi_handle *h, const double *v_init, const char *output_dir, doubl
 /*
  * Block LOBPCG for the exct lowest states (CalcType 3, "CG"; preconditioned when PreCG = 1).
  * v_init: exct start vectors in HPhi's layout, back to back (any norm), or NULL for the
- * reference's single-element starts (initial_iv > 0 on canonical models) or seeded random
- * ones.  Writes zvo_Lanczos_Step.dat and, when converged, zvo_energy.dat into output_dir
- * (NULL: no files).  result (may be NULL, nresult values at most): [0] converged (1/0),
- * [1] steps, [2] last residual 2-norm, then per state [3 + 4i] energy, [4 + 4i] <Hx|Hx>,
- * [5 + 4i] doublon, [6 + 4i] Sz.  exct <= 4.
+ * reference's single-element starts (initial_iv > 0 on canonical models) or its random
+ * ones (see hphi_reference_start).  Writes zvo_Lanczos_Step.dat and, when converged,
+ * zvo_energy.dat into output_dir (NULL: no files).  result (may be NULL, nresult values at
+ * most): [0] converged (1/0), [1] steps, [2] last residual 2-norm, then per state
+ * [3 + 4i] energy, [4 + 4i] <Hx|Hx>, [5 + 4i] doublon, [6 + 4i] Sz.  Any exct up to dim / 3.
  * Replaces: CalcByLOBPCG / LOBPCG_Main (src/CalcByLOBPCG.c:328-776) with phys (src/phys.c:48).
  */
 int hphi_lobpcg(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult);

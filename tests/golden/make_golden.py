@@ -112,6 +112,9 @@ def _cases():
     m = expert.kitaev_heisenberg(2, 2, -1.0, 0.2, calc_type="CG", lanczos_max=400, lanczos_eps=12)
     m.initial_vec_type = 0
     c["lobpcg_kitaev2x2"] = m
+    # six states (more than one block of the engine's linear-combination kernel), random start
+    c["lobpcg_chain10_k6"] = expert.heisenberg(10, expert.chain_bonds(10), calc_type="CG", exct=6,
+                                               lanczos_max=600)
     # Kondo lattices (itinerant ring + one local spin per cell, J S.s as InterAll): canonical
     # with real and complex vectors, and the grand-canonical KondoGC sector.
     c["kondo_chain4"] = expert.kondo_chain(4, 1.0, 1.5, lanczos_max=300)

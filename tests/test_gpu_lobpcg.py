@@ -23,14 +23,14 @@ def _steps_file(path):
 
 
 @pytest.mark.parametrize("name", golden_cases("lobpcg"))
-def test_lobpcg_matches_reference(name, tmp_path):
+def test_lobpcg_matches_reference(name, tmp_path, monkeypatch):
+    # the reference's own start vectors: single-element ones (initial_iv > 0 on canonical
+    # models) or its random ones drawn with one OpenMP thread, as the fixtures were made
+    monkeypatch.setenv("HPHI_B200_REF_THREADS", "1")
     g = load_golden(name)
     ref_steps, ref_states = g["lobpcg_steps"], g["lobpcg_states"]
     with hphi_b200.Hamiltonian(os.path.join(case_dir(name), "namelist.def")) as H:
-        # canonical cases use the reference's single-element starts (initial_iv > 0);
-        # the grand-canonical case gets the reference's own random start injected
-        v_init = None if "list_1" in g else [g["hv0_v1"]]
-        r = H.calc_by_lobpcg(v_init=v_init, output_dir=str(tmp_path))
+        r = H.calc_by_lobpcg(output_dir=str(tmp_path))
     assert r["converged"]
     assert abs(r["steps"] - ref_steps.shape[0]) <= 1, (r["steps"], ref_steps.shape[0])
     np.testing.assert_allclose(r["energy"], ref_states[:, 0], rtol=0, atol=1e-10)

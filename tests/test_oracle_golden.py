@@ -116,11 +116,15 @@ def test_oracle_tpq_energies(name):
 
 def lobpcg_start(d, g):
     """The reference's start vectors: single-element ones for initial_iv > 0 on canonical
-    models (Initialize_wave, src/CalcByLOBPCG.c:220-251), else its dumped first mltply input."""
+    models (Initialize_wave, src/CalcByLOBPCG.c:220-251), else its random ones (one thread,
+    as the fixtures were made; the first equals the dumped first mltply input)."""
+    import hphi_b200
     dim = g["diag"].size - 1
     k = d.k_exct
     if "list_1" not in g or d.initial_iv <= 0:
-        return g["hv0_v1"][None, :]
+        x0 = hphi_b200.reference_start(dim, hphi_b200.REF_LOBPCG, d.initial_iv, 0, d.initial_vec_type, 1, k)
+        assert np.max(np.abs(x0[0, 1:] - g["hv0_v1"][1:])) < 1e-15
+        return x0
     x0 = np.zeros((k, dim + 1), complex)
     for ie in range(k):
         iv = (dim // 2 + d.initial_iv + ie) % dim + 1
@@ -138,8 +142,9 @@ def test_oracle_lobpcg_matches_reference(name):
     rows, x = O.lobpcg(d, lists, diag, lobpcg_start(d, g))
     ref = g["lobpcg_steps"]
     assert rows.shape[0] == ref.shape[0]
-    # the step file prints 6 significant digits
-    np.testing.assert_allclose(rows[:, 1:], ref[:, 1:], rtol=1e-5, atol=0)
+    # the step file prints 6 significant digits; residuals near 1e-7 of degenerate states
+    # differ by rounding at the 1e-11 level
+    np.testing.assert_allclose(rows[:, 1:], ref[:, 1:], rtol=1e-5, atol=1e-10)
     H = O.dense_hamiltonian(d, lists, diag)
     e = np.real(np.sum(x.conj() * (x @ H.T), axis=1))
     np.testing.assert_allclose(e, g["lobpcg_states"][:, 0], rtol=0, atol=1e-12)
