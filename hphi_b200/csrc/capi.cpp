@@ -326,9 +326,19 @@ int hphi_lanczos(hphi_handle *h, const double *v_init, const char *output_dir, d
   LanczosOptions opt;
   opt.eigenvector = (s->model.calc_eigenvec != -1);
   opt.copy_eigenvector = opt.eigenvector;
+  // ReStart (src/Lanczos_EigenValue.c:80-101, 287-297): 1 writes the restart files, 3 reads
+  // them, 2 does both; they live in output_dir
+  LanczosRestart resume;
+  const int rmode = s->model.restart;
+  if (output_dir && (rmode == 2 || rmode == 3)) {
+    if (read_lanczos_restart(*s, output_dir, &resume) != 0) return -1;
+    opt.resume = &resume;
+  }
+  opt.restart_out = output_dir && (rmode == 1 || rmode == 2);
   LanczosResult &r = h->last_lanczos;
   r = LanczosResult();
   const int rc = lanczos_run(s, vt, v_init, opt, &r);
+  if (rc == 0 && r.has_restart && write_lanczos_restart(*s, r.restart, output_dir) != 0) return -1;
   if (result && nresult > 0) {
     double v[17] = {r.converged ? 1.0 : 0.0, (double)r.steps, r.e_target, 0, 0, 0, 0, r.energy, r.var, r.doublon, r.sz,
                     r.check_diff, r.check_var, (double)r.cg_rounds, (double)r.cg_iterations, r.cg_diff, r.cg_var};

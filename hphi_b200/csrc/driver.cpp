@@ -319,8 +319,15 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   RET(cuda_ok(cudaMalloc(&Q.p, esz * dim), "alloc Q"));
   RET(cuda_ok(cudaMalloc(&ST.p, sizeof(double) * 32), "alloc scalars"));  // slots used: [0, 29)
   const bool fixed = opt.fixed_steps > 0;
-  int max_steps = fixed ? opt.fixed_steps : m.lanczos_max;
+  const LanczosRestart *rs = opt.resume;
+  const int n0 = rs ? rs->steps : 0;  // steps already done (restart)
+  res->resumed = (rs != nullptr);
+  int max_steps = fixed ? opt.fixed_steps : n0 + m.lanczos_max;
   if ((int64_t)max_steps > dim) max_steps = (int)dim;
+  if (rs && (n0 < 1 || n0 >= max_steps)) {
+    set_error("Lanczos restart: the stored step count leaves no step to run");
+    return -1;
+  }
   if (!fixed && dim < m.lanczos_target) max_steps = (int)dim;
   RET(cuda_ok(cudaMalloc(&AL.p, sizeof(double) * (max_steps + 2)), "alloc alpha"));
   RET(cuda_ok(cudaMalloc(&BE.p, sizeof(double) * (max_steps + 2)), "alloc beta"));
@@ -333,11 +340,28 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
     RET(cuda_ok(cudaMemcpyAsync(V0.p, Q.p, esz * dim, cudaMemcpyDeviceToDevice, s->stream), "copy V0"));
   }
   double *st = (double *)ST.p;
-  const double init_st[6] = {0.0, 0.0, 0.0, 1.0, 0.0, 0.0};  // acc = 0, s = 1
-  RET(cuda_ok(cudaMemcpyAsync(st, init_st, sizeof(init_st), cudaMemcpyHostToDevice, s->stream), "init scalars"));
-  RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
-
   std::vector<double> alpha(max_steps + 2, 0.0), beta(max_steps + 2, 0.0);
+  if (rs) {
+    // HPhi's next step takes v1' = (v0 - alpha_n v1) / beta_n: here Q = v0 - alpha_n v1 with
+    // scale 1/beta_n and P = v1 with acc = -beta_n (src/Lanczos_EigenValue.c:80-101, 153-160)
+    DevBuf T;
+    RET(cuda_ok(cudaMalloc(&T.p, esz * dim), "alloc restart"));
+    RET(vec_from_host_c128(s, vt, rs->v1.data(), T.p));
+    RET(to_native(s, vt, T.p, P.p));
+    RET(vec_from_host_c128(s, vt, rs->v0.data(), T.p));
+    RET(to_native(s, vt, T.p, Q.p));
+    RET(vec_axpby(s, vt, -rs->alpha[n0], P.p, 1.0, Q.p));
+    for (int i = 1; i <= n0; i++) { alpha[i] = rs->alpha[i]; beta[i] = rs->beta[i]; }
+    RET(cuda_ok(cudaMemcpyAsync(AL.p, alpha.data(), sizeof(double) * (n0 + 1), cudaMemcpyHostToDevice, s->stream), "alpha"));
+    RET(cuda_ok(cudaMemcpyAsync(BE.p, beta.data(), sizeof(double) * (n0 + 1), cudaMemcpyHostToDevice, s->stream), "beta"));
+    const double rs_st[6] = {0.0, 0.0, -rs->beta[n0], 1.0 / rs->beta[n0], 0.0, 0.0};
+    RET(cuda_ok(cudaMemcpyAsync(st, rs_st, sizeof(rs_st), cudaMemcpyHostToDevice, s->stream), "restart scalars"));
+    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+  } else {
+    const double init_st[6] = {0.0, 0.0, 0.0, 1.0, 0.0, 0.0};  // acc = 0, s = 1
+    RET(cuda_ok(cudaMemcpyAsync(st, init_st, sizeof(init_st), cudaMemcpyHostToDevice, s->stream), "init scalars"));
+    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+  }
   void *pp = P.p, *qq = Q.p;
   auto do_step = [&](int k) -> int {
     RET(hv_native(s, vt, qq, pp, st + 2, st + 0));
@@ -353,9 +377,10 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   res->lines.clear();
   res->converged = false;
   res->steps = 0;
-  const int batch = opt.batch > 0 ? opt.batch : (fixed ? 32 : (dim >= (1 << 20) ? 1 : 16));
-  int done = 0;       // steps executed on the device
-  int checked = 1;    // steps examined on the host
+  // restart output needs the device state of the exact last step: check every step
+  const int batch = opt.restart_out ? 1 : (opt.batch > 0 ? opt.batch : (fixed ? 32 : (dim >= (1 << 20) ? 1 : 16)));
+  int done = n0;            // steps executed on the device
+  int checked = rs ? n0 : 1;  // steps examined on the host
   double ebefor = 0.0;
   std::vector<double> E(5, 0.0);
   const double ns = (double)m.nsite;
@@ -432,6 +457,37 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   if (!res->converged) {
     res->steps = checked;
   }
+  if (opt.restart_out && dim > 1) {
+    // HPhi's v0 and v1 after the last step k (src/Lanczos_EigenValue.c:287-291): v1 = q_k =
+    // P / beta_{k-1} (P holds q_k unscaled; beta_0 = 1, or the stored beta_n when resumed),
+    // v0 = H q_k - beta_{k-1} q_{k-1} = Q + alpha_k v1.  The files record (exit step - 1)
+    // coefficients: the converged step, or one past the last step when none converged.
+    const int k = checked;
+    LanczosRestart &R = res->restart;
+    R.dnorm = rs ? rs->dnorm : 0.0;
+    R.steps = res->converged ? k - 1 : k;
+    R.vec_steps = R.steps;
+    R.alpha.assign(alpha.begin(), alpha.begin() + R.steps + 1);
+    R.beta.assign(beta.begin(), beta.begin() + R.steps + 1);
+    const double bprev = (k >= 2) ? beta[k - 1] : 1.0;
+    DevBuf A, B;
+    RET(cuda_ok(cudaMalloc(&A.p, esz * dim), "alloc restart"));
+    RET(cuda_ok(cudaMalloc(&B.p, esz * dim), "alloc restart"));
+    RET(cuda_ok(cudaMemcpyAsync(A.p, pp, esz * dim, cudaMemcpyDeviceToDevice, s->stream), "copy"));
+    RET(vec_scale(s, vt, 1.0 / bprev, A.p));                 // v1 (native)
+    RET(cuda_ok(cudaMemcpyAsync(B.p, qq, esz * dim, cudaMemcpyDeviceToDevice, s->stream), "copy"));
+    RET(vec_axpby(s, vt, alpha[k], A.p, 1.0, B.p));          // v0 (native)
+    R.v0.assign(2 * (dim + 1), 0.0);
+    R.v1.assign(2 * (dim + 1), 0.0);
+    RET(from_native(s, vt, B.p, pp));
+    RET(vec_to_host_c128(s, vt, pp, R.v0.data()));
+    RET(from_native(s, vt, A.p, pp));
+    RET(vec_to_host_c128(s, vt, pp, R.v1.data()));
+    // HPhi's loop variable ends at the converged step or one past the last step, and it
+    // skips the files when that is two steps past the run's start
+    const int exit_stp = res->converged ? k : k + 1;
+    res->has_restart = (exit_stp != (rs ? n0 : 1) + 2);
+  }
   const int itr = res->steps;
   res->alpha.assign(alpha.begin() + 1, alpha.begin() + 1 + itr);
   res->beta.assign(beta.begin() + 1, beta.begin() + 1 + itr);
@@ -439,6 +495,7 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   const int nev = std::min(itr, std::max(m.nvec, m.lanczos_target + 1));
   for (int q = 0; q < nev && q < itr; q++) res->energies.push_back(tridiag_eigenvalue(res->alpha.data(), res->beta.data(), itr, q));
   if (!res->converged) {
+    if (opt.restart_out) return 0;  // restart mode: the files carry the run on
     set_error("Lanczos Eigenvalue is not converged in this process.");
     return -1;
   }
@@ -516,15 +573,82 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   return 0;
 }
 
+// OutputTMComponents / OutputLanczosVector (src/Lanczos_EigenValue.c:457-500, 697-720).
+int write_lanczos_restart(const Sector &s, const LanczosRestart &r, const std::string &outdir) {
+  RET(ensure_dir(outdir));
+  const std::string head = s.model.data_head;
+  const std::string tm = join(outdir, head + "_TMComponents.dat");
+  FILE *f = fopen(tm.c_str(), "w");
+  if (!f) { set_error("cannot write " + tm); return -1; }
+  fprintf(f, "%d \n", r.steps);
+  fprintf(f, "%.10lf \n", r.dnorm);
+  for (int i = 1; i <= r.steps; i++) fprintf(f, "%.10lf %.10lf \n", r.alpha[i], r.beta[i]);
+  fclose(f);
+  const std::string vf = join(outdir, head + "_recalcvec_rank_0.dat");
+  f = fopen(vf.c_str(), "wb");
+  if (!f) { set_error("cannot write " + vf); return -1; }
+  const unsigned long stp = (unsigned long)r.vec_steps;
+  const long dim = (long)s.dim;
+  fwrite(&stp, sizeof(stp), 1, f);
+  fwrite(&dim, sizeof(dim), 1, f);
+  fwrite(r.v0.data(), sizeof(double), r.v0.size(), f);
+  fwrite(r.v1.data(), sizeof(double), r.v1.size(), f);
+  fclose(f);
+  return 0;
+}
+
+// ReadInitialVector / ReadTMComponents (src/Lanczos_EigenValue.c:428-455, 624-695): the
+// coefficients come back with the 10 decimals they were printed with.
+int read_lanczos_restart(const Sector &s, const std::string &outdir, LanczosRestart *r) {
+  const std::string head = s.model.data_head;
+  const std::string vf = join(outdir, head + "_recalcvec_rank_0.dat");
+  FILE *f = fopen(vf.c_str(), "rb");
+  if (!f) { set_error("Lanczos restart: cannot open " + vf); return -1; }
+  unsigned long stp = 0;
+  long dim = 0;
+  const size_t n = 2 * (size_t)(s.dim + 1);
+  r->v0.assign(n, 0.0);
+  r->v1.assign(n, 0.0);
+  const bool ok = fread(&stp, sizeof(stp), 1, f) == 1 && fread(&dim, sizeof(dim), 1, f) == 1 && dim == (long)s.dim &&
+                  fread(r->v0.data(), sizeof(double), n, f) == n && fread(r->v1.data(), sizeof(double), n, f) == n;
+  fclose(f);
+  if (!ok) { set_error("Lanczos restart: " + vf + " does not hold vectors of this sector"); return -1; }
+  const std::string tm = join(outdir, head + "_TMComponents.dat");
+  f = fopen(tm.c_str(), "r");
+  if (!f) { set_error("Lanczos restart: cannot open " + tm); return -1; }
+  long steps = 0;
+  char buf[256];
+  if (!fgets(buf, sizeof(buf), f) || sscanf(buf, "%ld", &steps) != 1 || !fgets(buf, sizeof(buf), f) ||
+      sscanf(buf, "%lf", &r->dnorm) != 1) {
+    fclose(f);
+    set_error("Lanczos restart: malformed " + tm);
+    return -1;
+  }
+  r->alpha.assign(1, 0.0);
+  r->beta.assign(1, 0.0);
+  double a, b;
+  while (fgets(buf, sizeof(buf), f))
+    if (sscanf(buf, "%lf %lf", &a, &b) == 2) { r->alpha.push_back(a); r->beta.push_back(b); }
+  fclose(f);
+  if ((long)r->alpha.size() - 1 != steps || (unsigned long)steps != stp) {
+    set_error("Lanczos restart: input files for vector and TMcomponents are incorrect");
+    return -1;
+  }
+  r->steps = (int)steps;
+  r->vec_steps = (int)stp;
+  return 0;
+}
+
 int write_lanczos_outputs(const Sector &s, const LanczosResult &r, const std::string &outdir) {
   RET(ensure_dir(outdir));
   const Model &m = s.model;
   const std::string step_file = join(outdir, m.data_head + "_Lanczos_Step.dat");
-  FILE *f = fopen(step_file.c_str(), "w");
+  // a continued run appends to the step file (src/Lanczos_EigenValue.c:200-222)
+  FILE *f = fopen(step_file.c_str(), r.resumed ? "a" : "w");
   if (!f) { set_error("cannot write " + step_file); return -1; }
   for (const auto &l : r.lines) fputs(l.c_str(), f);
   fclose(f);
-  if (m.calc_eigenvec == -1) return 0;
+  if (m.calc_eigenvec == -1 || !r.converged) return 0;
   const std::string ef = join(outdir, m.data_head + "_energy.dat");
   f = fopen(ef.c_str(), "w");
   if (!f) { set_error("cannot write " + ef); return -1; }

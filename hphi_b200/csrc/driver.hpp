@@ -7,11 +7,26 @@
 
 namespace hphi {
 
+// Lanczos restart data in HPhi's files (src/Lanczos_EigenValue.c:419-500, 620-720):
+// zvo_TMComponents.dat holds the step count, dnorm and alpha_i, beta_i printed with 10
+// decimals; zvo_recalcvec_rank_0.dat the step, dim and HPhi's v0 and v1 (1-based complex128)
+// of the last step: v1 = q_n, v0 = H q_n - beta_{n-1} q_{n-1}.
+struct LanczosRestart {
+  int steps = 0;                     // alpha / beta entries
+  int vec_steps = 0;                 // step recorded with the vectors
+  double dnorm = 0.0;
+  std::vector<double> alpha, beta;   // [1 .. steps] (index 0 unused)
+  std::vector<double> v0, v1;        // 2 * (dim + 1) doubles each
+};
+
 struct LanczosOptions {
   bool eigenvector = false;       // replay the recurrence for the k_exct-th eigenvector
   bool copy_eigenvector = false;  // copy it back to the host (HPhi layout)
   int batch = 0;                  // steps between host convergence checks (0: automatic)
   int fixed_steps = 0;            // > 0: exactly this many steps, convergence test off
+  bool restart_out = false;       // fill LanczosResult::restart (ReStart 1 / 2); then a run
+                                  // that does not converge is not an error
+  const LanczosRestart *resume = nullptr;  // continue from these (ReStart 2 / 3)
 };
 
 struct LanczosResult {
@@ -22,6 +37,9 @@ struct LanczosResult {
   std::vector<double> alpha, beta;   // alpha[0..steps), beta[0..steps)
   std::vector<double> energies;      // lowest eigenvalues of the final tridiagonal matrix
   std::vector<std::string> lines;    // zvo_Lanczos_Step.dat
+  bool resumed = false;              // continued from restart files (step lines are appended)
+  bool has_restart = false;          // restart files to write (restart_out)
+  LanczosRestart restart;
   double energy = 0.0, var = 0.0, doublon = 0.0, sz = 0.0;
   // accuracy check of the Lanczos vector (src/CalcByLanczos.c:120-121) and, when it fails
   // with CalcEigenVec 0, the CG refinement (src/CG_EigenVector.c): relative variance and
@@ -61,6 +79,8 @@ int hashed_start(const Sector &s, uint64_t seed, bool complex_vec, std::vector<d
 // h_init: normalised start vector in HPhi's 1-based complex128 layout.
 int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOptions &opt, LanczosResult *res);
 int write_lanczos_outputs(const Sector &s, const LanczosResult &r, const std::string &outdir);
+int write_lanczos_restart(const Sector &s, const LanczosRestart &r, const std::string &outdir);
+int read_lanczos_restart(const Sector &s, const std::string &outdir, LanczosRestart *r);
 // h_init: start vector (any norm) of sample rand_i; writes SS/Norm/Flct_rand<rand_i>.dat.
 int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::string &outdir, TpqResult *res);
 // Block LOBPCG for the exct lowest states (CalcType 3).  h_init: exct start vectors in

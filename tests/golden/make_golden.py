@@ -14,6 +14,8 @@ of oracle/ref_hooks.c:
   tpq                            SS_rand0.dat rows (TPQ cases)
 refstart_* directories hold start.npz: the first mltply input of a golden case's input rerun
 with several OpenMP threads (the reference's per-thread random start vectors).
+restart_* directories hold inputs a/ and b/ and restart.npz: the restart files run a wrote
+and the steps and energy of run b continued from them.
 Large cases store only SHA-256 digests of the lists (sha_list_1 ...).
 
 Run in a container that has the reference sources and oracle/_ref/HPhi_ref
@@ -232,17 +234,64 @@ def make_start_case(name: str, src: str, threads: int) -> None:
     np.savez_compressed(os.path.join(out, "start.npz"), source=np.array(src), threads=np.array(threads), v1=v1)
 
 
+def _restart_cases():
+    """Lanczos restart: input a/ (ReStart 1, Lanczos_max 20: stops unconverged and writes the
+    restart files) and b/ (ReStart 3: continues from them to convergence)."""
+    def model(restart, lmax):
+        m = expert.heisenberg(14, expert.chain_bonds(14), lanczos_max=lmax, calc_eigenvec=0)
+        m.restart = restart
+        return m
+    return {"restart_chain14": (model(1, 20), model(3, 200))}
+
+
+def make_restart_case(name: str, ma, mb) -> None:
+    out = os.path.join(HERE, name)
+    shutil.rmtree(out, ignore_errors=True)
+    ma.write(os.path.join(out, "a"))
+    mb.write(os.path.join(out, "b"))
+    data = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for f in os.listdir(os.path.join(out, "a")):
+            shutil.copy(os.path.join(out, "a", f), tmp)
+        if run_ref.run(tmp, threads=1, dump_call=-1).returncode != 0:
+            raise RuntimeError(f"{name}: reference run a failed")
+        od = os.path.join(tmp, "output")
+        lines = open(os.path.join(od, "zvo_TMComponents.dat")).read().split("\n")
+        data["tm_steps"] = np.array(int(lines[0].split()[0]))
+        data["tm_dnorm"] = np.array(float(lines[1].split()[0]))
+        ab = np.array([[float(x) for x in l.split()] for l in lines[2:] if l.strip()])
+        data["tm_alpha"], data["tm_beta"] = ab[:, 0], ab[:, 1]
+        with open(os.path.join(od, "zvo_recalcvec_rank_0.dat"), "rb") as f:
+            stp, dim = np.frombuffer(f.read(16), dtype=np.int64)
+            v = np.frombuffer(f.read(), dtype=np.complex128)
+        data["rv_step"] = np.array(stp)
+        data["rv_v0"], data["rv_v1"] = v[:dim + 1].copy(), v[dim + 1:2 * (dim + 1)].copy()
+        data["a_step_lines"] = np.array(open(os.path.join(od, "zvo_Lanczos_Step.dat")).read().splitlines())
+        for f in os.listdir(os.path.join(out, "b")):
+            shutil.copy(os.path.join(out, "b", f), tmp)
+        if run_ref.run(tmp, threads=1, dump_call=-1).returncode != 0:
+            raise RuntimeError(f"{name}: reference run b failed")
+        steps = run_ref.lanczos_steps(tmp)
+        data["b_steps"] = np.array([s for s, _ in steps])
+        data["b_step_vals"] = np.array([[np.nan if v is None else v for v in (vals + [None] * 6)[:6]]
+                                        for _, vals in steps])
+        data["b_energy_state"] = run_ref.energy_states(tmp)[0]
+    np.savez_compressed(os.path.join(out, "restart.npz"), **data)
+
+
 def main(argv) -> None:
     if not run_ref.available():
         raise SystemExit("oracle/_ref/HPhi_ref is missing: run `make -C oracle` first")
-    small, large, starts = _cases(), _large_cases(), _start_cases()
-    names = argv or list(small) + list(large) + list(starts)
+    small, large, starts, restarts = _cases(), _large_cases(), _start_cases(), _restart_cases()
+    names = argv or list(small) + list(large) + list(starts) + list(restarts)
     for n in names:
         print("case", n, flush=True)
         if n in small:
             make_case(n, small[n])
         elif n in starts:
             make_start_case(n, *starts[n])
+        elif n in restarts:
+            make_restart_case(n, *restarts[n])
         else:
             make_case(n, large[n], large=True)
 
