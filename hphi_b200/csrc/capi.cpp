@@ -30,6 +30,9 @@ struct hphi_handle {
   void *d_stage1 = nullptr;
   void *d_perm0 = nullptr;   // native-order scratch of the HPhi-order device entry points
   void *d_perm1 = nullptr;
+  cudaStream_t copy_up = nullptr;    // hphi_mltply: v0 upload, overlapping the H v1 compute
+  cudaStream_t copy_back = nullptr;  // hphi_mltply: v0 download
+  std::vector<cudaEvent_t> ev;       // hphi_mltply: per chunk uploaded / updated, plus v1 consumed
 };
 
 namespace hphi {
@@ -118,6 +121,10 @@ void hphi_close(hphi_handle *h) {
     cudaFree(h->d_stage1);
     cudaFree(h->d_perm0);
     cudaFree(h->d_perm1);
+    if (h->copy_up) cudaStreamDestroy(h->copy_up);
+    if (h->copy_back) cudaStreamDestroy(h->copy_back);
+    for (cudaEvent_t e : h->ev)
+      if (e) cudaEventDestroy(e);
     sector_free(h->sector);
   }
   delete h;
@@ -247,23 +254,120 @@ int hphi_from_native(hphi_handle *h, int vec_type, const void *d_native, void *d
 }
 
 int hphi_mltply(hphi_handle *h, double *v0, const double *v1, double *prdct) {
+  // HPhi's mltply on host vectors.  Stream st: upload v1, H v1 on the device (a real H takes
+  // the real kernels on the real and imaginary parts), then chunk by chunk v0 += H v1.  Once
+  // v1 has been read, v0 uploads chunk by chunk into v1's buffer on copy_up (overlapping the
+  // H v1 compute), and each updated chunk downloads on copy_back while the next one uploads.
   CHECK_HANDLE(h);
   Sector *s = h->sector;
   cudaSetDevice(s->device);
-  const size_t bytes = sizeof(cplx) * (size_t)s->dim;
+  const int64_t dim = s->dim;
+  const size_t bytes = sizeof(cplx) * (size_t)dim;
+  constexpr int64_t kChunk = 4 << 20;  // complex elements per chunk (64 MB)
+  const int nchunk = (int)((dim + kChunk - 1) / kChunk);
   if (!h->d_stage0) {
-    if (cuda_fail(cudaMalloc(&h->d_stage0, bytes), "alloc v0")) return -1;
-    if (cuda_fail(cudaMalloc(&h->d_stage1, bytes), "alloc v1")) {
-      cudaFree(h->d_stage0);
-      h->d_stage0 = nullptr;
+    void *a = nullptr, *b = nullptr;
+    if (cuda_fail(cudaMalloc(&a, bytes), "alloc") || cuda_fail(cudaMalloc(&b, bytes), "alloc") ||
+        cuda_fail(cudaStreamCreateWithFlags(&h->copy_up, cudaStreamNonBlocking), "stream") ||
+        cuda_fail(cudaStreamCreateWithFlags(&h->copy_back, cudaStreamNonBlocking), "stream")) {
+      cudaFree(a); cudaFree(b);
+      return -1;
+    }
+    h->d_stage0 = a; h->d_stage1 = b;
+  }
+  if (!h->d_perm0) {
+    if (cuda_fail(cudaMalloc(&h->d_perm0, bytes), "alloc scratch")) return -1;
+    if (cuda_fail(cudaMalloc(&h->d_perm1, bytes), "alloc scratch")) {
+      cudaFree(h->d_perm0);
+      h->d_perm0 = nullptr;
       return -1;
     }
   }
-  int rc = vec_from_host_c128(s, kComplex128, v1, h->d_stage1);
-  if (rc == 0) rc = vec_from_host_c128(s, kComplex128, v0, h->d_stage0);
-  if (rc == 0) rc = hphi_mltply_device(h, HPHI_COMPLEX128, h->d_stage0, h->d_stage1, 1.0, 1.0, prdct);
-  if (rc == 0) rc = vec_to_host_c128(s, kComplex128, h->d_stage0, v0);
-  return rc;
+  while ((int)h->ev.size() < 2 * nchunk + 1) {
+    cudaEvent_t e;
+    if (cuda_fail(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event")) return -1;
+    h->ev.push_back(e);
+  }
+  cudaEvent_t v1_done = h->ev[2 * nchunk];
+  cudaStream_t st = s->stream;
+  // v1 (elements 1 .. dim of the 1-based array)
+  if (cuda_fail(cudaMemcpyAsync(h->d_stage1, v1 + 2, bytes, cudaMemcpyHostToDevice, st), "copy v1")) return -1;
+  double out[4] = {0, 0, 0, 0};
+  const double c01[2] = {0.0, 1.0};
+  if (cuda_fail(cudaMemcpyAsync(h->d_scal, c01, sizeof(c01), cudaMemcpyHostToDevice, st), "coef")) return -1;
+  const bool nat = has_native_order(s);
+  const bool real_h = !s->model.complex_terms;
+  double *re = (double *)h->d_perm0, *im = re + dim, *hre = (double *)h->d_perm1, *him = hre + dim;
+  // read v1 into the compute buffers, then free its buffer for v0
+  if (real_h) {
+    const void *src = h->d_stage1;
+    if (nat) {
+      if (to_native(s, kComplex128, h->d_stage1, h->d_stage0) != 0) return -1;
+      src = h->d_stage0;
+    }
+    if (vec_split_c128(s, src, re, im) != 0) return -1;
+  } else if (nat) {
+    if (to_native(s, kComplex128, h->d_stage1, h->d_perm1) != 0) return -1;
+  } else if (cuda_fail(cudaMemcpyAsync(h->d_perm1, h->d_stage1, bytes, cudaMemcpyDeviceToDevice, st), "copy")) {
+    return -1;
+  }
+  if (cuda_fail(cudaEventRecord(v1_done, st), "event") || cuda_fail(cudaStreamWaitEvent(h->copy_up, v1_done, 0), "wait"))
+    return -1;
+  cplx *v0d = (cplx *)h->d_stage1;
+  for (int k = 0; k < nchunk; k++) {
+    const int64_t c0 = (int64_t)k * kChunk, n = std::min<int64_t>(kChunk, dim - c0);
+    if (cuda_fail(cudaMemcpyAsync(v0d + c0, v0 + 2 * (1 + c0), sizeof(cplx) * n, cudaMemcpyHostToDevice, h->copy_up),
+                  "copy v0") ||
+        cuda_fail(cudaEventRecord(h->ev[k], h->copy_up), "event"))
+      return -1;
+  }
+  // H v1 into d_stage0 (HPhi order)
+  if (real_h) {
+    if ((nat ? hv_native(s, kReal64, re, hre, h->d_scal, h->d_scal + 2)
+             : hv_launch(s, kReal64, re, hre, h->d_scal, h->d_scal + 2)) != 0)
+      return -1;
+    if ((nat ? hv_native(s, kReal64, im, him, h->d_scal, h->d_scal + 4)
+             : hv_launch(s, kReal64, im, him, h->d_scal, h->d_scal + 4)) != 0)
+      return -1;
+    if (nat) {
+      if (vec_join_c128(s, hre, him, h->d_perm0) != 0 || from_native(s, kComplex128, h->d_perm0, h->d_stage0) != 0)
+        return -1;
+    } else if (vec_join_c128(s, hre, him, h->d_stage0) != 0) {
+      return -1;
+    }
+  } else {
+    if ((nat ? hv_native(s, kComplex128, h->d_perm1, h->d_perm0, h->d_scal, h->d_scal + 2)
+             : hv_launch(s, kComplex128, h->d_perm1, h->d_perm0, h->d_scal, h->d_scal + 2)) != 0)
+      return -1;
+    if (nat ? from_native(s, kComplex128, h->d_perm0, h->d_stage0) != 0
+            : cuda_fail(cudaMemcpyAsync(h->d_stage0, h->d_perm0, bytes, cudaMemcpyDeviceToDevice, st), "copy"))
+      return -1;
+  }
+  if (cuda_fail(cudaMemcpyAsync(out, h->d_scal + 2, sizeof(out), cudaMemcpyDeviceToHost, st), "prdct")) return -1;
+  // v0 += H v1 per chunk, downloaded as it is done
+  const cplx *hv = (const cplx *)h->d_stage0;
+  for (int k = 0; k < nchunk; k++) {
+    const int64_t c0 = (int64_t)k * kChunk, n = std::min<int64_t>(kChunk, dim - c0);
+    if (cuda_fail(cudaStreamWaitEvent(st, h->ev[k], 0), "wait") || vec_add_c128(s, st, n, v0d + c0, hv + c0) != 0 ||
+        cuda_fail(cudaEventRecord(h->ev[nchunk + k], st), "event") ||
+        cuda_fail(cudaStreamWaitEvent(h->copy_back, h->ev[nchunk + k], 0), "wait") ||
+        cuda_fail(cudaMemcpyAsync(v0 + 2 * (1 + c0), v0d + c0, sizeof(cplx) * n, cudaMemcpyDeviceToHost, h->copy_back),
+                  "copy back"))
+      return -1;
+  }
+  if (cuda_fail(cudaStreamSynchronize(h->copy_back), "sync") || cuda_fail(cudaStreamSynchronize(st), "sync") ||
+      cuda_fail(cudaStreamSynchronize(h->copy_up), "sync"))
+    return -1;
+  if (prdct) {
+    if (real_h) {
+      prdct[0] = out[0] + out[2];  // <a|Ha> + <b|Hb>; a real symmetric H has no imaginary part
+      prdct[1] = 0.0;
+    } else {
+      prdct[0] = out[0];
+      prdct[1] = out[1];
+    }
+  }
+  return 0;
 }
 
 int hphi_mltply_device_async(hphi_handle *h, int vec_type, void *d_v0, const void *d_v1, const double *d_coef,

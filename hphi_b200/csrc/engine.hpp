@@ -137,6 +137,11 @@ int vec_cg_sweep(Sector *s, VecType vt, double a, double shift, const void *p, c
 // x[i] += amp * start_value(seed, configuration of row i, 0) on the real part (HPhi order).
 int vec_add_hashed(Sector *s, VecType vt, uint64_t seed, double amp, void *d_x);
 
+// complex128 <-> real and imaginary parts (n = dim); y[0, n) += x[0, n) on stream st.
+int vec_split_c128(Sector *s, const void *d_c, double *d_re, double *d_im);
+int vec_join_c128(Sector *s, const double *d_re, const double *d_im, void *d_c);
+int vec_add_c128(Sector *s, cudaStream_t st, int64_t n, void *d_y, const void *d_x);
+
 // Copies between HPhi's 1-based complex128 host layout and a device vector.
 int vec_from_host_c128(Sector *s, VecType vt, const double *h_v_1based, void *d_v);
 int vec_to_host_c128(Sector *s, VecType vt, const void *d_v, double *h_v_1based);

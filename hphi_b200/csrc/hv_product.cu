@@ -223,6 +223,8 @@ __global__ void __launch_bounds__(kProdThreads, 2) prod_hv_kernel(ProdArgs a, co
 constexpr int kDownThreads = 1024;            // row pass: one CTA per SM, two rows at a time
 constexpr int kRow2Bytes = 103168;            // shared-memory offset of the second row (>= (12870 + 16) * 8)
 constexpr int kUpThreads = 128;               // column pass
+constexpr int kUpBatch = 8;                   // source loads in flight per thread
+constexpr int kUpMinBlocks = 12;               // CTAs per SM (40 registers)
 constexpr int kUpChunk = 2 * kUpThreads;      // columns per column-pass task (two per thread)
 
 struct TwoPassArgs {
@@ -371,7 +373,7 @@ __global__ void __launch_bounds__(kDownThreads, 1) prod_down_kernel(ProdArgs a, 
 // striding; part[blockIdx] = sum of v1 . (up hops) v1 over the CTA's tasks.  VEC2: Dc is even,
 // so a thread's two columns are one aligned 16-byte load.
 template <bool VEC2, bool UNIFORM>
-__global__ void __launch_bounds__(kUpThreads, 2048 / kUpThreads) prod_up_kernel(ProdArgs a, TwoPassArgs b, const double *__restrict__ v1,
+__global__ void __launch_bounds__(kUpThreads, kUpMinBlocks) prod_up_kernel(ProdArgs a, TwoPassArgs b, const double *__restrict__ v1,
                                                              double *__restrict__ v0, const double *__restrict__ coef,
                                                              double *__restrict__ part) {
   __shared__ int s_src[kMaxUpWidth];
@@ -395,10 +397,10 @@ __global__ void __launch_bounds__(kUpThreads, 2048 / kUpThreads) prod_up_kernel(
     const bool pair = VEC2 || d + 1 < Dc;
     double h0 = 0.0, h1 = 0.0;
     int k = 0;
-    for (; k + 4 <= nu; k += 4) {
-      double w0[4], w1[4];
+    for (; k + kUpBatch <= nu; k += kUpBatch) {
+      double w0[kUpBatch], w1[kUpBatch];
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
+      for (int q = 0; q < kUpBatch; q++) {
         const double *sp = v1 + (int64_t)(s_src[k + q] & 0x7FFFFFFF) * Dc + d;
         if (VEC2) {
           const double2 sv = __ldg(reinterpret_cast<const double2 *>(sp));
@@ -409,7 +411,7 @@ __global__ void __launch_bounds__(kUpThreads, 2048 / kUpThreads) prod_up_kernel(
         }
       }
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
+      for (int q = 0; q < kUpBatch; q++) {
         if (UNIFORM) {
           const uint32_t sg = (uint32_t)s_src[k + q] & 0x80000000u;
           h0 += flip_sign(w0[q], sg);

@@ -358,3 +358,42 @@ int vec_add_hashed(Sector *s, VecType vt, uint64_t seed, double amp, void *x) {
 }
 
 }  // namespace hphi
+
+namespace hphi {
+namespace {
+__global__ void split_c128_kernel(int64_t n, const cplx *__restrict__ c, double *__restrict__ re,
+                                  double *__restrict__ im) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const cplx v = c[i];
+    re[i] = v.x;
+    im[i] = v.y;
+  }
+}
+__global__ void join_c128_kernel(int64_t n, const double *__restrict__ re, const double *__restrict__ im,
+                                 cplx *__restrict__ c) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    c[i] = cplx{re[i], im[i]};
+}
+__global__ void add_c128_kernel(int64_t n, cplx *__restrict__ y, const cplx *__restrict__ x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = y[i] + x[i];
+}
+}  // namespace
+
+int vec_split_c128(Sector *s, const void *c, double *re, double *im) {
+  split_c128_kernel<<<s->red_blocks, kThreads, 0, s->stream>>>(s->dim, (const cplx *)c, re, im);
+  return check_launch("vec_split_c128");
+}
+
+int vec_join_c128(Sector *s, const double *re, const double *im, void *c) {
+  join_c128_kernel<<<s->red_blocks, kThreads, 0, s->stream>>>(s->dim, re, im, (cplx *)c);
+  return check_launch("vec_join_c128");
+}
+
+int vec_add_c128(Sector *s, cudaStream_t st, int64_t n, void *y, const void *x) {
+  add_c128_kernel<<<s->num_sms * 4, kThreads, 0, st>>>(n, (cplx *)y, (const cplx *)x);
+  return check_launch("vec_add_c128");
+}
+
+}  // namespace hphi
+
