@@ -27,14 +27,15 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-__all__ = ["Hamiltonian", "Batch", "Server", "HPhiError", "inspect_terms", "load_library", "library_path", "REAL64", "COMPLEX128",
-           "INFO_FIELDS", "EXPORTED_SYMBOLS"]
+__all__ = ["Hamiltonian", "Batch", "Server", "HPhiError", "inspect_terms", "inspect_green", "load_library",
+           "library_path", "REAL64", "COMPLEX128", "INFO_FIELDS", "EXPORTED_SYMBOLS"]
 
 REAL64 = 0
 COMPLEX128 = 1
 _HERE = os.path.dirname(os.path.abspath(__file__))
 INFO_FIELDS = ["dim", "nsite", "calc_model", "calc_type", "size_list_2_1", "size_list_2_2", "is_gc",
-               "vec_type", "n_offdiag", "n_diag", "lanczos_max", "num_ave", "native_order", "exct", "kernel"]
+               "vec_type", "n_offdiag", "n_diag", "lanczos_max", "num_ave", "native_order", "exct", "kernel",
+               "n_green_one", "n_green_two"]
 EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi_close", "hphi_info",
                     "hphi_sz", "hphi_diagonalcalc", "hphi_mltply", "hphi_mltply_device", "hphi_lanczos",
                     "hphi_lanczos_eigenvector", "hphi_tpq", "hphi_run", "hphi_inspect_terms",
@@ -43,7 +44,8 @@ EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi
                     "hphi_lanczos_steps", "hphi_batch_create", "hphi_batch_lanczos", "hphi_batch_tuning",
                     "hphi_batch_free", "hphi_server_create", "hphi_server_submit", "hphi_server_step",
                     "hphi_server_poll", "hphi_server_clock", "hphi_server_free", "hphi_lobpcg",
-                    "hphi_reference_start"]
+                    "hphi_reference_start", "hphi_expec_green", "hphi_expec_cisajs", "hphi_expec_cisajscktaltdc",
+                    "hphi_inspect_green"]
 FP64 = 0
 FP32 = 1
 BATCH_GRAPH = 1
@@ -116,6 +118,11 @@ def load_library() -> ctypes.CDLL:
     lib.hphi_server_free.argtypes = [P]
     lib.hphi_server_free.restype = None
     lib.hphi_reference_start.argtypes = [ctypes.c_int64, I, I, I, I, I, I, pd]
+    pint = ctypes.POINTER(I)
+    lib.hphi_expec_green.argtypes = [P, I, I, pint, pd, pd]
+    lib.hphi_expec_cisajs.argtypes = [P, pd, pd, ctypes.c_char_p]
+    lib.hphi_expec_cisajscktaltdc.argtypes = [P, pd, pd, ctypes.c_char_p]
+    lib.hphi_inspect_green.argtypes = [ctypes.c_char_p, I, pint, I]
     for name in EXPORTED_SYMBOLS:
         if name not in ("hphi_version", "hphi_last_error", "hphi_close", "hphi_stream", "hphi_batch_free",
                         "hphi_server_clock", "hphi_server_free"):
@@ -172,6 +179,23 @@ def inspect_terms(namelist_def: str):
     _check(lib.hphi_inspect_terms(path, masks.ctypes.data_as(pu), _dptr(coefs), no, dmasks.ctypes.data_as(pu),
                                   _dptr(dcoefs), nd, counts))
     return masks[:no], coefs[:no, 0] + 1j * coefs[:no, 1], dmasks[:nd], dcoefs[:nd]
+
+
+def inspect_green(namelist_def: str, body: int) -> np.ndarray:
+    """OneBodyG (body 1: rows of 4 ints) or TwoBodyG (body 2: rows of 8 ints) rows of an
+    expert-mode input as the reader keeps them, read on the host (no device needed)."""
+    lib = load_library()
+    path = os.fsencode(namelist_def)
+    w = 4 if body == 1 else 8
+    cap = 1 << 16
+    while True:  # one read (and one set of reader warnings) unless the rows exceed the buffer
+        rows = np.zeros((cap, w), dtype=np.int32)
+        n = lib.hphi_inspect_green(path, int(body), rows.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), cap)
+        if n < 0:
+            raise HPhiError(lib.hphi_last_error().decode())
+        if n <= cap:
+            return rows[:n]
+        cap = n
 
 
 class Hamiltonian:
@@ -236,6 +260,34 @@ class Hamiltonian:
         _check(load_library().hphi_mltply(self._h, _dptr(v0.view(np.float64)), _dptr(v1.view(np.float64)),
                                           _dptr(pr)))
         return complex(pr[0], pr[1])
+
+    def expec_green(self, vec: np.ndarray, rows, body: int) -> np.ndarray:
+        """<vec| O |vec> for Green's function rows (body 1: (i, s1, j, s2) -> c+_{i s1} c_{j s2};
+        body 2: (i, s1, j, s2, k, s3, l, s4) -> c+ c c+ c; spin models: site transitions),
+        with the reference's rules per model; vec in HPhi's layout.  Complex array per row."""
+        vec = _as_hphi_vector(vec, self.dim)
+        r = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).reshape(-1, 4 if body == 1 else 8))
+        out = np.zeros(2 * max(len(r), 1))
+        _check(load_library().hphi_expec_green(self._h, int(body), len(r),
+                                               r.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                               _dptr(vec.view(np.float64)), _dptr(out)))
+        return out[0:2 * len(r):2] + 1j * out[1:2 * len(r):2]
+
+    def expec_cisajs(self, vec: np.ndarray, path: Optional[str] = None) -> np.ndarray:
+        """expec_cisajs for the input's OneBodyG rows; writes the reference's file when path is given."""
+        return self._expec_model_green(1, vec, path)
+
+    def expec_cisajscktaltdc(self, vec: np.ndarray, path: Optional[str] = None) -> np.ndarray:
+        """expec_cisajscktaltdc for the input's TwoBodyG rows; writes the reference's file when path is given."""
+        return self._expec_model_green(2, vec, path)
+
+    def _expec_model_green(self, body: int, vec: np.ndarray, path: Optional[str]) -> np.ndarray:
+        vec = _as_hphi_vector(vec, self.dim)
+        n = self.info["n_green_one" if body == 1 else "n_green_two"]
+        out = np.zeros(2 * max(n, 1))
+        fn = load_library().hphi_expec_cisajs if body == 1 else load_library().hphi_expec_cisajscktaltdc
+        _check(fn(self._h, _dptr(vec.view(np.float64)), _dptr(out), os.fsencode(path) if path else None))
+        return out[0:2 * n:2] + 1j * out[1:2 * n:2]
 
     def mltply_device(self, v0_ptr: int, v1_ptr: int, vec_type: int, acc: float = 1.0,
                       scale: float = 1.0) -> complex:

@@ -112,6 +112,18 @@ int hphi_inspect_terms(const char *namelist_def, uint64_t *masks, double *coefs,
   return 0;
 }
 
+int hphi_inspect_green(const char *namelist_def, int body, int *rows, int cap) {
+  if (!namelist_def || (body != 1 && body != 2)) { set_error("bad argument"); return -1; }
+  Model m;
+  std::string err;
+  if (read_expert(namelist_def, &m, &err) != 0) { set_error(err); return -1; }
+  const int n = body == 1 ? (int)m.green_one.size() : (int)m.green_two.size();
+  const int w = body == 1 ? 4 : 8;
+  for (int e = 0; rows && e < n && e < cap; e++)
+    for (int q = 0; q < w; q++) rows[w * e + q] = body == 1 ? m.green_one[e][q] : m.green_two[e][q];
+  return n;
+}
+
 void hphi_close(hphi_handle *h) {
   if (!h) return;
   if (h->sector) {
@@ -149,6 +161,8 @@ int hphi_info(const hphi_handle *h, int64_t *info, int n) {
   v[HPHI_INFO_NATIVE_ORDER] = has_native_order(&s) ? 1 : 0;
   v[HPHI_INFO_EXCT] = s.model.k_exct;
   v[HPHI_INFO_KERNEL] = s.prod ? (prod_two_pass(&s) ? 3 : 2) : (s.hub ? 1 : 0);
+  v[HPHI_INFO_N_GREEN_ONE] = (int64_t)s.model.green_one.size();
+  v[HPHI_INFO_N_GREEN_TWO] = (int64_t)s.model.green_two.size();
   for (int i = 0; i < n && i < HPHI_INFO_COUNT; i++) info[i] = v[i];
   return 0;
 }
@@ -510,6 +524,7 @@ int hphi_lobpcg(hphi_handle *h, const double *v_init, const char *output_dir, do
     v_init = start.data();
   }
   LobpcgResult r;
+  r.copy_vectors = s->model.output_eigenvec != 0 && output_dir;  // OutputEigenVec files
   const int rc = lobpcg_run(s, vt, v_init, &r);
   if (result && nresult > 0) {
     std::vector<double> v = {r.converged ? 1.0 : 0.0, (double)r.steps, r.residual};
@@ -552,6 +567,68 @@ int hphi_reference_start(int64_t dim, int kind, int initial_iv, int sample, int 
   reference_random_start(dim, (RefStartKind)kind, initial_iv, sample, vec_type, threads, count, &out);
   std::memcpy(v, out.data(), sizeof(double) * out.size());
   return 0;
+}
+
+// Green's functions of host vector `vec` (HPhi layout); a vector with no imaginary part and a
+// real Hamiltonian run through the real kernels.
+static int green_host(hphi_handle *h, int body, int n, const int *rows, const double *vec, std::vector<double> *out,
+                      std::vector<char> *trail) {
+  Sector *s = h->sector;
+  std::vector<GreenTerm> terms;
+  std::string err;
+  if (compile_green(s->model, body, rows, n, &terms, trail, &err) != 0) {
+    set_error(err);
+    return -1;
+  }
+  bool real = true;
+  for (int64_t i = 1; i <= s->dim && real; i++) real = vec[2 * i + 1] == 0.0;
+  const VecType vt = real ? kReal64 : kComplex128;
+  cudaSetDevice(s->device);
+  void *d = nullptr;
+  if (cuda_fail(cudaMalloc(&d, (real ? sizeof(double) : sizeof(cplx)) * (size_t)s->dim), "alloc")) return -1;
+  int rc = vec_from_host_c128(s, vt, vec, d);
+  if (rc == 0) rc = green_expect(s, vt, d, terms, out);
+  cudaStreamSynchronize(s->stream);
+  cudaFree(d);
+  return rc;
+}
+
+int hphi_expec_green(hphi_handle *h, int body, int n, const int *rows, const double *vec, double *out) {
+  CHECK_HANDLE(h);
+  if ((body != 1 && body != 2) || n < 0 || (n > 0 && (!rows || !vec || !out))) {
+    set_error("hphi_expec_green: bad arguments");
+    return -1;
+  }
+  if (n == 0) return 0;
+  std::vector<double> g;
+  std::vector<char> trail;
+  if (green_host(h, body, n, rows, vec, &g, &trail) != 0) return -1;
+  std::memcpy(out, g.data(), sizeof(double) * g.size());
+  return 0;
+}
+
+static int expec_model_green(hphi_handle *h, int body, const double *vec, double *out, const char *path) {
+  CHECK_HANDLE(h);
+  const Model &m = h->sector->model;
+  const int n = body == 1 ? (int)m.green_one.size() : (int)m.green_two.size();
+  if (n == 0) return 0;  // the reference returns without a file (src/expec_cisajs.c:80)
+  if (!vec) { set_error("null vector"); return -1; }
+  GreenValues g;
+  std::vector<char> trail;
+  if (green_host(h, body, n, body == 1 ? m.green_one[0].data() : m.green_two[0].data(), vec,
+                 body == 1 ? &g.one : &g.two, body == 1 ? &trail : &g.trail_two) != 0)
+    return -1;
+  if (out) std::memcpy(out, (body == 1 ? g.one : g.two).data(), sizeof(double) * 2 * (size_t)n);
+  if (path && write_green_files(m, g, "", body == 1 ? path : "", body == 2 ? path : "") != 0) return -1;
+  return 0;
+}
+
+int hphi_expec_cisajs(hphi_handle *h, const double *vec, double *out, const char *path) {
+  return expec_model_green(h, 1, vec, out, path);
+}
+
+int hphi_expec_cisajscktaltdc(hphi_handle *h, const double *vec, double *out, const char *path) {
+  return expec_model_green(h, 2, vec, out, path);
 }
 
 }  // extern "C"

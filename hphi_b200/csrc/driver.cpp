@@ -309,6 +309,61 @@ int cg_eigenvector(Sector *s, VecType vt, double eig, uint64_t seed, void *vg, v
 }  // namespace
 
 // ------------------------------------------------------------------- Lanczos
+int model_green(Sector *s, VecType vt, const void *d_hphi, double scale, GreenValues *g) {
+  const Model &m = s->model;
+  std::string err;
+  std::vector<GreenTerm> terms;
+  std::vector<char> trail;
+  g->one.clear();
+  g->two.clear();
+  g->trail_two.clear();
+  if (!m.green_one.empty()) {
+    if (compile_green(m, 1, m.green_one[0].data(), (int)m.green_one.size(), &terms, &trail, &err) != 0) {
+      set_error(err);
+      return -1;
+    }
+    RET(green_expect(s, vt, d_hphi, terms, &g->one));
+  }
+  if (!m.green_two.empty()) {
+    if (compile_green(m, 2, m.green_two[0].data(), (int)m.green_two.size(), &terms, &g->trail_two, &err) != 0) {
+      set_error(err);
+      return -1;
+    }
+    RET(green_expect(s, vt, d_hphi, terms, &g->two));
+  }
+  for (double &x : g->one) x *= scale;
+  for (double &x : g->two) x *= scale;
+  return 0;
+}
+
+int write_green_files(const Model &m, const GreenValues &g, const std::string &dir, const std::string &name1,
+                      const std::string &name2) {
+  if (!m.green_one.empty() && !name1.empty()) {
+    const std::string p = join(dir, name1);
+    FILE *f = fopen(p.c_str(), "w");
+    if (!f) { set_error("cannot write " + p); return -1; }
+    for (size_t e = 0; e < m.green_one.size(); e++) {
+      const auto &r = m.green_one[e];
+      fprintf(f, " %4ld %4ld %4ld %4ld %.10lf %.10lf\n", (long)r[0], (long)r[1], (long)r[2], (long)r[3],
+              g.one[2 * e], g.one[2 * e + 1]);
+    }
+    fclose(f);
+  }
+  if (!m.green_two.empty() && !name2.empty()) {
+    const std::string p = join(dir, name2);
+    FILE *f = fopen(p.c_str(), "w");
+    if (!f) { set_error("cannot write " + p); return -1; }
+    for (size_t e = 0; e < m.green_two.size(); e++) {
+      const auto &r = m.green_two[e];
+      fprintf(f, " %4ld %4ld %4ld %4ld %4ld %4ld %4ld %4ld %.10lf %.10lf%s\n", (long)r[0], (long)r[1], (long)r[2],
+              (long)r[3], (long)r[4], (long)r[5], (long)r[6], (long)r[7], g.two[2 * e], g.two[2 * e + 1],
+              g.trail_two[e] ? " " : "");
+    }
+    fclose(f);
+  }
+  return 0;
+}
+
 int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOptions &opt, LanczosResult *res) {
   const Model &m = s->model;
   const int64_t dim = s->dim;
@@ -563,6 +618,11 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
     res->cg_var = rel_var();
     res->cg_diff = rel_diff();
   }
+  // expec_cisajs / expec_cisajscktaltdc of the eigenvector (src/CalcByLanczos.c:229-240)
+  if (!m.green_one.empty() || !m.green_two.empty()) {
+    RET(from_native(s, vt, VG.p, pp));
+    RET(model_green(s, vt, pp, 1.0, &res->green));
+  }
   res->eigenvector.assign(2 * (dim + 1), 0.0);
   if (opt.copy_eigenvector) {
     RET(from_native(s, vt, VG.p, pp));
@@ -656,6 +716,7 @@ int write_lanczos_outputs(const Sector &s, const LanczosResult &r, const std::st
   fprintf(f, "Doublon  %.16lf \n", r.doublon);
   fprintf(f, "Sz  %.16lf \n", r.sz);
   fclose(f);
+  RET(write_green_files(m, r.green, outdir, m.data_head + "_cisajs.dat", m.data_head + "_cisajscktalt.dat"));
   if (m.output_eigenvec && !r.eigenvector.empty()) {
     // zvo_eigenvec_%d_rank_%d.dat: int step, long dim, complex128[dim+1] (src/CalcByLanczos.c:262-273)
     char name[256];
@@ -749,10 +810,25 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
     sv = 1.0 / *gnorm;
     return 0;
   };
+  // Green's functions of the normalised state sv*V at step 0 and at every ExpecInterval-th
+  // step from 2 on (src/CalcByTPQ.c:170-179, 261-271), files %s_cisajs_set%dstep%d.dat
+  const bool green = !m.green_one.empty() || !m.green_two.empty();
+  DevBuf GV;
+  if (green) RET(cuda_ok(cudaMalloc(&GV.p, esz * dim), "alloc Green's function staging"));
+  auto green_step = [&](int step) -> int {
+    RET(from_native(s, vt, V.p, GV.p));
+    GreenValues g;
+    RET(model_green(s, vt, GV.p, sv * sv, &g));
+    char n1[256], n2[256];
+    snprintf(n1, sizeof(n1), "%s_cisajs_set%dstep%d.dat", m.data_head.c_str(), rand_i, step);
+    snprintf(n2, sizeof(n2), "%s_cisajscktalt_set%dstep%d.dat", m.data_head.c_str(), rand_i, step);
+    return write_green_files(m, g, outdir, n1, n2);
+  };
   res->energy.clear();
   res->inv_temp.clear();
   // FirstMultiply: expec on the start vector, then v = (L - H/Ns) v normalised.
   RET(expec());
+  if (green) RET(green_step(0));
   double gnorm = 0.0;
   RET(multiply(&gnorm));
   write_lines(0.0, first_norm, 0, false);
@@ -771,6 +847,7 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
     write_lines(inv_temp, gnorm, step, true);
     res->energy.push_back(E);
     res->inv_temp.push_back(inv_temp);
+    if (green && m.expec_interval > 0 && step % m.expec_interval == 0) RET(green_step(step));
   }
   fclose(fss);
   fclose(fnorm);

@@ -29,6 +29,23 @@ struct LanczosOptions {
   const LanczosRestart *resume = nullptr;  // continue from these (ReStart 2 / 3)
 };
 
+// Green's function values of the model's OneBodyG / TwoBodyG rows (expec_cisajs,
+// src/expec_cisajs.c:66-641; expec_cisajscktaltdc, src/expec_cisajscktaltdc.c:87-1647):
+// (re, im) per row, with the reference's line endings of the two-body rows.
+struct GreenValues {
+  std::vector<double> one, two;
+  std::vector<char> trail_two;
+};
+
+// The model's Green's functions of the vector d_hphi (device, HPhi row order), multiplied
+// by `scale`; nothing when the model requests none.
+int model_green(Sector *s, VecType vt, const void *d_hphi, double scale, GreenValues *g);
+// Writes dir/name1 (one-body) and dir/name2 (two-body) in the reference's formats; a file
+// whose request list or name is empty is not written (src/expec_cisajs.c:80,
+// src/expec_cisajscktaltdc.c:102).
+int write_green_files(const Model &m, const GreenValues &g, const std::string &dir, const std::string &name1,
+                      const std::string &name2);
+
 struct LanczosResult {
   bool converged = false;
   int steps = 0;                     // X->Large.itr
@@ -48,6 +65,7 @@ struct LanczosResult {
   bool cg_ran = false;
   int cg_rounds = 0, cg_iterations = 0;
   std::vector<double> eigenvector;   // 1-based complex128 (HPhi layout) when requested
+  GreenValues green;                 // of the eigenvector (src/CalcByLanczos.c:229-240)
 };
 
 struct LobpcgResult {
@@ -59,6 +77,7 @@ struct LobpcgResult {
   std::vector<double> energy, var, doublon, sz;  // phys() of each converged vector
   std::vector<std::string> lines;    // zvo_Lanczos_Step.dat
   std::vector<double> eigenvectors;  // exct x (dim + 1) complex128 when copy_vectors
+  std::vector<GreenValues> green;    // of each vector (phys, src/phys.c:100-110)
 };
 
 struct TpqResult {

@@ -136,6 +136,10 @@ int vec_cg_sweep(Sector *s, VecType vt, double a, double shift, const void *p, c
                  double *d_out);
 // x[i] += amp * start_value(seed, configuration of row i, 0) on the real part (HPhi order).
 int vec_add_hashed(Sector *s, VecType vt, uint64_t seed, double amp, void *d_x);
+// <v| O_e |v> of compiled Green's function entries (compile_green) on a device vector in
+// HPhi's row order; out = (re, im) per entry (green.cu).
+int green_expect(Sector *s, VecType vt, const void *d_v, const std::vector<GreenTerm> &terms,
+                 std::vector<double> *out);
 
 // complex128 <-> real and imaginary parts (n = dim); y[0, n) += x[0, n) on stream st.
 int vec_split_c128(Sector *s, const void *d_c, double *d_re, double *d_im);

@@ -522,6 +522,7 @@ int lobpcg_run(Sector *s, VecType vt, const double *h_init, LobpcgResult *res) {
   res->doublon.assign(k, 0.0);
   res->sz.assign(k, 0.0);
   res->eigenvectors.clear();
+  res->green.clear();
   double *obs = ops.d_out;
   for (int i = 0; i < k; i++) {
     LRET(ops.hv(vec(1, i), vec(6, i)));
@@ -536,6 +537,12 @@ int lobpcg_run(Sector *s, VecType vt, const double *h_init, LobpcgResult *res) {
     res->var[i] = h2[0].real();
     res->doublon[i] = o[0];
     res->sz[i] = o[4];
+    if (!m.green_one.empty() || !m.green_two.empty()) {
+      // expec_cisajs / expec_cisajscktaltdc of each vector (phys, src/phys.c:100-110)
+      LRET(from_native(s, vt, vec(1, i), HOST_TMP.p));
+      res->green.emplace_back();
+      LRET(model_green(s, vt, HOST_TMP.p, 1.0, &res->green.back()));
+    }
     if (res->copy_vectors) {
       std::vector<double> hv(2 * (dim + 1), 0.0);
       LRET(from_native(s, vt, vec(1, i), HOST_TMP.p));
@@ -577,6 +584,34 @@ int write_lobpcg_outputs(const Sector &s, const LobpcgResult &r, const std::stri
     fprintf(f, "\n");
   }
   fclose(f);
+  if (m.output_eigenvec && !r.eigenvectors.empty()) {
+    // zvo_eigenvec_%d_rank_%d.dat per state: int itr, long dim, complex128[dim+1]
+    // (src/CalcByLOBPCG.c:754-771)
+    const size_t per = 2 * (size_t)(s.dim + 1);
+    for (size_t i = 0; i * per < r.eigenvectors.size(); i++) {
+      char name[256];
+      snprintf(name, sizeof(name), "%s_eigenvec_%d_rank_%d.dat", m.data_head.c_str(), (int)i, 0);
+      const std::string vf = outdir + sep + name;
+      FILE *fv = fopen(vf.c_str(), "wb");
+      if (!fv) {
+        set_error("cannot write " + vf);
+        return -1;
+      }
+      const int itr = r.steps;
+      const long dim = (long)s.dim;
+      fwrite(&itr, sizeof(int), 1, fv);
+      fwrite(&dim, sizeof(long), 1, fv);
+      fwrite(r.eigenvectors.data() + i * per, sizeof(double), per, fv);
+      fclose(fv);
+    }
+  }
+  for (size_t i = 0; i < r.green.size(); i++) {
+    // FullDiag/CG file names (src/global.c:85-86) with the vector's index
+    char n1[256], n2[256];
+    snprintf(n1, sizeof(n1), "%s_cisajs_eigen%d.dat", m.data_head.c_str(), (int)i);
+    snprintf(n2, sizeof(n2), "%s_cisajscktalt_eigen%d.dat", m.data_head.c_str(), (int)i);
+    LRET(write_green_files(m, r.green[i], outdir, n1, n2));
+  }
   return 0;
 }
 

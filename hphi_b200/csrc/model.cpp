@@ -91,6 +91,36 @@ bool read_table(const Model &m, const std::string &fname, std::vector<std::vecto
   return true;
 }
 
+// Reads an integer table (OneBodyG / TwoBodyG): the count on the 2nd header line, then that
+// many lines of ncol integers.
+bool read_int_table(const Model &m, const std::string &fname, int ncol, std::vector<std::vector<int>> *rows,
+                    std::string *err) {
+  std::ifstream f;
+  if (!open_def(m, fname, &f)) { *err = "cannot open " + fname; return false; }
+  std::string line;
+  int count = -1;
+  for (int i = 0; i < 5; i++) {
+    if (!std::getline(f, line)) { *err = fname + ": truncated header"; return false; }
+    if (i == 1) {
+      std::istringstream ss(line);
+      std::string kw;
+      ss >> kw >> count;
+      if (ss.fail() || count < 0) { *err = fname + ": bad header line 2"; return false; }
+    }
+  }
+  rows->clear();
+  while ((int)rows->size() < count && std::getline(f, line)) {
+    if (line.find_first_not_of(" \t\r\n") == std::string::npos) continue;
+    std::istringstream ss(line);
+    std::vector<int> r(ncol, 0);
+    for (int q = 0; q < ncol; q++)
+      if (!(ss >> r[q])) { *err = fname + ": malformed line: " + line; return false; }
+    rows->push_back(r);
+  }
+  if ((int)rows->size() != count) { *err = fname + ": fewer entries than the header count"; return false; }
+  return true;
+}
+
 // Compiles a fermion operator string (ops applied right to left) in the
 // Jordan-Wigner ordering of configuration bits.  Push form: a source s with
 // (s & req_mask) == req_val maps to s ^ flip with sign (-1)^(sign0 + popc(s & sm)).
@@ -176,6 +206,77 @@ bool add_spin_string(Model *m, const std::vector<SpinOp> &ops, std::complex<doub
   return true;
 }
 
+int compile_green(const Model &m, int body, const int *rows, int n, std::vector<GreenTerm> *terms,
+                  std::vector<char> *trailing_space, std::string *err) {
+  terms->assign((size_t)n, GreenTerm{0, 0, 0, 0, 0.0, 0.0});
+  trailing_space->assign((size_t)n, 0);
+  const bool spin = m.is_spin();
+  const bool kondo = m.is_kondo();
+  // Hubbard-type dispatch of both functions (HubbardNConserved runs as Hubbard after sz,
+  // src/sz.c:802-806); iFlgSzConserved is set by a 2Sz line (src/readdef.c:570-573)
+  const bool canonical_fermion = m.calc_model == kHubbard || m.calc_model == kHubbardNConserved || kondo;
+  const int stride = body == 1 ? 4 : 8;
+  auto fbit = [](int site, int s) { return 2 * site + s; };
+  auto bad = [&](int site, int g) {
+    return site < 0 || site >= m.nsite || g < 0 || g > (spin ? m.locspn[site] : 1);
+  };
+  auto set_fermion = [&](int e, const std::vector<FermionOp> &ops) {
+    uint64_t rm, rv, fl, sm;
+    int s0;
+    if (compile_fermion(ops, &rm, &rv, &fl, &sm, &s0)) (*terms)[e] = GreenTerm{rm, rv, fl, sm, s0 ? -1.0 : 1.0, 0.0};
+  };
+  auto set_spin = [&](int e, const std::vector<SpinOp> &ops) {
+    uint64_t rm, rv, fl;
+    if (compile_spin(ops, m.site_bits, &rm, &rv, &fl)) (*terms)[e] = GreenTerm{rm, rv, fl, 0, 1.0, 0.0};
+  };
+  for (int e = 0; e < n; e++) {
+    const int *r = rows + (size_t)stride * e;
+    for (int q = 0; q < stride / 2; q++)
+      if (bad(r[2 * q], r[2 * q + 1])) {
+        *err = "Green's function entry " + std::to_string(e) + ": site or spin index out of range";
+        return -1;
+      }
+    if (body == 1) {
+      const int i = r[0], s1 = r[1], j = r[2], s2 = r[3];
+      if (spin) {
+        // spin sites never hop (src/expec_cisajs.c:349-398, 446-450, 526-530, 626-629)
+        if (i != j) continue;
+        if (s1 == s2) set_spin(e, {{i, s1, s1}});                  // longitudinal: [digit == s1]
+        else if (m.calc_model == kSpinGC) set_spin(e, {{i, s1, s2}});  // transverse |s1><s2| (:512-521, :609-621)
+        continue;                                                   // canonical: zero
+      }
+      if (canonical_fermion && m.sz_conserved && s1 != s2) continue;  // :276-282
+      if (kondo && ((m.locspn[i] == 1 && m.locspn[j] == 0) || (m.locspn[i] == 0 && m.locspn[j] == 1)))
+        continue;                                                   // :284-293
+      // c+_{i s1} c_{j s2} (general_hopp / GC_general_hopp, CisAjt src/mltplyHubbardCore.c:305-347)
+      set_fermion(e, {{fbit(i, s1), true}, {fbit(j, s2), false}});
+    } else {
+      const int i = r[0], s1 = r[1], j = r[2], s2 = r[3], k = r[4], s3 = r[5], l = r[6], s4 = r[7];
+      if (spin) {
+        // on-site pairs (the reader enforces i == j, k == l); Rearray_Interactions orders the
+        // pairs by site (:274-391), which commute on different sites.  Every spin branch
+        // prints "value \n" (:682-886, :1423-1647).
+        (*trailing_space)[e] = 1;
+        // a canonical sector holds one Sz: rows that change it are zero without a lookup
+        // (the 2Sz test of SpinGeneral :801-817; SpinHalf reaches its lookups only through
+        // Sz-conserving branches :700-760), since the half tables would map such a
+        // configuration to an unrelated row
+        if (m.calc_model == kSpin && (s1 - s2) + (s3 - s4) != 0) continue;
+        set_spin(e, {{i, s1, s2}, {k, s3, s4}});
+        continue;
+      }
+      if (canonical_fermion && m.sz_conserved && s1 + s3 != s2 + s4) {  // :535-541
+        (*trailing_space)[e] = 1;
+        continue;
+      }
+      // c+_{i s1} c_{j s2} c+_{k s3} c_{l s4}, right pair first (CisAjtCkuAlv_element and
+      // relatives, src/mltplyHubbardCore.c:689-1000)
+      set_fermion(e, {{fbit(i, s1), true}, {fbit(j, s2), false}, {fbit(k, s3), true}, {fbit(l, s4), false}});
+    }
+  }
+  return 0;
+}
+
 void canonicalize_terms(Model *m) {
   std::map<std::tuple<uint64_t, uint64_t, uint64_t, uint64_t>, std::complex<double>> off;
   std::vector<std::tuple<uint64_t, uint64_t, uint64_t, uint64_t>> order;
@@ -234,7 +335,7 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
   for (const char *must : {"calcmod", "modpara", "locspin"})
     if (!files.count(must)) { *err = std::string("namelist.def: missing ") + must; return -1; }
   for (const char *unsupported : {"boost", "laser", "teonebody", "tetwobody", "singleexcitation",
-                                  "pairexcitation", "spectrumvec"})
+                                  "pairexcitation", "spectrumvec", "threebodyg", "fourbodyg", "sixbodyg"})
     if (files.count(unsupported)) {
       *err = std::string("namelist.def: keyword not supported by this engine: ") + unsupported;
       return -1;
@@ -606,6 +707,40 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       }
     }
     m->n_interall = (int)rows.size();
+  }
+  // ---- Green's function requests (src/readdef.c:1441-1523)
+  if (files.count("onebodyg")) {
+    std::vector<std::vector<int>> g;
+    if (!read_int_table(*m, files["onebodyg"], 4, &g, err)) return -1;
+    for (const auto &r : g) {
+      if (!check_site(r[0]) || !check_site(r[2]) || !sigma_ok(r[0], r[1]) || !sigma_ok(r[2], r[3])) {
+        *err = files["onebodyg"] + ": bad index"; return -1;
+      }
+      if (m->calc_model == kSpin && r[0] != r[2]) {
+        // the reference skips the row (cWarningIncorrectFormatForSpin2, src/readdef.c:1455-1460)
+        printf("Warning: Site component of (i, j) =(%d, %d) is ignored.\n", r[0], r[2]);
+        continue;
+      }
+      m->green_one.push_back({r[0], r[1], r[2], r[3]});
+    }
+  }
+  if (files.count("twobodyg")) {
+    std::vector<std::vector<int>> g;
+    if (!read_int_table(*m, files["twobodyg"], 8, &g, err)) return -1;
+    for (const auto &r : g) {
+      if (spin && (r[0] != r[2] || r[4] != r[6])) {
+        // CheckFormatForSpinInt (src/readdef.c:2637-2651): a fatal input error in the reference
+        *err = files["twobodyg"] + ": Site component of (i, j, k, l) =(" + std::to_string(r[0]) + ", " +
+               std::to_string(r[2]) + ", " + std::to_string(r[4]) + ", " + std::to_string(r[6]) +
+               ") is not correct; i=j and k=l must be satisfied.";
+        return -1;
+      }
+      for (int q = 0; q < 4; q++)
+        if (!check_site(r[2 * q]) || !sigma_ok(r[2 * q], r[2 * q + 1])) {
+          *err = files["twobodyg"] + ": bad index"; return -1;
+        }
+      m->green_two.push_back({r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7]});
+    }
   }
   canonicalize_terms(m);
   return 0;

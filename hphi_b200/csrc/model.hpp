@@ -10,6 +10,7 @@
 // src/mltplyHubbardCore.c and src/mltplySpinCore.c (masks from the *_GetInfo
 // functions, fermion signs from SgnBit, src/bitcalc.c:338-352).
 #pragma once
+#include <array>
 #include <complex>
 #include <cstdint>
 #include <string>
@@ -67,6 +68,11 @@ struct Model {
   // numeric order is HPhi's mixed-radix order.  Spin-1/2 models have site_bits = 1.
   bool general_spin = false;
   int site_bits = 1;
+  // Green's function requests as read (0-based sites): OneBodyG rows (i, s1, j, s2) and
+  // TwoBodyG rows (i, s1, j, s2, k, s3, l, s4) (src/readdef.c:1441-1523).  A canonical Spin
+  // model drops one-body rows with i != j, as the reference does with a warning.
+  std::vector<std::array<int, 4>> green_one;
+  std::vector<std::array<int, 8>> green_two;
   // Raw term counts as read (for logs).
   int n_trans = 0, n_coulomb_intra = 0, n_coulomb_inter = 0, n_hund = 0, n_exchange = 0;
   int n_ising = 0, n_pairhop = 0, n_pairlift = 0, n_interall = 0;
@@ -97,5 +103,22 @@ bool add_spin_string(Model *m, const std::vector<SpinOp> &ops, std::complex<doub
 
 // Merges duplicate terms (same masks) by adding their coefficients, drops zeros.
 void canonicalize_terms(Model *m);
+
+// One Green's function entry <v| O |v> in push form: a row whose configuration c has
+// (c & cm) == cv contributes coef * (-1)^popcount(c & sm) * conj(v[row(c ^ flip)]) * v[row(c)]
+// (no contribution when c ^ flip is outside the sector).  coef == 0 marks an entry that is
+// zero by the reference's rules.
+struct GreenTerm {
+  uint64_t cm, cv, flip, sm;
+  double coef, unused;
+};
+
+// Compiles Green's function rows (body 1: OneBodyG rows i s1 j s2; body 2: TwoBodyG rows
+// i s1 j s2 k s3 l s4; 0-based sites) following expec_cisajs (src/expec_cisajs.c:66-641) and
+// expec_cisajscktaltdc (src/expec_cisajscktaltdc.c:87-1647).  trailing_space[e] != 0 where
+// the reference prints the entry's line with a space before the newline.  Returns 0, or -1
+// with a message for an index out of range.
+int compile_green(const Model &m, int body, const int *rows, int n, std::vector<GreenTerm> *terms,
+                  std::vector<char> *trailing_space, std::string *err);
 
 }  // namespace hphi

@@ -70,6 +70,10 @@ class ExpertModel:
     pairhop: List[Tuple] = field(default_factory=list)
     pairlift: List[Tuple] = field(default_factory=list)
     interall: List[Tuple] = field(default_factory=list)
+    # Green's function requests: OneBodyG rows (i, s1, j, s2) and TwoBodyG rows
+    # (i, s1, j, s2, k, s3, l, s4) (src/readdef.c:1441-1523)
+    greenone: List[Tuple] = field(default_factory=list)
+    greentwo: List[Tuple] = field(default_factory=list)
 
     # ------------------------------------------------------------------ writers
     def write(self, directory: str) -> str:
@@ -91,6 +95,9 @@ class ExpertModel:
             ("PairLift", "pairlift.def", "NPairlift", self.pairlift, "{:d} {:d} {:.17g}"),
             ("InterAll", "interall.def", "NInterAll", self.interall,
              "{:d} {:d} {:d} {:d} {:d} {:d} {:d} {:d} {:.17g} {:.17g}"),
+            ("OneBodyG", "greenone.def", "NCisAjs", self.greenone, "{:d} {:d} {:d} {:d}"),
+            ("TwoBodyG", "greentwo.def", "NCisAjsCktAltDC", self.greentwo,
+             "{:d} {:d} {:d} {:d} {:d} {:d} {:d} {:d}"),
         ]
         for kw, fname, head, rows, fmt in tables:
             if not rows:

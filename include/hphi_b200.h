@@ -41,7 +41,9 @@ typedef struct hphi_handle hphi_handle;
 #define HPHI_INFO_NATIVE_ORDER 12 /* 1 if the engine's native vector order differs from HPhi's */
 #define HPHI_INFO_EXCT 13         /* exct: states of LOBPCG / the Lanczos eigenvector index */
 #define HPHI_INFO_KERNEL 14       /* native H*v kernel: 0 general, 1 Hubbard block plan, 2 Hubbard product layout, 3 product layout two-pass (real vectors) */
-#define HPHI_INFO_COUNT 15
+#define HPHI_INFO_N_GREEN_ONE 15  /* OneBodyG rows read (NCisAjt) */
+#define HPHI_INFO_N_GREEN_TWO 16  /* TwoBodyG rows read (NCisAjtCkuAlvDC) */
+#define HPHI_INFO_COUNT 17
 
 /* Library version string. */
 const char *hphi_version(void);
@@ -305,6 +307,35 @@ void hphi_server_free(hphi_server *s);
  */
 int hphi_reference_start(int64_t dim, int kind, int initial_iv, int sample, int vec_type, int threads, int count,
                          double *v);
+
+/*
+ * Green's functions <v| O |v> of the rows `rows` on the host vector vec (HPhi's layout,
+ * complex128[dim+1], element 0 unused): body 1 rows are OneBodyG rows (i, s1, j, s2),
+ * O = c+_{i s1} c_{j s2}; body 2 rows are TwoBodyG rows (i, s1, j, s2, k, s3, l, s4),
+ * O = c+_{i s1} c_{j s2} c+_{k s3} c_{l s4} (spin models: |s><s'| on a site), with the
+ * reference's rules for each model.  out receives (re, im) per row.
+ * Replaces the entry loops of expec_cisajs (src/expec_cisajs.c:66-641) and
+ * expec_cisajscktaltdc (src/expec_cisajscktaltdc.c:87-1647), one batch of rows per pass.
+ */
+int hphi_expec_green(hphi_handle *h, int body, int n, const int *rows, const double *vec, double *out);
+
+/*
+ * expec_cisajs (src/expec_cisajs.c:66) and expec_cisajscktaltdc (src/expec_cisajscktaltdc.c:87)
+ * for the rows of the input's OneBodyG / TwoBodyG files: out receives (re, im) per row
+ * (HPHI_INFO_N_GREEN_ONE / _TWO rows; may be NULL), and when path is not NULL the file is
+ * written there in the reference's format (zvo_cisajs.dat, zvo_cisajscktalt.dat).
+ */
+int hphi_expec_cisajs(hphi_handle *h, const double *vec, double *out, const char *path);
+int hphi_expec_cisajscktaltdc(hphi_handle *h, const double *vec, double *out, const char *path);
+
+/*
+ * Reads an expert-mode input on the host only and copies its OneBodyG (body 1, 4 ints per
+ * row) or TwoBodyG (body 2, 8 ints per row) rows as the reader keeps them (a canonical Spin
+ * model drops one-body rows with i != j, src/readdef.c:1455-1460).  Returns the row count
+ * (at most cap rows are written; rows may be NULL), or -1 with a message for an input the
+ * reference rejects (spin two-body rows need i == j and k == l, src/readdef.c:1497-1503).
+ */
+int hphi_inspect_green(const char *namelist_def, int body, int *rows, int cap);
 
 #ifdef __cplusplus
 }

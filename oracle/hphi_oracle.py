@@ -56,6 +56,9 @@ class Def:
     pairlift: List[Tuple[int, int, float]] = field(default_factory=list)
     interall_diag: List[Tuple[int, int, int, int, float]] = field(default_factory=list)
     interall_off: List[Tuple[int, int, int, int, int, int, int, int, complex]] = field(default_factory=list)
+    sz_conserved: bool = False        # iFlgSzConserved: a 2Sz line (src/readdef.c:570-573)
+    green_one: List[Tuple[int, int, int, int]] = field(default_factory=list)      # OneBodyG rows
+    green_two: List[Tuple[int, int, int, int, int, int, int, int]] = field(default_factory=list)  # TwoBodyG rows
 
 
 def _table(path: str) -> List[List[float]]:
@@ -63,6 +66,14 @@ def _table(path: str) -> List[List[float]]:
         lines = f.read().splitlines()
     n = int(lines[1].split()[1])
     rows = [list(map(float, l.split())) for l in lines[5:] if l.strip()]
+    return rows[:n]
+
+
+def _int_table(path: str) -> List[List[int]]:
+    with open(path) as f:
+        lines = f.read().splitlines()
+    n = int(lines[1].split()[1])
+    rows = [list(map(int, l.split())) for l in lines[5:] if l.strip()]
     return rows[:n]
 
 
@@ -166,6 +177,18 @@ def read_expert(namelist: str) -> Def:
                 d.interall_diag.append((i, s1, k, s3, v.real))
             else:
                 d.interall_off.append((i, s1, j, s2, k, s3, l, s4, v))
+    d.sz_conserved = sz_cons
+    # Green's function rows (src/readdef.c:1441-1523)
+    if "onebodyg" in files:
+        for r in _int_table(files["onebodyg"]):
+            if d.calc_model == SPIN and r[0] != r[2]:   # skipped with a warning (:1455-1460)
+                continue
+            d.green_one.append(tuple(r[:4]))
+    if "twobodyg" in files:
+        for r in _int_table(files["twobodyg"]):
+            if _is_spin(d) and (r[0] != r[2] or r[4] != r[6]):   # CheckFormatForSpinInt (:1497-1503)
+                raise ValueError("spin two-body Green's function rows need i == j and k == l")
+            d.green_two.append(tuple(r[:8]))
     return d
 
 
@@ -774,3 +797,167 @@ def lobpcg(d: Def, lists, diag, x_init: np.ndarray):
         np_ = np.linalg.norm(p, axis=1)[:, None]
         x, hx, p, hp = x / nx, hx / nx, p / np_, hp / np_
     return np.array(rows), x
+
+
+# ------------------------------------------------------------- Green's functions
+def _fbit(site: int, s: int) -> int:
+    return 2 * site + s
+
+
+def _sum_pairs(d: Def, lists, ok, target, coef, vec, x):
+    """sum over rows j with ok of conj(vec[off(target_j)]) * coef_j * vec[j] (M_CORR mode of
+    the element routines: the scatter into v0 is skipped, dam_pr is returned)."""
+    off = np.zeros(x.size, dtype=np.int64)
+    off[ok] = get_off(d, lists, target[ok])
+    ok = ok & (off > 0)
+    return complex(np.sum(np.conj(vec[off[ok]]) * coef[ok] * x[ok]))
+
+
+def expec_cisajs(d: Def, lists, vec: np.ndarray) -> np.ndarray:
+    """expec_cisajs (src/expec_cisajs.c:66-641): <vec| c+_{i s1} c_{j s2} |vec> per OneBodyG
+    row (spin models: |s1><s2| on site i, zero for i != j); vec is 1-based complex."""
+    vec = vec.astype(np.complex128)
+    cj = configs(d, lists)[1:]
+    x = vec[1:]
+    one = np.ones(x.size)
+    out = []
+    for (i, s1, j, s2) in d.green_one:
+        val = 0j
+        if d.calc_model == HUBBARDGC:                                   # :193-243
+            ok, t, sg = _hop(cj, _fbit(i, s1), _fbit(j, s2))
+            val = _sum_pairs(d, lists, ok, t, sg, vec, x)
+        elif d.calc_model in (HUBBARD, HUBBARD_NCONS, KONDO, KONDOGC):   # :254-316
+            if d.sz_conserved and s1 != s2:
+                val = 0j
+            elif d.calc_model in (KONDO, KONDOGC) and (
+                    (d.locspn[i] == 1 and d.locspn[j] == 0) or (d.locspn[i] == 0 and d.locspn[j] == 1)):
+                val = 0j
+            elif i == j and s1 == s2:
+                n = ((cj >> np.uint64(_fbit(i, s1))) & np.uint64(1)).astype(np.float64)
+                val = complex(np.sum(n * np.abs(x) ** 2))
+            else:
+                ok, t, sg = _hop(cj, _fbit(i, s1), _fbit(j, s2))
+                val = _sum_pairs(d, lists, ok, t, sg, vec, x)
+        elif d.calc_model == SPIN:                                     # :329-470
+            if i == j and s1 == s2:
+                hit = (_digit(d, cj, i) if _general(d) else ((cj >> np.uint64(i)) & np.uint64(1)).astype(np.int64)) == s1
+                val = complex(np.sum(hit * np.abs(x) ** 2))
+        elif d.calc_model == SPINGC:                                   # :496-641
+            if i == j:
+                if _general(d):
+                    dig = _digit(d, cj, i)
+                    if s1 == s2:
+                        val = complex(np.sum((dig == s1) * np.abs(x) ** 2))
+                    else:   # GetOffCompGeneralSpin(j-1, site, s2 -> s1)
+                        tp = _tpow(d)
+                        ok = dig == s2
+                        t = (cj.astype(np.int64) + (s1 - s2) * tp[i]).astype(np.uint64)
+                        val = _sum_pairs(d, lists, ok, np.where(ok, t, cj), one, vec, x)
+                else:
+                    b = ((cj >> np.uint64(i)) & np.uint64(1)).astype(np.int64)
+                    if s1 == s2:   # child_SpinGC_CisAis = bit ^ (1 - s1)
+                        val = complex(np.sum((b == s1) * np.abs(x) ** 2))
+                    else:          # child_SpinGC_CisAit(j, site, s2): bit == s2 flips
+                        ok = b == s2
+                        val = _sum_pairs(d, lists, ok, cj ^ np.uint64(1 << i), one, vec, x)
+        out.append(val)
+    return np.array(out, dtype=np.complex128)
+
+
+def _rearray(r):
+    """Rearray_Interactions (src/expec_cisajscktaltdc.c:274-391): on-site pairs ordered by
+    site; returns (i, s1, j, s2, k, s3, l, s4, V) or None."""
+    i, s1, j, s2, k, s3, l, s4 = r
+    if i == j and k == l:
+        return (k, s3, l, s4, i, s1, j, s2, 1.0) if i > k else (i, s1, j, s2, k, s3, l, s4, 1.0)
+    if i == l and k == j:
+        return (k, s3, j, s2, i, s1, l, s4, -1.0) if i > k else (i, s1, l, s4, k, s3, j, s2, -1.0)
+    return None
+
+
+def expec_cisajscktalt(d: Def, lists, vec: np.ndarray) -> np.ndarray:
+    """expec_cisajscktaltdc (src/expec_cisajscktaltdc.c:87-1647): <vec| c+_{i s1} c_{j s2}
+    c+_{k s3} c_{l s4} |vec> per TwoBodyG row; spin models through Rearray_Interactions and
+    the per-model branches."""
+    vec = vec.astype(np.complex128)
+    cj = configs(d, lists)[1:]
+    x = vec[1:]
+    one = np.ones(x.size)
+    out = []
+    general = _general(d)
+    tp = _tpow(d) if general else None
+
+    def sbit(c, site):
+        return _digit(d, c, site) if general else ((c >> np.uint64(site)) & np.uint64(1)).astype(np.int64)
+
+    def sflip(c, site, to, frm):
+        """|to><frm| on a site: (ok, new configurations)."""
+        ok = sbit(c, site) == frm
+        if general:
+            return ok, (c.astype(np.int64) + (to - frm) * tp[site]).astype(np.uint64)
+        return ok, (c ^ np.uint64(1 << site)) if to != frm else c
+
+    for row in d.green_two:
+        val = 0j
+        if not _is_spin(d):
+            i, s1, j, s2, k, s3, l, s4 = row
+            if d.calc_model in (HUBBARD, HUBBARD_NCONS, KONDO, KONDOGC) and d.sz_conserved and s1 + s3 != s2 + s4:
+                out.append(0j)                                          # :535-541
+                continue
+            # general_int_GetInfo + CisAjtCkuAlv_element and its relatives (:393-618):
+            # c+_k c_l first, then c+_i c_j on the intermediate configuration
+            ok2, t2, sg2 = _hop(cj, _fbit(k, s3), _fbit(l, s4))
+            ok1, t1, sg1 = _hop(t2, _fbit(i, s1), _fbit(j, s2))
+            val = _sum_pairs(d, lists, ok1 & ok2, t1, (sg1 * sg2).astype(np.float64), vec, x)
+            out.append(val)
+            continue
+        rr = _rearray(row)
+        if rr is None:
+            out.append(0j)
+            continue
+        i, s1, j, s2, k, s3, l, s4, V = rr
+        if d.calc_model == SPIN and not general:                       # :652-770
+            if s1 == s2 and s3 == s4:
+                val = complex(V * np.sum(((sbit(cj, i) == s2) & (sbit(cj, k) == s4)) * np.abs(x) ** 2))
+            elif i == k and s1 == s4 and s3 == s2:
+                val = complex(V * np.sum((sbit(cj, i) == s1) * np.abs(x) ** 2))
+            elif s1 == s4 and s2 == s3:   # child_exchange_spin_element; tmp_V is not applied
+                ok = (sbit(cj, i) == s2) & (sbit(cj, k) == s4)
+                val = _sum_pairs(d, lists, ok, cj ^ np.uint64((1 << i) | (1 << k)), one, vec, x)
+        elif d.calc_model == SPIN:                                     # :784-890
+            two_sz = lambda site, g: 2 * g - d.locspn[site]   # GetLocal2Sz
+            o = row
+            dsz = two_sz(o[0], o[1]) - two_sz(o[2], o[3]) + two_sz(o[4], o[5]) - two_sz(o[6], o[7])
+            if dsz != 0:
+                val = 0j
+            elif s1 == s2 and s3 == s4:
+                val = complex(V * np.sum(((sbit(cj, i) == s1) & (sbit(cj, k) == s3)) * np.abs(x) ** 2))
+            elif s1 != s2 and s3 != s4:
+                ok2, t2 = sflip(cj, k, s3, s4)
+                ok1, t1 = sflip(np.where(ok2, t2, cj), i, s1, s2)
+                ok = ok1 & ok2
+                val = _sum_pairs(d, lists, ok, np.where(ok, t1, cj), V * one, vec, x)
+        else:                                                          # SpinGC :1423-1647
+            if s1 == s2 and s3 == s4:
+                val = complex(V * np.sum(((sbit(cj, i) == s2) & (sbit(cj, k) == s4)) * np.abs(x) ** 2))
+            else:
+                # the right pair on the initial configuration, the left pair after it
+                ok2, t2 = sflip(cj, k, s3, s4)
+                ok1, t1 = sflip(np.where(ok2, t2, cj), i, s1, s2)
+                ok = ok1 & ok2
+                val = _sum_pairs(d, lists, ok, np.where(ok, t1, cj), V * one, vec, x)
+        out.append(val)
+    return np.array(out, dtype=np.complex128)
+
+
+def read_green_file(path: str) -> Tuple[np.ndarray, np.ndarray]:
+    """Rows and complex values of a zvo_cisajs*.dat / zvo_cisajscktalt*.dat file."""
+    rows, vals = [], []
+    for line in open(path):
+        p = line.split()
+        if not p:
+            continue
+        rows.append([int(t) for t in p[:-2]])
+        vals.append(complex(float(p[-2]), float(p[-1])))
+    return np.array(rows, dtype=np.int64), np.array(vals, dtype=np.complex128)
+

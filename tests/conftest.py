@@ -22,6 +22,9 @@ def golden_cases(kind=None):
             continue
         z = np.load(p)
         large = "sha_list_1" in z.files
+        green = "green_files" in z.files
+        if (kind == "green") != green:
+            continue
         if kind == "large" and not large:
             continue
         if kind == "small" and large:
@@ -46,3 +49,25 @@ def case_dir(name):
 
 def load_golden(name):
     return dict(np.load(os.path.join(GOLDEN, name, "golden.npz")))
+
+
+def green_reference(z, fname):
+    """(rows, values, text lines) of a reference Green's function file stored in a fixture."""
+    lines = str(z["text_" + fname]).splitlines()
+    rows = np.array([[int(t) for t in l.split()[:-2]] for l in lines], dtype=np.int64)
+    vals = np.array([complex(float(l.split()[-2]), float(l.split()[-1])) for l in lines])
+    return rows, vals, lines
+
+
+def tpq_state(O, d, lists, start, step):
+    """The normalised TPQ state of `step` from the normalised start vector (oracle H*v):
+    v <- (L v - H v / Ns) / |.| (src/Multiply.c:42-68)."""
+    v = start.astype(np.complex128).copy()
+    diag = O.diagonalcalc(d, lists)
+    for _ in range(step):
+        hv, _ = O.mltply(d, lists, diag, np.zeros_like(v), v)
+        v = d.large_value * v - hv / d.nsite
+        v[0] = 0
+        v /= np.linalg.norm(v[1:])
+    return v
+

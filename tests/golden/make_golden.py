@@ -16,6 +16,9 @@ refstart_* directories hold start.npz: the first mltply input of a golden case's
 with several OpenMP threads (the reference's per-thread random start vectors).
 restart_* directories hold inputs a/ and b/ and restart.npz: the restart files run a wrote
 and the steps and energy of run b continued from them.
+green_* directories hold inputs with OneBodyG / TwoBodyG files and golden.npz with the
+reference's Green's function files (text_<file>), the eigenvectors it wrote (vec_<file>,
+OutputEigenVec), the first mltply input (start) and its energies (states, or tpq rows).
 Large cases store only SHA-256 digests of the lists (sha_list_1 ...).
 
 Run in a container that has the reference sources and oracle/_ref/HPhi_ref
@@ -279,11 +282,128 @@ def make_restart_case(name: str, ma, mb) -> None:
     np.savez_compressed(os.path.join(out, "restart.npz"), **data)
 
 
+def _green_rows(nsite: int, nsig: int, seed: int, n_one: int, n_two: int, spin: bool):
+    """OneBodyG / TwoBodyG rows: every one-body (i, s1, j, s2) (spin models: plus the
+    off-site rows the reader drops or zeroes) when n_one < 0, else n_one random rows;
+    structured two-body rows (densities, spin flips, overlapping indices) plus n_two
+    random rows (spin models: on-site pairs only)."""
+    rng = np.random.RandomState(seed)
+    sig = range(nsig)
+    if n_one < 0:
+        one = [(i, a, j, b) for i in range(nsite) for a in sig for j in range(nsite) for b in sig]
+    else:
+        one = [tuple(int(x) for x in (rng.randint(nsite), rng.randint(nsig), rng.randint(nsite), rng.randint(nsig)))
+               for _ in range(n_one)]
+    two = []
+    if spin:
+        for i, k in [(0, 0), (0, 1), (1, 0), (0, nsite - 1), (nsite - 1, 1)]:
+            for a in sig:
+                for b in sig:
+                    for c in sig:
+                        for dd in sig:
+                            if rng.rand() < (1.0 if nsig == 2 else 0.3):
+                                two.append((i, a, i, b, k, c, k, dd))
+        for _ in range(n_two):
+            i, k = rng.randint(nsite), rng.randint(nsite)
+            two.append((int(i), int(rng.randint(nsig)), int(i), int(rng.randint(nsig)), int(k),
+                        int(rng.randint(nsig)), int(k), int(rng.randint(nsig))))
+    else:
+        for i, j in [(0, 1), (1, 0), (0, 0), (0, nsite - 1)]:
+            two += [(i, a, i, a, j, b, j, b) for a in sig for b in sig]          # n n
+            two += [(i, 0, i, 1, j, 1, j, 0), (i, 1, j, 1, j, 0, i, 0)]          # spin flip / exchange order
+            two += [(i, 0, j, 0, j, 0, i, 0), (i, 0, j, 1, j, 1, i, 0)]          # overlapping middle indices
+            two += [(i, 0, j, 0, i, 1, j, 1), (i, 0, j, 0, j, 1, i, 1)]          # pair hopping orders
+        for _ in range(n_two):
+            two.append(tuple(int(rng.randint(m)) for m in (nsite, 2, nsite, 2, nsite, 2, nsite, 2)))
+    return one, two
+
+
+def _green_cases():
+    """Lanczos (eigenvector and Green's functions), TPQ and LOBPCG inputs with OneBodyG /
+    TwoBodyG files, one per model branch of expec_cisajs / expec_cisajscktaltdc."""
+    c = {}
+
+    def lanczos(m, seed, n_one=-1, n_two=40, nsig=2):
+        m.calc_eigenvec, m.output_eigenvec = 0, 1
+        m.greenone, m.greentwo = _green_rows(m.nsite, nsig, seed, n_one, n_two, m.model.startswith("Spin"))
+        return m
+
+    c["green_hub6"] = lanczos(expert.hubbard(6, expert.square_bonds(2, 3), 1.0, 4.0, 3, 3, lanczos_max=300), 1)
+    m = expert.ExpertModel(model="HubbardGC", nsite=4, two_sz=None, initial_vec_type=0, lanczos_max=300)
+    for i, j in expert.chain_bonds(4):
+        for s in (0, 1):
+            m.trans += [(i, s, j, s, 1.0, 0.0), (j, s, i, s, 1.0, 0.0)]
+    m.trans += [(0, 0, 0, 1, 0.3, 0.2), (0, 1, 0, 0, 0.3, -0.2)]   # a spin-mixing field: complex vectors
+    m.coulombintra = [(i, 3.0) for i in range(4)]
+    c["green_hubgc4"] = lanczos(m, 2)
+    m = expert.hubbard(6, expert.square_bonds(2, 3), 1.0, 4.0, 3, 3, lanczos_max=300)
+    m.two_sz = None
+    c["green_ncons"] = lanczos(m, 3)
+    c["green_kondo3"] = lanczos(expert.kondo_chain(3, 1.0, 1.5, lanczos_max=300), 4)
+    c["green_spin10"] = lanczos(expert.heisenberg(10, expert.chain_bonds(10), lanczos_max=300), 5)
+    m = expert.kitaev_heisenberg(2, 2, -1.0, 0.2, lanczos_max=300)
+    m.initial_vec_type = 0
+    c["green_kitaev2x2"] = lanczos(m, 6)
+    c["green_gspin6"] = lanczos(expert.general_heisenberg([2] * 6, expert.chain_bonds(6), lanczos_max=300), 7,
+                                n_two=60, nsig=3)
+    m = expert.general_heisenberg([2] * 5, expert.chain_bonds(5), two_sz=None, D=0.2, hx=0.4, lanczos_max=300)
+    m.initial_vec_type = 0
+    c["green_gspingc5"] = lanczos(m, 8, n_two=60, nsig=3)
+    m = expert.hubbard(6, expert.chain_bonds(6), 1.0, 4.0, 3, 3, calc_type="TPQ", lanczos_max=12, num_ave=1,
+                       large_value=6.0, expec_interval=4)
+    m.initial_vec_type = 0
+    m.greenone, m.greentwo = _green_rows(6, 2, 9, 40, 20, False)
+    c["green_tpq_hub6"] = m
+    m = expert.heisenberg(10, expert.chain_bonds(10), calc_type="CG", exct=2, lanczos_max=600)
+    m.output_eigenvec = 1
+    m.greenone, m.greentwo = _green_rows(10, 2, 10, -1, 30, True)
+    c["green_lobpcg_chain10"] = m
+    return c
+
+
+def _read_eigvec(path: str) -> np.ndarray:
+    """zvo_eigenvec_%d_rank_%d.dat: int step, long dim, complex128[dim+1] (src/CalcByLanczos.c:262-273)."""
+    with open(path, "rb") as f:
+        f.read(4)
+        dim = int(np.frombuffer(f.read(8), dtype=np.int64)[0])
+        return np.frombuffer(f.read(16 * (dim + 1)), dtype=np.complex128).copy()
+
+
+def make_green_case(name: str, m) -> None:
+    out = os.path.join(HERE, name)
+    shutil.rmtree(out, ignore_errors=True)
+    m.write(out)
+    data = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for f in os.listdir(out):
+            shutil.copy(os.path.join(out, f), tmp)
+        p = run_ref.run(tmp, threads=1, dump_call=0)
+        if p.returncode != 0:
+            raise RuntimeError(f"{name}: reference failed\n{p.stdout[-3000:]}\n{p.stderr[-3000:]}")
+        od = os.path.join(tmp, "output")
+        v1, _, _, _ = run_ref.read_hv(tmp)
+        data["start"] = v1
+        files = sorted(f for f in os.listdir(od) if "cisajs" in f)
+        data["green_files"] = np.array(files)
+        for f in files:
+            text = open(os.path.join(od, f)).read()
+            data["text_" + f] = np.array(text)
+        for f in sorted(os.listdir(od)):
+            if f.startswith("zvo_eigenvec_"):
+                data["vec_" + f] = _read_eigvec(os.path.join(od, f))
+        if m.calc_type == "TPQ":
+            data["tpq"] = run_ref.tpq_table(tmp, 0)
+        else:
+            data["states"] = run_ref.energy_states(tmp)
+    np.savez_compressed(os.path.join(out, "golden.npz"), **data)
+
+
 def main(argv) -> None:
     if not run_ref.available():
         raise SystemExit("oracle/_ref/HPhi_ref is missing: run `make -C oracle` first")
     small, large, starts, restarts = _cases(), _large_cases(), _start_cases(), _restart_cases()
-    names = argv or list(small) + list(large) + list(starts) + list(restarts)
+    greens = _green_cases()
+    names = argv or list(small) + list(large) + list(starts) + list(restarts) + list(greens)
     for n in names:
         print("case", n, flush=True)
         if n in small:
@@ -292,6 +412,8 @@ def main(argv) -> None:
             make_start_case(n, *starts[n])
         elif n in restarts:
             make_restart_case(n, *restarts[n])
+        elif n in greens:
+            make_green_case(n, greens[n])
         else:
             make_case(n, large[n], large=True)
 

@@ -138,3 +138,42 @@ def test_compiled_terms_reproduce_reference_hv(name):
         _, y3 = emulate_hv(name, g["hv3_v1"])
         ref3 = g["hv3_v0a"][1:] - g["hv3_v0b"][1:]
         assert np.max(np.abs(y3 - ref3)) <= 1e-11 * np.max(np.abs(g["hv3_v0a"][1:]))
+
+
+@pytest.mark.parametrize("name", golden_cases("green"))
+def test_green_rows_read_as_the_reference_keeps_them(name):
+    """OneBodyG / TwoBodyG rows after the reader: the rows of the reference's output files
+    (a canonical Spin model drops one-body rows with i != j)."""
+    from conftest import green_reference
+    z = load_golden(name)
+    nl = os.path.join(case_dir(name), "namelist.def")
+    one, two = hphi_b200.inspect_green(nl, 1), hphi_b200.inspect_green(nl, 2)
+    for f in (str(x) for x in z["green_files"]):
+        rows, _, _ = green_reference(z, f)
+        np.testing.assert_array_equal(rows, two if "cktalt" in f else one)
+
+
+def test_green_reader_warnings_and_rejections(tmp_path, capfd):
+    src = case_dir("green_spin10")
+    d = tmp_path / "in"
+    shutil.copytree(src, d)
+    n_file = int(open(d / "greenone.def").read().splitlines()[1].split()[1])
+    rows = hphi_b200.inspect_green(str(d / "namelist.def"), 1)
+    out = capfd.readouterr().out
+    # the reference's warning for every skipped off-site row
+    assert out.count("Warning: Site component of (i, j) =(") == n_file - len(rows)
+    assert (rows[:, 0] == rows[:, 2]).all()
+    # a spin two-body row with i != j is a fatal input error (CheckFormatForSpinInt)
+    lines = open(d / "greentwo.def").read().splitlines()
+    n = int(lines[1].split()[1])
+    lines[1] = f"NCisAjsCktAltDC {n + 1}"
+    lines.append("0 0 1 0 1 0 0 0")
+    open(d / "greentwo.def", "w").write("\n".join(lines) + "\n")
+    with pytest.raises(hphi_b200.HPhiError, match="i=j and k=l must be satisfied"):
+        hphi_b200.inspect_green(str(d / "namelist.def"), 2)
+    # out-of-range spin index
+    lines = open(src + "/greenone.def").read().splitlines()
+    lines[5] = "0 2 0 2"
+    open(d / "greenone.def", "w").write("\n".join(lines) + "\n")
+    with pytest.raises(hphi_b200.HPhiError, match="bad index"):
+        hphi_b200.inspect_green(str(d / "namelist.def"), 1)

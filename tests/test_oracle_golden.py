@@ -148,3 +148,28 @@ def test_oracle_lobpcg_matches_reference(name):
     H = O.dense_hamiltonian(d, lists, diag)
     e = np.real(np.sum(x.conj() * (x @ H.T), axis=1))
     np.testing.assert_allclose(e, g["lobpcg_states"][:, 0], rtol=0, atol=1e-12)
+
+
+def _green_vector(O, d, lists, z, fname):
+    if "step" in fname:
+        from conftest import tpq_state
+        return tpq_state(O, d, lists, z["start"], int(fname.split("step")[1].split(".")[0]))
+    k = int(fname.split("eigen")[1].split(".")[0]) if "eigen" in fname else 0
+    return z[f"vec_zvo_eigenvec_{k}_rank_0.dat"]
+
+
+@pytest.mark.parametrize("name", golden_cases("green"))
+def test_oracle_green_functions_match_reference(name):
+    """expec_cisajs / expec_cisajscktaltdc restated: every value the reference printed
+    (%.10lf) for the eigenvector(s) it wrote, or for its TPQ states, and the same rows."""
+    from conftest import green_reference
+    z = load_golden(name)
+    d = O.read_expert(case_dir(name) + "/namelist.def")
+    lists = None if O._rows_are_configs(d) else O.sz(d)
+    for f in (str(x) for x in z["green_files"]):
+        rows, vals, _ = green_reference(z, f)
+        v = _green_vector(O, d, lists, z, f)
+        two = "cktalt" in f
+        got = O.expec_cisajscktalt(d, lists, v) if two else O.expec_cisajs(d, lists, v)
+        np.testing.assert_array_equal(rows, np.array(d.green_two if two else d.green_one))
+        np.testing.assert_allclose(got, vals, rtol=0, atol=1e-10, err_msg=f)
