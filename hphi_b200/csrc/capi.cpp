@@ -3,7 +3,9 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <cerrno>
 #include <cstring>
+#include <sys/stat.h>
 #include <string>
 #include <vector>
 
@@ -434,6 +436,18 @@ int hphi_lanczos(hphi_handle *h, const double *v_init, const char *output_dir, d
   CHECK_HANDLE(h);
   Sector *s = h->sector;
   const VecType vt = default_vec_type(*s);
+  const int iev = s->model.input_eigenvec;
+  if (iev == 1 || iev == 2) {
+    // InputEigenVec: the stored eigenvector (in output_dir) instead of a Lanczos run
+    LanczosResult &r = h->last_lanczos;
+    r = LanczosResult();
+    if (lanczos_input_vector(s, vt, output_dir ? output_dir : "", iev, &r) != 0) return -1;
+    if (result && nresult > 0) {
+      double v[17] = {1.0, 0, 0, 0, 0, 0, 0, r.energy, r.var, r.doublon, r.sz, 0, 0, 0, 0, 0, 0};
+      for (int i = 0; i < nresult && i < 17; i++) result[i] = v[i];
+    }
+    return output_dir ? write_lanczos_outputs(*s, r, output_dir) : 0;
+  }
   std::vector<double> start;
   if (!v_init) {
     if (!single_element_start(*s, &start))
@@ -495,16 +509,53 @@ int hphi_tpq(hphi_handle *h, const double *v_init, const char *output_dir, doubl
   const int64_t stride = 2 * (s->dim + 1);
   TpqResult r;
   std::vector<double> start;
+  const int restart = s->model.restart;  // RESTART_OUT 1, RESTART_INOUT 2, RESTART_IN 3
   for (int rand_i = 0; rand_i < s->model.num_ave; rand_i++) {
+    TpqOptions opt;
+    opt.keep_vector = restart == 1 || restart == 2;
     const double *v = nullptr;
-    if (v_init) {
+    char vname[256];
+    snprintf(vname, sizeof(vname), "tmpvec_set%d_rank_%d.dat", rand_i, 0);
+    const std::string vpath = out + "/" + vname;
+    FILE *fin = (restart == 2 || restart == 3) ? fopen(vpath.c_str(), "rb") : nullptr;
+    if (fin) {
+      // stored state: int step, long dim, complex128[dim+1] (src/CalcByTPQ.c:86-104)
+      int stp = 0;
+      long dim = 0;
+      start.assign(stride, 0.0);
+      const bool ok = fread(&stp, sizeof(int), 1, fin) == 1 && fread(&dim, sizeof(long), 1, fin) == 1 &&
+                      dim == (long)s->dim && fread(start.data(), sizeof(double), stride, fin) == (size_t)stride;
+      fclose(fin);
+      if (!ok) {
+        set_error("Error: A file of Inputvector is incorrect.");
+        return -1;
+      }
+      opt.resume_step = stp;
+      v = start.data();
+    } else if (v_init) {
+      // a missing stored state starts the sample normally, as the reference announces
+      // (src/CalcByTPQ.c:93-96; it then reads from the missing file, here it does not)
       v = v_init + stride * rand_i;
     } else {
       reference_random_start(s->dim, kRefTPQ, s->model.initial_iv, rand_i, s->model.initial_vec_type,
                              reference_threads(), 1, &start);
       v = start.data();
     }
-    if (tpq_run(s, vt, v, rand_i, out, &r) != 0) return -1;
+    if (tpq_run(s, vt, v, rand_i, out, &r, opt) != 0) return -1;
+    if (opt.keep_vector) {
+      // tmpvec_set%d_rank_%d.dat after the loop (src/CalcByTPQ.c:275-290)
+      FILE *fo = fopen(vpath.c_str(), "wb");
+      if (!fo) {
+        set_error("cannot write " + vpath);
+        return -1;
+      }
+      const int stp = r.final_step;
+      const long dim = (long)s->dim;
+      fwrite(&stp, sizeof(int), 1, fo);
+      fwrite(&dim, sizeof(long), 1, fo);
+      fwrite(r.final_vector.data(), sizeof(double), r.final_vector.size(), fo);
+      fclose(fo);
+    }
   }
   if (result)
     for (int i = 0; i < nresult && i < (int)r.energy.size(); i++) result[i] = r.energy[i];
@@ -517,6 +568,36 @@ int hphi_lobpcg(hphi_handle *h, const double *v_init, const char *output_dir, do
   const VecType vt = default_vec_type(*s);
   const int k = std::max(1, s->model.k_exct);
   std::vector<double> start;
+  const int restart = s->model.restart;  // RESTART_OUT 1, RESTART_INOUT 2, RESTART_IN 3
+  const std::string out = output_dir ? output_dir : "";
+  const int64_t stride = 2 * (s->dim + 1);
+  auto tmpvec = [&](int ie) {
+    char name[64];
+    snprintf(name, sizeof(name), "tmpvec_set%d_rank_%d.dat", ie, 0);
+    return out.empty() ? std::string(name) : out + "/" + name;
+  };
+  if ((restart == 2 || restart == 3) && output_dir) {
+    // Initialize_wave (A): the stored vectors of every state, else the usual start
+    // (src/CalcByLOBPCG.c:175-212)
+    std::vector<double> stored((size_t)stride * k, 0.0);
+    bool all = true;
+    for (int ie = 0; ie < k && all; ie++) {
+      FILE *f = fopen(tmpvec(ie).c_str(), "rb");
+      if (!f) { all = false; break; }
+      int itr = 0;
+      unsigned long dim = 0;
+      const bool ok = fread(&itr, sizeof(int), 1, f) == 1 && fread(&dim, sizeof(dim), 1, f) == 1 &&
+                      dim == (unsigned long)s->dim &&
+                      fread(stored.data() + (size_t)stride * ie, sizeof(double), stride, f) == (size_t)stride;
+      fclose(f);
+      if (!ok) { set_error("Error: Invalid restart file."); return -1; }
+      stored[(size_t)stride * ie] = stored[(size_t)stride * ie + 1] = 0.0;
+    }
+    if (all && !v_init) {
+      start.swap(stored);
+      v_init = start.data();
+    }
+  }
   if (!v_init) {
     if (!lobpcg_single_element_start(*s, &start))
       reference_random_start(s->dim, kRefLOBPCG, s->model.initial_iv, 0, s->model.initial_vec_type,
@@ -524,8 +605,38 @@ int hphi_lobpcg(hphi_handle *h, const double *v_init, const char *output_dir, do
     v_init = start.data();
   }
   LobpcgResult r;
-  r.copy_vectors = s->model.output_eigenvec != 0 && output_dir;  // OutputEigenVec files
+  const bool restart_out = (restart == 1 || restart == 2) && output_dir;
+  // OutputEigenVec files and the restart vectors need the states on the host
+  r.copy_vectors = (s->model.output_eigenvec != 0 && output_dir) || restart_out;
   const int rc = lobpcg_run(s, vt, v_init, &r);
+  if (restart_out && !r.eigenvectors.empty()) {
+    // Output_restart (src/CalcByLOBPCG.c:295-319, called at :600-606): the current vectors
+    if (!out.empty() && mkdir(out.c_str(), 0755) != 0 && errno != EEXIST) {
+      set_error("cannot create output directory " + out);
+      return -1;
+    }
+    for (int ie = 0; ie < k; ie++) {
+      FILE *f = fopen(tmpvec(ie).c_str(), "wb");
+      if (!f) { set_error("cannot write " + tmpvec(ie)); return -1; }
+      const int itr = r.itr;
+      const long dim = (long)s->dim;
+      fwrite(&itr, sizeof(int), 1, f);
+      fwrite(&dim, sizeof(long), 1, f);
+      fwrite(r.eigenvectors.data() + (size_t)stride * ie, sizeof(double), stride, f);
+      fclose(f);
+    }
+    if (!r.converged) {
+      // an unconverged run in restart mode ends here without error (LOBPCG_Main returns 1,
+      // CalcByLOBPCG returns TRUE, :650-656): the step file only
+      if (write_lobpcg_outputs(*s, r, out) != 0) return -1;
+      if (result && nresult > 0) {
+        result[0] = 0.0;
+        if (nresult > 1) result[1] = (double)r.steps;
+        if (nresult > 2) result[2] = r.residual;
+      }
+      return 0;
+    }
+  }
   if (result && nresult > 0) {
     std::vector<double> v = {r.converged ? 1.0 : 0.0, (double)r.steps, r.residual};
     for (int i = 0; i < k; i++) {

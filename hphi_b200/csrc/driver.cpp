@@ -633,6 +633,62 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   return 0;
 }
 
+int lanczos_input_vector(Sector *s, VecType vt, const std::string &outdir, int mode, LanczosResult *res) {
+  const Model &m = s->model;
+  const int64_t dim = s->dim;
+  char name[256];
+  snprintf(name, sizeof(name), "%s_eigenvec_%d_rank_%d.dat", m.data_head.c_str(), std::max(1, m.k_exct) - 1, 0);
+  const std::string path = join(outdir, name);
+  FILE *f = fopen(path.c_str(), "rb");
+  if (!f) { set_error("Error: A file of Inputvector does not exist."); return -1; }
+  int itr = 0;
+  long fdim = 0;
+  std::vector<double> h(2 * (size_t)(dim + 1), 0.0);
+  const bool ok = fread(&itr, sizeof(int), 1, f) == 1 && fread(&fdim, sizeof(long), 1, f) == 1 && fdim == (long)dim &&
+                  fread(h.data(), sizeof(double), h.size(), f) == h.size();
+  fclose(f);
+  if (!ok) { set_error("Error: A file of Inputvector is incorrect."); return -1; }
+  h[0] = h[1] = 0.0;
+  for (int64_t i = 1; i <= dim && vt == kReal64; i++)
+    if (h[2 * i + 1] != 0.0) vt = kComplex128;  // a complex stored vector keeps its phases
+  const size_t esz = (vt == kReal64) ? sizeof(double) : sizeof(cplx);
+  RET(cuda_ok(cudaSetDevice(s->device), "cudaSetDevice"));
+  DevBuf A, B, C, ST;
+  RET(cuda_ok(cudaMalloc(&A.p, esz * dim), "alloc"));
+  RET(cuda_ok(cudaMalloc(&B.p, esz * dim), "alloc"));
+  RET(cuda_ok(cudaMalloc(&ST.p, sizeof(double) * 32), "alloc scalars"));
+  double *st = (double *)ST.p;
+  RET(vec_from_host_c128(s, vt, h.data(), A.p));
+  RET(to_native(s, vt, A.p, B.p));
+  if (mode == 2) {
+    // v0 = H v1 (v0 starts at zero), v1 = v0 / |v0| (src/CalcByLanczos.c:208-223)
+    RET(cuda_ok(cudaMalloc(&C.p, esz * dim), "alloc"));
+    const double coef[2] = {0.0, 1.0};
+    RET(cuda_ok(cudaMemcpyAsync(st, coef, sizeof(coef), cudaMemcpyHostToDevice, s->stream), "coef"));
+    RET(hv_native(s, vt, B.p, C.p, st, st + 2, false));
+    RET(vec_norm2(s, vt, C.p, st + 4));
+    double n2 = 0.0;
+    RET(cuda_ok(cudaMemcpyAsync(&n2, st + 4, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "read"));
+    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+    RET(vec_scale(s, vt, 1.0 / std::sqrt(n2), C.p));
+    std::swap(B.p, C.p);
+    RET(from_native(s, vt, B.p, A.p));
+  }
+  RET(model_green(s, vt, A.p, 1.0, &res->green));
+  RET(native_observables(s, vt, B.p, st + 8));  // expec_totalSz
+  double ob[6];
+  RET(cuda_ok(cudaMemcpyAsync(ob, st + 8, sizeof(ob), cudaMemcpyDeviceToHost, s->stream), "read"));
+  RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+  res->sz = ob[4];
+  res->energy = res->doublon = 0.0;
+  res->converged = true;
+  res->from_input = true;
+  res->steps = 0;
+  res->eigenvector.assign(2 * (dim + 1), 0.0);
+  RET(vec_to_host_c128(s, vt, A.p, res->eigenvector.data()));
+  return cuda_ok(cudaStreamSynchronize(s->stream), "sync");
+}
+
 // OutputTMComponents / OutputLanczosVector (src/Lanczos_EigenValue.c:457-500, 697-720).
 int write_lanczos_restart(const Sector &s, const LanczosRestart &r, const std::string &outdir) {
   RET(ensure_dir(outdir));
@@ -702,13 +758,16 @@ int read_lanczos_restart(const Sector &s, const std::string &outdir, LanczosRest
 int write_lanczos_outputs(const Sector &s, const LanczosResult &r, const std::string &outdir) {
   RET(ensure_dir(outdir));
   const Model &m = s.model;
-  const std::string step_file = join(outdir, m.data_head + "_Lanczos_Step.dat");
-  // a continued run appends to the step file (src/Lanczos_EigenValue.c:200-222)
-  FILE *f = fopen(step_file.c_str(), r.resumed ? "a" : "w");
-  if (!f) { set_error("cannot write " + step_file); return -1; }
-  for (const auto &l : r.lines) fputs(l.c_str(), f);
-  fclose(f);
-  if (m.calc_eigenvec == -1 || !r.converged) return 0;
+  FILE *f = nullptr;
+  if (!r.from_input) {
+    const std::string step_file = join(outdir, m.data_head + "_Lanczos_Step.dat");
+    // a continued run appends to the step file (src/Lanczos_EigenValue.c:200-222)
+    f = fopen(step_file.c_str(), r.resumed ? "a" : "w");
+    if (!f) { set_error("cannot write " + step_file); return -1; }
+    for (const auto &l : r.lines) fputs(l.c_str(), f);
+    fclose(f);
+    if (m.calc_eigenvec == -1 || !r.converged) return 0;
+  }
   const std::string ef = join(outdir, m.data_head + "_energy.dat");
   f = fopen(ef.c_str(), "w");
   if (!f) { set_error("cannot write " + ef); return -1; }
@@ -735,7 +794,8 @@ int write_lanczos_outputs(const Sector &s, const LanczosResult &r, const std::st
 }
 
 // ------------------------------------------------------------------------ TPQ
-int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::string &outdir, TpqResult *res) {
+int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::string &outdir, TpqResult *res,
+            const TpqOptions &opt) {
   const Model &m = s->model;
   const int64_t dim = s->dim;
   const size_t esz = (vt == kReal64) ? sizeof(double) : sizeof(cplx);
@@ -754,8 +814,10 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
   RET(vec_norm2(s, vt, V.p, st + 0));
   RET(cuda_ok(cudaMemcpyAsync(&n0, st, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "read"));
   RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
-  const double first_norm = std::sqrt(n0);
-  double sv = 1.0 / first_norm;  // V holds the current vector times 1/sv
+  const bool resumed = opt.resume_step > 0;
+  // global_1st_norm is only set by MakeIniVec, so a continued run prints 0 (its initial value)
+  const double first_norm = resumed ? 0.0 : std::sqrt(n0);
+  double sv = 1.0 / std::sqrt(n0);  // V holds the current vector times 1/sv
   RET(ensure_dir(outdir));
   char name[256];
   snprintf(name, sizeof(name), "SS_rand%d.dat", rand_i);
@@ -764,7 +826,8 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
   const std::string norm_file = join(outdir, name);
   snprintf(name, sizeof(name), "Flct_rand%d.dat", rand_i);
   const std::string flct_file = join(outdir, name);
-  FILE *fss = fopen(ss_file.c_str(), "w"), *fnorm = fopen(norm_file.c_str(), "w"), *fflct = fopen(flct_file.c_str(), "w");
+  const char *mode = resumed ? "a" : "w";  // a continued run appends (src/CalcByTPQ.c:118-136)
+  FILE *fss = fopen(ss_file.c_str(), mode), *fnorm = fopen(norm_file.c_str(), mode), *fflct = fopen(flct_file.c_str(), mode);
   if (!fss || !fnorm || !fflct) {
     if (fss) fclose(fss);
     if (fnorm) fclose(fnorm);
@@ -772,9 +835,11 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
     set_error("cannot write TPQ output files in " + outdir);
     return -1;
   }
-  fprintf(fss, " # inv_tmp, energy, phys_var, phys_doublon, phys_num, step_i\n");
-  fprintf(fnorm, " # inv_temp, global_norm, global_1st_norm, step_i \n");
-  fprintf(fflct, " # inv_temp, N, N^2, D, D^2, Sz, Sz^2, step_i \n");
+  if (!resumed) {
+    fprintf(fss, " # inv_tmp, energy, phys_var, phys_doublon, phys_num, step_i\n");
+    fprintf(fnorm, " # inv_temp, global_norm, global_1st_norm, step_i \n");
+    fprintf(fflct, " # inv_temp, N, N^2, D, D^2, Sz, Sz^2, step_i \n");
+  }
   // expec_energy_flct on the current vector (sv*V): observables, H = H*(sv V), E, var.
   double ob[6], E = 0.0, var = 0.0;
   auto expec = [&]() -> int {
@@ -826,21 +891,27 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
   };
   res->energy.clear();
   res->inv_temp.clear();
-  // FirstMultiply: expec on the start vector, then v = (L - H/Ns) v normalised.
-  RET(expec());
-  if (green) RET(green_step(0));
-  double gnorm = 0.0;
-  RET(multiply(&gnorm));
-  write_lines(0.0, first_norm, 0, false);
-  res->energy.push_back(E);
-  res->inv_temp.push_back(0.0);
-  RET(expec());
-  int step = 1;
-  double inv_temp = (2.0 / Ns) / (L - E / Ns);
-  write_lines(inv_temp, gnorm, step, true);
-  res->energy.push_back(E);
-  res->inv_temp.push_back(inv_temp);
-  for (step = 2; step < m.lanczos_max; step++) {
+  double gnorm = 0.0, inv_temp = 0.0;
+  int step = 2;
+  if (resumed) {
+    // expec_energy_flct on the stored state, then the loop from its step (src/CalcByTPQ.c:107-113)
+    RET(expec());
+    step = opt.resume_step;
+  } else {
+    // FirstMultiply: expec on the start vector, then v = (L - H/Ns) v normalised.
+    RET(expec());
+    if (green) RET(green_step(0));
+    RET(multiply(&gnorm));
+    write_lines(0.0, first_norm, 0, false);
+    res->energy.push_back(E);
+    res->inv_temp.push_back(0.0);
+    RET(expec());
+    inv_temp = (2.0 / Ns) / (L - E / Ns);
+    write_lines(inv_temp, gnorm, 1, true);
+    res->energy.push_back(E);
+    res->inv_temp.push_back(inv_temp);
+  }
+  for (; step < m.lanczos_max; step++) {
     RET(multiply(&gnorm));
     RET(expec());
     inv_temp = (2.0 * step / Ns) / (L - E / Ns);
@@ -852,6 +923,15 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
   fclose(fss);
   fclose(fnorm);
   fclose(fflct);
+  res->final_step = step;
+  if (opt.keep_vector) {
+    // the normalised state sv*V in HPhi's order
+    RET(from_native(s, vt, V.p, H.p));
+    res->final_vector.assign(2 * (dim + 1), 0.0);
+    RET(vec_to_host_c128(s, vt, H.p, res->final_vector.data()));
+    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+    for (double &x : res->final_vector) x *= sv;
+  }
   return 0;
 }
 

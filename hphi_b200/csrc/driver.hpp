@@ -66,12 +66,20 @@ struct LanczosResult {
   int cg_rounds = 0, cg_iterations = 0;
   std::vector<double> eigenvector;   // 1-based complex128 (HPhi layout) when requested
   GreenValues green;                 // of the eigenvector (src/CalcByLanczos.c:229-240)
+  bool from_input = false;           // InputEigenVec: no Lanczos run, no step file
 };
+
+// CalcByLanczos with InputEigenVec 1 or 2 (src/CalcByLanczos.c:160-225): the vector stored in
+// <outdir>/<head>_eigenvec_<exct-1>_rank_0.dat replaces the Lanczos run (mode 2 takes
+// H v / |H v|); its Green's functions and Sz follow.  Energy and Doublon are not computed
+// on this path (they print as 0, as in the reference).
+int lanczos_input_vector(Sector *s, VecType vt, const std::string &outdir, int mode, LanczosResult *res);
 
 struct LobpcgResult {
   bool converged = false;
   bool copy_vectors = false;         // copy the eigenvectors back (HPhi layout, exct blocks)
-  int steps = 0;                     // X->Large.itr
+  int steps = 0;                     // steps run (at most Lanczos_max)
+  int itr = 0;                       // X->Large.itr: the loop counter (Lanczos_max + 1 when unconverged)
   double residual = 0.0;             // largest residual 2-norm of the last step
   std::vector<double> eig;           // LOBPCG eigenvalue estimates of the last step
   std::vector<double> energy, var, doublon, sz;  // phys() of each converged vector
@@ -82,6 +90,16 @@ struct LobpcgResult {
 
 struct TpqResult {
   std::vector<double> inv_temp, energy;
+  int final_step = 0;                // step_i after the loop (the restart file's step)
+  std::vector<double> final_vector;  // the last state (HPhi layout) when TpqOptions::keep_vector
+};
+
+// TPQ restart (ReStart, src/CalcByTPQ.c:86-110, 275-290): resume_step > 0 continues from a
+// stored state (h_init) at that step, appending to the sample's files; keep_vector returns
+// the last state for tmpvec_set%d_rank_%d.dat.
+struct TpqOptions {
+  int resume_step = 0;
+  bool keep_vector = false;
 };
 
 // k-th smallest eigenvalue (0-based) of the symmetric tridiagonal matrix with diagonal
@@ -101,7 +119,8 @@ int write_lanczos_outputs(const Sector &s, const LanczosResult &r, const std::st
 int write_lanczos_restart(const Sector &s, const LanczosRestart &r, const std::string &outdir);
 int read_lanczos_restart(const Sector &s, const std::string &outdir, LanczosRestart *r);
 // h_init: start vector (any norm) of sample rand_i; writes SS/Norm/Flct_rand<rand_i>.dat.
-int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::string &outdir, TpqResult *res);
+int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::string &outdir, TpqResult *res,
+            const TpqOptions &opt = TpqOptions());
 // Block LOBPCG for the exct lowest states (CalcType 3).  h_init: exct start vectors in
 // HPhi's 1-based complex128 layout, back to back (any norm).
 bool lobpcg_single_element_start(const Sector &s, std::vector<double> *v);

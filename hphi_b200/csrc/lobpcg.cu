@@ -515,6 +515,7 @@ int lobpcg_run(Sector *s, VecType vt, const double *h_init, LobpcgResult *res) {
     }
   }
   res->steps = std::min(stp, m.lanczos_max);
+  res->itr = stp;
   res->eig = eig;
   // phys() / expec_energy_flct for each x: energy, <Hx|Hx>, doublon, Sz
   res->energy.assign(k, 0.0);
@@ -597,7 +598,7 @@ int write_lobpcg_outputs(const Sector &s, const LobpcgResult &r, const std::stri
         set_error("cannot write " + vf);
         return -1;
       }
-      const int itr = r.steps;
+      const int itr = r.itr;
       const long dim = (long)s.dim;
       fwrite(&itr, sizeof(int), 1, fv);
       fwrite(&dim, sizeof(long), 1, fv);

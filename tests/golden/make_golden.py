@@ -16,6 +16,9 @@ refstart_* directories hold start.npz: the first mltply input of a golden case's
 with several OpenMP threads (the reference's per-thread random start vectors).
 restart_* directories hold inputs a/ and b/ and restart.npz: the restart files run a wrote
 and the steps and energy of run b continued from them.
+tpqrestart_* directories hold inputs a/ (ReStart 1) and b/ (ReStart 3, continuing a) and
+restart.npz: the TPQ files and the stored states (tmpvec_set%d_rank_0.dat) after each run;
+lobpcgrestart_* the same for LOBPCG (step rows of both runs, a's stored vectors, b's states).
 green_* directories hold inputs with OneBodyG / TwoBodyG files and golden.npz with the
 reference's Green's function files (text_<file>), the eigenvectors it wrote (vec_<file>,
 OutputEigenVec), the first mltply input (start) and its energies (states, or tpq rows).
@@ -398,12 +401,90 @@ def make_green_case(name: str, m) -> None:
     np.savez_compressed(os.path.join(out, "golden.npz"), **data)
 
 
+def _tpq_restart_cases():
+    """TPQ restart: input a/ (ReStart 1, Lanczos_max 12, two samples: writes
+    tmpvec_set%d_rank_0.dat) and b/ (ReStart 3, Lanczos_max 25: continues both samples; the reference
+    divides by (Lanczos_max - step + 1) / 10 for its progress log, so it needs 10 more steps)."""
+    def model(restart, lmax):
+        m = expert.hubbard(6, expert.chain_bonds(6), 1.0, 4.0, 3, 3, calc_type="TPQ", lanczos_max=lmax,
+                           num_ave=2, large_value=6.0, expec_interval=100)
+        m.initial_vec_type = 0
+        m.restart = restart
+        return m
+    return {"tpqrestart_hub6": (model(1, 12), model(3, 25))}
+
+
+def make_tpq_restart_case(name: str, ma, mb) -> None:
+    out = os.path.join(HERE, name)
+    shutil.rmtree(out, ignore_errors=True)
+    ma.write(os.path.join(out, "a"))
+    mb.write(os.path.join(out, "b"))
+    data = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        od = os.path.join(tmp, "output")
+        for tag, sub in (("a", "a"), ("b", "b")):
+            for f in os.listdir(os.path.join(out, sub)):
+                shutil.copy(os.path.join(out, sub, f), tmp)
+            if run_ref.run(tmp, threads=1, dump_call=-1).returncode != 0:
+                raise RuntimeError(f"{name}: reference run {tag} failed")
+            for r in range(2):
+                for base in ("SS_rand", "Norm_rand", "Flct_rand"):
+                    data[f"{tag}_{base}{r}"] = np.array(open(os.path.join(od, f"{base}{r}.dat")).read())
+                with open(os.path.join(od, f"tmpvec_set{r}_rank_0.dat"), "rb") as f:
+                    data[f"{tag}_step{r}"] = np.array(int(np.frombuffer(f.read(4), dtype=np.int32)[0]))
+                    dim = int(np.frombuffer(f.read(8), dtype=np.int64)[0])
+                    v = np.frombuffer(f.read(16 * (dim + 1)), dtype=np.complex128).copy()
+                    v[0] = 0
+                    data[f"{tag}_vec{r}"] = v
+    np.savez_compressed(os.path.join(out, "restart.npz"), **data)
+
+
+def _lobpcg_restart_cases():
+    """LOBPCG restart: input a/ (ReStart 1, Lanczos_max 8: stops unconverged and writes
+    tmpvec_set%d_rank_0.dat per state) and b/ (ReStart 3: continues from them)."""
+    def model(restart, lmax):
+        m = expert.heisenberg(12, expert.chain_bonds(12), calc_type="CG", exct=2, lanczos_max=lmax)
+        m.restart = restart
+        return m
+    return {"lobpcgrestart_chain12": (model(1, 8), model(3, 500))}
+
+
+def make_lobpcg_restart_case(name: str, ma, mb) -> None:
+    out = os.path.join(HERE, name)
+    shutil.rmtree(out, ignore_errors=True)
+    ma.write(os.path.join(out, "a"))
+    mb.write(os.path.join(out, "b"))
+    data = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        od = os.path.join(tmp, "output")
+        for tag, sub in (("a", "a"), ("b", "b")):
+            for f in os.listdir(os.path.join(out, sub)):
+                shutil.copy(os.path.join(out, sub, f), tmp)
+            p = run_ref.run(tmp, threads=1, dump_call=-1)
+            if p.returncode != 0:
+                raise RuntimeError(f"{name}: reference run {tag} failed")
+            data[f"{tag}_steps"] = run_ref.lobpcg_steps(tmp)
+            if tag == "a":
+                for ie in range(2):
+                    with open(os.path.join(od, f"tmpvec_set{ie}_rank_0.dat"), "rb") as f:
+                        data[f"a_itr{ie}"] = np.array(int(np.frombuffer(f.read(4), dtype=np.int32)[0]))
+                        dim = int(np.frombuffer(f.read(8), dtype=np.int64)[0])
+                        v = np.frombuffer(f.read(16 * (dim + 1)), dtype=np.complex128).copy()
+                        v[0] = 0
+                        data[f"a_vec{ie}"] = v
+                data["a_energy_exists"] = np.array(os.path.exists(os.path.join(od, "zvo_energy.dat")))
+            else:
+                data["b_states"] = run_ref.energy_states(tmp)
+    np.savez_compressed(os.path.join(out, "restart.npz"), **data)
+
+
 def main(argv) -> None:
     if not run_ref.available():
         raise SystemExit("oracle/_ref/HPhi_ref is missing: run `make -C oracle` first")
     small, large, starts, restarts = _cases(), _large_cases(), _start_cases(), _restart_cases()
-    greens = _green_cases()
-    names = argv or list(small) + list(large) + list(starts) + list(restarts) + list(greens)
+    greens, tpq_restarts, lobpcg_restarts = _green_cases(), _tpq_restart_cases(), _lobpcg_restart_cases()
+    names = argv or (list(small) + list(large) + list(starts) + list(restarts) + list(greens) + list(tpq_restarts)
+                     + list(lobpcg_restarts))
     for n in names:
         print("case", n, flush=True)
         if n in small:
@@ -414,6 +495,10 @@ def main(argv) -> None:
             make_restart_case(n, *restarts[n])
         elif n in greens:
             make_green_case(n, greens[n])
+        elif n in tpq_restarts:
+            make_tpq_restart_case(n, *tpq_restarts[n])
+        elif n in lobpcg_restarts:
+            make_lobpcg_restart_case(n, *lobpcg_restarts[n])
         else:
             make_case(n, large[n], large=True)
 
