@@ -25,6 +25,9 @@ metric (solves/s and latency against the plain FP64 GPU path):
              half-filled Hubbard chains L=10..14 (U in [2,10]) and 24-site Kitaev-Heisenberg
              honeycomb (SpinGC, complex) through the continuous-batching server: solves/s,
              p50/p99 latency, |dE| against each request solved alone by the plain driver.
+  green      expec_cisajs on the 4x4 Hubbard sector: the 512 spin-conserving one-body rows of a
+             normalised random vector (rows x sector rows per second), the reference's
+             expec_cisajs timed on 8 of the rows as the CPU baseline.
 
 Multi-GPU (--gpus N under torchrun): the path does not shard for this workload, so
 N independent replicas run (one per GPU); value = total bytes / max-over-ranks time.
@@ -321,6 +324,117 @@ def run_precision_mode(args):
     print(json.dumps(out))
 
 
+def reference_green_times(model, vec_c128: np.ndarray, threads: int, timeout: float = 3000.0):
+    """Wall time of the reference's expec_cisajs (oracle/_ref/HPhi_ref, link-time hook) on
+    the vector vec_c128 (HPhi layout), read through CalcByLanczos with InputEigenVec 1."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import run_ref
+    if not run_ref.available():
+        return None, "oracle/_ref/HPhi_ref not built"
+    with tempfile.TemporaryDirectory() as tmp:
+        model.calc_eigenvec, model.output_eigenvec = 0, 0
+        model.write(tmp)
+        txt = open(os.path.join(tmp, "calcmod.def")).read() + "InputEigenVec 1\n"
+        open(os.path.join(tmp, "calcmod.def"), "w").write(txt)
+        os.makedirs(os.path.join(tmp, "output"))
+        with open(os.path.join(tmp, "output", "zvo_eigenvec_0_rank_0.dat"), "wb") as f:
+            f.write(np.array([0], dtype=np.int32).tobytes())
+            f.write(np.array([vec_c128.size - 1], dtype=np.int64).tobytes())
+            f.write(vec_c128.tobytes())
+        t0 = time.time()
+        run_ref.run(tmp, threads=threads, dump_call=-1, timeout=timeout, extra_env={"HPHI_DUMP_LISTS": "0"})
+        wall = time.time() - t0
+        p = os.path.join(tmp, "green_times.txt")
+        if not os.path.exists(p):
+            return None, "reference produced no timing"
+        vals = open(p).read().split()
+        return float(vals[1]), f"{wall:.1f} s wall"
+
+
+def run_green_mode(args):
+    """One-body Green's functions (expec_cisajs) on the half-filled 4x4 Hubbard sector: all 512
+    spin-conserving rows <c+_{i s} c_{j s}> of a normalised random real vector."""
+    import torch
+    import hphi_b200
+    from hphi_b200 import expert
+    model, desc = workload_model(args.workload)
+    n_elec = model.ncond
+    rows = np.array([(i, s_, j, s_) for s_ in (0, 1) for i in range(16) for j in range(16)], dtype=np.int32)
+    model.greenone = [tuple(int(x) for x in r) for r in rows]
+    tmp = tempfile.mkdtemp()
+    H = hphi_b200.Hamiltonian(model.write(tmp))
+    dim = H.dim
+    gen = torch.Generator(device="cuda").manual_seed(77)
+    v = torch.rand(dim, dtype=torch.float64, device="cuda", generator=gen) - 0.5
+    v /= torch.linalg.vector_norm(v)
+    stream = torch.cuda.ExternalStream(H.stream)
+    for _ in range(args.warmup):
+        g = H.expec_green_device(v.data_ptr(), hphi_b200.REAL64, rows, 1)
+    clocks = _clock_start()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        g = H.expec_green_device(v.data_ptr(), hphi_b200.REAL64, rows, 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    cl = clocks.stop()
+    t = e0.elapsed_time(e1) / 1e3 / args.steps
+    n_rows = len(rows)
+    per_pass = 16                                   # real rows evaluated per pass over the sector
+    passes = (n_rows + per_pass - 1) // per_pass
+    stream_bytes = passes * dim * 16.0              # list_1 + the vector, once per pass
+    value = n_rows * dim / t / 1e9
+    # checks: densities sum to the electron number, every <n_i s> in [0, 1]
+    dens = np.array([g[k] for k in range(n_rows) if rows[k, 0] == rows[k, 2]]).real
+    ok = abs(dens.sum() - n_elec) < 1e-9 and dens.min() > -1e-12 and dens.max() < 1 + 1e-12
+    # end to end: the reference-facing call on a pinned HPhi-layout complex128 host vector
+    vh = torch.zeros(dim + 1, dtype=torch.complex128).pin_memory()
+    vh[1:].real.copy_(v.cpu())
+    vnp = vh.numpy()
+    e2e = None
+    if args.e2e_steps > 0:
+        H.expec_green(vnp, rows, 1)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            ge = H.expec_green(vnp, rows, 1)
+        te = (time.perf_counter() - t0) / args.e2e_steps
+        e2e = {"value": n_rows * dim / te / 1e9, "unit": "G row-elements/s", "h2d_bytes_per_step": 16 * (dim + 1),
+               "d2h_bytes_per_step": 16 * n_rows, "ms_per_step": 1e3 * te,
+               "max_abs_diff_vs_device": float(np.max(np.abs(ge - g)))}
+    peak, peak_src = peak_hbm()
+    traffic = profile_traffic("green_kernel", args.workload)
+    roof = {"bound": "hbm", "achieved": stream_bytes / t / 1e9, "peak": peak, "unit": "GB/s",
+            "frac": stream_bytes / t / 1e9 / peak, "traffic": traffic, "peak_source": peak_src,
+            "kernel": "green_kernel<double,false> + finalize_partials_kernel<16>, one pass per 16 rows; "
+                      "achieved counts 16 bytes per sector row per pass (list_1 and the vector), traffic is "
+                      "DRAM bytes per green_kernel launch"}
+    cpu = None
+    if not args.no_cpu_baseline:
+        sample = 8
+        mref, _ = workload_model(args.workload)
+        mref.greenone = [tuple(int(x) for x in r) for r in rows[:sample]]
+        threads = os.cpu_count()
+        tr, note = reference_green_times(mref, vnp, threads)
+        if tr is not None:
+            cpu = {"value": sample * dim / tr / 1e9, "unit": "G row-elements/s", "cores": threads,
+                   "kind": "reference", "sample": f"the reference's expec_cisajs on the first {sample} rows "
+                                                 f"(OMP_NUM_THREADS={threads}), {tr:.2f} s; whole run {note}"}
+        else:
+            cpu = {"unavailable": note}
+    H.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    out = {"metric": METRIC, "mode": "green", "value": value, "unit": "G row-elements/s", "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"{args.workload} expec_cisajs", "desc": desc, "dim": dim, "rows": n_rows,
+                      "rows_desc": "c+_{i s} c_{j s}, i, j = 0..15, s = 0, 1",
+                      "l2": "vectors and list_1 (1.3 GB each) exceed L2; no flush"},
+           "checks_ok": bool(ok), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+           "gpu_launches": 2 * passes * args.steps, "clocks": cl}
+    print(json.dumps(out))
+
+
 def serve_requests(n: int, seed: int = 50):
     from hphi_b200 import expert
     rng = np.random.default_rng(seed)
@@ -406,7 +520,7 @@ def run_serve_mode(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", default="hv", choices=["hv", "batch", "precision", "serve"])
+    ap.add_argument("--mode", default="hv", choices=["hv", "batch", "precision", "serve", "green"])
     ap.add_argument("--batch-size", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=300)
     ap.add_argument("--precision-steps", type=int, default=300)
@@ -432,7 +546,8 @@ def main():
             return
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        {"batch": run_batch_mode, "precision": run_precision_mode, "serve": run_serve_mode}[args.mode](args)
+        {"batch": run_batch_mode, "precision": run_precision_mode, "serve": run_serve_mode,
+         "green": run_green_mode}[args.mode](args)
         return
 
     import torch

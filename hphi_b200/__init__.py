@@ -45,7 +45,7 @@ EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi
                     "hphi_batch_free", "hphi_server_create", "hphi_server_submit", "hphi_server_step",
                     "hphi_server_poll", "hphi_server_clock", "hphi_server_free", "hphi_lobpcg",
                     "hphi_reference_start", "hphi_expec_green", "hphi_expec_cisajs", "hphi_expec_cisajscktaltdc",
-                    "hphi_inspect_green"]
+                    "hphi_inspect_green", "hphi_expec_green_device"]
 FP64 = 0
 FP32 = 1
 BATCH_GRAPH = 1
@@ -123,6 +123,7 @@ def load_library() -> ctypes.CDLL:
     lib.hphi_expec_cisajs.argtypes = [P, pd, pd, ctypes.c_char_p]
     lib.hphi_expec_cisajscktaltdc.argtypes = [P, pd, pd, ctypes.c_char_p]
     lib.hphi_inspect_green.argtypes = [ctypes.c_char_p, I, pint, I]
+    lib.hphi_expec_green_device.argtypes = [P, I, I, pint, I, VP, pd]
     for name in EXPORTED_SYMBOLS:
         if name not in ("hphi_version", "hphi_last_error", "hphi_close", "hphi_stream", "hphi_batch_free",
                         "hphi_server_clock", "hphi_server_free"):
@@ -271,6 +272,15 @@ class Hamiltonian:
         _check(load_library().hphi_expec_green(self._h, int(body), len(r),
                                                r.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
                                                _dptr(vec.view(np.float64)), _dptr(out)))
+        return out[0:2 * len(r):2] + 1j * out[1:2 * len(r):2]
+
+    def expec_green_device(self, vec_ptr: int, vec_type: int, rows, body: int) -> np.ndarray:
+        """expec_green on a device vector in HPhi's row order (REAL64 or COMPLEX128)."""
+        r = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).reshape(-1, 4 if body == 1 else 8))
+        out = np.zeros(2 * max(len(r), 1))
+        _check(load_library().hphi_expec_green_device(self._h, int(body), len(r),
+                                                      r.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                                      int(vec_type), ctypes.c_void_p(vec_ptr), _dptr(out)))
         return out[0:2 * len(r):2] + 1j * out[1:2 * len(r):2]
 
     def expec_cisajs(self, vec: np.ndarray, path: Optional[str] = None) -> np.ndarray:

@@ -565,7 +565,7 @@ int hphi_tpq(hphi_handle *h, const double *v_init, const char *output_dir, doubl
 int hphi_lobpcg(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult) {
   CHECK_HANDLE(h);
   Sector *s = h->sector;
-  const VecType vt = default_vec_type(*s);
+  VecType vt = default_vec_type(*s);
   const int k = std::max(1, s->model.k_exct);
   std::vector<double> start;
   const int restart = s->model.restart;  // RESTART_OUT 1, RESTART_INOUT 2, RESTART_IN 3
@@ -598,6 +598,30 @@ int hphi_lobpcg(hphi_handle *h, const double *v_init, const char *output_dir, do
       v_init = start.data();
     }
   }
+  bool from_input = false;
+  if (s->model.input_eigenvec != 0 && !v_init) {
+    // InputEigenVec: the states stored in <head>_eigenvec_%d_rank_0.dat (src/CalcByLOBPCG.c:688-716)
+    start.assign((size_t)stride * k, 0.0);
+    for (int ie = 0; ie < k; ie++) {
+      char name[256];
+      snprintf(name, sizeof(name), "%s_eigenvec_%d_rank_%d.dat", s->model.data_head.c_str(), ie, 0);
+      const std::string path = out.empty() ? std::string(name) : out + "/" + name;
+      FILE *f = fopen(path.c_str(), "rb");
+      if (!f) { set_error("Error: Inputvector file is not found."); return -1; }
+      int itr = 0;
+      long dim = 0;
+      const bool ok = fread(&itr, sizeof(int), 1, f) == 1 && fread(&dim, sizeof(long), 1, f) == 1 &&
+                      dim == (long)s->dim &&
+                      fread(start.data() + (size_t)stride * ie, sizeof(double), stride, f) == (size_t)stride;
+      fclose(f);
+      if (!ok) { set_error("Error: Invalid Inputvector file."); return -1; }
+      start[(size_t)stride * ie] = start[(size_t)stride * ie + 1] = 0.0;
+    }
+    v_init = start.data();
+    from_input = true;
+    for (size_t q = 1; q < start.size() && vt == kReal64; q += 2)
+      if (start[q] != 0.0) vt = kComplex128;  // complex stored states keep their phases
+  }
   if (!v_init) {
     if (!lobpcg_single_element_start(*s, &start))
       reference_random_start(s->dim, kRefLOBPCG, s->model.initial_iv, 0, s->model.initial_vec_type,
@@ -605,6 +629,7 @@ int hphi_lobpcg(hphi_handle *h, const double *v_init, const char *output_dir, do
     v_init = start.data();
   }
   LobpcgResult r;
+  r.phys_only = from_input;
   const bool restart_out = (restart == 1 || restart == 2) && output_dir;
   // OutputEigenVec files and the restart vectors need the states on the host
   r.copy_vectors = (s->model.output_eigenvec != 0 && output_dir) || restart_out;
@@ -714,6 +739,29 @@ int hphi_expec_green(hphi_handle *h, int body, int n, const int *rows, const dou
   std::vector<double> g;
   std::vector<char> trail;
   if (green_host(h, body, n, rows, vec, &g, &trail) != 0) return -1;
+  std::memcpy(out, g.data(), sizeof(double) * g.size());
+  return 0;
+}
+
+int hphi_expec_green_device(hphi_handle *h, int body, int n, const int *rows, int vec_type, const void *d_vec,
+                            double *out) {
+  CHECK_HANDLE(h);
+  if ((body != 1 && body != 2) || n < 0 || (vec_type != kReal64 && vec_type != kComplex128) ||
+      (n > 0 && (!rows || !d_vec || !out))) {
+    set_error("hphi_expec_green_device: bad arguments");
+    return -1;
+  }
+  if (n == 0) return 0;
+  Sector *s = h->sector;
+  std::vector<GreenTerm> terms;
+  std::vector<char> trail;
+  std::string err;
+  if (compile_green(s->model, body, rows, n, &terms, &trail, &err) != 0) {
+    set_error(err);
+    return -1;
+  }
+  std::vector<double> g;
+  if (green_expect(s, (VecType)vec_type, d_vec, terms, &g) != 0) return -1;
   std::memcpy(out, g.data(), sizeof(double) * g.size());
   return 0;
 }

@@ -78,6 +78,7 @@ int lanczos_input_vector(Sector *s, VecType vt, const std::string &outdir, int m
 struct LobpcgResult {
   bool converged = false;
   bool copy_vectors = false;         // copy the eigenvectors back (HPhi layout, exct blocks)
+  bool phys_only = false;            // InputEigenVec: the start block is the result (no iteration, no step file)
   int steps = 0;                     // steps run (at most Lanczos_max)
   int itr = 0;                       // X->Large.itr: the loop counter (Lanczos_max + 1 when unconverged)
   double residual = 0.0;             // largest residual 2-norm of the last step

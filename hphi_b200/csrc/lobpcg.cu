@@ -415,7 +415,7 @@ int lobpcg_run(Sector *s, VecType vt, const double *h_init, LobpcgResult *res) {
   res->converged = false;
   int stp;
   char line[512];
-  for (stp = 1; stp <= m.lanczos_max; stp++) {
+  for (stp = 1; !res->phys_only && stp <= m.lanczos_max; stp++) {
     double eabs = 0.0;
     for (int i = 0; i < k; i++) eabs = std::max(eabs, std::fabs(eig[i]));
     double eps = std::pow(10.0, -0.5 * m.lanczos_eps);
@@ -516,6 +516,12 @@ int lobpcg_run(Sector *s, VecType vt, const double *h_init, LobpcgResult *res) {
   }
   res->steps = std::min(stp, m.lanczos_max);
   res->itr = stp;
+  if (res->phys_only) {
+    // CalcByLOBPCG with InputEigenVec (src/CalcByLOBPCG.c:688-722): phys() of the read vectors
+    res->steps = res->itr = 0;
+    res->converged = true;
+    res->lines.clear();
+  }
   res->eig = eig;
   // phys() / expec_energy_flct for each x: energy, <Hx|Hx>, doublon, Sz
   res->energy.assign(k, 0.0);
@@ -563,13 +569,16 @@ int write_lobpcg_outputs(const Sector &s, const LobpcgResult &r, const std::stri
   const Model &m = s.model;
   const std::string sep = outdir.empty() ? "" : "/";
   const std::string step_file = outdir + sep + m.data_head + "_Lanczos_Step.dat";
-  FILE *f = fopen(step_file.c_str(), "w");
-  if (!f) {
-    set_error("cannot write " + step_file);
-    return -1;
+  FILE *f = nullptr;
+  if (!r.phys_only) {
+    f = fopen(step_file.c_str(), "w");
+    if (!f) {
+      set_error("cannot write " + step_file);
+      return -1;
+    }
+    for (const auto &l : r.lines) fputs(l.c_str(), f);
+    fclose(f);
   }
-  for (const auto &l : r.lines) fputs(l.c_str(), f);
-  fclose(f);
   if (!r.converged) return 0;
   const std::string ef = outdir + sep + m.data_head + "_energy.dat";
   f = fopen(ef.c_str(), "w");

@@ -318,6 +318,10 @@ int hphi_reference_start(int64_t dim, int kind, int initial_iv, int sample, int 
  * expec_cisajscktaltdc (src/expec_cisajscktaltdc.c:87-1647), one batch of rows per pass.
  */
 int hphi_expec_green(hphi_handle *h, int body, int n, const int *rows, const double *vec, double *out);
+/* The same on a device vector in HPhi's row order (d_vec[r] for row r + 1; vec_type 0 real
+ * float64, 1 complex128), on the handle's stream; returns when out is filled. */
+int hphi_expec_green_device(hphi_handle *h, int body, int n, const int *rows, int vec_type, const void *d_vec,
+                            double *out);
 
 /*
  * expec_cisajs (src/expec_cisajs.c:66) and expec_cisajscktaltdc (src/expec_cisajscktaltdc.c:87)

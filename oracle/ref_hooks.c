@@ -2,7 +2,8 @@
  * Link-time hooks around the reference HPhi executable (test infrastructure).
  *
  * This file is linked into oracle/_ref/HPhi_ref together with the unmodified
- * reference sources (-Wl,--wrap=mltply -Wl,--wrap=sz -Wl,--wrap=diagonalcalc).
+ * reference sources (-Wl,--wrap=mltply -Wl,--wrap=sz -Wl,--wrap=diagonalcalc
+ * -Wl,--wrap=expec_cisajs).
  * It never changes what the reference computes; it only records it:
  *
  *   HPHI_DUMP_DIR=<dir>      enables the dumps below (nothing is written otherwise)
@@ -15,11 +16,13 @@
  *   <dir>/hv.bin      around mltply call k: int64 idim, v1[0..idim], v0_before[0..idim],
  *                                            v0_after[0..idim] (complex128), prdct (complex128)
  *   <dir>/mltply_times.txt at exit:          number of mltply calls and their wall times (s)
+ *   <dir>/green_times.txt at exit:           number of expec_cisajs calls and their wall times (s)
  *
  * Reference interfaces wrapped:
  *   int mltply(struct BindStruct*, double complex*, double complex*)   src/mltply.c:56
  *   int sz(struct BindStruct*, long unsigned int*, ...)                 src/sz.c:62
  *   int diagonalcalc(struct BindStruct*)                                src/diagonalcalc.c:84
+ *   int expec_cisajs(struct BindStruct*, double complex*)               src/expec_cisajs.c:66
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -32,6 +35,7 @@
 int __real_mltply(struct BindStruct *X, double complex *v0_, double complex *v1_);
 int __real_sz(struct BindStruct *X, long unsigned int *a, long unsigned int *b, long unsigned int *c);
 int __real_diagonalcalc(struct BindStruct *X);
+int __real_expec_cisajs(struct BindStruct *X, double complex *vec);
 
 static long g_ncall = 0;
 static double *g_times = NULL;
@@ -62,6 +66,9 @@ static double now_s(void) {
   return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
 }
 
+static long g_ngreen = 0;
+static double g_green_times[64];
+
 static void write_times(void) {
   char path[4096];
   const char *d = dump_dir();
@@ -72,6 +79,23 @@ static void write_times(void) {
   fprintf(f, "%ld\n", g_ncall);
   for (long i = 0; i < g_ncall && i < g_cap; i++) fprintf(f, "%.9e\n", g_times[i]);
   fclose(f);
+  if (g_ngreen == 0) return;
+  snprintf(path, sizeof(path), "%s/green_times.txt", d);
+  f = fopen(path, "w");
+  if (!f) return;
+  fprintf(f, "%ld\n", g_ngreen);
+  for (long i = 0; i < g_ngreen && i < 64; i++) fprintf(f, "%.9e\n", g_green_times[i]);
+  fclose(f);
+}
+
+int __wrap_expec_cisajs(struct BindStruct *X, double complex *vec) {
+  double t0 = now_s();
+  int r = __real_expec_cisajs(X, vec);
+  double t1 = now_s();
+  if (g_ngreen < 64) g_green_times[g_ngreen] = t1 - t0;
+  g_ngreen++;
+  if (!g_atexit) { atexit(write_times); g_atexit = 1; }
+  return r;
 }
 
 int __wrap_sz(struct BindStruct *X, long unsigned int *a, long unsigned int *b, long unsigned int *c) {

@@ -150,3 +150,32 @@ def test_green_on_the_full_size_sector():
     assert abs(dens.sum() - 16.0) < 1e-9
     assert (dens >= -1e-12).all() and (dens <= 1 + 1e-12).all()
     assert abs(g[32] - np.conj(g[33])) < 1e-12 and abs(g[34] - np.conj(g[35])) < 1e-12
+
+
+def test_lobpcg_input_eigenvectors(tmp_path, monkeypatch):
+    """CalcByLOBPCG with InputEigenVec: the reference's stored states replace the iteration;
+    phys() of them gives the reference's energies and, per state, the reference's Green's
+    function files (same vectors, so the excited state's files compare too)."""
+    name = "green_lobpcg_chain10"
+    z = load_golden(name)
+    d = tmp_path / "in"
+    shutil.copytree(case_dir(name), d)
+    os.remove(d / "golden.npz")
+    txt = open(d / "calcmod.def").read().replace("OutputEigenVec 1", "InputEigenVec 1")
+    open(d / "calcmod.def", "w").write(txt)
+    out = tmp_path / "output"
+    os.makedirs(out)
+    for k in range(2):
+        v = z[f"vec_zvo_eigenvec_{k}_rank_0.dat"]
+        with open(out / f"zvo_eigenvec_{k}_rank_0.dat", "wb") as f:
+            f.write(np.array([0], dtype=np.int32).tobytes())
+            f.write(np.array([v.size - 1], dtype=np.int64).tobytes())
+            f.write(v.astype(np.complex128).tobytes())
+    with hphi_b200.Hamiltonian(str(d / "namelist.def")) as H:
+        r = H.calc_by_lobpcg(output_dir=str(out))
+    assert r["converged"] and r["steps"] == 0
+    assert not (out / "zvo_Lanczos_Step.dat").exists()
+    np.testing.assert_allclose(r["energy"], z["states"][:, 0], rtol=0, atol=1e-10)
+    for f in (str(x) for x in z["green_files"]):
+        _, _, lines = green_reference(z, f)
+        _same_layout(open(out / f).read().splitlines(), lines, 1e-10)
