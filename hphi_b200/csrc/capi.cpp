@@ -705,8 +705,8 @@ int hphi_reference_start(int64_t dim, int kind, int initial_iv, int sample, int 
   return 0;
 }
 
-// Green's functions of host vector `vec` (HPhi layout); a vector with no imaginary part and a
-// real Hamiltonian run through the real kernels.
+// Green's functions of host vector `vec` (HPhi layout); a vector with no imaginary part runs
+// through the real kernels (checked on the device after one upload).
 static int green_host(hphi_handle *h, int body, int n, const int *rows, const double *vec, std::vector<double> *out,
                       std::vector<char> *trail) {
   Sector *s = h->sector;
@@ -716,14 +716,11 @@ static int green_host(hphi_handle *h, int body, int n, const int *rows, const do
     set_error(err);
     return -1;
   }
-  bool real = true;
-  for (int64_t i = 1; i <= s->dim && real; i++) real = vec[2 * i + 1] == 0.0;
-  const VecType vt = real ? kReal64 : kComplex128;
   cudaSetDevice(s->device);
   void *d = nullptr;
-  if (cuda_fail(cudaMalloc(&d, (real ? sizeof(double) : sizeof(cplx)) * (size_t)s->dim), "alloc")) return -1;
-  int rc = vec_from_host_c128(s, vt, vec, d);
-  if (rc == 0) rc = green_expect(s, vt, d, terms, out);
+  VecType vt = kComplex128;
+  if (green_stage_host_vector(s, vec, &d, &vt) != 0) return -1;
+  const int rc = green_expect(s, vt, d, terms, out);
   cudaStreamSynchronize(s->stream);
   cudaFree(d);
   return rc;

@@ -140,6 +140,9 @@ int vec_add_hashed(Sector *s, VecType vt, uint64_t seed, double amp, void *d_x);
 // HPhi's row order; out = (re, im) per entry (green.cu).
 int green_expect(Sector *s, VecType vt, const void *d_v, const std::vector<GreenTerm> &terms,
                  std::vector<double> *out);
+// Uploads a host vector in HPhi's layout for green_expect: real parts only (*vt = kReal64)
+// when every imaginary part is zero, else complex.  *d_vec is the caller's to cudaFree.
+int green_stage_host_vector(Sector *s, const double *h_v_1based, void **d_vec, VecType *vt);
 
 // complex128 <-> real and imaginary parts (n = dim); y[0, n) += x[0, n) on stream st.
 int vec_split_c128(Sector *s, const void *d_c, double *d_re, double *d_im);
