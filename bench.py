@@ -65,6 +65,12 @@ def workload_model(name: str):
     if name == "hubbard3x4":
         m = expert.hubbard(12, expert.square_bonds(3, 4), 1.0, 8.0, 6, 6)
         return m, "Hubbard 3x4 periodic, t=1, U=8, half filling (dim 853,776)"
+    if name == "heisenberg4x8":
+        m = expert.heisenberg(32, expert.square_bonds(4, 8), 1.0)
+        return m, "Heisenberg 4x8 periodic, J=1, Sz=0 (dim 601,080,390)"
+    if name == "heisenberg4x7":
+        m = expert.heisenberg(28, expert.square_bonds(4, 7), 1.0)
+        return m, "Heisenberg 4x7 periodic, J=1, Sz=0 (dim 40,116,600; profiling case)"
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -160,7 +166,7 @@ def run_reference_arm(args):
         return
     model, desc = workload_model(args.workload)
     dim = {"hubbard4x4": 165636900, "chain16": 12870, "hubbard3x4": 853776,
-           "hubbard4x4_6e": 64128064}[args.workload]
+           "hubbard4x4_6e": 64128064, "heisenberg4x8": 601080390, "heisenberg4x7": 40116600}[args.workload]
     threads = os.cpu_count()
     times, note = reference_mltply_times(model, args.warmup + args.steps, threads)
     if times is None:
