@@ -814,39 +814,51 @@ int batch_autotune(Batch *b, bool force) {
   cudaEventCreate(&e1);
   BatchTuning best;
   best.hv_ms = 1e30f;
-  const int threads_c[] = {128, 256, 512};
-  const int rows_c[] = {1, 2, 4, 8};
-  const int ctas_c[] = {2, 4, 8, 16};
+  // candidate launch shapes, the usual winners first: the search stops once it has spent
+  // kTuneBudgetS seconds (after at least three shapes), so a single very large instance is
+  // not timed 36 x 4 times while a batch of small instances still tries every shape
+  constexpr double kTuneBudgetS = 2.0;
+  std::vector<std::array<int, 3>> cand;  // threads, rows per thread, CTAs per SM
+  for (int rp : {1, 2})
+    for (int th : {256, 128, 512})
+      for (int cs : {8, 16, 4, 2})
+        if (th * cs <= 2048) cand.push_back({th, rp, cs});
+  for (int rp : {4, 8})
+    for (int th : {256, 128, 512})
+      for (int cs : {8, 16, 4, 2})
+        if (th * cs <= 2048) cand.push_back({th, rp, cs});
   const BatchTuning saved = b->tune;
   int rc = 0;
-  for (int th : threads_c)
-    for (int rp : rows_c)
-      for (int cs : ctas_c) {
-        if (th * cs > 2048 || rc) continue;
-        BatchTuning t;
-        t.threads = th;
-        t.rows_per_thread = rp;
-        t.ctas_per_sm = cs;
-        b->tune = t;
-        b->plan_dirty = true;
-        if ((rc = upload(b))) break;
-        auto trial = [&]() {
-          if (b->prec == kFP32) launch_hv<float>(b, t, 0, kTuneKind);
-          else launch_hv<double>(b, t, 0, kTuneKind);
-        };
-        trial();
-        cudaEventRecord(e0, b->stream);
-        for (int r = 0; r < 3; r++) trial();
-        cudaEventRecord(e1, b->stream);
-        if ((rc = cuda_ok(cudaEventSynchronize(e1), "tune sync"))) break;
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        ms /= 3.0f;
-        if (ms < best.hv_ms) {
-          best = t;
-          best.hv_ms = ms;
-        }
-      }
+  const auto t_start = std::chrono::steady_clock::now();
+  int tried = 0;
+  for (const auto &cnd : cand) {
+    const double spent = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    if (rc || (tried >= 3 && spent > kTuneBudgetS)) break;
+    tried++;
+    BatchTuning t;
+    t.threads = cnd[0];
+    t.rows_per_thread = cnd[1];
+    t.ctas_per_sm = cnd[2];
+    b->tune = t;
+    b->plan_dirty = true;
+    if ((rc = upload(b))) break;
+    auto trial = [&]() {
+      if (b->prec == kFP32) launch_hv<float>(b, t, 0, kTuneKind);
+      else launch_hv<double>(b, t, 0, kTuneKind);
+    };
+    trial();
+    cudaEventRecord(e0, b->stream);
+    for (int r = 0; r < 3; r++) trial();
+    cudaEventRecord(e1, b->stream);
+    if ((rc = cuda_ok(cudaEventSynchronize(e1), "tune sync"))) break;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= 3.0f;
+    if (ms < best.hv_ms) {
+      best = t;
+      best.hv_ms = ms;
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) {
