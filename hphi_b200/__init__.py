@@ -187,7 +187,7 @@ def inspect_green(namelist_def: str, body: int) -> np.ndarray:
     expert-mode input as the reader keeps them, read on the host (no device needed)."""
     lib = load_library()
     path = os.fsencode(namelist_def)
-    w = 4 if body == 1 else 8
+    w = 4 * (1 if body == 1 else 2 if body == 2 else body)
     cap = 1 << 16
     while True:  # one read (and one set of reader warnings) unless the rows exceed the buffer
         rows = np.zeros((cap, w), dtype=np.int32)
@@ -267,7 +267,8 @@ class Hamiltonian:
         body 2: (i, s1, j, s2, k, s3, l, s4) -> c+ c c+ c; spin models: site transitions),
         with the reference's rules per model; vec in HPhi's layout.  Complex array per row."""
         vec = _as_hphi_vector(vec, self.dim)
-        r = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).reshape(-1, 4 if body == 1 else 8))
+        r = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).reshape(-1, 4 * (1 if body == 1 else 2 if body == 2
+                                                                                     else body)))
         out = np.zeros(2 * max(len(r), 1))
         _check(load_library().hphi_expec_green(self._h, int(body), len(r),
                                                r.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
@@ -276,7 +277,8 @@ class Hamiltonian:
 
     def expec_green_device(self, vec_ptr: int, vec_type: int, rows, body: int) -> np.ndarray:
         """expec_green on a device vector in HPhi's row order (REAL64 or COMPLEX128)."""
-        r = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).reshape(-1, 4 if body == 1 else 8))
+        r = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).reshape(-1, 4 * (1 if body == 1 else 2 if body == 2
+                                                                                     else body)))
         out = np.zeros(2 * max(len(r), 1))
         _check(load_library().hphi_expec_green_device(self._h, int(body), len(r),
                                                       r.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),

@@ -115,14 +115,19 @@ int hphi_inspect_terms(const char *namelist_def, uint64_t *masks, double *coefs,
 }
 
 int hphi_inspect_green(const char *namelist_def, int body, int *rows, int cap) {
-  if (!namelist_def || (body != 1 && body != 2)) { set_error("bad argument"); return -1; }
+  if (!namelist_def || (body != 1 && body != 2 && body != 3 && body != 4 && body != 6)) {
+    set_error("bad argument");
+    return -1;
+  }
   Model m;
   std::string err;
   if (read_expert(namelist_def, &m, &err) != 0) { set_error(err); return -1; }
-  const int n = body == 1 ? (int)m.green_one.size() : (int)m.green_two.size();
-  const int w = body == 1 ? 4 : 8;
+  const std::vector<std::vector<int>> &multi = body == 3 ? m.green_three : body == 4 ? m.green_four : m.green_six;
+  const int n = body == 1 ? (int)m.green_one.size() : body == 2 ? (int)m.green_two.size() : (int)multi.size();
+  const int w = 4 * (body == 1 ? 1 : body == 2 ? 2 : body);
   for (int e = 0; rows && e < n && e < cap; e++)
-    for (int q = 0; q < w; q++) rows[w * e + q] = body == 1 ? m.green_one[e][q] : m.green_two[e][q];
+    for (int q = 0; q < w; q++)
+      rows[w * e + q] = body == 1 ? m.green_one[e][q] : body == 2 ? m.green_two[e][q] : multi[e][q];
   return n;
 }
 
@@ -728,7 +733,7 @@ static int green_host(hphi_handle *h, int body, int n, const int *rows, const do
 
 int hphi_expec_green(hphi_handle *h, int body, int n, const int *rows, const double *vec, double *out) {
   CHECK_HANDLE(h);
-  if ((body != 1 && body != 2) || n < 0 || (n > 0 && (!rows || !vec || !out))) {
+  if ((body != 1 && body != 2 && body != 3 && body != 4 && body != 6) || n < 0 || (n > 0 && (!rows || !vec || !out))) {
     set_error("hphi_expec_green: bad arguments");
     return -1;
   }
@@ -743,7 +748,8 @@ int hphi_expec_green(hphi_handle *h, int body, int n, const int *rows, const dou
 int hphi_expec_green_device(hphi_handle *h, int body, int n, const int *rows, int vec_type, const void *d_vec,
                             double *out) {
   CHECK_HANDLE(h);
-  if ((body != 1 && body != 2) || n < 0 || (vec_type != kReal64 && vec_type != kComplex128) ||
+  if ((body != 1 && body != 2 && body != 3 && body != 4 && body != 6) || n < 0 ||
+      (vec_type != kReal64 && vec_type != kComplex128) ||
       (n > 0 && (!rows || !d_vec || !out))) {
     set_error("hphi_expec_green_device: bad arguments");
     return -1;
@@ -775,7 +781,7 @@ static int expec_model_green(hphi_handle *h, int body, const double *vec, double
                  body == 1 ? &g.one : &g.two, body == 1 ? &trail : &g.trail_two) != 0)
     return -1;
   if (out) std::memcpy(out, (body == 1 ? g.one : g.two).data(), sizeof(double) * 2 * (size_t)n);
-  if (path && write_green_files(m, g, "", body == 1 ? path : "", body == 2 ? path : "") != 0) return -1;
+  if (path && write_green_file(m, g, body, path) != 0) return -1;
   return 0;
 }
 

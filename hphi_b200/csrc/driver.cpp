@@ -314,9 +314,7 @@ int model_green(Sector *s, VecType vt, const void *d_hphi, double scale, GreenVa
   std::string err;
   std::vector<GreenTerm> terms;
   std::vector<char> trail;
-  g->one.clear();
-  g->two.clear();
-  g->trail_two.clear();
+  *g = GreenValues();
   if (!m.green_one.empty()) {
     if (compile_green(m, 1, m.green_one[0].data(), (int)m.green_one.size(), &terms, &trail, &err) != 0) {
       set_error(err);
@@ -331,36 +329,65 @@ int model_green(Sector *s, VecType vt, const void *d_hphi, double scale, GreenVa
     }
     RET(green_expect(s, vt, d_hphi, terms, &g->two));
   }
+  const std::vector<std::vector<int>> *multi[3] = {&m.green_three, &m.green_four, &m.green_six};
+  const int body[3] = {3, 4, 6};
+  for (int q = 0; q < 3; q++) {
+    if (multi[q]->empty()) continue;
+    std::vector<int> flat;
+    for (const auto &r : *multi[q]) flat.insert(flat.end(), r.begin(), r.end());
+    if (compile_green(m, body[q], flat.data(), (int)multi[q]->size(), &terms, &g->multi_short[q], &err) != 0) {
+      set_error(err);
+      return -1;
+    }
+    RET(green_expect(s, vt, d_hphi, terms, &g->multi[q]));
+  }
   for (double &x : g->one) x *= scale;
   for (double &x : g->two) x *= scale;
+  for (auto &v : g->multi)
+    for (double &x : v) x *= scale;
   return 0;
 }
 
-int write_green_files(const Model &m, const GreenValues &g, const std::string &dir, const std::string &name1,
-                      const std::string &name2) {
-  if (!m.green_one.empty() && !name1.empty()) {
-    const std::string p = join(dir, name1);
-    FILE *f = fopen(p.c_str(), "w");
-    if (!f) { set_error("cannot write " + p); return -1; }
-    for (size_t e = 0; e < m.green_one.size(); e++) {
+int write_green_file(const Model &m, const GreenValues &g, int kind, const std::string &path) {
+  FILE *f = fopen(path.c_str(), "w");
+  if (!f) { set_error("cannot write " + path); return -1; }
+  if (kind == 1) {
+    for (size_t e = 0; e < m.green_one.size() && 2 * e + 1 < g.one.size(); e++) {
       const auto &r = m.green_one[e];
       fprintf(f, " %4ld %4ld %4ld %4ld %.10lf %.10lf\n", (long)r[0], (long)r[1], (long)r[2], (long)r[3],
               g.one[2 * e], g.one[2 * e + 1]);
     }
-    fclose(f);
-  }
-  if (!m.green_two.empty() && !name2.empty()) {
-    const std::string p = join(dir, name2);
-    FILE *f = fopen(p.c_str(), "w");
-    if (!f) { set_error("cannot write " + p); return -1; }
-    for (size_t e = 0; e < m.green_two.size(); e++) {
+  } else if (kind == 2) {
+    for (size_t e = 0; e < m.green_two.size() && 2 * e + 1 < g.two.size(); e++) {
       const auto &r = m.green_two[e];
       fprintf(f, " %4ld %4ld %4ld %4ld %4ld %4ld %4ld %4ld %.10lf %.10lf%s\n", (long)r[0], (long)r[1], (long)r[2],
               (long)r[3], (long)r[4], (long)r[5], (long)r[6], (long)r[7], g.two[2 * e], g.two[2 * e + 1],
               g.trail_two[e] ? " " : "");
     }
-    fclose(f);
+  } else if (m.calc_model == kSpinGC && !m.general_spin) {
+    // expec_Threebody / Fourbody / Sixbody_SpinGCHalf lines (src/expec_cisajscktaltdc.c:1064,
+    // 1256, 1402): an extra space before indices 12 and 16 of the four- and six-body rows;
+    // other models leave the file empty (:1092-1107)
+    const int q = kind == 3 ? 0 : kind == 4 ? 1 : 2;
+    const std::vector<std::vector<int>> &rows = kind == 3 ? m.green_three : kind == 4 ? m.green_four : m.green_six;
+    for (size_t e = 0; e < rows.size() && 2 * e + 1 < g.multi[q].size(); e++) {
+      const int n = g.multi_short[q][e] ? 8 : (int)rows[e].size();
+      for (int i = 0; i < n; i++) fprintf(f, "%s %4ld", (kind != 3 && !g.multi_short[q][e] && (i == 12 || (kind == 6 && i == 16))) ? " " : "", (long)rows[e][i]);
+      fprintf(f, " %.10lf %.10lf \n", g.multi[q][2 * e], g.multi[q][2 * e + 1]);
+    }
   }
+  fclose(f);
+  return 0;
+}
+
+int write_green_files(const Model &m, const GreenValues &g, const std::string &dir, const std::string &suffix) {
+  const std::string h = m.data_head;
+  if (!m.green_one.empty()) RET(write_green_file(m, g, 1, join(dir, h + "_cisajs" + suffix + ".dat")));
+  if (!m.green_two.empty() || !m.green_three.empty() || !m.green_four.empty() || !m.green_six.empty())
+    RET(write_green_file(m, g, 2, join(dir, h + "_cisajscktalt" + suffix + ".dat")));
+  if (!m.green_three.empty()) RET(write_green_file(m, g, 3, join(dir, h + "_ThreeBody" + suffix + ".dat")));
+  if (!m.green_four.empty()) RET(write_green_file(m, g, 4, join(dir, h + "_FourBody" + suffix + ".dat")));
+  if (!m.green_six.empty()) RET(write_green_file(m, g, 6, join(dir, h + "_SixBody" + suffix + ".dat")));
   return 0;
 }
 
@@ -619,7 +646,8 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
     res->cg_diff = rel_diff();
   }
   // expec_cisajs / expec_cisajscktaltdc of the eigenvector (src/CalcByLanczos.c:229-240)
-  if (!m.green_one.empty() || !m.green_two.empty()) {
+  if (!m.green_one.empty() || !m.green_two.empty() || !m.green_three.empty() || !m.green_four.empty() ||
+      !m.green_six.empty()) {
     RET(from_native(s, vt, VG.p, pp));
     RET(model_green(s, vt, pp, 1.0, &res->green));
   }
@@ -775,7 +803,7 @@ int write_lanczos_outputs(const Sector &s, const LanczosResult &r, const std::st
   fprintf(f, "Doublon  %.16lf \n", r.doublon);
   fprintf(f, "Sz  %.16lf \n", r.sz);
   fclose(f);
-  RET(write_green_files(m, r.green, outdir, m.data_head + "_cisajs.dat", m.data_head + "_cisajscktalt.dat"));
+  RET(write_green_files(m, r.green, outdir, ""));
   if (m.output_eigenvec && !r.eigenvector.empty()) {
     // zvo_eigenvec_%d_rank_%d.dat: int step, long dim, complex128[dim+1] (src/CalcByLanczos.c:262-273)
     char name[256];
@@ -877,17 +905,17 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
   };
   // Green's functions of the normalised state sv*V at step 0 and at every ExpecInterval-th
   // step from 2 on (src/CalcByTPQ.c:170-179, 261-271), files %s_cisajs_set%dstep%d.dat
-  const bool green = !m.green_one.empty() || !m.green_two.empty();
+  const bool green = !m.green_one.empty() || !m.green_two.empty() || !m.green_three.empty() ||
+                     !m.green_four.empty() || !m.green_six.empty();
   DevBuf GV;
   if (green) RET(cuda_ok(cudaMalloc(&GV.p, esz * dim), "alloc Green's function staging"));
   auto green_step = [&](int step) -> int {
     RET(from_native(s, vt, V.p, GV.p));
     GreenValues g;
     RET(model_green(s, vt, GV.p, sv * sv, &g));
-    char n1[256], n2[256];
-    snprintf(n1, sizeof(n1), "%s_cisajs_set%dstep%d.dat", m.data_head.c_str(), rand_i, step);
-    snprintf(n2, sizeof(n2), "%s_cisajscktalt_set%dstep%d.dat", m.data_head.c_str(), rand_i, step);
-    return write_green_files(m, g, outdir, n1, n2);
+    char suffix[64];
+    snprintf(suffix, sizeof(suffix), "_set%dstep%d", rand_i, step);
+    return write_green_files(m, g, outdir, suffix);
   };
   res->energy.clear();
   res->inv_temp.clear();

@@ -35,16 +35,22 @@ struct LanczosOptions {
 struct GreenValues {
   std::vector<double> one, two;
   std::vector<char> trail_two;
+  std::vector<double> multi[3];       // three-, four- and six-body rows
+  std::vector<char> multi_short[3];   // rows the reference prints with 8 indices
 };
 
 // The model's Green's functions of the vector d_hphi (device, HPhi row order), multiplied
 // by `scale`; nothing when the model requests none.
 int model_green(Sector *s, VecType vt, const void *d_hphi, double scale, GreenValues *g);
-// Writes dir/name1 (one-body) and dir/name2 (two-body) in the reference's formats; a file
-// whose request list or name is empty is not written (src/expec_cisajs.c:80,
-// src/expec_cisajscktaltdc.c:102).
-int write_green_files(const Model &m, const GreenValues &g, const std::string &dir, const std::string &name1,
-                      const std::string &name2);
+// One Green's function file (kind 1, 2, 3, 4, 6) in the reference's format at `path`.
+int write_green_file(const Model &m, const GreenValues &g, int kind, const std::string &path);
+// Every requested Green's function file in dir: <head>_cisajs<suffix>.dat,
+// <head>_cisajscktalt<suffix>.dat, <head>_ThreeBody<suffix>.dat, ... (src/global.c:43-89;
+// suffix "" for Lanczos, "_set%dstep%d" for TPQ, "_eigen%d" for LOBPCG).  A file whose rows
+// were not requested is not written (src/expec_cisajs.c:80, src/expec_cisajscktaltdc.c:102),
+// except that the two-body file exists whenever any of the two-, three-, four- or six-body
+// lists is requested (src/expec_cisajscktaltdc.c:102-180).
+int write_green_files(const Model &m, const GreenValues &g, const std::string &dir, const std::string &suffix);
 
 struct LanczosResult {
   bool converged = false;

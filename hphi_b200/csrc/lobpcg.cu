@@ -544,7 +544,8 @@ int lobpcg_run(Sector *s, VecType vt, const double *h_init, LobpcgResult *res) {
     res->var[i] = h2[0].real();
     res->doublon[i] = o[0];
     res->sz[i] = o[4];
-    if (!m.green_one.empty() || !m.green_two.empty()) {
+    if (!m.green_one.empty() || !m.green_two.empty() || !m.green_three.empty() || !m.green_four.empty() ||
+        !m.green_six.empty()) {
       // expec_cisajs / expec_cisajscktaltdc of each vector (phys, src/phys.c:100-110)
       LRET(from_native(s, vt, vec(1, i), HOST_TMP.p));
       res->green.emplace_back();
@@ -617,10 +618,9 @@ int write_lobpcg_outputs(const Sector &s, const LobpcgResult &r, const std::stri
   }
   for (size_t i = 0; i < r.green.size(); i++) {
     // FullDiag/CG file names (src/global.c:85-86) with the vector's index
-    char n1[256], n2[256];
-    snprintf(n1, sizeof(n1), "%s_cisajs_eigen%d.dat", m.data_head.c_str(), (int)i);
-    snprintf(n2, sizeof(n2), "%s_cisajscktalt_eigen%d.dat", m.data_head.c_str(), (int)i);
-    LRET(write_green_files(m, r.green[i], outdir, n1, n2));
+    char suffix[64];
+    snprintf(suffix, sizeof(suffix), "_eigen%d", (int)i);
+    LRET(write_green_files(m, r.green[i], outdir, suffix));
   }
   return 0;
 }

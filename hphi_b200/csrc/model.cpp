@@ -215,7 +215,7 @@ int compile_green(const Model &m, int body, const int *rows, int n, std::vector<
   // Hubbard-type dispatch of both functions (HubbardNConserved runs as Hubbard after sz,
   // src/sz.c:802-806); iFlgSzConserved is set by a 2Sz line (src/readdef.c:570-573)
   const bool canonical_fermion = m.calc_model == kHubbard || m.calc_model == kHubbardNConserved || kondo;
-  const int stride = body == 1 ? 4 : 8;
+  const int stride = 4 * (body == 1 ? 1 : body == 2 ? 2 : body);  // 4 integers per site pair
   auto fbit = [](int site, int s) { return 2 * site + s; };
   auto bad = [&](int site, int g) {
     return site < 0 || site >= m.nsite || g < 0 || g > (spin ? m.locspn[site] : 1);
@@ -236,6 +236,39 @@ int compile_green(const Model &m, int body, const int *rows, int n, std::vector<
         *err = "Green's function entry " + std::to_string(e) + ": site or spin index out of range";
         return -1;
       }
+    if (body >= 3) {
+      // expec_Threebody / Fourbody / Sixbody_SpinGCHalf (src/expec_cisajscktaltdc.c:901-1420):
+      // spin-1/2 SpinGC only; the last pairs act first through mltplyHalfSpinGC_mini
+      // (src/mltplySpin.c:416-500, nothing for a pair on two sites), the first two pairs go
+      // through Rearray_Interactions (:274-391) and the SpinGC element routines
+      if (m.calc_model != kSpinGC || m.general_spin) continue;
+      int a[4], g[4];
+      for (int q = 0; q < 4; q++) { a[q] = r[2 * q]; g[q] = r[2 * q + 1]; }
+      int p1, q1, q2, p3, q3, q4;  // pairs (site, to, from) after Rearray
+      double V;
+      if (a[0] == a[1] && a[2] == a[3]) {
+        V = 1.0;
+        if (a[0] > a[2]) { p1 = a[2]; q1 = g[2]; q2 = g[3]; p3 = a[0]; q3 = g[0]; q4 = g[1]; }
+        else { p1 = a[0]; q1 = g[0]; q2 = g[1]; p3 = a[2]; q3 = g[2]; q4 = g[3]; }
+      } else if (a[0] == a[3] && a[2] == a[1]) {
+        V = -1.0;
+        if (a[0] > a[2]) { p1 = a[2]; q1 = g[2]; q2 = g[1]; p3 = a[0]; q3 = g[0]; q4 = g[3]; }
+        else { p1 = a[0]; q1 = g[0]; q2 = g[3]; p3 = a[2]; q3 = g[2]; q4 = g[1]; }
+      } else {
+        (*trailing_space)[e] = 1;  // printed with its first 8 indices only
+        continue;
+      }
+      std::vector<SpinOp> ops = {{p1, q1, q2}, {p3, q3, q4}};
+      bool onsite = true;
+      for (int k = 2; k < body; k++) {  // pair k: (r[4k], r[4k+1]) created, (r[4k+2], r[4k+3]) annihilated
+        if (r[4 * k] != r[4 * k + 2]) { onsite = false; break; }
+        ops.push_back({r[4 * k], r[4 * k + 1], r[4 * k + 3]});
+      }
+      if (!onsite) continue;
+      uint64_t rm, rv, fl;
+      if (compile_spin(ops, m.site_bits, &rm, &rv, &fl)) (*terms)[e] = GreenTerm{rm, rv, fl, 0, V, 0.0};
+      continue;
+    }
     if (body == 1) {
       const int i = r[0], s1 = r[1], j = r[2], s2 = r[3];
       if (spin) {
@@ -335,7 +368,7 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
   for (const char *must : {"calcmod", "modpara", "locspin"})
     if (!files.count(must)) { *err = std::string("namelist.def: missing ") + must; return -1; }
   for (const char *unsupported : {"boost", "laser", "teonebody", "tetwobody", "singleexcitation",
-                                  "pairexcitation", "spectrumvec", "threebodyg", "fourbodyg", "sixbodyg"})
+                                  "pairexcitation", "spectrumvec"})
     if (files.count(unsupported)) {
       *err = std::string("namelist.def: keyword not supported by this engine: ") + unsupported;
       return -1;
@@ -740,6 +773,22 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
           *err = files["twobodyg"] + ": bad index"; return -1;
         }
       m->green_two.push_back({r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7]});
+    }
+  }
+  // three-, four- and six-body rows: read as written (the reference's format check of these
+  // rows is disabled, src/readdef.c:1547-1555); indices must be in range here
+  const std::pair<const char *, std::vector<std::vector<int>> *> multi[] = {
+      {"threebodyg", &m->green_three}, {"fourbodyg", &m->green_four}, {"sixbodyg", &m->green_six}};
+  const int multi_pairs[] = {3, 4, 6};
+  for (int q = 0; q < 3; q++) {
+    if (!files.count(multi[q].first)) continue;
+    std::vector<std::vector<int>> g;
+    const std::string fn = files[multi[q].first];
+    if (!read_int_table(*m, fn, 4 * multi_pairs[q], &g, err)) return -1;
+    for (const auto &r : g) {
+      for (int k = 0; k < 2 * multi_pairs[q]; k++)
+        if (!check_site(r[2 * k]) || !sigma_ok(r[2 * k], r[2 * k + 1])) { *err = fn + ": bad index"; return -1; }
+      multi[q].second->push_back(r);
     }
   }
   canonicalize_terms(m);

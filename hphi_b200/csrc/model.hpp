@@ -73,6 +73,10 @@ struct Model {
   // model drops one-body rows with i != j, as the reference does with a warning.
   std::vector<std::array<int, 4>> green_one;
   std::vector<std::array<int, 8>> green_two;
+  // ThreeBodyG / FourBodyG / SixBodyG rows (3, 4, 6 site pairs of 4 integers each,
+  // src/readdef.c:1525-1700);
+  // the reference evaluates them for spin-1/2 SpinGC only.
+  std::vector<std::vector<int>> green_three, green_four, green_six;
   // Raw term counts as read (for logs).
   int n_trans = 0, n_coulomb_intra = 0, n_coulomb_inter = 0, n_hund = 0, n_exchange = 0;
   int n_ising = 0, n_pairhop = 0, n_pairlift = 0, n_interall = 0;
@@ -114,10 +118,12 @@ struct GreenTerm {
 };
 
 // Compiles Green's function rows (body 1: OneBodyG rows i s1 j s2; body 2: TwoBodyG rows
-// i s1 j s2 k s3 l s4; 0-based sites) following expec_cisajs (src/expec_cisajs.c:66-641) and
-// expec_cisajscktaltdc (src/expec_cisajscktaltdc.c:87-1647).  trailing_space[e] != 0 where
-// the reference prints the entry's line with a space before the newline.  Returns 0, or -1
-// with a message for an index out of range.
+// i s1 j s2 k s3 l s4; body 3 / 4 / 6: ThreeBodyG / FourBodyG / SixBodyG rows of 3 / 4 / 6
+// site pairs; 0-based sites) following expec_cisajs (src/expec_cisajs.c:66-641) and
+// expec_cisajscktaltdc (src/expec_cisajscktaltdc.c:87-1647).  flag[e] (bodies 1, 2):
+// the reference prints the entry's line with a space before the newline; (bodies 3, 4, 6):
+// the reference prints only the first 8 indices (its Rearray_Interactions rejected the row).
+// Returns 0, or -1 with a message for an index out of range.
 int compile_green(const Model &m, int body, const int *rows, int n, std::vector<GreenTerm> *terms,
                   std::vector<char> *trailing_space, std::string *err);
 

@@ -74,6 +74,10 @@ class ExpertModel:
     # (i, s1, j, s2, k, s3, l, s4) (src/readdef.c:1441-1523)
     greenone: List[Tuple] = field(default_factory=list)
     greentwo: List[Tuple] = field(default_factory=list)
+    # ThreeBodyG / FourBodyG / SixBodyG rows: 3, 4, 6 site pairs (i, s, j, t) flattened
+    greenthree: List[Tuple] = field(default_factory=list)
+    greenfour: List[Tuple] = field(default_factory=list)
+    greensix: List[Tuple] = field(default_factory=list)
 
     # ------------------------------------------------------------------ writers
     def write(self, directory: str) -> str:
@@ -98,6 +102,9 @@ class ExpertModel:
             ("OneBodyG", "greenone.def", "NCisAjs", self.greenone, "{:d} {:d} {:d} {:d}"),
             ("TwoBodyG", "greentwo.def", "NCisAjsCktAltDC", self.greentwo,
              "{:d} {:d} {:d} {:d} {:d} {:d} {:d} {:d}"),
+            ("ThreeBodyG", "greenthree.def", "NThreeBody", self.greenthree, " ".join(["{:d}"] * 12)),
+            ("FourBodyG", "greenfour.def", "NFourBody", self.greenfour, " ".join(["{:d}"] * 16)),
+            ("SixBodyG", "greensix.def", "NSixBody", self.greensix, " ".join(["{:d}"] * 24)),
         ]
         for kw, fname, head, rows, fmt in tables:
             if not rows:

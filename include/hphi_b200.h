@@ -312,8 +312,10 @@ int hphi_reference_start(int64_t dim, int kind, int initial_iv, int sample, int 
  * Green's functions <v| O |v> of the rows `rows` on the host vector vec (HPhi's layout,
  * complex128[dim+1], element 0 unused): body 1 rows are OneBodyG rows (i, s1, j, s2),
  * O = c+_{i s1} c_{j s2}; body 2 rows are TwoBodyG rows (i, s1, j, s2, k, s3, l, s4),
- * O = c+_{i s1} c_{j s2} c+_{k s3} c_{l s4} (spin models: |s><s'| on a site), with the
- * reference's rules for each model.  out receives (re, im) per row.
+ * O = c+_{i s1} c_{j s2} c+_{k s3} c_{l s4} (spin models: |s><s'| on a site); body 3, 4, 6
+ * rows are ThreeBodyG / FourBodyG / SixBodyG rows of 3, 4, 6 such pairs (4 integers each,
+ * spin-1/2 SpinGC only, zero otherwise), with the reference's rules for each model.  out
+ * receives (re, im) per row.
  * Replaces the entry loops of expec_cisajs (src/expec_cisajs.c:66-641) and
  * expec_cisajscktaltdc (src/expec_cisajscktaltdc.c:87-1647), one batch of rows per pass.
  */
@@ -334,7 +336,8 @@ int hphi_expec_cisajscktaltdc(hphi_handle *h, const double *vec, double *out, co
 
 /*
  * Reads an expert-mode input on the host only and copies its OneBodyG (body 1, 4 ints per
- * row) or TwoBodyG (body 2, 8 ints per row) rows as the reader keeps them (a canonical Spin
+ * row), TwoBodyG (body 2, 8 ints per row) or ThreeBodyG / FourBodyG / SixBodyG (body 3, 4,
+ * 6: 12, 16, 24 ints per row) rows as the reader keeps them (a canonical Spin
  * model drops one-body rows with i != j, src/readdef.c:1455-1460).  Returns the row count
  * (at most cap rows are written; rows may be NULL), or -1 with a message for an input the
  * reference rejects (spin two-body rows need i == j and k == l, src/readdef.c:1497-1503).

@@ -59,6 +59,7 @@ class Def:
     sz_conserved: bool = False        # iFlgSzConserved: a 2Sz line (src/readdef.c:570-573)
     green_one: List[Tuple[int, int, int, int]] = field(default_factory=list)      # OneBodyG rows
     green_two: List[Tuple[int, int, int, int, int, int, int, int]] = field(default_factory=list)  # TwoBodyG rows
+    green_multi: Dict[int, List[Tuple[int, ...]]] = field(default_factory=dict)  # 3/4/6: ThreeBodyG ... rows
 
 
 def _table(path: str) -> List[List[float]]:
@@ -189,6 +190,9 @@ def read_expert(namelist: str) -> Def:
             if _is_spin(d) and (r[0] != r[2] or r[4] != r[6]):   # CheckFormatForSpinInt (:1497-1503)
                 raise ValueError("spin two-body Green's function rows need i == j and k == l")
             d.green_two.append(tuple(r[:8]))
+    for key, npairs in (("threebodyg", 3), ("fourbodyg", 4), ("sixbodyg", 6)):   # :1525-1700
+        if key in files:
+            d.green_multi[npairs] = [tuple(r[:4 * npairs]) for r in _int_table(files[key])]
     return d
 
 
@@ -960,4 +964,42 @@ def read_green_file(path: str) -> Tuple[np.ndarray, np.ndarray]:
         rows.append([int(t) for t in p[:-2]])
         vals.append(complex(float(p[-2]), float(p[-1])))
     return np.array(rows, dtype=np.int64), np.array(vals, dtype=np.complex128)
+
+
+def expec_multibody(d: Def, vec: np.ndarray, npairs: int):
+    """expec_Threebody / Fourbody / Sixbody_SpinGCHalf (src/expec_cisajscktaltdc.c:901-1420)
+    for the ThreeBodyG / FourBodyG / SixBodyG rows: the pairs after the second act first,
+    last pair first, through mltplyHalfSpinGC_mini (src/mltplySpin.c:416-500: |s><t| on one
+    site, nothing for a pair on two sites); then Rearray_Interactions on the first two pairs
+    (None: the reference prints 8 indices and zero) and <vec| O_12 O_34 |vec_pr>.  Returns
+    (values, short) or None when the model is not spin-1/2 SpinGC (the file stays empty)."""
+    if d.calc_model != SPINGC or _general(d):
+        return None
+    vec = vec.astype(np.complex128)
+    n = vec.size - 1
+    c = np.arange(n, dtype=np.uint64)
+
+    def apply(site, to, frm, x):
+        y = np.zeros_like(x)
+        ok = ((c >> np.uint64(site)) & np.uint64(1)) == np.uint64(frm)
+        tgt = (c ^ np.uint64(1 << site)) if to != frm else c
+        y[(tgt[ok] + np.uint64(1)).astype(np.int64)] += x[1:][ok]
+        return y
+
+    vals, short = [], []
+    for row in d.green_multi.get(npairs, []):
+        pairs = [row[4 * k:4 * k + 4] for k in range(npairs)]
+        vp = vec.copy()
+        for (i, s_, j, t) in reversed(pairs[2:]):
+            vp = apply(i, s_, t, vp) if i == j else np.zeros_like(vp)
+        rr = _rearray(tuple(row[:8]))
+        if rr is None:
+            vals.append(0j)
+            short.append(True)
+            continue
+        i1, s1, _, s2, k1, s3, _, s4, V = rr
+        w = apply(i1, s1, s2, apply(k1, s3, s4, vp))
+        vals.append(complex(V * np.vdot(vec[1:], w[1:])))
+        short.append(False)
+    return np.array(vals, dtype=np.complex128), np.array(short, dtype=bool)
 

@@ -54,7 +54,7 @@ def load_golden(name):
 def green_reference(z, fname):
     """(rows, values, text lines) of a reference Green's function file stored in a fixture."""
     lines = str(z["text_" + fname]).splitlines()
-    rows = np.array([[int(t) for t in l.split()[:-2]] for l in lines], dtype=np.int64)
+    rows = [[int(t) for t in l.split()[:-2]] for l in lines]  # short multi-body lines have 8 indices
     vals = np.array([complex(float(l.split()[-2]), float(l.split()[-1])) for l in lines])
     return rows, vals, lines
 
@@ -71,3 +71,32 @@ def tpq_state(O, d, lists, start, step):
         v /= np.linalg.norm(v[1:])
     return v
 
+
+
+def oracle_green_file(O, d, lists, v, fname):
+    """(rows, values) the reference writes into Green's function file `fname` for the
+    vector v, from the oracle: rows as printed (8 indices for rows Rearray_Interactions
+    rejects), empty arrays for a file the reference leaves empty."""
+    empty = (np.zeros((0,), dtype=np.int64), np.zeros(0, dtype=np.complex128))
+    for key, npairs in (("ThreeBody", 3), ("FourBody", 4), ("SixBody", 6)):
+        if key in fname:
+            res = O.expec_multibody(d, v, npairs)
+            if res is None:
+                return empty
+            vals, short = res
+            rows = [list(r[:8]) if sh else list(r) for r, sh in zip(d.green_multi[npairs], short)]
+            return rows, vals
+    if "cktalt" in fname:
+        if not d.green_two:
+            return empty
+        return [list(r) for r in d.green_two], O.expec_cisajscktalt(d, lists, v)
+    return [list(r) for r in d.green_one], O.expec_cisajs(d, lists, v)
+
+
+def check_green_lines(lines, rows, vals, atol):
+    """Parsed lines of a Green's function file against (rows, values)."""
+    assert len(lines) == len(rows), (len(lines), len(rows))
+    for line, r, v in zip(lines, rows, vals):
+        p = line.split()
+        assert [int(t) for t in p[:-2]] == list(r), (line, r)
+        assert abs(complex(float(p[-2]), float(p[-1])) - v) <= atol, (line, v)

@@ -361,7 +361,43 @@ def _green_cases():
     m.output_eigenvec = 1
     m.greenone, m.greentwo = _green_rows(10, 2, 10, -1, 30, True)
     c["green_lobpcg_chain10"] = m
+    # three-, four- and six-body rows (spin-1/2 SpinGC with a transverse field, complex vectors)
+    m = expert.heisenberg(8, expert.chain_bonds(8), lanczos_max=300)
+    m.model, m.two_sz, m.initial_vec_type = "SpinGC", None, 0
+    m.trans = [(i, 0, i, 1, 0.3, 0.0) for i in range(8)] + [(i, 1, i, 0, 0.3, 0.0) for i in range(8)]
+    m.calc_eigenvec, m.output_eigenvec = 0, 1
+    m.greenthree, m.greenfour, m.greensix = (_multi_rows(8, 11 + k, n, 30) for k, n in enumerate((3, 4, 6)))
+    c["green_multi_spingc8"] = m
+    # a Hubbard input with ThreeBodyG only: the reference leaves the two- and three-body files empty
+    m = expert.hubbard(6, expert.square_bonds(2, 3), 1.0, 4.0, 3, 3, lanczos_max=300)
+    m.calc_eigenvec, m.output_eigenvec = 0, 1
+    m.greenthree = _multi_rows(6, 12, 3, 5)
+    c["green_multi_hub6"] = m
     return c
+
+
+def _multi_rows(nsite: int, seed: int, npairs: int, n: int):
+    """Rows of npairs site pairs (i, s, j, t): the first two pairs on-site, in Rearray's
+    exchanged form (i, j)(j, i), or neither; the later pairs on-site except in some rows."""
+    rng = np.random.RandomState(seed)
+    rows = []
+    for r in range(n):
+        g = [int(x) for x in rng.randint(2, size=2 * npairs)]
+        i, j = (int(x) for x in rng.choice(nsite, 2, replace=False))
+        k = int(rng.randint(nsite))
+        if r % 5 == 0:
+            first = [i, g[0], j, g[1], j, g[2], i, g[3]]
+        elif r % 5 == 1:
+            first = [i, g[0], j, g[1], k, g[2], int((k + 1) % nsite), g[3]]
+        else:
+            first = [i, g[0], i, g[1], k, g[2], k, g[3]]
+        rest = []
+        for q in range(2, npairs):
+            a = int(rng.randint(nsite))
+            b = int((a + 1) % nsite) if (r % 5 == 4 and q == npairs - 1) else a
+            rest += [a, g[2 * q], b, g[2 * q + 1]]
+        rows.append(tuple(first + rest))
+    return rows
 
 
 def _read_eigvec(path: str) -> np.ndarray:
@@ -386,7 +422,7 @@ def make_green_case(name: str, m) -> None:
         od = os.path.join(tmp, "output")
         v1, _, _, _ = run_ref.read_hv(tmp)
         data["start"] = v1
-        files = sorted(f for f in os.listdir(od) if "cisajs" in f)
+        files = sorted(f for f in os.listdir(od) if "cisajs" in f or "Body" in f)
         data["green_files"] = np.array(files)
         for f in files:
             text = open(os.path.join(od, f)).read()

@@ -52,14 +52,28 @@ def test_green_kernels_match_oracle_and_reference(name, tmp_path):
         for f in (str(x) for x in z["green_files"]):
             rows, vals, lines = green_reference(z, f)
             v = _vector(d, lists, z, f)
-            two = "cktalt" in f
-            got = H.expec_green(v, rows, 2 if two else 1)
-            want = O.expec_cisajscktalt(d, lists, v) if two else O.expec_cisajs(d, lists, v)
+            multi = {"ThreeBody": 3, "FourBody": 4, "SixBody": 6}
+            body = next((n for k, n in multi.items() if k in f), 2 if "cktalt" in f else 1)
+            if body >= 3:
+                full = d.green_multi[body]
+                res = O.expec_multibody(d, v, body)
+                got = H.expec_green(v, full, body)
+                if res is None:
+                    np.testing.assert_array_equal(got, 0)   # the reference leaves the file empty
+                    assert lines == []
+                    continue
+                np.testing.assert_allclose(got, res[0], rtol=0, atol=1e-12, err_msg=f)
+                np.testing.assert_allclose(got, vals, rtol=0, atol=1e-10, err_msg=f)
+                continue
+            if not lines:
+                continue
+            got = H.expec_green(v, rows, body)
+            want = O.expec_cisajscktalt(d, lists, v) if body == 2 else O.expec_cisajs(d, lists, v)
             np.testing.assert_allclose(got, want, rtol=0, atol=1e-12, err_msg=f)
             np.testing.assert_allclose(got, vals, rtol=0, atol=1e-10, err_msg=f)
             # the input's rows through the reference-named entry points, and the file they write
             path = str(tmp_path / f)
-            g2 = H.expec_cisajscktaltdc(v, path) if two else H.expec_cisajs(v, path)
+            g2 = H.expec_cisajscktaltdc(v, path) if body == 2 else H.expec_cisajs(v, path)
             np.testing.assert_array_equal(g2, got)
             _same_layout(open(path).read().splitlines(), lines, 1e-10)
 
@@ -77,20 +91,21 @@ def _run_case(name, tmp_path, monkeypatch, run):
 
 @pytest.mark.parametrize("name", [n for n in golden_cases("green") if "tpq" not in n and "lobpcg" not in n])
 def test_lanczos_writes_green_files(name, tmp_path, monkeypatch):
-    """calc_by_lanczos with OneBodyG / TwoBodyG: zvo_cisajs.dat and zvo_cisajscktalt.dat of
-    its own eigenvector (oracle on the eigenvector file it wrote, 1e-10) and the reference's
-    values for the same input and start vector."""
+    """calc_by_lanczos with Green's function requests: every file of the reference (same
+    names, rows, line layout), equal to the oracle on the eigenvector file the engine wrote
+    (1e-10) and to the reference's values for the same input and start vector."""
+    from conftest import check_green_lines, oracle_green_file
     z = load_golden(name)
     d, lists = _oracle(name)
     out = _run_case(name, tmp_path, monkeypatch, lambda H, o: H.calc_by_lanczos(output_dir=o))
     v = _read_eigvec(out / "zvo_eigenvec_0_rank_0.dat")
-    for f in (str(x) for x in z["green_files"]):
-        _, vals, lines = green_reference(z, f)
+    written = sorted(f for f in os.listdir(out) if "cisajs" in f or "Body" in f)
+    assert written == sorted(str(x) for x in z["green_files"])
+    for f in written:
+        _, _, lines = green_reference(z, f)
         mine = open(out / f).read().splitlines()
-        rows, got = O.read_green_file(str(out / f))
-        two = "cktalt" in f
-        want = O.expec_cisajscktalt(d, lists, v) if two else O.expec_cisajs(d, lists, v)
-        np.testing.assert_allclose(got, want, rtol=0, atol=1e-10, err_msg=f)
+        rows, want = oracle_green_file(O, d, lists, v, f)
+        check_green_lines(mine, rows, want, 1e-10)
         _same_layout(mine, lines, 1e-6)
 
 

@@ -160,16 +160,14 @@ def _green_vector(O, d, lists, z, fname):
 
 @pytest.mark.parametrize("name", golden_cases("green"))
 def test_oracle_green_functions_match_reference(name):
-    """expec_cisajs / expec_cisajscktaltdc restated: every value the reference printed
-    (%.10lf) for the eigenvector(s) it wrote, or for its TPQ states, and the same rows."""
-    from conftest import green_reference
+    """expec_cisajs / expec_cisajscktaltdc (and the three-, four-, six-body functions)
+    restated: every value the reference printed (%.10lf) for the eigenvector(s) it wrote, or
+    for its TPQ states, with the same rows (and the same empty files)."""
+    from conftest import check_green_lines, oracle_green_file
     z = load_golden(name)
     d = O.read_expert(case_dir(name) + "/namelist.def")
     lists = None if O._rows_are_configs(d) else O.sz(d)
     for f in (str(x) for x in z["green_files"]):
-        rows, vals, _ = green_reference(z, f)
-        v = _green_vector(O, d, lists, z, f)
-        two = "cktalt" in f
-        got = O.expec_cisajscktalt(d, lists, v) if two else O.expec_cisajs(d, lists, v)
-        np.testing.assert_array_equal(rows, np.array(d.green_two if two else d.green_one))
-        np.testing.assert_allclose(got, vals, rtol=0, atol=1e-10, err_msg=f)
+        lines = str(z["text_" + f]).splitlines()
+        rows, vals = oracle_green_file(O, d, lists, _green_vector(O, d, lists, z, f), f)
+        check_green_lines(lines, rows, vals, 1e-10)
