@@ -690,10 +690,11 @@ int hphi_run(hphi_handle *h, const char *output_dir) {
   const std::string out = output_dir ? output_dir : "output";
   switch (h->sector->model.calc_type) {
     case kLanczos: return hphi_lanczos(h, nullptr, out.c_str(), nullptr, 0);
-    case kTPQ: return hphi_tpq(h, nullptr, out.c_str(), nullptr, 0);
+    case kTPQ:
+    case kcTPQ: return hphi_tpq(h, nullptr, out.c_str(), nullptr, 0);
     case kCG: return hphi_lobpcg(h, nullptr, out.c_str(), nullptr, 0);
     default:
-      set_error("CalcType not supported by this engine (Lanczos = 0, TPQ = 1 and LOBPCG = 3 are)");
+      set_error("CalcType not supported by this engine (Lanczos = 0, TPQ = 1, LOBPCG = 3 and cTPQ = 5 are)");
       return -1;
   }
 }

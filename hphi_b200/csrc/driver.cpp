@@ -919,12 +919,62 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
   };
   res->energy.clear();
   res->inv_temp.clear();
+  // canonical TPQ (CalcType 5, CalcByCanonicalTPQ src/CalcByCanonicalTPQ.c:52-287): the step
+  // is v <- exp(-dtau H / 2) v / |.|, dtau = 1/LargeValue, by a Taylor sum of ExpandCoef terms
+  // (MultiplyForCanonicalTPQ src/Multiply.c:162-203), and the inverse temperature grows by dtau
+  const bool canonical = m.calc_type == kcTPQ;
+  const int expand = m.expand_coef > 0 ? m.expand_coef : 10;
+  const double dtau = 1.0 / L;
+  DevBuf CA, CT, CU;
+  if (canonical) {
+    RET(cuda_ok(cudaMalloc(&CA.p, esz * dim), "alloc cTPQ sum"));
+    RET(cuda_ok(cudaMalloc(&CT.p, esz * dim), "alloc cTPQ term"));
+    RET(cuda_ok(cudaMalloc(&CU.p, esz * dim), "alloc cTPQ term"));
+  }
+  auto ctpq_multiply = [&](double *gnorm_out) -> int {
+    // x = sv V and h = H x (expec left H x in H): sum = x + a h + sum_c a^c/c! H^c x;
+    // scalar slots [26, 31) (expec and the observables use [0, 22))
+    const double a = -0.5 * dtau;
+    RET(cuda_ok(cudaMemcpyAsync(CA.p, V.p, esz * dim, cudaMemcpyDeviceToDevice, s->stream), "copy"));
+    RET(vec_scale(s, vt, sv, CA.p));
+    RET(vec_axpby(s, vt, a, H.p, 1.0, CA.p));
+    RET(cuda_ok(cudaMemcpyAsync(CT.p, H.p, esz * dim, cudaMemcpyDeviceToDevice, s->stream), "copy"));
+    double coeff = a;
+    const double c01[2] = {0.0, 1.0};
+    RET(cuda_ok(cudaMemcpyAsync(st + 26, c01, sizeof(c01), cudaMemcpyHostToDevice, s->stream), "coef"));
+    for (int c = 2; c <= expand; c++) {
+      coeff *= a / (double)c;
+      RET(hv_native(s, vt, CT.p, CU.p, st + 26, st + 28, false));
+      RET(vec_axpby(s, vt, coeff, CU.p, 1.0, CA.p));
+      std::swap(CT.p, CU.p);
+    }
+    RET(vec_norm2(s, vt, CA.p, st + 30));
+    double n2 = 0.0;
+    RET(cuda_ok(cudaMemcpyAsync(&n2, st + 30, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "read"));
+    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+    *gnorm_out = std::sqrt(n2);
+    std::swap(V.p, CA.p);
+    sv = 1.0 / *gnorm_out;
+    return 0;
+  };
+  if (canonical && m.expand_coef <= 0) printf("In cTPQ calc., the default value of ExpandCoef (=10) is used. \n");
   double gnorm = 0.0, inv_temp = 0.0;
   int step = 2;
   if (resumed) {
-    // expec_energy_flct on the stored state, then the loop from its step (src/CalcByTPQ.c:107-113)
+    // expec_energy_flct on the stored state, then the loop from its step (src/CalcByTPQ.c:107-113);
+    // a continued cTPQ run resumes its inverse temperature at (step - 1) dtau (the reference
+    // leaves it unset on this path)
     RET(expec());
     step = opt.resume_step;
+    if (canonical) inv_temp = (step - 1) * dtau;
+  } else if (canonical) {
+    // step 0: the normalised start vector, its Green's functions, expec (with the Flct line)
+    RET(expec());
+    if (green) RET(green_step(0));
+    write_lines(0.0, first_norm, 0, true);
+    res->energy.push_back(E);
+    res->inv_temp.push_back(0.0);
+    step = 1;
   } else {
     // FirstMultiply: expec on the start vector, then v = (L - H/Ns) v normalised.
     RET(expec());
@@ -940,9 +990,15 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
     res->inv_temp.push_back(inv_temp);
   }
   for (; step < m.lanczos_max; step++) {
-    RET(multiply(&gnorm));
-    RET(expec());
-    inv_temp = (2.0 * step / Ns) / (L - E / Ns);
+    if (canonical) {
+      RET(ctpq_multiply(&gnorm));
+      RET(expec());
+      inv_temp += dtau;
+    } else {
+      RET(multiply(&gnorm));
+      RET(expec());
+      inv_temp = (2.0 * step / Ns) / (L - E / Ns);
+    }
     write_lines(inv_temp, gnorm, step, true);
     res->energy.push_back(E);
     res->inv_temp.push_back(inv_temp);

@@ -445,7 +445,8 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       else if (k == "expecinterval") m->expec_interval = (int)v;
       else if (k == "calchs") m->read_hacker = (int)v;
       else if (k == "precg") m->pre_cg = (int)v;
-      else if (k == "timeslice" || k == "expandcoef" || k == "outputinterval" || k == "tinit" ||
+      else if (k == "expandcoef") m->expand_coef = (int)v;
+      else if (k == "timeslice" || k == "outputinterval" || k == "tinit" ||
                k == "omegamax" || k == "omegamin" || k == "omegaim" || k == "omegaorg" || k == "nomega" ||
                k == "targettpqrand") {
         // accepted and ignored: parameters of modes outside this engine

@@ -52,6 +52,7 @@ struct Model {
   int lanczos_max = 0, initial_iv = 0, nvec = 0, k_exct = 0, lanczos_eps = 0, lanczos_target = 0;
   int num_ave = 1, expec_interval = 1, read_hacker = 1;
   int pre_cg = 0;               // PreCG: point-Jacobi preconditioning in LOBPCG (src/readdef.c:646)
+  int expand_coef = 0;          // ExpandCoef: Taylor order of the cTPQ step (0: 10, src/CalcByCanonicalTPQ.c:81-86)
   double large_value = 0.0;
   std::string data_head = "zvo", para_head = "zqp";
   // locspn.def

@@ -45,6 +45,7 @@ class Def:
     large_value: float = 0.0
     num_ave: int = 1
     pre_cg: int = 0
+    expand_coef: int = 0              # ExpandCoef of cTPQ (0: 10)
     locspn: List[int] = field(default_factory=list)   # 0 itinerant, 1 local spin (Kondo)
     trans: List[Tuple[int, int, int, int, complex]] = field(default_factory=list)   # off-diagonal, Hermitian pairs
     chemi: List[Tuple[int, int, float]] = field(default_factory=list)                # (site, spin, mu): -mu n
@@ -114,6 +115,7 @@ def read_expert(namelist: str) -> Def:
         elif k == "initial_iv": d.initial_iv = int(v)
         elif k == "exct": d.k_exct = int(v)
         elif k == "precg": d.pre_cg = int(v)
+        elif k == "expandcoef": d.expand_coef = int(v)
         elif k == "lanczoseps": d.lanczos_eps = int(v)
         elif k == "lanczostarget": d.lanczos_target = int(v)
         elif k == "largevalue": d.large_value = v

@@ -61,12 +61,22 @@ def green_reference(z, fname):
 
 def tpq_state(O, d, lists, start, step):
     """The normalised TPQ state of `step` from the normalised start vector (oracle H*v):
-    v <- (L v - H v / Ns) / |.| (src/Multiply.c:42-68)."""
+    microcanonical v <- (L v - H v / Ns) / |.| (src/Multiply.c:42-68); canonical (CalcType 5)
+    v <- sum_{c <= ExpandCoef} (-dtau H / 2)^c / c! v / |.|, dtau = 1 / L (src/Multiply.c:162-203)."""
     v = start.astype(np.complex128).copy()
     diag = O.diagonalcalc(d, lists)
+    H = lambda x: O.mltply(d, lists, diag, np.zeros_like(x), x)[0]
     for _ in range(step):
-        hv, _ = O.mltply(d, lists, diag, np.zeros_like(v), v)
-        v = d.large_value * v - hv / d.nsite
+        if d.calc_type == 5:
+            a = -0.5 / d.large_value
+            acc, term, coef = v.copy(), v.copy(), 1.0
+            for c in range(1, (d.expand_coef or 10) + 1):
+                term = H(term)
+                coef *= a / c
+                acc = acc + coef * term
+            v = acc
+        else:
+            v = d.large_value * v - H(v) / d.nsite
         v[0] = 0
         v /= np.linalg.norm(v[1:])
     return v

@@ -361,6 +361,12 @@ def _green_cases():
     m.output_eigenvec = 1
     m.greenone, m.greentwo = _green_rows(10, 2, 10, -1, 30, True)
     c["green_lobpcg_chain10"] = m
+    # canonical TPQ (CalcType 5): exp(-dtau H / 2) steps, Green's functions every 4 steps
+    m = expert.hubbard(6, expert.chain_bonds(6), 1.0, 4.0, 3, 3, calc_type="cTPQ", lanczos_max=12, num_ave=1,
+                       large_value=6.0, expec_interval=4)
+    m.initial_vec_type = 0
+    m.greenone, m.greentwo = _green_rows(6, 2, 13, 30, 10, False)
+    c["green_ctpq_hub6"] = m
     # three-, four- and six-body rows (spin-1/2 SpinGC with a transverse field, complex vectors)
     m = expert.heisenberg(8, expert.chain_bonds(8), lanczos_max=300)
     m.model, m.two_sz, m.initial_vec_type = "SpinGC", None, 0
@@ -430,8 +436,10 @@ def make_green_case(name: str, m) -> None:
         for f in sorted(os.listdir(od)):
             if f.startswith("zvo_eigenvec_"):
                 data["vec_" + f] = _read_eigvec(os.path.join(od, f))
-        if m.calc_type == "TPQ":
+        if m.calc_type in ("TPQ", "cTPQ"):
             data["tpq"] = run_ref.tpq_table(tmp, 0)
+            for base in ("SS_rand0", "Norm_rand0", "Flct_rand0"):
+                data["text_" + base] = np.array(open(os.path.join(od, base + ".dat")).read())
         else:
             data["states"] = run_ref.energy_states(tmp)
     np.savez_compressed(os.path.join(out, "golden.npz"), **data)

@@ -194,3 +194,24 @@ def test_lobpcg_input_eigenvectors(tmp_path, monkeypatch):
     for f in (str(x) for x in z["green_files"]):
         _, _, lines = green_reference(z, f)
         _same_layout(open(out / f).read().splitlines(), lines, 1e-10)
+
+
+def test_canonical_tpq_files_match_reference(tmp_path, monkeypatch):
+    """calc_by_tpq with CalcType 5 (cTPQ): SS_rand0.dat, Norm_rand0.dat and Flct_rand0.dat (a
+    Flct line at step 0, the inverse temperature growing by 1/LargeValue) and the Green's
+    function files of steps 0, 4 and 8, against the reference's run from the same start."""
+    name = "green_ctpq_hub6"
+    z = load_golden(name)
+    out = _run_case(name, tmp_path, monkeypatch, lambda H, o: H.calc_by_tpq(output_dir=o))
+    for base in ("SS_rand0", "Norm_rand0", "Flct_rand0"):
+        mine = [l for l in open(out / f"{base}.dat").read().splitlines()]
+        ref = str(z["text_" + base]).splitlines()
+        assert len(mine) == len(ref) and mine[0] == ref[0]
+        a = np.array([[float(x) for x in l.split()] for l in mine[1:]])
+        b = np.array([[float(x) for x in l.split()] for l in ref[1:]])
+        np.testing.assert_allclose(a, b, rtol=1e-10, atol=1e-10, err_msg=base)
+    written = sorted(f for f in os.listdir(out) if "cisajs" in f)
+    assert written == sorted(str(x) for x in z["green_files"])
+    for f in written:
+        _, _, lines = green_reference(z, f)
+        _same_layout(open(out / f).read().splitlines(), lines, 1e-9)
