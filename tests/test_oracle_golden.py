@@ -171,3 +171,42 @@ def test_oracle_green_functions_match_reference(name):
         lines = str(z["text_" + f]).splitlines()
         rows, vals = oracle_green_file(O, d, lists, _green_vector(O, d, lists, z, f), f)
         check_green_lines(lines, rows, vals, 1e-10)
+
+
+def _known_answers():
+    import json
+    import os
+    from conftest import GOLDEN
+    base = os.path.join(GOLDEN, "known_answers")
+    exp = json.load(open(os.path.join(base, "expected.json")))
+    return base, exp
+
+
+@pytest.mark.parametrize("name", sorted(_known_answers()[1]))
+def test_oracle_reproduces_reference_test_values(name):
+    """The reference's own known-answer tests (test/*.sh, standard-mode inputs) in expert
+    mode: the oracle's lowest eigenvalues of the same Hamiltonian equal the values those
+    tests check (1e-10), and so does the ground state's doublon."""
+    import os
+    base, exp = _known_answers()
+    from scipy.sparse.linalg import LinearOperator, eigsh
+    d = O.read_expert(os.path.join(base, name, "namelist.def"))
+    lists = None if O._rows_are_configs(d) else O.sz(d)
+    diag = O.diagonalcalc(d, lists)
+    dim = diag.size - 1
+
+    def hv(x):
+        v1 = np.zeros(dim + 1, dtype=np.complex128)
+        v1[1:] = np.ravel(x)
+        return O.mltply(d, lists, diag, np.zeros_like(v1), v1)[0][1:]
+
+    want = np.array(exp[name])
+    op = LinearOperator((dim, dim), matvec=hv, dtype=np.complex128)
+    w, V = eigsh(op, k=len(want) + 1, which="SA", tol=1e-14, v0=np.ones(dim, dtype=np.complex128))
+    order = np.argsort(w)
+    w, V = w[order], V[:, order]
+    np.testing.assert_allclose(w[:len(want)], want[:, 0], rtol=0, atol=1e-10)
+    v = np.zeros(dim + 1, dtype=np.complex128)
+    v[1:] = V[:, 0]
+    _, _, doublon, _ = O.expec_energy(d, lists, diag, v)
+    assert abs(doublon - want[0, 1]) < 1e-10
