@@ -48,7 +48,7 @@ def ritz_table(alpha, beta, steps):
 
 def check_lanczos_against_reference(g, E1, alpha, beta, nsteps_checked=30):
     """Lanczos without reorthogonalisation amplifies rounding differences once Ritz values
-    converge (ghost copies appear at different steps), so parity is judged on the
+    converge (ghost copies appear at different steps), so parity is checked on the
     ground-state energy at convergence (1e-10) and on the Ritz values E[1..4] of the
     early steps, printed by the reference with 10 decimals."""
     ref_last = g["step_vals"][-1]
