@@ -184,3 +184,11 @@ def test_green_reader_warnings_and_rejections(tmp_path, capfd):
     open(d / "greenone.def", "w").write("\n".join(lines) + "\n")
     with pytest.raises(hphi_b200.HPhiError, match="bad index"):
         hphi_b200.inspect_green(str(d / "namelist.def"), 1)
+
+
+def test_green_inspect_rejects_unknown_body():
+    nl = os.path.join(case_dir("green_multi_spingc8"), "namelist.def")
+    for body in (0, 5, 7):
+        with pytest.raises(hphi_b200.HPhiError):
+            hphi_b200.inspect_green(nl, body)
+    assert hphi_b200.inspect_green(nl, 6).shape[1] == 24
