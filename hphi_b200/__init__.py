@@ -38,7 +38,7 @@ INFO_FIELDS = ["dim", "nsite", "calc_model", "calc_type", "size_list_2_1", "size
                "n_green_one", "n_green_two"]
 EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi_close", "hphi_info",
                     "hphi_sz", "hphi_diagonalcalc", "hphi_mltply", "hphi_mltply_device", "hphi_lanczos",
-                    "hphi_lanczos_eigenvector", "hphi_tpq", "hphi_run", "hphi_inspect_terms",
+                    "hphi_lanczos_eigenvector", "hphi_tpq", "hphi_tem", "hphi_run", "hphi_inspect_terms",
                     "hphi_lanczos_tridiagonal", "hphi_mltply_device_async", "hphi_stream",
                     "hphi_synchronize", "hphi_to_native", "hphi_from_native", "hphi_mltply_device_noalloc",
                     "hphi_lanczos_steps", "hphi_batch_create", "hphi_batch_lanczos", "hphi_batch_tuning",
@@ -92,6 +92,7 @@ def load_library() -> ctypes.CDLL:
     lib.hphi_lanczos.argtypes = [P, pd, ctypes.c_char_p, pd, I]
     lib.hphi_lanczos_eigenvector.argtypes = [P, pd]
     lib.hphi_tpq.argtypes = [P, pd, ctypes.c_char_p, pd, I]
+    lib.hphi_tem.argtypes = [P, pd, ctypes.c_char_p, pd, I]
     lib.hphi_run.argtypes = [P, ctypes.c_char_p]
     lib.hphi_mltply_device_async.argtypes = [P, I, VP, VP, VP, VP]
     lib.hphi_mltply_device_noalloc.argtypes = [P, I, VP, VP, D, D, pd]
@@ -389,6 +390,18 @@ class Hamiltonian:
             if buf.shape[0] < self.info["num_ave"]:
                 raise ValueError("need one start vector per TPQ sample (NumAve)")
         _check(load_library().hphi_tpq(self._h, None if buf is None else _dptr(buf.view(np.float64)),
+                                       None if output_dir is None else os.fsencode(output_dir), _dptr(res), n))
+        return res
+
+    def calc_by_tem(self, v_init: Optional[np.ndarray] = None, output_dir: Optional[str] = None,
+                    nresult: Optional[int] = None) -> np.ndarray:
+        """Real-time evolution (CalcByTEM, CalcType 4) from v_init (HPhi layout, dim+1
+        complex128) or, when None, from <SpectrumVec>_rank_0.dat in output_dir.  Writes SS.dat,
+        Norm.dat, Flct.dat and the step files; returns the energy of each step."""
+        n = nresult or self.info["lanczos_max"]
+        res = np.zeros(n)
+        buf = None if v_init is None else np.ascontiguousarray(_as_hphi_vector(v_init, self.dim))
+        _check(load_library().hphi_tem(self._h, None if buf is None else _dptr(buf.view(np.float64)),
                                        None if output_dir is None else os.fsencode(output_dir), _dptr(res), n))
         return res
 

@@ -685,6 +685,51 @@ int hphi_lobpcg(hphi_handle *h, const double *v_init, const char *output_dir, do
   return rc;
 }
 
+int hphi_tem(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult) {
+  CHECK_HANDLE(h);
+  Sector *s = h->sector;
+  const Model &m = s->model;
+  const std::string out = output_dir ? output_dir : "output";
+  const int64_t stride = 2 * (s->dim + 1);
+  std::vector<double> start;
+  int step_initial = 0;
+  if (!v_init) {
+    // the input state <SpectrumVec>_rank_0.dat in the output folder (src/CalcByTEM.c:74-103)
+    if (!m.input_eigenvec) {
+      set_error("Error: A file of Inputvector is not inputted.");
+      return -1;
+    }
+    const std::string path = out + "/" + m.spectrum_vec + "_rank_0.dat";
+    FILE *fin = m.spectrum_vec.empty() ? nullptr : fopen(path.c_str(), "rb");
+    if (!fin) {
+      set_error("Error: A file of Inputvector does not exist.");
+      return -1;
+    }
+    int stp = 0;
+    long dim = 0;
+    start.assign(stride, 0.0);
+    const bool ok = fread(&stp, sizeof(int), 1, fin) == 1 && fread(&dim, sizeof(long), 1, fin) == 1 &&
+                    dim == (long)s->dim && fread(start.data(), sizeof(double), stride, fin) == (size_t)stride;
+    fclose(fin);
+    if (!ok) {
+      set_error("Error: A file of Inputvector is incorrect.");
+      return -1;
+    }
+    // ReStart 2 / 3 continues from the file's step (RESTART_NOT / RESTART_OUT start at 0)
+    if (m.restart == 2 || m.restart == 3) step_initial = stp;
+    if (step_initial < 0) {
+      set_error("Error: A file of Inputvector is incorrect.");
+      return -1;
+    }
+    v_init = start.data();
+  }
+  TeResult r;
+  if (te_run(s, v_init, step_initial, out, &r) != 0) return -1;
+  if (result)
+    for (int i = 0; i < nresult && i < (int)r.energy.size(); i++) result[i] = r.energy[i];
+  return 0;
+}
+
 int hphi_run(hphi_handle *h, const char *output_dir) {
   CHECK_HANDLE(h);
   const std::string out = output_dir ? output_dir : "output";
@@ -693,8 +738,10 @@ int hphi_run(hphi_handle *h, const char *output_dir) {
     case kTPQ:
     case kcTPQ: return hphi_tpq(h, nullptr, out.c_str(), nullptr, 0);
     case kCG: return hphi_lobpcg(h, nullptr, out.c_str(), nullptr, 0);
+    case kTimeEvolution: return hphi_tem(h, nullptr, out.c_str(), nullptr, 0);
     default:
-      set_error("CalcType not supported by this engine (Lanczos = 0, TPQ = 1, LOBPCG = 3 and cTPQ = 5 are)");
+      set_error("CalcType not supported by this engine (Lanczos = 0, TPQ = 1, LOBPCG = 3, time evolution = 4 "
+                "and cTPQ = 5 are)");
       return -1;
   }
 }

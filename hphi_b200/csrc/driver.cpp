@@ -1019,4 +1019,154 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
   return 0;
 }
 
+int te_run(Sector *s, const double *h_init, int step_initial, const std::string &outdir, TeResult *res) {
+  const Model &m = s->model;
+  const int64_t dim = s->dim;
+  const VecType vt = kComplex128;
+  const size_t esz = sizeof(cplx);
+  if ((int)m.te_time.size() < m.lanczos_max) {
+    set_error("Error: NTETimeSteps must be larger than Lanczos_max.");
+    return -1;
+  }
+  if (m.output_eigenvec && m.output_interval <= 0) {
+    set_error("OutputEigenVec in time evolution needs a positive OutputInterval");
+    return -1;
+  }
+  RET(cuda_ok(cudaSetDevice(s->device), "cudaSetDevice"));
+  // every time index's terms, back to back
+  std::vector<BitTerm> off;
+  std::vector<DiagTerm> dg;
+  std::vector<size_t> off_at, dg_at;
+  for (size_t k = 0; k < m.te_time.size(); k++) {
+    off_at.push_back(off.size());
+    dg_at.push_back(dg.size());
+    off.insert(off.end(), m.te_offdiag[k].begin(), m.te_offdiag[k].end());
+    dg.insert(dg.end(), m.te_diag[k].begin(), m.te_diag[k].end());
+  }
+  off_at.push_back(off.size());
+  dg_at.push_back(dg.size());
+  DevBuf OFF, DG, P, HP, ACC, U, ST;
+  if (!off.empty()) {
+    RET(cuda_ok(cudaMalloc(&OFF.p, sizeof(BitTerm) * off.size()), "alloc terms"));
+    RET(cuda_ok(cudaMemcpyAsync(OFF.p, off.data(), sizeof(BitTerm) * off.size(), cudaMemcpyHostToDevice, s->stream),
+                "upload terms"));
+  }
+  if (!dg.empty()) {
+    RET(cuda_ok(cudaMalloc(&DG.p, sizeof(DiagTerm) * dg.size()), "alloc terms"));
+    RET(cuda_ok(cudaMemcpyAsync(DG.p, dg.data(), sizeof(DiagTerm) * dg.size(), cudaMemcpyHostToDevice, s->stream),
+                "upload terms"));
+  }
+  for (DevBuf *b : {&P, &HP, &ACC, &U}) RET(cuda_ok(cudaMalloc(&b->p, esz * dim), "alloc vector"));
+  RET(cuda_ok(cudaMalloc(&ST.p, sizeof(double) * 32), "alloc scalars"));
+  double *st = (double *)ST.p;
+  const double c01[2] = {0.0, 1.0};
+  RET(cuda_ok(cudaMemcpyAsync(st, c01, sizeof(c01), cudaMemcpyHostToDevice, s->stream), "coef"));
+  // y = H(step) x: the static part (general row kernel) plus the step's terms
+  auto apply_h = [&](int step, const void *x, void *y) -> int {
+    RET(hv_launch(s, vt, x, y, st, st + 2));
+    return te_terms_apply(s, (const BitTerm *)OFF.p + off_at[step], (int)(off_at[step + 1] - off_at[step]),
+                          (const DiagTerm *)DG.p + dg_at[step], (int)(dg_at[step + 1] - dg_at[step]), x, y);
+  };
+  RET(vec_from_host_c128(s, vt, h_init, P.p));
+  // the reference's v0 (H psi of the previous step) is zero before the first step
+  RET(cuda_ok(cudaMemsetAsync(HP.p, 0, esz * dim, s->stream), "zero"));
+  RET(ensure_dir(outdir));
+  const std::string ss_file = join(outdir, "SS.dat"), norm_file = join(outdir, "Norm.dat"),
+                    flct_file = join(outdir, "Flct.dat");
+  FILE *fss = fopen(ss_file.c_str(), "w"), *fnorm = fopen(norm_file.c_str(), "w"), *fflct = fopen(flct_file.c_str(), "w");
+  if (!fss || !fnorm || !fflct) {
+    if (fss) fclose(fss);
+    if (fnorm) fclose(fnorm);
+    if (fflct) fclose(fflct);
+    set_error("cannot write time-evolution output files in " + outdir);
+    return -1;
+  }
+  struct Closer {
+    FILE *a, *b, *c;
+    ~Closer() { fclose(a); fclose(b); fclose(c); }
+  } closer{fss, fnorm, fflct};
+  fprintf(fss, " # time, energy, phys_var, phys_doublon, phys_num, step_i\n");
+  fprintf(fnorm, " # time, norm, step_i \n");
+  fprintf(fflct, " # time, N, N^2, D, D^2, Sz, Sz^2, step_i \n");
+  const bool green = !m.green_one.empty() || !m.green_two.empty() || !m.green_three.empty() ||
+                     !m.green_four.empty() || !m.green_six.empty();
+  std::vector<double> host;
+  auto write_state = [&](int step, int label) -> int {
+    // <head>_eigenvec_<label>_rank_0.dat: int step, long dim, complex128[dim + 1]
+    host.assign(2 * (dim + 1), 0.0);
+    RET(vec_to_host_c128(s, vt, P.p, host.data()));
+    char name[256];
+    snprintf(name, sizeof(name), "%s_eigenvec_%d_rank_%d.dat", m.data_head.c_str(), label, 0);
+    FILE *f = fopen(join(outdir, name).c_str(), "wb");
+    if (!f) { set_error(std::string("cannot write ") + name); return -1; }
+    const long ld = (long)dim;
+    fwrite(&step, sizeof(int), 1, f);
+    fwrite(&ld, sizeof(long), 1, f);
+    fwrite(host.data(), sizeof(double), host.size(), f);
+    fclose(f);
+    return 0;
+  };
+  res->time.clear();
+  res->energy.clear();
+  res->norm.clear();
+  const std::complex<double> mi(0.0, -1.0);
+  int step = step_initial;
+  for (; step < m.lanczos_max; step++) {
+    const double time = m.te_time[step];
+    const double dt = step == 0 ? 0.0 : m.te_time[step] - m.te_time[step - 1];
+    // MultiplyForTEM: psi <- (psi - i dt H' psi + sum_{k=2}^{ExpandCoef} (-i dt)^k / k! H^k psi) / |.|
+    // where H' psi is the previous step's H psi; a step with dt < 1e-14 keeps psi
+    if (dt >= 1e-14) {
+      RET(cuda_ok(cudaMemcpyAsync(ACC.p, P.p, esz * dim, cudaMemcpyDeviceToDevice, s->stream), "copy"));
+      std::complex<double> coef = mi * dt;
+      RET(vec_caxpy(s, coef.real(), coef.imag(), HP.p, ACC.p));
+      void *t = HP.p, *u = U.p;
+      for (int k = 2; k <= m.expand_coef; k++) {
+        coef *= mi * dt / (double)k;
+        RET(apply_h(step, t, u));
+        RET(vec_caxpy(s, coef.real(), coef.imag(), u, ACC.p));
+        std::swap(t, u);
+      }
+      std::swap(P.p, ACC.p);
+    }
+    RET(vec_norm2(s, vt, P.p, st + 4));
+    double n2 = 0.0;
+    RET(cuda_ok(cudaMemcpyAsync(&n2, st + 4, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "read"));
+    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+    const double gnorm = std::sqrt(n2);
+    RET(vec_scale(s, vt, 1.0 / gnorm, P.p));
+    // expec_energy_flct: observables of psi, H psi with this step's terms, E, var
+    RET(vec_diag_observables(s, vt, P.p, st + 16));
+    RET(apply_h(step, P.p, HP.p));
+    RET(vec_dot(s, vt, P.p, HP.p, st + 6));
+    RET(vec_norm2(s, vt, HP.p, st + 8));
+    double sc[4], ob[6];
+    RET(cuda_ok(cudaMemcpyAsync(sc, st + 6, sizeof(sc), cudaMemcpyDeviceToHost, s->stream), "read"));
+    RET(cuda_ok(cudaMemcpyAsync(ob, st + 16, sizeof(ob), cudaMemcpyDeviceToHost, s->stream), "read"));
+    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+    const double E = sc[0], var = sc[2];
+    fprintf(fss, "%.16lf  %.16lf %.16lf %.16lf %.16lf %d\n", time, E, var, ob[0], ob[2], step);
+    fprintf(fnorm, "%.16lf %.16lf %d\n", time, gnorm, step);
+    fprintf(fflct, "%.16lf %.16lf %.16lf %.16lf %.16lf %.16lf %.16lf %d\n", time, ob[2], ob[3], ob[0], ob[1], ob[4],
+            ob[5], step);
+    fflush(fss);
+    fflush(fnorm);
+    fflush(fflct);
+    res->time.push_back(time);
+    res->energy.push_back(E);
+    res->norm.push_back(gnorm);
+    if (green && m.expec_interval > 0 && step % m.expec_interval == 0) {
+      GreenValues g;
+      RET(model_green(s, vt, P.p, 1.0, &g));
+      char suffix[64];
+      snprintf(suffix, sizeof(suffix), "_step%d", step);
+      RET(write_green_files(m, g, outdir, suffix));
+    }
+    if (m.output_eigenvec && step % m.output_interval == 0) RET(write_state(step, step));
+  }
+  res->final_step = step;
+  if (m.output_eigenvec) RET(write_state(step, 0));
+  return 0;
+}
+
 }  // namespace hphi

@@ -109,6 +109,15 @@ struct TpqOptions {
   bool keep_vector = false;
 };
 
+// Real-time evolution (CalcType 4, CalcByTEM src/CalcByTEM.c:52-234): per step the state
+// is advanced by the Taylor sum of exp(-i dt H) (MultiplyForTEM src/Multiply.c:79-139),
+// normalised, and measured (SS.dat, Norm.dat, Flct.dat, Green's function files every
+// ExpecInterval steps, eigenvector files every OutputInterval steps with OutputEigenVec).
+struct TeResult {
+  std::vector<double> time, energy, norm;
+  int final_step = 0;
+};
+
 // k-th smallest eigenvalue (0-based) of the symmetric tridiagonal matrix with diagonal
 // a[0..n) and off-diagonal b[0..n-1), by Sturm bisection; its eigenvector by inverse iteration.
 double tridiag_eigenvalue(const double *a, const double *b, int n, int k);
@@ -128,6 +137,9 @@ int read_lanczos_restart(const Sector &s, const std::string &outdir, LanczosRest
 // h_init: start vector (any norm) of sample rand_i; writes SS/Norm/Flct_rand<rand_i>.dat.
 int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::string &outdir, TpqResult *res,
             const TpqOptions &opt = TpqOptions());
+// h_init: the input state (SpectrumVec file contents, HPhi's 1-based complex128 layout);
+// step_initial: the first time index (the file's step on a ReStart 2 / 3 run, else 0).
+int te_run(Sector *s, const double *h_init, int step_initial, const std::string &outdir, TeResult *res);
 // Block LOBPCG for the exct lowest states (CalcType 3).  h_init: exct start vectors in
 // HPhi's 1-based complex128 layout, back to back (any norm).
 bool lobpcg_single_element_start(const Sector &s, std::vector<double> *v);

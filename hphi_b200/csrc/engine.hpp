@@ -144,6 +144,13 @@ int green_expect(Sector *s, VecType vt, const void *d_v, const std::vector<Green
 // when every imaginary part is zero, else complex.  *d_vec is the caller's to cudaFree.
 int green_stage_host_vector(Sector *s, const double *h_v_1based, void **d_vec, VecType *vt);
 
+// Real-time evolution (te.cu), complex vectors in HPhi's row order:
+// v0 += (terms of one time index) v1, the terms compiled like the static ones;
+// y += (a_re + i a_im) x.
+int te_terms_apply(Sector *s, const BitTerm *d_off, int noff, const DiagTerm *d_diag, int ndiag, const void *d_v1,
+                   void *d_v0);
+int vec_caxpy(Sector *s, double a_re, double a_im, const void *d_x, void *d_y);
+
 // complex128 <-> real and imaginary parts (n = dim); y[0, n) += x[0, n) on stream st.
 int vec_split_c128(Sector *s, const void *d_c, double *d_re, double *d_im);
 int vec_join_c128(Sector *s, const double *d_re, const double *d_im, void *d_c);

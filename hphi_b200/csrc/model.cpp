@@ -367,8 +367,7 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
   }
   for (const char *must : {"calcmod", "modpara", "locspin"})
     if (!files.count(must)) { *err = std::string("namelist.def: missing ") + must; return -1; }
-  for (const char *unsupported : {"boost", "laser", "teonebody", "tetwobody", "singleexcitation",
-                                  "pairexcitation", "spectrumvec"})
+  for (const char *unsupported : {"boost", "laser", "singleexcitation", "pairexcitation"})
     if (files.count(unsupported)) {
       *err = std::string("namelist.def: keyword not supported by this engine: ") + unsupported;
       return -1;
@@ -446,7 +445,8 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       else if (k == "calchs") m->read_hacker = (int)v;
       else if (k == "precg") m->pre_cg = (int)v;
       else if (k == "expandcoef") m->expand_coef = (int)v;
-      else if (k == "timeslice" || k == "outputinterval" || k == "tinit" ||
+      else if (k == "outputinterval") m->output_interval = (int)v;
+      else if (k == "timeslice" || k == "tinit" ||
                k == "omegamax" || k == "omegamin" || k == "omegaim" || k == "omegaorg" || k == "nomega" ||
                k == "targettpqrand") {
         // accepted and ignored: parameters of modes outside this engine
@@ -791,6 +791,112 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
         if (!check_site(r[2 * k]) || !sigma_ok(r[2 * k], r[2 * k + 1])) { *err = fn + ": bad index"; return -1; }
       multi[q].second->push_back(r);
     }
+  }
+  if (files.count("spectrumvec")) m->spectrum_vec = files["spectrumvec"];
+  // ---- TEOneBody / TETwoBody, read for CalcType 4 only (src/readdef.c:755-797, 1752-1840):
+  // 5 header lines (the 2nd: "AllTimeStep n"), then per time index a line "time count"
+  // followed by count transfer rows (i s1 j s2 re im) or InterAll rows (8 indices, re im)
+  if (m->calc_type == kTimeEvolution && (files.count("teonebody") || files.count("tetwobody"))) {
+    if (files.count("teonebody") && files.count("tetwobody")) {
+      *err = "Time Evolution mode does not support TEOneBody and TETwoBody at the same time";
+      return -1;
+    }
+    const bool one = files.count("teonebody") > 0;
+    const std::string fn = files[one ? "teonebody" : "tetwobody"];
+    const int ncol = one ? 6 : 10;
+    std::ifstream f;
+    if (!open_def(*m, fn, &f)) { *err = "cannot open " + fn; return -1; }
+    int nsteps = -1;
+    for (int i = 0; i < 5; i++) {
+      if (!std::getline(f, line)) { *err = fn + ": truncated header"; return -1; }
+      std::istringstream ss(line);
+      std::string kw;
+      if (i == 1 && !(ss >> kw >> nsteps)) { *err = fn + ": bad step count line"; return -1; }
+    }
+    if (nsteps < 0) { *err = fn + ": negative step count"; return -1; }
+    Model scratch = *m;
+    auto next_line = [&](std::string *out) {
+      while (std::getline(f, *out))
+        if (out->find_first_not_of(" \t\r") != std::string::npos) return true;
+      return false;
+    };
+    // a canonical sector admits only terms that keep its particle numbers (and Sz where fixed)
+    const uint64_t up_bits = 0x5555555555555555ull, dn_bits = 0xAAAAAAAAAAAAAAAAull;
+    auto delta = [](const BitTerm &t, uint64_t mask) {
+      return 2 * __builtin_popcountll(t.cv & t.flip & mask) - __builtin_popcountll(t.flip & mask);
+    };
+    auto keeps_sector = [&](const BitTerm &t) {
+      if (m->is_gc() || m->general_spin) return true;
+      if (spin) return delta(t, ~0ull) == 0;
+      if (m->calc_model == kHubbardNConserved) return delta(t, ~0ull) == 0;
+      return delta(t, up_bits) == 0 && delta(t, dn_bits) == 0;
+    };
+    for (int step = 0; step < nsteps; step++) {
+      if (!next_line(&line)) break;
+      std::istringstream hs(line);
+      double time;
+      int count;
+      if (!(hs >> time >> count) || count < 0) { *err = fn + ": bad time line: " + line; return -1; }
+      std::vector<std::vector<double>> trows;
+      for (int q = 0; q < count; q++) {
+        std::string row;
+        if (!next_line(&row)) { *err = fn + ": truncated at time index " + std::to_string(step); return -1; }
+        std::istringstream rs(row);
+        std::vector<double> r(ncol);
+        for (double &x : r)
+          if (!(rs >> x)) { *err = fn + ": malformed line: " + row; return -1; }
+        trows.push_back(r);
+      }
+      scratch.offdiag.clear();
+      scratch.diag.clear();
+      if (one) {
+        // CheckTETransferHermite (src/readdef.c:3100-3220): every row needs its conjugate
+        // partner; a site-diagonal row keeps its real part
+        for (const auto &r : trows) {
+          const int i = (int)r[0], s1 = (int)r[1], j = (int)r[2], s2 = (int)r[3];
+          if (!check_site(i) || !check_site(j) || !sigma_ok(i, s1) || !sigma_ok(j, s2)) {
+            *err = fn + ": bad site or spin index"; return -1;
+          }
+          if (spin && i != j) { *err = fn + ": spin models need site-diagonal transfers"; return -1; }
+          bool partner = false;
+          for (const auto &p : trows)
+            if ((int)p[0] == j && (int)p[1] == s2 && (int)p[2] == i && (int)p[3] == s1 &&
+                std::abs(std::complex<double>(r[4], r[5]) - std::complex<double>(p[4], -p[5])) <= 1e-12)
+              partner = true;
+          if (!partner) { *err = fn + ": transfer integrals are not Hermitian"; return -1; }
+          std::complex<double> t(r[4], r[5]);
+          if (i == j && s1 == s2) t = t.real();
+          if (spin) add_spin_string(&scratch, {{i, s1, s2}}, -t);
+          else add_fermion_string(&scratch, {{fbit(i, s1), true}, {fbit(j, s2), false}}, -t);
+        }
+      } else {
+        for (const auto &r : trows) {
+          int s[4], g[4];
+          for (int q = 0; q < 4; q++) { s[q] = (int)r[2 * q]; g[q] = (int)r[2 * q + 1]; }
+          for (int q = 0; q < 4; q++)
+            if (!check_site(s[q]) || !sigma_ok(s[q], g[q])) { *err = fn + ": bad index"; return -1; }
+          const std::complex<double> V(r[8], r[9]);
+          if (spin) {
+            if (s[0] != s[1] || s[2] != s[3]) { *err = fn + ": spin InterAll needs i==j and k==l"; return -1; }
+            add_spin_string(&scratch, {{s[0], g[0], g[1]}, {s[2], g[2], g[3]}}, V);
+          } else {
+            add_fermion_string(&scratch, {{fbit(s[0], g[0]), true}, {fbit(s[1], g[1]), false},
+                                          {fbit(s[2], g[2]), true}, {fbit(s[3], g[3]), false}}, V);
+          }
+        }
+      }
+      canonicalize_terms(&scratch);
+      for (const auto &t : scratch.offdiag)
+        if (!keeps_sector(t)) {
+          *err = fn + ": a term at time index " + std::to_string(step) + " leaves the sector";
+          return -1;
+        }
+      m->te_time.push_back(time);
+      m->te_offdiag.push_back(scratch.offdiag);
+      m->te_diag.push_back(scratch.diag);
+    }
+    if ((int)m->te_time.size() != nsteps) { *err = fn + ": fewer time indices than AllTimeStep"; return -1; }
+    m->te_kind = one ? 1 : 2;
   }
   canonicalize_terms(m);
   return 0;

@@ -78,6 +78,16 @@ struct Model {
   // src/readdef.c:1525-1700);
   // the reference evaluates them for spin-1/2 SpinGC only.
   std::vector<std::vector<int>> green_three, green_four, green_six;
+  // Time evolution (CalcType 4, src/CalcByTEM.c:52-234): the terms of TEOneBody (te_kind 1,
+  // transfers) or TETwoBody (te_kind 2, InterAll) at each time index, compiled like the static
+  // terms and added to H at that step (MakeTEDTransfer / MakeTEDInterAll :237-279 for the
+  // off-diagonal part, diagonalcalcForTE src/diagonalcalc.c:195-245 for the diagonal part).
+  int te_kind = 0;
+  std::vector<double> te_time;                   // TETime[step]
+  std::vector<std::vector<BitTerm>> te_offdiag;  // per step
+  std::vector<std::vector<DiagTerm>> te_diag;    // per step
+  std::string spectrum_vec;                      // SpectrumVec: head of the input vector file
+  int output_interval = 0;                       // OutputInterval (eigenvector files)
   // Raw term counts as read (for logs).
   int n_trans = 0, n_coulomb_intra = 0, n_coulomb_inter = 0, n_hund = 0, n_exchange = 0;
   int n_ising = 0, n_pairhop = 0, n_pairlift = 0, n_interall = 0;

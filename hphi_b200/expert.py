@@ -78,6 +78,15 @@ class ExpertModel:
     greenthree: List[Tuple] = field(default_factory=list)
     greenfour: List[Tuple] = field(default_factory=list)
     greensix: List[Tuple] = field(default_factory=list)
+    # time evolution (calc_type "TimeEvolution"): per time index (time, rows), TEOneBody rows
+    # (i, s1, j, s2, t_re, t_im) or TETwoBody rows (i, s1, j, s2, k, s3, l, s4, V_re, V_im)
+    # (src/readdef.c:1752-1840); the start state is <spectrum_vec>_rank_0.dat
+    te_onebody: List[Tuple[float, List[Tuple]]] = field(default_factory=list)
+    te_twobody: List[Tuple[float, List[Tuple]]] = field(default_factory=list)
+    spectrum_vec: Optional[str] = None
+    input_eigenvec: int = 0
+    expand_coef: int = 0
+    output_interval: int = 0
 
     # ------------------------------------------------------------------ writers
     def write(self, directory: str) -> str:
@@ -114,6 +123,21 @@ class ExpertModel:
                 for r in rows:
                     f.write(fmt.format(*r) + "\n")
             names.append((kw, fname))
+        for kw, fname, steps, fmt in (
+                ("TEOneBody", "teonebody.def", self.te_onebody, "{:d} {:d} {:d} {:d} {:.17g} {:.17g}"),
+                ("TETwoBody", "tetwobody.def", self.te_twobody,
+                 "{:d} {:d} {:d} {:d} {:d} {:d} {:d} {:d} {:.17g} {:.17g}")):
+            if not steps:
+                continue
+            with open(os.path.join(directory, fname), "w") as f:
+                f.write(f"{_SEP}\nAllTimeStep {len(steps)}\n{_SEP}\n{_SEP}\n{_SEP}\n")
+                for t, rows in steps:
+                    f.write(f"{t!r} {len(rows)}\n")
+                    for r in rows:
+                        f.write(fmt.format(*r) + "\n")
+            names.append((kw, fname))
+        if self.spectrum_vec:
+            names.append(("SpectrumVec", self.spectrum_vec))
         path = os.path.join(directory, "namelist.def")
         with open(path, "w") as f:
             for kw, fname in names:
@@ -130,6 +154,8 @@ class ExpertModel:
             f.write(f"InitialVecType {self.initial_vec_type}\n")
             if self.output_eigenvec:
                 f.write(f"OutputEigenVec {self.output_eigenvec}\n")
+            if self.input_eigenvec:
+                f.write(f"InputEigenVec {self.input_eigenvec}\n")
             if self.restart:
                 f.write(f"ReStart {self.restart}\n")
 
@@ -151,6 +177,10 @@ class ExpertModel:
                   f"NumAve         {self.num_ave}", f"ExpecInterval  {self.expec_interval}"]
         if self.pre_cg:
             lines.append(f"PreCG          {self.pre_cg}")
+        if self.expand_coef:
+            lines.append(f"ExpandCoef     {self.expand_coef}")
+        if self.output_interval:
+            lines.append(f"OutputInterval {self.output_interval}")
         with open(path, "w") as f:
             f.write("\n".join(lines) + "\n")
 

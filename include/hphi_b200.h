@@ -195,6 +195,22 @@ int hphi_lanczos_eigenvector(hphi_handle *h, double *v);
 int hphi_tpq(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult);
 
 /*
+ * Real-time evolution (CalcType 4) under H(t) = H + the TEOneBody / TETwoBody terms of each
+ * time index.  Per step: psi <- sum_{k<=ExpandCoef} (-i dt H)^k / k! psi, normalised (the
+ * first-order term uses the previous step's H psi; ExpandCoef 0 keeps first order only), then
+ * E, var and the diagonal observables of psi.  v_init: the start state in HPhi's layout
+ * ((dim + 1) complex128), or NULL to read <SpectrumVec>_rank_0.dat from output_dir (needs
+ * InputEigenVec; ReStart 2 / 3 continue from the file's step).  Writes SS.dat, Norm.dat,
+ * Flct.dat, <head>_cisajs_step%d.dat (every ExpecInterval steps) and, with OutputEigenVec,
+ * <head>_eigenvec_%d_rank_0.dat (every OutputInterval steps and at the end, as index 0).
+ * result (may be NULL) receives the energy of each step (nresult values at most).
+ * Replaces: CalcByTEM (src/CalcByTEM.c:52-234), MultiplyForTEM (src/Multiply.c:79-139),
+ * MakeTEDTransfer / MakeTEDInterAll (src/CalcByTEM.c:237-279), diagonalcalcForTE
+ * (src/diagonalcalc.c:195-245).
+ */
+int hphi_tem(hphi_handle *h, const double *v_init, const char *output_dir, double *result, int nresult);
+
+/*
  * Block LOBPCG for the exct lowest states (CalcType 3, "CG"; preconditioned when PreCG = 1).
  * v_init: exct start vectors in HPhi's layout, back to back (any norm), or NULL for the
  * reference's single-element starts (initial_iv > 0 on canonical models) or its random

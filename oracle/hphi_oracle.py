@@ -61,6 +61,11 @@ class Def:
     green_one: List[Tuple[int, int, int, int]] = field(default_factory=list)      # OneBodyG rows
     green_two: List[Tuple[int, int, int, int, int, int, int, int]] = field(default_factory=list)  # TwoBodyG rows
     green_multi: Dict[int, List[Tuple[int, ...]]] = field(default_factory=dict)  # 3/4/6: ThreeBodyG ... rows
+    expec_interval: int = 1
+    # time evolution (CalcType 4): TEOneBody (te_kind 1) / TETwoBody (te_kind 2) rows per time index
+    te_kind: int = 0
+    te_time: List[float] = field(default_factory=list)
+    te_rows: List[List[Tuple]] = field(default_factory=list)
 
 
 def _table(path: str) -> List[List[float]]:
@@ -120,6 +125,7 @@ def read_expert(namelist: str) -> Def:
         elif k == "lanczostarget": d.lanczos_target = int(v)
         elif k == "largevalue": d.large_value = v
         elif k == "numave": d.num_ave = int(v)
+        elif k == "expecinterval": d.expec_interval = int(v)
     loc_lines = open(files["locspin"]).read().splitlines()
     d.nlocspn = int(loc_lines[1].split()[1])
     d.locspn = [0] * d.nsite
@@ -195,6 +201,19 @@ def read_expert(namelist: str) -> Def:
     for key, npairs in (("threebodyg", 3), ("fourbodyg", 4), ("sixbodyg", 6)):   # :1525-1700
         if key in files:
             d.green_multi[npairs] = [tuple(r[:4 * npairs]) for r in _int_table(files[key])]
+    # TEOneBody / TETwoBody (src/readdef.c:755-797, 1752-1840), read for CalcType 4 only:
+    # 5 header lines (2nd: "AllTimeStep n"), then per time index "time count" and count rows
+    for key, kind in (("teonebody", 1), ("tetwobody", 2)):
+        if key in files and d.calc_type == 4:
+            lines = [l for l in open(files[key]).read().splitlines()[5:] if l.strip()]
+            pos = 0
+            while pos < len(lines):
+                t, n = lines[pos].split()[:2]
+                rows = [tuple(float(x) for x in l.split()) for l in lines[pos + 1: pos + 1 + int(n)]]
+                d.te_time.append(float(t))
+                d.te_rows.append(rows)
+                pos += 1 + int(n)
+            d.te_kind = kind
     return d
 
 
@@ -1005,3 +1024,81 @@ def expec_multibody(d: Def, vec: np.ndarray, npairs: int):
         short.append(False)
     return np.array(vals, dtype=np.complex128), np.array(short, dtype=bool)
 
+
+
+def _te_def(d: Def, step: int) -> Def:
+    """H at time index `step`: the static terms plus that index's TE rows, as MakeTEDTransfer /
+    MakeTEDInterAll (src/CalcByTEM.c:237-279) and diagonalcalcForTE (src/diagonalcalc.c:195-245)
+    add them: a site-diagonal transfer is -t n (real part), other transfers -t c+c, InterAll
+    rows split as the static InterAll."""
+    import dataclasses
+    e = dataclasses.replace(d, trans=list(d.trans), chemi=list(d.chemi),
+                            interall_diag=list(d.interall_diag), interall_off=list(d.interall_off))
+    for r in d.te_rows[step]:
+        if d.te_kind == 1:
+            i, s1, j, s2 = (int(x) for x in r[:4])
+            t = complex(r[4], r[5])
+            if i == j and s1 == s2:
+                e.chemi.append((i, s1, t.real))
+            else:
+                e.trans.append((i, s1, j, s2, t))
+        else:
+            i, s1, j, s2, k, s3, l, s4 = (int(x) for x in r[:8])
+            v = complex(r[8], r[9])
+            if i == j and k == l and s1 == s2 and s3 == s4:
+                e.interall_diag.append((i, s1, k, s3, v.real))
+            else:
+                e.interall_off.append((i, s1, j, s2, k, s3, l, s4, v))
+    return e
+
+
+def te_flct(d: Def, lists, v: np.ndarray):
+    """Diagonal observables of expec_energy_flct (src/expec_energy_flct.c:186-666) for a
+    normalised vector: (doublon, doublon^2, N, N^2, Sz, Sz^2); a canonical spin model gives
+    the constants of :92-101."""
+    w = np.abs(v[1:]) ** 2
+    if d.calc_model == SPIN:
+        sz = 0.5 * d.total_2sz
+        return 0.0, 0.0, float(d.nsite), float(d.nsite) ** 2, sz, sz * sz
+    c = configs(d, lists)[1:].astype(np.uint64)
+    even = np.uint64(0x5555555555555555)
+    up, dn = _popcount(c & even).astype(float), _popcount(c & ~even).astype(float)
+    dbl = _popcount(c & (c >> np.uint64(1)) & even).astype(float)
+    n, sz = up + dn, 0.5 * (up - dn)
+    return (float(w @ dbl), float(w @ dbl ** 2), float(w @ n), float(w @ n ** 2), float(w @ sz),
+            float(w @ sz ** 2))
+
+
+def te_run(d: Def, lists, v_init: np.ndarray, step_initial: int = 0, keep_states=()):
+    """CalcByTEM (src/CalcByTEM.c:52-234) with MultiplyForTEM (src/Multiply.c:79-139).  Per time
+    index: dt = TETime[i] - TETime[i-1] (0 at index 0); for dt >= 1e-14 the state becomes
+    psi - i dt H' psi + sum_{k=2}^{ExpandCoef} (-i dt)^k / k! H^k psi, where H' psi is the H psi
+    of the previous index (zero before the first one) and H is this index's Hamiltonian; then it
+    is normalised (norm = global_norm) and measured: E = <psi|H psi>, var = <H psi|H psi> and the
+    Flct observables.  Returns per-index rows (time, E, var, norm, flct...) and the states at
+    the indices in keep_states."""
+    psi = np.asarray(v_init, dtype=np.complex128).copy()
+    hpsi = np.zeros_like(psi)
+    rows, states = [], {}
+    for step in range(step_initial, d.lanczos_max):
+        e = _te_def(d, step)
+        diag = diagonalcalc(e, lists)
+        dt = 0.0 if step == 0 else d.te_time[step] - d.te_time[step - 1]
+        if dt >= 1e-14:
+            acc = psi + (-1j * dt) * hpsi
+            term, coef = hpsi, -1j * dt
+            for k in range(2, d.expand_coef + 1):
+                coef *= -1j * dt / k
+                term, _ = mltply(e, lists, diag, np.zeros_like(psi), term)
+                acc = acc + coef * term
+            psi = acc
+        psi[0] = 0.0
+        norm = float(np.sqrt(np.sum(np.abs(psi[1:]) ** 2)))
+        psi = psi / norm
+        hpsi, _ = mltply(e, lists, diag, np.zeros_like(psi), psi)
+        energy = float(np.vdot(psi[1:], hpsi[1:]).real)
+        var = float(np.sum(np.abs(hpsi[1:]) ** 2))
+        rows.append((d.te_time[step], energy, var, norm) + te_flct(d, lists, psi) + (step,))
+        if step in keep_states:
+            states[step] = psi.copy()
+    return rows, states

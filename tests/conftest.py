@@ -22,8 +22,11 @@ def golden_cases(kind=None):
             continue
         z = np.load(p)
         large = "sha_list_1" in z.files
+        te = "text_SS" in z.files          # time-evolution cases
+        if (kind == "te") != te:
+            continue
         green = "green_files" in z.files
-        if (kind == "green") != green:
+        if kind != "te" and (kind == "green") != green:
             continue
         if kind == "large" and not large:
             continue

@@ -22,6 +22,10 @@ lobpcgrestart_* the same for LOBPCG (step rows of both runs, a's stored vectors,
 green_* directories hold inputs with OneBodyG / TwoBodyG files and golden.npz with the
 reference's Green's function files (text_<file>), the eigenvectors it wrote (vec_<file>,
 OutputEigenVec), the first mltply input (start) and its energies (states, or tpq rows).
+te_* directories hold time-evolution inputs (CalcType 4, TEOneBody / TETwoBody) and golden.npz
+with the seeded start state written as zvo_eigenvec_0_rank_0.dat before the run (start), the
+reference's SS.dat, Norm.dat, Flct.dat (text_SS ...), its Green's function step files and the
+eigenvector files of OutputEigenVec (vec_<file>).
 Large cases store only SHA-256 digests of the lists (sha_list_1 ...).
 
 Run in a container that has the reference sources and oracle/_ref/HPhi_ref
@@ -522,13 +526,126 @@ def make_lobpcg_restart_case(name: str, ma, mb) -> None:
     np.savez_compressed(os.path.join(out, "restart.npz"), **data)
 
 
+def _te_times(n: int, dt: float, repeat_at: int = -1):
+    """Time grid accumulated as t += dt (a repeated time at index repeat_at: a zero step)."""
+    out, t = [], 0.0
+    for k in range(n):
+        out.append(t)
+        if k != repeat_at:
+            t += dt
+    return out
+
+
+def _te_cases():
+    import math
+    cases = {}
+    # Hubbard chain L=6 (3+3 electrons): a time-dependent exchange-like InterAll on every bond
+    # and a time-dependent density-density row, 30 steps of 0.02, ExpandCoef 4, Green's
+    # functions every 10 steps, eigenvector files every 10 steps
+    L = 6
+    m = expert.hubbard(L, expert.chain_bonds(L), 1.0, 4.0, 3, 3, calc_type="TimeEvolution", lanczos_max=30,
+                       expec_interval=10, input_eigenvec=1, spectrum_vec="zvo_eigenvec_0", expand_coef=4,
+                       output_eigenvec=1, output_interval=10)
+    m.greenone = [(i, s, i, s) for i in range(L) for s in (0, 1)] + [(0, 0, 1, 0), (1, 0, 0, 0), (2, 1, 4, 1)]
+    m.greentwo = [(i, 0, i, 0, (i + 1) % L, 1, (i + 1) % L, 1) for i in range(L)]
+    steps = []
+    for k, t in enumerate(_te_times(30, 0.02)):
+        v = 0.5 * math.cos(2.0 * t)
+        rows = []
+        for x in range(L):
+            f = (x + 1) % L
+            r = (x, 0, f, 0, f, 1, x, 1)
+            rows.append(r + (v, 0.0))
+            rows.append((r[6], r[7], r[4], r[5], r[2], r[3], r[0], r[1], v, 0.0))
+        rows.append((0, 0, 0, 0, 3, 1, 3, 1, 0.3 * t, 0.0))
+        steps.append((t, rows))
+    m.te_twobody = steps
+    cases["te_hub_chain6_two"] = (m, 11)
+    # the same chain driven by a Peierls phase on the hoppings, t e^{i A(t)}, with a site
+    # potential; non-uniform time steps with one repeated time, ExpandCoef 10
+    m = expert.hubbard(L, [], 1.0, 4.0, 3, 3, calc_type="TimeEvolution", lanczos_max=25, expec_interval=6,
+                       input_eigenvec=1, spectrum_vec="zvo_eigenvec_0", expand_coef=10)
+    m.greenone = [(i, s, i, s) for i in range(L) for s in (0, 1)] + [(0, 0, 1, 0), (1, 0, 0, 0)]
+    steps = []
+    times = [0.03 * k + 0.002 * k * k for k in range(25)]
+    times[7] = times[6]
+    for t in times:
+        a = 0.8 * math.sin(3.0 * t)
+        rows = []
+        for x in range(L):
+            f = (x + 1) % L
+            for sg in (0, 1):
+                rows.append((x, sg, f, sg, math.cos(a), math.sin(a)))
+                rows.append((f, sg, x, sg, math.cos(a), -math.sin(a)))
+        rows.append((2, 0, 2, 0, 0.5 * math.cos(t), 0.0))
+        steps.append((t, rows))
+    m.te_onebody = steps
+    cases["te_hub_chain6_one"] = (m, 12)
+    # Heisenberg chain L=10 (Sz=0): the exchange of every bond modulated in time through
+    # TETwoBody spin rows plus a time-dependent Ising-type row; ExpandCoef 6
+    L = 10
+    m = expert.heisenberg(L, expert.chain_bonds(L), 1.0, calc_type="TimeEvolution", lanczos_max=30,
+                          input_eigenvec=1, spectrum_vec="zvo_eigenvec_0", expand_coef=6, expec_interval=15)
+    m.greenone = [(i, s, i, s) for i in range(L) for s in (0, 1)]
+    steps = []
+    for t in _te_times(30, 0.05):
+        j = 0.5 * (1.0 + 0.5 * math.sin(t))
+        rows = []
+        for x in range(L):
+            f = (x + 1) % L
+            rows.append((x, 0, x, 1, f, 1, f, 0, j, 0.0))
+            rows.append((f, 0, f, 1, x, 1, x, 0, j, 0.0))
+        rows.append((0, 1, 0, 1, 5, 1, 5, 1, 0.2 * t, 0.0))
+        steps.append((t, rows))
+    m.te_twobody = steps
+    cases["te_spin_chain10_two"] = (m, 13)
+    return cases
+
+
+def make_te_case(name: str, m, seed: int) -> None:
+    import hphi_oracle as O
+    out = os.path.join(HERE, name)
+    shutil.rmtree(out, ignore_errors=True)
+    m.write(out)
+    d = O.read_expert(os.path.join(out, "namelist.def"))
+    dim = len(O.sz(d)[0]) - 1
+    rng = np.random.default_rng(seed)
+    v = np.zeros(dim + 1, dtype=np.complex128)
+    v[1:] = rng.standard_normal(dim) + 1j * rng.standard_normal(dim)
+    v[1:] /= np.linalg.norm(v[1:])
+    data = {"start": v}
+    with tempfile.TemporaryDirectory() as tmp:
+        for f in os.listdir(out):
+            shutil.copy(os.path.join(out, f), tmp)
+        od = os.path.join(tmp, "output")
+        os.makedirs(od)
+        with open(os.path.join(od, "zvo_eigenvec_0_rank_0.dat"), "wb") as f:
+            f.write(np.array([0], dtype=np.int32).tobytes())
+            f.write(np.array([dim], dtype=np.int64).tobytes())
+            f.write(v.tobytes())
+        p = run_ref.run(tmp, threads=1)
+        if p.returncode != 0:
+            raise RuntimeError(f"{name}: reference failed\n{p.stdout[-3000:]}\n{p.stderr[-3000:]}")
+        for base in ("SS", "Norm", "Flct"):
+            data["text_" + base] = np.array(open(os.path.join(od, base + ".dat")).read())
+        files = sorted(f for f in os.listdir(od) if "cisajs" in f or "Body" in f)
+        data["green_files"] = np.array(files)
+        for f in files:
+            data["text_" + f] = np.array(open(os.path.join(od, f)).read())
+        for f in sorted(os.listdir(od)):
+            if f.startswith("zvo_eigenvec_"):
+                data["vec_" + f] = _read_eigvec(os.path.join(od, f))
+    np.savez_compressed(os.path.join(out, "golden.npz"), **data)
+
+
 def main(argv) -> None:
     if not run_ref.available():
         raise SystemExit("oracle/_ref/HPhi_ref is missing: run `make -C oracle` first")
     small, large, starts, restarts = _cases(), _large_cases(), _start_cases(), _restart_cases()
     greens, tpq_restarts, lobpcg_restarts = _green_cases(), _tpq_restart_cases(), _lobpcg_restart_cases()
+    tes = _te_cases()
     names = argv or (list(small) + list(large) + list(starts) + list(restarts) + list(greens) + list(tpq_restarts)
-                     + list(lobpcg_restarts))
+                     + list(lobpcg_restarts) + list(tes))
     for n in names:
         print("case", n, flush=True)
         if n in small:
@@ -543,6 +660,8 @@ def main(argv) -> None:
             make_tpq_restart_case(n, *tpq_restarts[n])
         elif n in lobpcg_restarts:
             make_lobpcg_restart_case(n, *lobpcg_restarts[n])
+        elif n in tes:
+            make_te_case(n, *tes[n])
         else:
             make_case(n, large[n], large=True)
 

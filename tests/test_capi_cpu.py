@@ -192,3 +192,21 @@ def test_green_inspect_rejects_unknown_body():
         with pytest.raises(hphi_b200.HPhiError):
             hphi_b200.inspect_green(nl, body)
     assert hphi_b200.inspect_green(nl, 6).shape[1] == 24
+
+
+def test_time_evolution_inputs_are_checked(tmp_path):
+    """TEOneBody / TETwoBody are read for CalcType 4: both at once is an error (as the
+    reference's CalcByTEM reports), so is a time-dependent term that leaves a canonical sector;
+    a valid TETwoBody file reads."""
+    from hphi_b200 import expert
+    m = expert.hubbard(4, expert.chain_bonds(4), 1.0, 4.0, 2, 2, calc_type="TimeEvolution", lanczos_max=2,
+                       input_eigenvec=1, spectrum_vec="zvo_eigenvec_0")
+    m.te_twobody = [(0.0, [(0, 0, 1, 0, 1, 1, 0, 1, 1.0, 0.0), (0, 1, 1, 1, 1, 0, 0, 0, 1.0, 0.0)]), (0.1, [])]
+    hphi_b200.inspect_terms(m.write(str(tmp_path / "ok")))
+    m.te_onebody = [(0.0, [(0, 0, 1, 0, 1.0, 0.0), (1, 0, 0, 0, 1.0, 0.0)]), (0.1, [])]
+    with pytest.raises(hphi_b200.HPhiError, match="TEOneBody and TETwoBody at the same time"):
+        hphi_b200.inspect_terms(m.write(str(tmp_path / "both")))
+    m.te_twobody = []
+    m.te_onebody = [(0.0, [(0, 0, 1, 1, 1.0, 0.0), (1, 1, 0, 0, 1.0, 0.0)]), (0.1, [])]
+    with pytest.raises(hphi_b200.HPhiError, match="leaves the sector"):
+        hphi_b200.inspect_terms(m.write(str(tmp_path / "flip")))
