@@ -28,6 +28,9 @@ metric (solves/s and latency against the plain FP64 GPU path):
   green      expec_cisajs on the 4x4 Hubbard sector: the 512 spin-conserving one-body rows of a
              normalised random vector (rows x sector rows per second), the reference's
              expec_cisajs timed on 8 of the rows as the CPU baseline.
+  tem        real-time evolution (CalcByTEM) on the 4x4 Hubbard sector under a TEOneBody
+             Peierls pulse, ExpandCoef 10: time steps per second through the C-ABI, the
+             reference's mltply inside its own CalcByTEM as the CPU baseline.
 
 Multi-GPU (--gpus N under torchrun): the path does not shard for this workload, so
 N independent replicas run (one per GPU); value = total bytes / max-over-ranks time.
@@ -444,6 +447,113 @@ def run_green_mode(args):
     print(json.dumps(out))
 
 
+def tem_model(workload: str, nsteps: int, expand: int):
+    """The workload's static H plus a Peierls phase pulse on its hoppings as TEOneBody rows:
+    t -> t e^{i A(t)} with A(t) = 0.5 sin(4 t), dt = 0.01."""
+    import math
+    m, desc = workload_model(workload)
+    m.calc_type, m.lanczos_max, m.input_eigenvec, m.spectrum_vec = "TimeEvolution", nsteps, 1, "zvo_eigenvec_0"
+    m.expand_coef, m.expec_interval = expand, 100000
+    hops = [r for r in m.trans if (r[0], r[1]) != (r[2], r[3])]
+    m.trans = []
+    m.te_onebody = []
+    for k in range(nsteps):
+        t = 0.01 * k
+        a = 0.5 * math.sin(4.0 * t)
+        rows = []
+        for (i, s1, j, s2, tr, ti) in hops:
+            sign = 1.0 if i < j else -1.0
+            rows.append((i, s1, j, s2, tr * math.cos(a), sign * tr * math.sin(a)))
+        m.te_onebody.append((t, rows))
+    return m, desc + "; TEOneBody Peierls pulse A(t) = 0.5 sin(4t), dt = 0.01"
+
+
+def reference_tem_times(model, vec_c128: np.ndarray, threads: int, timeout: float = 3000.0):
+    """Wall times of the reference's mltply calls (oracle/_ref/HPhi_ref, link-time hook) inside
+    its CalcByTEM on the same input, started from vec_c128 (HPhi layout)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import run_ref
+    if not run_ref.available():
+        return None, "oracle/_ref/HPhi_ref not built"
+    with tempfile.TemporaryDirectory() as tmp:
+        model.write(tmp)
+        os.makedirs(os.path.join(tmp, "output"))
+        with open(os.path.join(tmp, "output", "zvo_eigenvec_0_rank_0.dat"), "wb") as f:
+            f.write(np.array([0], dtype=np.int32).tobytes())
+            f.write(np.array([vec_c128.size - 1], dtype=np.int64).tobytes())
+            f.write(vec_c128.tobytes())
+        t0 = time.time()
+        run_ref.run(tmp, threads=threads, dump_call=-1, timeout=timeout, extra_env={"HPHI_DUMP_LISTS": "0"})
+        wall = time.time() - t0
+        if not os.path.exists(os.path.join(tmp, "mltply_times.txt")):
+            return None, "reference produced no timing"
+        return run_ref.read_times(tmp), f"{wall:.1f} s wall"
+
+
+def run_tem_mode(args):
+    """Real-time evolution (CalcByTEM) on the workload's sector: K timed steps of the Taylor
+    propagator (ExpandCoef 10) under a time-dependent Peierls pulse, through the C-ABI."""
+    import hphi_b200
+    expand = 10
+    W, K = max(args.warmup, 1), args.steps
+    tmp = tempfile.mkdtemp()
+    times = {}
+    e_last = None
+    for n in (W, W + K):
+        m, desc = tem_model(args.workload, n, expand)
+        d = os.path.join(tmp, f"run{n}")
+        H = hphi_b200.Hamiltonian(m.write(d))
+        dim = H.dim
+        if n == W:
+            rng = np.random.default_rng(21)
+            v = np.zeros(dim + 1, dtype=np.complex128)
+            v[1:] = rng.standard_normal(dim)
+            v[1:] /= np.linalg.norm(v[1:])
+            H.calc_by_tem(v_init=v, output_dir=os.path.join(d, "output"))    # first-call setup
+            clocks = _clock_start()
+        t0 = time.perf_counter()
+        e = H.calc_by_tem(v_init=v, output_dir=os.path.join(d, "output"))
+        times[n] = time.perf_counter() - t0
+        e_last = e
+        H.close()
+    cl = clocks.stop()
+    t_step = (times[W + K] - times[W]) / K
+    hv_bytes = 3.0 * dim * 16
+    peak, peak_src = peak_hbm()
+    achieved = expand * hv_bytes / t_step / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "peak_source": peak_src,
+            "kernel": "one time step = ExpandCoef applications of H(t) (hv_general_kernel<cplx> + te_terms_kernel) "
+                      "and the vector updates; achieved counts 3 * dim * 16 bytes per application (the complex "
+                      "H*v's algorithmic bytes), not the axpy / norm passes"}
+    norm = np.loadtxt(os.path.join(tmp, f"run{W + K}", "output", "Norm.dat"), comments="#")
+    cpu = None
+    if not args.no_cpu_baseline:
+        mref, _ = tem_model(args.workload, 2, 2)
+        threads = os.cpu_count()
+        tr, note = reference_tem_times(mref, v, threads)
+        if tr is not None:
+            tm = float(np.median(tr))
+            cpu = {"value": hv_bytes / tm / 1e9, "unit": "GB/s", "cores": threads, "kind": "reference",
+                   "sample": f"the reference's CalcByTEM, 2 steps with ExpandCoef 2 (OMP_NUM_THREADS={threads}): "
+                             f"median of its {len(tr)} mltply calls {tm:.2f} s, counted with the same 3*dim*16 "
+                             f"bytes; whole run {note}"}
+        else:
+            cpu = {"unavailable": note}
+    shutil.rmtree(tmp, ignore_errors=True)
+    out = {"metric": METRIC, "mode": "tem", "value": 1.0 / t_step, "unit": "time steps/s", "n_gpus": 1,
+           "steps": K, "warmup": W, "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+           "config": {"workload": f"{args.workload} time evolution", "desc": desc, "dim": dim,
+                      "expand_coef": expand, "timing": "host clock around calc_by_tem with W and W+K steps "
+                                                      "(difference / K; each step reads its norm to the host)",
+                      "l2": "vectors (2.65 GB each) exceed L2; no flush"},
+           "hv_equivalent_gbs": achieved, "norm_before_normalisation_max_dev": float(np.max(np.abs(norm[:, 1] - 1.0))),
+           "energy_last": float(e_last[-1]), "roofline": roof, "cpu_baseline": cpu,
+           "gpu_launches_per_step": 4 * expand + 8, "clocks": cl}
+    print(json.dumps(out))
+
+
 def serve_requests(n: int, seed: int = 50):
     from hphi_b200 import expert
     rng = np.random.default_rng(seed)
@@ -529,7 +639,7 @@ def run_serve_mode(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", default="hv", choices=["hv", "batch", "precision", "serve", "green"])
+    ap.add_argument("--mode", default="hv", choices=["hv", "batch", "precision", "serve", "green", "tem"])
     ap.add_argument("--batch-size", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=300)
     ap.add_argument("--precision-steps", type=int, default=300)
@@ -556,7 +666,7 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         {"batch": run_batch_mode, "precision": run_precision_mode, "serve": run_serve_mode,
-         "green": run_green_mode}[args.mode](args)
+         "green": run_green_mode, "tem": run_tem_mode}[args.mode](args)
         return
 
     import torch
