@@ -529,13 +529,13 @@ def run_tem_mode(args):
     norm = np.loadtxt(os.path.join(tmp, f"run{W + K}", "output", "Norm.dat"), comments="#")
     cpu = None
     if not args.no_cpu_baseline:
-        mref, _ = tem_model(args.workload, 2, 2)
+        mref, _ = tem_model(args.workload, 10, 1)    # its progress log divides by Lanczos_max / 10
         threads = os.cpu_count()
         tr, note = reference_tem_times(mref, v, threads)
         if tr is not None:
             tm = float(np.median(tr))
             cpu = {"value": hv_bytes / tm / 1e9, "unit": "GB/s", "cores": threads, "kind": "reference",
-                   "sample": f"the reference's CalcByTEM, 2 steps with ExpandCoef 2 (OMP_NUM_THREADS={threads}): "
+                   "sample": f"the reference's CalcByTEM, 10 first-order steps (OMP_NUM_THREADS={threads}): "
                              f"median of its {len(tr)} mltply calls {tm:.2f} s, counted with the same 3*dim*16 "
                              f"bytes; whole run {note}"}
         else:

@@ -18,11 +18,21 @@ namespace {
 
 constexpr int kThreads = 256;
 
-template <bool GC>
+constexpr int kSmemTermMax = 1024;  // 48 KiB of BitTerm
+
+// SMEM: the step's off-diagonal terms are staged in shared memory (every row reads all of them).
+template <bool GC, bool SMEM>
 __global__ void __launch_bounds__(kThreads) te_terms_kernel(
     int64_t dim, const uint64_t *__restrict__ list_1, const uint32_t *__restrict__ l21,
-    const uint32_t *__restrict__ l22, int lo_bits, uint64_t lo_mask, const BitTerm *__restrict__ off, int noff,
+    const uint32_t *__restrict__ l22, int lo_bits, uint64_t lo_mask, const BitTerm *__restrict__ goff, int noff,
     const DiagTerm *__restrict__ dg, int ndg, const cplx *__restrict__ v1, cplx *__restrict__ v0) {
+  extern __shared__ BitTerm sterms[];
+  const BitTerm *off = goff;
+  if (SMEM) {
+    for (int k = threadIdx.x; k < noff; k += blockDim.x) sterms[k] = goff[k];
+    __syncthreads();
+    off = sterms;
+  }
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < dim; r += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t c = GC ? (uint64_t)r : list_1[r];
     const cplx x = v1[r];
@@ -72,14 +82,20 @@ int te_terms_apply(Sector *s, const BitTerm *d_off, int noff, const DiagTerm *d_
                    void *d_v0) {
   if (noff == 0 && ndiag == 0) return 0;
   const uint64_t lo_mask = s->ihfbit - 1;
-  if (s->gc)
-    te_terms_kernel<true><<<s->red_blocks, kThreads, 0, s->stream>>>(
-        s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, d_off, noff, d_diag, ndiag,
-        (const cplx *)d_v1, (cplx *)d_v0);
-  else
-    te_terms_kernel<false><<<s->red_blocks, kThreads, 0, s->stream>>>(
-        s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, d_off, noff, d_diag, ndiag,
-        (const cplx *)d_v1, (cplx *)d_v0);
+  const bool smem = noff <= kSmemTermMax;
+  const size_t bytes = smem ? sizeof(BitTerm) * (size_t)noff : 0;
+#define HPHI_TE_LAUNCH(GC, SM)                                                                              \
+  te_terms_kernel<GC, SM><<<s->red_blocks, kThreads, bytes, s->stream>>>(                                   \
+      s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, d_off, noff, d_diag, ndiag, \
+      (const cplx *)d_v1, (cplx *)d_v0)
+  if (s->gc) {
+    if (smem) HPHI_TE_LAUNCH(true, true);
+    else HPHI_TE_LAUNCH(true, false);
+  } else {
+    if (smem) HPHI_TE_LAUNCH(false, true);
+    else HPHI_TE_LAUNCH(false, false);
+  }
+#undef HPHI_TE_LAUNCH
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_error(std::string("te_terms launch failed: ") + cudaGetErrorString(e));
