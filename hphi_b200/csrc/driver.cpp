@@ -23,7 +23,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
+#include <tuple>
 #include <sys/stat.h>
 #include <vector>
 
@@ -1033,19 +1035,65 @@ int te_run(Sector *s, const double *h_init, int step_initial, const std::string 
     return -1;
   }
   RET(cuda_ok(cudaSetDevice(s->device), "cudaSetDevice"));
-  // every time index's terms, back to back
+  // The off-diagonal terms of all time indices by their masks (the union), one split-term plan
+  // for the union, and per index its coefficient table and its generic terms (back to back);
+  // the diagonal terms of each index back to back.
+  std::vector<BitTerm> uni;
+  std::map<std::tuple<uint64_t, uint64_t, uint64_t, uint64_t>, int> where;
+  const size_t nidx = m.te_time.size();
+  std::vector<std::vector<std::pair<int, BitTerm>>> by_idx(nidx);
+  for (size_t k = 0; k < nidx; k++)
+    for (const BitTerm &t : m.te_offdiag[k]) {
+      const auto key = std::make_tuple(t.cm, t.cv, t.flip, t.sm);
+      auto it = where.find(key);
+      if (it == where.end()) {
+        it = where.emplace(key, (int)uni.size()).first;
+        uni.push_back(t);
+      }
+      by_idx[k].push_back({it->second, t});
+    }
+  SplitPlan plan;
+  struct PlanFree {
+    SplitPlan *p;
+    ~PlanFree() { split_plan_free(p); }
+  } plan_free{&plan};
+  std::vector<int> tab, gen_ids;
+  {
+    std::string err;
+    if (!uni.empty() && split_plan_for_terms(s, uni, &plan, &tab, &gen_ids, &err) != 0) {
+      set_error("time-evolution term plan: " + err);
+      return -1;
+    }
+  }
+  std::vector<int> tab_pos(uni.size(), -1), gen_pos(uni.size(), -1);
+  for (size_t i = 0; i < tab.size(); i++) tab_pos[tab[i]] = (int)i;
+  for (size_t i = 0; i < gen_ids.size(); i++) gen_pos[gen_ids[i]] = (int)i;
+  const size_t ncoef = 4 * tab.size() + 2;
+  std::vector<double> coefs(nidx * ncoef, 0.0);
   std::vector<BitTerm> off;
   std::vector<DiagTerm> dg;
   std::vector<size_t> off_at, dg_at;
-  for (size_t k = 0; k < m.te_time.size(); k++) {
+  for (size_t k = 0; k < nidx; k++) {
     off_at.push_back(off.size());
     dg_at.push_back(dg.size());
-    off.insert(off.end(), m.te_offdiag[k].begin(), m.te_offdiag[k].end());
+    for (const auto &e : by_idx[k]) {
+      if (tab_pos[e.first] >= 0) {
+        double *c = &coefs[k * ncoef + 4 * tab_pos[e.first]];
+        c[0] = e.second.re; c[1] = e.second.im; c[2] = -e.second.re; c[3] = -e.second.im;
+      } else {
+        off.push_back(e.second);
+      }
+    }
     dg.insert(dg.end(), m.te_diag[k].begin(), m.te_diag[k].end());
   }
   off_at.push_back(off.size());
   dg_at.push_back(dg.size());
-  DevBuf OFF, DG, P, HP, ACC, U, ST;
+  DevBuf OFF, DG, CO, P, HP, ACC, U, ST;
+  if (plan.lo_ptr) {
+    RET(cuda_ok(cudaMalloc(&CO.p, sizeof(double) * coefs.size()), "alloc coefficient tables"));
+    RET(cuda_ok(cudaMemcpyAsync(CO.p, coefs.data(), sizeof(double) * coefs.size(), cudaMemcpyHostToDevice,
+                                s->stream), "upload coefficient tables"));
+  }
   if (!off.empty()) {
     RET(cuda_ok(cudaMalloc(&OFF.p, sizeof(BitTerm) * off.size()), "alloc terms"));
     RET(cuda_ok(cudaMemcpyAsync(OFF.p, off.data(), sizeof(BitTerm) * off.size(), cudaMemcpyHostToDevice, s->stream),
@@ -1064,7 +1112,8 @@ int te_run(Sector *s, const double *h_init, int step_initial, const std::string 
   // y = H(step) x: the static part (general row kernel) plus the step's terms
   auto apply_h = [&](int step, const void *x, void *y) -> int {
     RET(hv_launch(s, vt, x, y, st, st + 2));
-    return te_terms_apply(s, (const BitTerm *)OFF.p + off_at[step], (int)(off_at[step + 1] - off_at[step]),
+    return te_terms_apply(s, plan, (const double *)CO.p + (plan.lo_ptr ? step * ncoef : 0),
+                          (const BitTerm *)OFF.p + off_at[step], (int)(off_at[step + 1] - off_at[step]),
                           (const DiagTerm *)DG.p + dg_at[step], (int)(dg_at[step + 1] - dg_at[step]), x, y);
   };
   RET(vec_from_host_c128(s, vt, h_init, P.p));

@@ -79,6 +79,14 @@ struct Sector {
   std::vector<uint64_t> gs_list_1, gs_list_2_1, gs_list_2_2;
 };
 
+// Builds the split-term plan of the term list T into *plan (device arrays; coefficients from
+// T).  tab_out: the tabulated terms in coefficient-table order (term tab[i] has entries 4i..4i+3:
+// re, im, -re, -im); gen_out: the terms left generic (plan->gen holds them in that order).  A
+// plan whose lo_ptr stays null tabulates nothing.  split_plan_free releases it.
+int split_plan_for_terms(Sector *s, const std::vector<BitTerm> &T, SplitPlan *plan, std::vector<int> *tab_out,
+                         std::vector<int> *gen_out, std::string *err);
+void split_plan_free(SplitPlan *p);
+
 // specialise = false skips the specialised kernel plans (the batched engine uses the
 // general row kernel only).
 int sector_build(const Model &m, int device, Sector **out, std::string *err, bool specialise = true);
@@ -147,8 +155,10 @@ int green_stage_host_vector(Sector *s, const double *h_v_1based, void **d_vec, V
 // Real-time evolution (te.cu), complex vectors in HPhi's row order:
 // v0 += (terms of one time index) v1, the terms compiled like the static ones;
 // y += (a_re + i a_im) x.
-int te_terms_apply(Sector *s, const BitTerm *d_off, int noff, const DiagTerm *d_diag, int ndiag, const void *d_v1,
-                   void *d_v0);
+// plan: split-term plan of the union of every time index's off-diagonal terms, with d_coef the
+// index's coefficient table (plan->coef is not read); d_off / noff: the index's generic terms.
+int te_terms_apply(Sector *s, const SplitPlan &plan, const double *d_coef, const BitTerm *d_off, int noff,
+                   const DiagTerm *d_diag, int ndiag, const void *d_v1, void *d_v0);
 int vec_caxpy(Sector *s, double a_re, double a_im, const void *d_x, void *d_y);
 
 // complex128 <-> real and imaginary parts (n = dim); y[0, n) += x[0, n) on stream st.

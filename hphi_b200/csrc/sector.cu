@@ -179,13 +179,17 @@ uint64_t binom_host(int n, int k) {
 
 }  // namespace
 
+static int split_plan_build(Sector *s, std::string *err) {
+  return split_plan_for_terms(s, s->model.offdiag, &s->split, nullptr, nullptr, err);
+}
+
 // Split-term plan (split.cuh): classifies the compiled terms by which half of the
 // configuration their masks touch and tabulates the lower-half and upper-half ones.
 // Skipped (every term generic) when a half has more than 18 bits or the entry fields
 // would overflow.
-static int split_plan_build(Sector *s, std::string *err) {
-  SplitPlan &P = s->split;
-  const std::vector<BitTerm> &T = s->model.offdiag;
+int split_plan_for_terms(Sector *s, const std::vector<BitTerm> &T, SplitPlan *plan, std::vector<int> *tab_out,
+                         std::vector<int> *gen_out, std::string *err) {
+  SplitPlan &P = *plan;
   const uint64_t lo_mask = s->ihfbit - 1;
   std::vector<int> lo_t, hi_t, gen_t;
   for (int q = 0; q < (int)T.size(); q++) {
@@ -204,6 +208,8 @@ static int split_plan_build(Sector *s, std::string *err) {
   }
   std::vector<BitTerm> gen;
   for (int q : gen_t) gen.push_back(T[q]);
+  if (gen_out) *gen_out = gen_t;
+  if (tab_out) tab_out->clear();
   P.ngen = (int)gen.size();
   if (P.ngen) {
     CK(cudaMalloc(&P.gen, sizeof(BitTerm) * gen.size()));
@@ -214,6 +220,7 @@ static int split_plan_build(Sector *s, std::string *err) {
   std::vector<int> tab;
   for (int q : lo_t) tab.push_back(q);
   for (int q : hi_t) tab.push_back(q);
+  if (tab_out) *tab_out = tab;
   std::vector<double> coef(4 * tab.size() + 2, 0.0);
   for (size_t i = 0; i < tab.size(); i++) {
     coef[4 * i] = T[tab[i]].re;
@@ -285,6 +292,12 @@ static int split_plan_build(Sector *s, std::string *err) {
   if (!hi_ent.empty()) CK(cudaMemcpy(P.hi_ent, hi_ent.data(), sizeof(HiEnt) * hi_ent.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(P.coef, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice));
   return 0;
+}
+
+void split_plan_free(SplitPlan *p) {
+  cudaFree(p->lo_ptr); cudaFree(p->lo_ent); cudaFree(p->hi_ptr); cudaFree(p->hi_ent);
+  cudaFree(p->coef); cudaFree(p->gen);
+  *p = SplitPlan();
 }
 
 int64_t sector_dim(const Model &m) {

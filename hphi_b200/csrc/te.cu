@@ -7,11 +7,15 @@
 // src/diagonalcalc.c:195-245, called from src/mltply.c:49).  Here the static part of H
 // runs through the general row kernel and te_terms_kernel adds the step's terms to the
 // same output rows: one thread per row in gather form, the same test / flip / two-level
-// lookup / parity sign as the static terms, so no output row is written twice.
+// lookup / parity sign as the static terms, so no output row is written twice.  The masks of
+// the time-dependent rows are fixed, their values change with the time index: the terms whose
+// masks lie in one half of the configuration go through a split-term plan (split.cuh) built
+// once for all indices, with one coefficient table per index; the others are tested per row.
 #include <cuda_runtime.h>
 
 #include "device_util.cuh"
 #include "engine.hpp"
+#include "split.cuh"
 
 namespace hphi {
 namespace {
@@ -24,8 +28,9 @@ constexpr int kSmemTermMax = 1024;  // 48 KiB of BitTerm
 template <bool GC, bool SMEM>
 __global__ void __launch_bounds__(kThreads) te_terms_kernel(
     int64_t dim, const uint64_t *__restrict__ list_1, const uint32_t *__restrict__ l21,
-    const uint32_t *__restrict__ l22, int lo_bits, uint64_t lo_mask, const BitTerm *__restrict__ goff, int noff,
-    const DiagTerm *__restrict__ dg, int ndg, const cplx *__restrict__ v1, cplx *__restrict__ v0) {
+    const uint32_t *__restrict__ l22, int lo_bits, uint64_t lo_mask, SplitView split,
+    const BitTerm *__restrict__ goff, int noff, const DiagTerm *__restrict__ dg, int ndg,
+    const cplx *__restrict__ v1, cplx *__restrict__ v0) {
   extern __shared__ BitTerm sterms[];
   const BitTerm *off = goff;
   if (SMEM) {
@@ -40,6 +45,12 @@ __global__ void __launch_bounds__(kThreads) te_terms_kernel(
     for (int k = 0; k < ndg; k++)
       if ((c & dg[k].cm) == dg[k].cv) d += dg[k].v;
     double yr = d * x.x, yi = d * x.y;
+    if (split.lo_ptr) {
+      const cplx t = split_terms<cplx, GC>(split, c, r, lo_bits, lo_mask, l22, [&](int64_t j) { return v1[j]; },
+                                           cplx{0.0, 0.0});
+      yr += t.x;
+      yi += t.y;
+    }
     for (int k = 0; k < noff; k++) {
       const BitTerm t = off[k];
       if ((c & t.cm) != t.cv) continue;
@@ -78,15 +89,17 @@ __global__ void caxpy_kernel(int64_t n, double ar, double ai, const cplx *__rest
 
 }  // namespace
 
-int te_terms_apply(Sector *s, const BitTerm *d_off, int noff, const DiagTerm *d_diag, int ndiag, const void *d_v1,
-                   void *d_v0) {
-  if (noff == 0 && ndiag == 0) return 0;
+int te_terms_apply(Sector *s, const SplitPlan &plan, const double *d_coef, const BitTerm *d_off, int noff,
+                   const DiagTerm *d_diag, int ndiag, const void *d_v1, void *d_v0) {
+  if (noff == 0 && ndiag == 0 && !plan.lo_ptr) return 0;
+  SplitView sv = split_view(plan);
+  sv.coef = d_coef;
   const uint64_t lo_mask = s->ihfbit - 1;
   const bool smem = noff <= kSmemTermMax;
   const size_t bytes = smem ? sizeof(BitTerm) * (size_t)noff : 0;
 #define HPHI_TE_LAUNCH(GC, SM)                                                                              \
   te_terms_kernel<GC, SM><<<s->red_blocks, kThreads, bytes, s->stream>>>(                                   \
-      s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, d_off, noff, d_diag, ndiag, \
+      s->dim, s->d_list_1, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask, sv, d_off, noff, d_diag, ndiag, \
       (const cplx *)d_v1, (cplx *)d_v0)
   if (s->gc) {
     if (smem) HPHI_TE_LAUNCH(true, true);
