@@ -127,3 +127,26 @@ def test_te_conserves_energy_on_the_full_size_sector():
             norm = table(open(os.path.join(tmp, "output", "Norm.dat")).read())
     assert np.all(np.abs(norm[:, 1] - 1.0) < 1e-9)
     assert np.all(np.abs(e - e[0]) < 1e-9 * abs(e[0]) + 1e-9)
+
+
+def test_te_restart_continues_from_the_stored_step(tmp_path):
+    """ReStart 3 reads the step of <SpectrumVec>_rank_0.dat and starts the loop there with no
+    previous H psi (src/CalcByTEM.c:99-102: the first step keeps the stored state), so a run
+    continued from the state OutputEigenVec wrote at step 10 repeats the reference's SS and Flct
+    rows from step 10 on."""
+    name = "te_hub_chain6_two"
+    z = load_golden(name)
+    d, out = _setup(case_dir(name), tmp_path, z["start"])
+    with hphi_b200.Hamiltonian(str(d / "namelist.def")) as H:
+        H.calc_by_tem(output_dir=str(out))
+    out2 = tmp_path / "output2"
+    os.makedirs(out2)
+    shutil.copy(out / "zvo_eigenvec_10_rank_0.dat", out2 / "zvo_eigenvec_0_rank_0.dat")
+    open(d / "calcmod.def", "a").write("ReStart 3\n")
+    with hphi_b200.Hamiltonian(str(d / "namelist.def")) as H:
+        H.calc_by_tem(output_dir=str(out2))
+    for base in ("SS", "Flct"):
+        mine = table(open(out2 / f"{base}.dat").read())
+        ref = table(z["text_" + base])
+        assert mine[0, -1] == 10 and len(mine) == len(ref) - 10
+        np.testing.assert_allclose(mine, ref[10:], rtol=0, atol=1e-10, err_msg=base)
