@@ -599,6 +599,44 @@ def _te_cases():
         steps.append((t, rows))
     m.te_twobody = steps
     cases["te_spin_chain10_two"] = (m, 13)
+    # HubbardGC chain L=4 (dim 256): Peierls-phase hoppings and a time-dependent spin-flip
+    # transfer on site 1 (grand-canonical: no sector to keep), ExpandCoef 5
+    L = 4
+    m = expert.ExpertModel(model="HubbardGC", nsite=L, two_sz=None, calc_type="TimeEvolution", lanczos_max=20,
+                           input_eigenvec=1, spectrum_vec="zvo_eigenvec_0", expand_coef=5, expec_interval=10)
+    m.coulombintra = [(i, 3.0) for i in range(L)]
+    m.greenone = [(i, s, i, s) for i in range(L) for s in (0, 1)] + [(1, 0, 1, 1), (1, 1, 1, 0)]
+    steps = []
+    for t in _te_times(20, 0.05):
+        a, h = 0.6 * math.sin(2.0 * t), 0.3 * math.cos(t)
+        rows = []
+        for x in range(L):
+            f = (x + 1) % L
+            for sg in (0, 1):
+                rows.append((x, sg, f, sg, math.cos(a), math.sin(a)))
+                rows.append((f, sg, x, sg, math.cos(a), -math.sin(a)))
+        rows += [(1, 0, 1, 1, h, 0.1 * t), (1, 1, 1, 0, h, -0.1 * t)]
+        steps.append((t, rows))
+    m.te_onebody = steps
+    cases["te_hubgc_chain4_one"] = (m, 14)
+    # Kondo chain of 3 cells (conduction sites 0, 2, 4; local spins 1, 3, 5; 3 electrons):
+    # the local-conduction exchange of every cell modulated in time through TETwoBody, plus a
+    # time-dependent density-density row on the conduction sites; ExpandCoef 3
+    m = expert.kondo_chain(3, 1.0, 2.0, U=1.0, calc_type="TimeEvolution", lanczos_max=20, input_eigenvec=1,
+                           spectrum_vec="zvo_eigenvec_0", expand_coef=3, expec_interval=10)
+    m.greenone = [(i, s, i, s) for i in range(6) for s in (0, 1)] + [(0, 0, 2, 0), (2, 0, 0, 0)]
+    steps = []
+    for t in _te_times(20, 0.05):
+        jt = 0.5 + 0.4 * math.sin(3.0 * t)
+        rows = []
+        for c in range(3):
+            l, e = 2 * c + 1, 2 * c
+            rows.append((l, 0, l, 1, e, 1, e, 0, jt, 0.0))
+            rows.append((l, 1, l, 0, e, 0, e, 1, jt, 0.0))
+        rows.append((0, 0, 0, 0, 2, 1, 2, 1, 0.2 * t, 0.0))
+        steps.append((t, rows))
+    m.te_twobody = steps
+    cases["te_kondo_chain3_two"] = (m, 15)
     return cases
 
 
@@ -608,7 +646,7 @@ def make_te_case(name: str, m, seed: int) -> None:
     shutil.rmtree(out, ignore_errors=True)
     m.write(out)
     d = O.read_expert(os.path.join(out, "namelist.def"))
-    dim = len(O.sz(d)[0]) - 1
+    dim = (1 << O.nbits(d)) if O._rows_are_configs(d) else len(O.sz(d)[0]) - 1
     rng = np.random.default_rng(seed)
     v = np.zeros(dim + 1, dtype=np.complex128)
     v[1:] = rng.standard_normal(dim) + 1j * rng.standard_normal(dim)

@@ -45,7 +45,7 @@ def test_oracle_te_known_answers(name):
 def test_oracle_te_matches_reference(name):
     z = load_golden(name)
     d = O.read_expert(os.path.join(case_dir(name), "namelist.def"))
-    lists = O.sz(d)
+    lists = None if O._rows_are_configs(d) else O.sz(d)
     green_steps = [s for s in range(d.lanczos_max) if d.green_one and s % d.expec_interval == 0]
     rows, states = O.te_run(d, lists, z["start"], keep_states=green_steps)
     r = np.array(rows)
