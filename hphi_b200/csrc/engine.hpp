@@ -108,10 +108,10 @@ int hv_native(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double 
 int to_native(Sector *s, VecType vt, const void *d_hphi, void *d_native);
 int from_native(Sector *s, VecType vt, const void *d_native, void *d_hphi);
 // hv_native with caller-provided scratch: d_part receives the per-block partial sums
-// (hv_scratch_doubles(s) doubles), d_counter the block counters (2 ints, zeroed on the stream).
+// (hv_scratch_doubles(s, vt) doubles), d_counter the block counters (2 ints, zeroed on the stream).
 int hv_native_scratch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out,
                       double *d_part, int *d_counter);
-size_t hv_scratch_doubles(const Sector *s);
+size_t hv_scratch_doubles(const Sector *s, VecType vt);
 
 // Diagonal observables of a native-order vector (as vec_diag_observables).
 int native_observables(Sector *s, VecType vt, const void *d_v, double *d_out);

@@ -153,8 +153,8 @@ int hv_launch_scratch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const
   return 0;
 }
 
-size_t hv_scratch_doubles(const Sector *s) {
-  if (s->prod) return prod_scratch_doubles(s);
+size_t hv_scratch_doubles(const Sector *s, VecType vt) {
+  if (s->prod) return prod_scratch_doubles(s, vt);
   if (s->hub) return hub_scratch_doubles(s);
   return 2 * (size_t)s->red_blocks;
 }

@@ -941,9 +941,12 @@ int prod_plan_build(Sector *s, std::string *err) {
 
 bool prod_two_pass(const Sector *s) { return s->prod && s->prod->two_pass; }
 
-size_t prod_scratch_doubles(const Sector *s) {
+size_t prod_scratch_doubles(const Sector *s, VecType vt) {
   const ProdPlan *p = s->prod;
-  return 2 * std::max((size_t)p->args.Uc, (size_t)(p->grid_dn + p->grid_up));
+  // the two-pass kernels (real vectors) keep one partial sum per CTA of each pass; the
+  // one-pass kernel one per row
+  if (vt == kReal64 && p->two_pass) return 2 * (size_t)(p->grid_dn + p->grid_up);
+  return 2 * (size_t)p->args.Uc;
 }
 
 namespace {

@@ -12,9 +12,13 @@
 // The array has a fixed size (kScratchDoubles doubles = 128 KiB) and exists on every
 // GPU that loads this library, until the process exits.  Calls share it: two calls whose
 // work overlaps on the GPU (different streams, different threads, or different handles on
-// the same device) race on it, so callers must order them.  The first call on a device
-// looks up the array's device address (cudaGetSymbolAddress, which may load the module);
-// make that first call before any stream capture.
+// the same device) race on it, so callers must order them.  Each call waits for its
+// stream before it returns (it reads <v1|H|v1> back to the host).  The first call on a
+// device looks up the array's device address (cudaGetSymbolAddress, which may load the
+// module); make that first call before any stream capture.  The partial sums it needs are
+// 2 per CTA of the two passes for real vectors on the product-layout Hubbard kernels
+// (a few thousand), 2 per row of the up-spin matrix for its complex one-pass kernel, 2 per
+// block otherwise; a sector that needs more than the array holds is refused.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -81,7 +85,7 @@ extern "C" int hphi_mltply_device_noalloc(hphi_handle *h, int vec_type, void *d_
     set_error("hphi_mltply_device_noalloc: cudaSetDevice failed");
     return -1;
   }
-  const size_t need = hv_scratch_doubles(s);
+  const size_t need = hv_scratch_doubles(s, (VecType)vec_type);
   if (need > kScratchDoubles - kPartialSlot) {
     set_error("hphi_mltply_device_noalloc: this sector needs " + std::to_string(need) +
               " partial sums, more than the fixed scratch of " + std::to_string(kScratchDoubles - kPartialSlot));

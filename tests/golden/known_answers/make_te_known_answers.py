@@ -13,7 +13,8 @@ are stored here in te_expected.json.  The start state is the chain's ground stat
 tests compute from the written input (it is non-degenerate).
 
 Run:  python tests/golden/known_answers/make_te_known_answers.py   (reads the reference's
-test scripts from /root/reference/test and writes the inputs and te_expected.json here)
+test scripts from $HPHI_REFERENCE/test, by default the checkout beside this repository, and
+writes the inputs and te_expected.json here)
 """
 import json
 import os
@@ -23,7 +24,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(HERE))))
 from hphi_b200 import expert  # noqa: E402
 
-REF_TEST = "/root/reference/test"
+REPO = os.path.dirname(os.path.dirname(os.path.dirname(HERE)))
+REF_TEST = os.path.join(os.environ.get("HPHI_REFERENCE", os.path.join(os.path.dirname(REPO), "reference")), "test")
 CASES = {"te_hubbard_chain_interall": "Normal", "te_hubbard_chain_interall_diagonal": "Diagonal"}
 
 
