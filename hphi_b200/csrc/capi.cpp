@@ -482,7 +482,16 @@ int hphi_lanczos(hphi_handle *h, const double *v_init, const char *output_dir, d
     for (int q = 0; q < 4 && q < (int)r.energies.size(); q++) v[3 + q] = r.energies[q];
     for (int i = 0; i < nresult && i < 17; i++) result[i] = v[i];
   }
-  if (rc != 0) return -1;
+  if (rc != 0) {
+    // HPhi writes its step lines while it iterates, so a run that stops unconverged leaves
+    // them behind (src/Lanczos_EigenValue.c:200-258, then exitMPI(-3) in src/HPhiMain.c:294-297)
+    if (output_dir && !r.converged && !r.lines.empty()) {
+      const std::string msg = hphi_last_error();
+      write_lanczos_outputs(*s, r, output_dir);
+      set_error(msg);
+    }
+    return -1;
+  }
   if (output_dir && write_lanczos_outputs(*s, r, output_dir) != 0) return -1;
   return 0;
 }

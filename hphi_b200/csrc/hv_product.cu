@@ -51,6 +51,7 @@
 #include "device_util.cuh"
 #include "engine.hpp"
 #include "hv_product.hpp"
+#include "tma.cuh"
 
 namespace hphi {
 namespace {
@@ -62,7 +63,8 @@ constexpr uint32_t kEllNone = 0xFFFFFFFFu;
 struct ProdArgs {
   int N, Uc, Dc;               // sites, rows (up configurations), columns (down configurations)
   int wd, wu;                  // ELL widths
-  const uint16_t *rank;        // [2^N]
+  const uint16_t *rank;        // [2^N] position of an up configuration (its rank)
+  const uint16_t *pos_dn;      // [2^N] position of a down configuration
   const uint16_t *unrank_up;   // [Uc]
   const uint16_t *unrank_dn;   // [Dc]
   const uint32_t *ell_dn;      // [wd][Dc]: source rank | coefficient index << 16
@@ -245,68 +247,79 @@ __device__ __forceinline__ double flip_sign(double x, uint32_t sg) {
 }
 
 // Row pass: v0[u, :] = acc * v0[u, :] + scale * (D + down hops) v1[u, :] for two rows at a time;
-// part[blockIdx] = sum over the CTA's rows of v1 . (D + down) v1.
+// part[blockIdx] = sum over the CTA's rows of v1 . (D + down) v1.  The two rows are staged
+// by bulk asynchronous copies completing on an mbarrier (per-thread cp.async when the rows
+// are not 16-byte aligned); a bounded wait that gives up makes the CTA's partial sum NaN.
+// Gathers: each 16-bit table entry (word | sign << 15) serves both rows.
 __global__ void __launch_bounds__(kDownThreads, 1) prod_down_kernel(ProdArgs a, TwoPassArgs b,
                                                                    const double *__restrict__ v1,
                                                                    double *__restrict__ v0,
                                                                    const double *__restrict__ coef,
                                                                    double *__restrict__ part) {
-  extern __shared__ double rows[];  // row 0 at 0, row 1 at kRow2Bytes; each Dc + 16 words
+  extern __shared__ __align__(128) double rows[];  // row 0 at 0, row 1 at kRow2Bytes; each Dc + 16 words
+  __shared__ uint64_t bar;
   double *row1 = rows + kRow2Bytes / 8;
   const double acc = coef[0], scale = coef[1];
   const int Dc = a.Dc, Uc = a.Uc;
-  const char *rb = reinterpret_cast<const char *>(rows);
+  const int tid = threadIdx.x;
   double pr = 0.0;
-  // rows are copied with cp.async: 16-byte pieces when the rows start on 16-byte boundaries
-  const bool v16 = (Dc % 2 == 0) && ((uintptr_t)v1 % 16 == 0);
-  const uint32_t sm0 = (uint32_t)__cvta_generic_to_shared(rows), sm1 = sm0 + kRow2Bytes;
+  // rows arrive by bulk copies when they start on 16-byte boundaries and are whole 16-byte units
+  const bool bulk = (Dc % 2 == 0) && ((uintptr_t)v1 % 16 == 0);
+  const uint32_t sm0 = smem_u32(rows), sm1 = sm0 + kRow2Bytes;
+  if (tid == 0) mbar_init(&bar, 1);
+  mbar_fence_init();
+  if (tid < 16) {  // zero words after each row (one per bank pair), never overwritten by the copies
+    rows[Dc + tid] = 0.0;
+    row1[Dc + tid] = 0.0;
+  }
+  uint32_t phase = 0;
+  bool ok = true;
   for (int u0 = 2 * blockIdx.x; u0 < Uc; u0 += 2 * gridDim.x) {
     const bool two = u0 + 1 < Uc;
     __syncthreads();  // the previous rows are no longer read
     const double *s0 = v1 + (int64_t)u0 * Dc;
     const double *s1 = two ? s0 + Dc : s0;
-    if (v16) {
-      for (int i = threadIdx.x; i < Dc / 2; i += kDownThreads) {
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sm0 + 16 * i), "l"(s0 + 2 * i) : "memory");
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sm1 + 16 * i), "l"(s1 + 2 * i) : "memory");
+    if (bulk) {
+      if (tid == 0) {
+        mbar_arrive_expect_tx(&bar, (uint32_t)(2 * Dc * 8));
+        bulk_g2s(rows, s0, (uint32_t)(Dc * 8), &bar);
+        bulk_g2s(row1, s1, (uint32_t)(Dc * 8), &bar);
       }
     } else {
-      for (int i = threadIdx.x; i < Dc; i += kDownThreads) {
+      for (int i = tid; i < Dc; i += kDownThreads) {
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sm0 + 8 * i), "l"(s0 + i) : "memory");
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sm1 + 8 * i), "l"(s1 + i) : "memory");
       }
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    if (threadIdx.x < 16) {
-      rows[Dc + threadIdx.x] = 0.0;
-      row1[Dc + threadIdx.x] = 0.0;
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
     // the next pair's rows toward L2 while this pair is processed (a hint, no completion)
     const int un = u0 + 2 * gridDim.x;
-    if (v16 && threadIdx.x < 2 && un + (int)threadIdx.x < Uc) {
-      const double *pf = v1 + (int64_t)(un + threadIdx.x) * Dc;
+    if (bulk && tid < 2 && un + tid < Uc) {
+      const double *pf = v1 + (int64_t)(un + tid) * Dc;
       asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(pf), "r"((uint32_t)(Dc * 8)) : "memory");
     }
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-    __syncthreads();
+    if (bulk) {
+      const bool got = mbar_wait(&bar, phase);
+      phase ^= 1;
+      if (__syncthreads_or(!got)) {
+        ok = false;
+        mbar_wait(&bar, phase ^ 1);  // copies still in flight land before the CTA leaves (bounded)
+        break;
+      }
+    } else {
+      asm volatile("cp.async.wait_all;\n" ::: "memory");
+      __syncthreads();
+    }
     const int ua1 = two ? u0 + 1 : u0;
     const uint32_t uc0 = a.unrank_up[u0], uc1 = a.unrank_up[ua1];
     const double du0 = a.du[u0], du1 = a.du[ua1];
-    const int lane = threadIdx.x & 31;
-    // entries of the first four slot groups of the next column block, loaded one block ahead
-    uint4 q[4];
-    auto load_block = [&](int pp, uint4 (&dst)[4]) {
-      const int w = pp >> 5, ng = (b.wslots[w] + 7) >> 3;
-      const uint4 *base = b.gat + ((int64_t)w * b.groups) * 32 + lane;
-#pragma unroll
-      for (int g = 0; g < 4; g++) dst[g] = (g < ng) ? __ldg(base + g * 32) : make_uint4(0, 0, 0, 0);
-    };
-    if ((int)threadIdx.x < b.npad) load_block(threadIdx.x, q);
-    for (int p = threadIdx.x; p < b.npad; p += kDownThreads) {
+    const int lane = tid & 31;
+    const double tdn = b.t_dn;
+    const char *rb = reinterpret_cast<const char *>(rows);
+    for (int p = tid; p < b.npad; p += kDownThreads) {
       const int w = p >> 5, ns = b.wslots[w];  // the same for the warp's 32 columns
-      uint4 cur[4] = {q[0], q[1], q[2], q[3]};
-      if (p + kDownThreads < b.npad) load_block(p + kDownThreads, q);
-      // per-column diagonal parts, loaded before the gathers
+      const uint4 *gp = b.gat + ((int64_t)w * b.groups) * 32 + lane;
+      // per-column diagonal parts and the old v0, loaded before the gathers
       const int pc = (p < Dc) ? p : Dc - 1;
       const double ddp = (a.cross_mode == 2) ? 0.0 : __ldg(a.dd + pc);
       const uint32_t cdp = __ldg(a.unrank_dn + pc);
@@ -314,32 +327,25 @@ __global__ void __launch_bounds__(kDownThreads, 1) prod_down_kernel(ProdArgs a, 
       const double y0old = (acc != 0.0) ? __ldcs(o0) : 0.0;
       const double y1old = (acc != 0.0 && two) ? __ldcs(o0 + Dc) : 0.0;
       double g0 = 0.0, g1 = 0.0;
-      auto gather2 = [&](uint32_t r, int slot) {
-        // two 16-bit entries: word index (15 bits) | sign << 15; every slot at or beyond the
-        // warp's count holds a zero word, so only whole words are skipped
-        if (slot < ns) {
-          const uint32_t o0 = (r << 3) & 0x3FFF8u, s0 = (r << 16) & 0x80000000u;
-          const uint32_t o1 = (r >> 13) & 0x3FFF8u, s1 = r & 0x80000000u;
-          g0 += flip_sign(*reinterpret_cast<const double *>(rb + o0), s0);
-          g1 += flip_sign(*reinterpret_cast<const double *>(rb + kRow2Bytes + o0), s0);
-          g0 += flip_sign(*reinterpret_cast<const double *>(rb + o1), s1);
-          g1 += flip_sign(*reinterpret_cast<const double *>(rb + kRow2Bytes + o1), s1);
-        }
+      // two 16-bit entries: word index (15 bits) | sign << 15; the sign is applied by flipping
+      // the sign bit of the gathered value; every slot at or beyond the warp's count holds a
+      // zero word, so only whole entry pairs are skipped
+      auto gather2 = [&](uint32_t r) {
+        const uint32_t o0 = (r << 3) & 0x3FFF8u, o1 = (r >> 13) & 0x3FFF8u;
+        const uint32_t s0 = r << 16;  // sign of the low entry at bit 31 (the high entry's is there already)
+        const double *x0 = reinterpret_cast<const double *>(rb + o0);
+        const double *x1 = reinterpret_cast<const double *>(rb + o1);
+        g0 += flip_sign(x0[0], s0 & 0x80000000u);
+        g1 += flip_sign(x0[kRow2Bytes / 8], s0 & 0x80000000u);
+        g0 += flip_sign(x1[0], r & 0x80000000u);
+        g1 += flip_sign(x1[kRow2Bytes / 8], r & 0x80000000u);
       };
-#pragma unroll
-      for (int g = 0; g < 4; g++) {
-        if (8 * g >= ns) break;
-        gather2(cur[g].x, 8 * g);
-        gather2(cur[g].y, 8 * g + 2);
-        gather2(cur[g].z, 8 * g + 4);
-        gather2(cur[g].w, 8 * g + 6);
-      }
-      for (int g = 4; 8 * g < ns; g++) {  // more than 32 slots: remaining groups loaded here
-        const uint4 e = __ldg(b.gat + ((int64_t)w * b.groups + g) * 32 + lane);
-        gather2(e.x, 8 * g);
-        gather2(e.y, 8 * g + 2);
-        gather2(e.z, 8 * g + 4);
-        gather2(e.w, 8 * g + 6);
+      for (int g = 0; 8 * g < ns; g++) {
+        const uint4 e = __ldg(gp + g * 32);
+        gather2(e.x);
+        if (8 * g + 2 < ns) gather2(e.y);
+        if (8 * g + 4 < ns) gather2(e.z);
+        if (8 * g + 6 < ns) gather2(e.w);
       }
       if (p < Dc) {
         auto diag = [&](int ua, uint32_t uc, double du) -> double {
@@ -350,20 +356,20 @@ __global__ void __launch_bounds__(kDownThreads, 1) prod_down_kernel(ProdArgs a, 
           else for (uint32_t m = ud; m; m &= m - 1) D += __ldg(a.usite + (__ffs(m) - 1));
           return D;
         };
-        const double x0 = rows[p], y0 = diag(u0, uc0, du0) * x0 + b.t_dn * g0;
+        const double x0 = rows[p], y0 = diag(u0, uc0, du0) * x0 + tdn * g0;
         __stcs(o0, (acc == 0.0) ? scale * y0 : acc * y0old + scale * y0);
         pr += x0 * y0;
         if (two) {
-          const double x1 = row1[p], y1 = diag(ua1, uc1, du1) * x1 + b.t_dn * g1;
+          const double x1 = row1[p], y1 = diag(ua1, uc1, du1) * x1 + tdn * g1;
           __stcs(o0 + Dc, (acc == 0.0) ? scale * y1 : acc * y1old + scale * y1);
           pr += x1 * y1;
         }
       }
     }
   }
-  double v[2] = {pr, 0.0};
+  double v[2] = {ok ? pr : __longlong_as_double(0x7FF8000000000000ll), 0.0};
   block_sum<2>(v);
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     part[2 * blockIdx.x] = v[0];
     part[2 * blockIdx.x + 1] = 0.0;
   }
@@ -487,10 +493,11 @@ __device__ __forceinline__ int species_parity(uint64_t c, int N) {
 // without it the values are moved as they are (functions of the configuration).
 template <typename T, bool TO_NATIVE, bool SIGN>
 __global__ void prod_permute_kernel(int64_t dim, int N, int Dc, const uint64_t *__restrict__ list_1,
-                                    const uint16_t *__restrict__ rank, const T *__restrict__ in, T *__restrict__ out) {
+                                    const uint16_t *__restrict__ rank, const uint16_t *__restrict__ pos_dn,
+                                    const T *__restrict__ in, T *__restrict__ out) {
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < dim; r += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t c = list_1[r];
-    const int64_t pos = (int64_t)rank[compress_species(c, 0, N)] * Dc + rank[compress_species(c, 1, N)];
+    const int64_t pos = (int64_t)rank[compress_species(c, 0, N)] * Dc + pos_dn[compress_species(c, 1, N)];
     const double sg = (SIGN && species_parity(c, N)) ? -1.0 : 1.0;
     if (TO_NATIVE) out[pos] = VT<T>::scale(sg, in[r]);
     else out[r] = VT<T>::scale(sg, in[pos]);
@@ -710,6 +717,95 @@ void build_gather(const std::vector<std::vector<uint32_t>> &rows_dn, const std::
   }
 }
 
+
+// Positions of the down configurations for the row pass.  The row pass gives column p to
+// lane p % 32 of warp p / 32, and an 8-byte gather of source column q hits the shared-memory
+// bank pair q % 16; a half-warp's slot count is max(largest lane degree, largest bank-pair
+// load) (the edge colouring of build_gather), so positions decide both.  Start from the
+// configurations sorted by hop count (equal lane degrees in a half-warp), then swap positions
+// (within a half-warp: a bank change; across half-warps: only between equal hop counts) when
+// that does not raise the summed slot counts of the half-warps it touches.  rows[r]: sources
+// of configuration r (ELL entries, source in the low 16 bits).  Returns the position of each
+// configuration; deterministic (fixed seed).
+std::vector<int> balance_positions(const std::vector<std::vector<uint32_t>> &rows) {
+  const int n = (int)rows.size();
+  constexpr int G = 16;
+  std::vector<int> order(n), pos(n);
+  for (int r = 0; r < n; r++) order[r] = r;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rows[a].size() > rows[b].size(); });
+  for (int p = 0; p < n; p++) pos[order[p]] = p;
+  const int ng = (n + G - 1) / G;
+  if (n < 4 * G) return pos;
+  std::vector<std::vector<int>> src(n), rdr(n);
+  for (int r = 0; r < n; r++)
+    for (uint32_t e : rows[r]) {
+      const int q = (int)(e & 0xFFFFu);
+      src[r].push_back(q);
+      rdr[q].push_back(r);
+    }
+  std::vector<int> at(order);  // configuration at each position
+  std::vector<int> load((size_t)ng * G, 0), lmax(ng, 0), D(ng, 0);
+  for (int r = 0; r < n; r++) {
+    const int g = pos[r] / G;
+    lmax[g] = std::max(lmax[g], (int)src[r].size());
+    for (int q : src[r]) load[(size_t)g * G + pos[q] % G]++;
+  }
+  auto eval = [&](int g) {
+    int m = lmax[g];
+    for (int k = 0; k < G; k++) m = std::max(m, load[(size_t)g * G + k]);
+    return m;
+  };
+  for (int g = 0; g < ng; g++) D[g] = eval(g);
+  uint64_t rng = 0x9E3779B97F4A7C15ull;
+  auto next = [&]() { rng ^= rng << 13; rng ^= rng >> 7; rng ^= rng << 17; return rng; };
+  std::vector<int> touched;
+  std::vector<char> mark(ng, 0);
+  auto touch = [&](int g) { if (!mark[g]) { mark[g] = 1; touched.push_back(g); } };
+  // adds (sgn = 1) or removes (-1) a configuration's edges: its reads (in its own half-warp)
+  // and the reads of it; edges to `other` are left to the other configuration's call
+  auto contrib = [&](int r, int p, int sgn, int other) {
+    const int g = p / G, bk = p % G;
+    for (int q : src[r])
+      if (q != other) load[(size_t)g * G + pos[q] % G] += sgn;
+    for (int rr : rdr[r])
+      if (rr != other) { const int gg = pos[rr] / G; load[(size_t)gg * G + bk] += sgn; touch(gg); }
+    touch(g);
+  };
+  const int64_t iters = std::min<int64_t>(200 * (int64_t)n, 4000000);
+  for (int64_t it = 0; it < iters; it++) {
+    const int p1 = (int)(next() % n);
+    int p2;
+    if (next() & 1) p2 = (p1 / G) * G + (int)(next() % G);
+    else p2 = (int)(next() % n);
+    if (p2 >= n || p2 == p1 || src[at[p1]].size() != src[at[p2]].size()) continue;
+    const int a = at[p1], b = at[p2];
+    touched.clear();
+    contrib(a, p1, -1, -1);
+    contrib(b, p2, -1, a);
+    pos[a] = p2; pos[b] = p1; at[p1] = b; at[p2] = a;
+    contrib(a, p2, +1, -1);
+    contrib(b, p1, +1, a);
+    long before = 0, after = 0;
+    std::vector<int> nd(touched.size());
+    for (size_t i = 0; i < touched.size(); i++) {
+      before += D[touched[i]];
+      nd[i] = eval(touched[i]);
+      after += nd[i];
+    }
+    if (after <= before) {
+      for (size_t i = 0; i < touched.size(); i++) D[touched[i]] = nd[i];
+    } else {
+      contrib(a, p2, -1, -1);
+      contrib(b, p1, -1, a);
+      pos[a] = p1; pos[b] = p2; at[p1] = a; at[p2] = b;
+      contrib(a, p1, +1, -1);
+      contrib(b, p2, +1, a);
+    }
+    for (int g : touched) mark[g] = 0;
+  }
+  return pos;
+}
+
 }  // namespace
 
 int prod_plan_build(Sector *s, std::string *err) {
@@ -747,6 +843,33 @@ int prod_plan_build(Sector *s, std::string *err) {
   int wd = 0, wu = 0;
   build_ell(hops[1], unrank_dn, rank, &rows_dn, &wd);
   build_ell(hops[0], unrank_up, rank, &rows_up, &wu);
+  // Two-pass kernels (real vectors): every down hop of one magnitude, real up hops, the
+  // second staged row at its fixed offset.  HPHI_B200_PROD=single keeps the one-pass kernel.
+  bool two_pass_ok;
+  double tmag;
+  {
+    const char *pe = getenv("HPHI_B200_PROD");
+    two_pass_ok = !(pe && std::string(pe) == "single") && !hops[1].empty() &&
+                  (size_t)(Dc + 16) * 8 <= (size_t)kRow2Bytes && wd <= 255;
+    tmag = hops[1].empty() ? 0.0 : std::fabs(hops[1][0].re);
+    for (const SpeciesHop &h : hops[1]) two_pass_ok = two_pass_ok && h.im == 0.0 && std::fabs(h.re) == tmag && tmag > 0.0;
+    for (const SpeciesHop &h : hops[0]) two_pass_ok = two_pass_ok && h.im == 0.0;
+  }
+  // Down configurations take the positions balanced for the row pass's gather table
+  // (balance_positions); HPHI_B200_BALANCE=0 keeps rank order.  Up configurations keep
+  // their rank.
+  std::vector<uint16_t> pos_dn(rank);
+  {
+    const char *bal = getenv("HPHI_B200_BALANCE");
+    if (two_pass_ok && !(bal && std::string(bal) == "0")) {
+      const std::vector<int> pos = balance_positions(rows_dn);
+      std::vector<uint16_t> un(Dc);
+      for (int r = 0; r < Dc; r++) un[pos[r]] = unrank_dn[r];
+      unrank_dn.swap(un);
+      for (int p = 0; p < Dc; p++) pos_dn[unrank_dn[p]] = (uint16_t)p;
+      build_ell(hops[1], unrank_dn, pos_dn, &rows_dn, &wd);
+    }
+  }
   if (wu > kMaxUpWidth || wd > 255) return 0;
   std::vector<uint32_t> ell_dn((size_t)std::max(wd, 1) * Dc, kEllNone), ell_up((size_t)Uc * std::max(wu, 1), kEllNone);
   std::vector<uint8_t> cnt_dn(Dc), wmax_dn((Dc + 31) / 32, 0);
@@ -828,7 +951,7 @@ int prod_plan_build(Sector *s, std::string *err) {
   std::vector<double> utab(17);
   for (int k = 0; k <= 16; k++) utab[k] = a.u0 * (double)k;
   auto fail = [&]() { prod_plan_free(p); return -1; };
-  if (upload(p, rank, &a.rank, err) || upload(p, unrank_up, &a.unrank_up, err) ||
+  if (upload(p, rank, &a.rank, err) || upload(p, pos_dn, &a.pos_dn, err) || upload(p, unrank_up, &a.unrank_up, err) ||
       upload(p, unrank_dn, &a.unrank_dn, err) || upload(p, ell_dn, &a.ell_dn, err) ||
       upload(p, ell_up, &a.ell_up, err) || upload(p, coef_table(hops[1]), &a.cf_dn, err) ||
       upload(p, coef_table(hops[0]), &a.cf_up, err) || upload(p, du, &a.du, err) || upload(p, dd, &a.dd, err) ||
@@ -843,7 +966,7 @@ int prod_plan_build(Sector *s, std::string *err) {
     }
     p->allocs.push_back(q);
     const unsigned nb = (unsigned)std::min<int64_t>((s->dim + 255) / 256, (int64_t)s->num_sms * 16);
-    prod_permute_kernel<double, true, false><<<nb, 256, 0, s->stream>>>(s->dim, N, Dc, s->d_list_1, a.rank,
+    prod_permute_kernel<double, true, false><<<nb, 256, 0, s->stream>>>(s->dim, N, Dc, s->d_list_1, a.rank, a.pos_dn,
                                                                         s->d_diag, (double *)q);
     if (cudaStreamSynchronize(s->stream) != cudaSuccess) {
       *err = "product plan: diagonal permutation failed";
@@ -874,16 +997,8 @@ int prod_plan_build(Sector *s, std::string *err) {
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, prod_hv_kernel<double>, kProdThreads, smem_r);
   p->grid = std::max(1, std::min(Uc, std::max(1, per_sm) * s->num_sms));
-  // Two-pass kernels (real vectors): every down hop of one magnitude, real up hops, the
-  // second staged row at its fixed offset.  HPHI_B200_PROD=single keeps the one-pass kernel.
   {
-    const char *pe = getenv("HPHI_B200_PROD");
-    bool ok = !(pe && std::string(pe) == "single") && !hops[1].empty() && (size_t)(Dc + 16) * 8 <= (size_t)kRow2Bytes &&
-              wd <= 255;
-    const double tmag = hops[1].empty() ? 0.0 : std::fabs(hops[1][0].re);
-    for (const SpeciesHop &h : hops[1]) ok = ok && h.im == 0.0 && std::fabs(h.re) == tmag && tmag > 0.0;
-    for (const SpeciesHop &h : hops[0]) ok = ok && h.im == 0.0;
-    if (ok) {
+    if (two_pass_ok) {
       TwoPassArgs &b = p->tp;
       b.npad = (Dc + 31) / 32 * 32;
       b.t_dn = tmag;
@@ -1020,17 +1135,17 @@ int prod_permute(Sector *s, VecType vt, const void *in, void *out, bool to_nativ
   const int N = p->args.N, Dc = p->args.Dc;
   if (vt == kReal64) {
     if (to_native)
-      prod_permute_kernel<double, true, true><<<nb, 256, 0, s->stream>>>(s->dim, N, Dc, s->d_list_1, p->args.rank,
+      prod_permute_kernel<double, true, true><<<nb, 256, 0, s->stream>>>(s->dim, N, Dc, s->d_list_1, p->args.rank, p->args.pos_dn,
                                                                          (const double *)in, (double *)out);
     else
-      prod_permute_kernel<double, false, true><<<nb, 256, 0, s->stream>>>(s->dim, N, Dc, s->d_list_1, p->args.rank,
+      prod_permute_kernel<double, false, true><<<nb, 256, 0, s->stream>>>(s->dim, N, Dc, s->d_list_1, p->args.rank, p->args.pos_dn,
                                                                           (const double *)in, (double *)out);
   } else {
     if (to_native)
-      prod_permute_kernel<cplx, true, true><<<nb, 256, 0, s->stream>>>(s->dim, N, Dc, s->d_list_1, p->args.rank,
+      prod_permute_kernel<cplx, true, true><<<nb, 256, 0, s->stream>>>(s->dim, N, Dc, s->d_list_1, p->args.rank, p->args.pos_dn,
                                                                        (const cplx *)in, (cplx *)out);
     else
-      prod_permute_kernel<cplx, false, true><<<nb, 256, 0, s->stream>>>(s->dim, N, Dc, s->d_list_1, p->args.rank,
+      prod_permute_kernel<cplx, false, true><<<nb, 256, 0, s->stream>>>(s->dim, N, Dc, s->d_list_1, p->args.rank, p->args.pos_dn,
                                                                         (const cplx *)in, (cplx *)out);
   }
   return cuda_ok(cudaGetLastError(), "permute");

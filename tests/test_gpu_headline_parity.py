@@ -44,8 +44,9 @@ def _step_lines(path):
         for line in f:
             if not line.startswith("stp"):
                 continue
-            tok = line.replace("stp =", "stp=").split()
-            out.append((int(tok[0][4:]), [None if "x" in t else float(t) for t in tok[1:]]))
+            head, rest = line.split("=", 1)
+            tok = rest.split()
+            out.append((int(tok[0]), [None if "x" in t else float(t) for t in tok[1:]]))
     return out
 
 
