@@ -32,6 +32,10 @@ metric (solves/s and latency against the plain FP64 GPU path):
              Peierls pulse, ExpandCoef 10: time steps per second through the C-ABI, the
              reference's mltply inside its own CalcByTEM as the CPU baseline.
 
+The default line also carries "modes": bounded runs of batch (64 of the 256 chains), serve
+(40 requests) and precision (the full 4x8 sector), each in its own process after the timed
+H*v (--no-modes skips them).
+
 Multi-GPU (--gpus N under torchrun): the path does not shard for this workload, so
 N independent replicas run (one per GPU); value = total bytes / max-over-ranks time.
 """
@@ -654,6 +658,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3, help="0 skips the end-to-end leg")
     ap.add_argument("--no-hphi-order", action="store_true", help="skip the HPhi-order device leg")
+    ap.add_argument("--no-modes", action="store_true",
+                    help="skip the bounded batch / serve / precision runs reported under 'modes'")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -757,6 +763,49 @@ def main():
            world, rank, dist)
 
 
+def _mode_line(argv, timeout):
+    """Runs `bench.py --mode ...` in a fresh process (its own device memory); its JSON line."""
+    cmd = [sys.executable, os.path.abspath(__file__)] + argv
+    try:
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    except subprocess.TimeoutExpired:
+        return {"error": f"timed out after {timeout} s"}
+    lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
+    if p.returncode != 0 or not lines:
+        return {"error": (p.stderr or p.stdout)[-300:]}
+    return json.loads(lines[-1])
+
+
+def run_modes():
+    """Bounded runs of the batching, serving and precision workloads after the timed H*v, so
+    the default line carries their solves/s, latency and accuracy: batch with 64 of the 256
+    J1-J2 chains (300 steps), serve with 40 Poisson requests, precision on the full 4x8
+    Heisenberg sector (300 steps).  The full-size runs are --mode batch / serve."""
+    modes = {}
+    b = _mode_line(["--mode", "batch", "--batch-size", "64", "--plain-sample", "16"], 600)
+    if "error" in b:
+        modes["batch"] = b
+    else:
+        modes["batch"] = {k: b[k] for k in ("config", "fp64_batched_solves_per_s", "fp32_batched_refined_solves_per_s",
+                                            "plain_fp64_solves_per_s", "plain_sample", "speedup_fp32_vs_plain",
+                                            "speedup_fp64_batched_vs_plain", "max_abs_dE_fp32_refined_vs_fp64",
+                                            "max_abs_dE_batched_fp64_vs_plain", "clocks")}
+    sv = _mode_line(["--mode", "serve", "--serve-requests", "40", "--plain-sample", "8"], 900)
+    if "error" in sv:
+        modes["serve"] = sv
+    else:
+        modes["serve"] = {k: sv[k] for k in ("config", "fp64", "fp32", "plain_fp64_solves_per_s", "plain_sample",
+                                             "clocks")}
+    pr = _mode_line(["--mode", "precision"], 900)
+    if "error" in pr:
+        modes["precision"] = pr
+    else:
+        modes["precision"] = {k: pr[k] for k in ("config", "plain_fp64_s", "fp32_s", "speedup_vs_plain",
+                                                 "abs_dE_refined", "abs_dE_unrefined", "e_fp64_plain",
+                                                 "fp32_phase_ms", "clocks")}
+    return modes
+
+
 def run_e2e(H, v1, dim, world, dist, args):
     import torch
     hv0 = torch.zeros(2 * (dim + 1), dtype=torch.float64).pin_memory()
@@ -813,6 +862,8 @@ def finish(args, H_native, kind, kname, kdesc, desc, dim, balg, value, t_max, ac
                         "traffic": profile_traffic(kname, args.workload),
                         "kernels": kdesc},
            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": (2 if kind == 2 else 3) * args.steps, "clocks": clocks}
+    if world == 1 and not args.no_modes:
+        out["modes"] = run_modes()
     print(json.dumps(out))
     if dist:
         dist.destroy_process_group()
