@@ -36,7 +36,9 @@
 // sign in bit 15, eight per lane in one 16-byte load issued a column block ahead, and empty
 // slots point at zero words placed one per bank.  The column pass walks
 // the matrix in column chunks (all rows of chunk 0, then chunk 1, ...) so the source rows of
-// the chunk being processed stay in L2 while every row gathers its ~N/2 up-hop sources.
+// the chunk being processed stay in L2 while every row gathers its ~N/2 up-hop sources; a
+// warp takes one row and 128 columns, its lanes hold the row's packed hop entries and
+// broadcast them by shuffles, and every source row is read as two 512-byte warp loads.
 // Both passes take their work by static striding (no dispenser) and keep per-CTA partial
 // sums of <v1|H v1>, so the result is reproducible.
 #include <cuda_runtime.h>
@@ -240,6 +242,8 @@ struct TwoPassArgs {
   const int *usrc;             // [Uc][wu] up-hop source rank
   const double *ucf;           // [Uc][wu] up-hop coefficient
   const uint8_t *nus;          // [Uc] up hops of each row
+  const uint32_t *usrc16;      // [Uc][wu2] two up hops per word: rank | sign << 15 (16 bits each)
+  int wu2;                     // words per row of usrc16 (0: no packed table)
 };
 
 __device__ __forceinline__ double flip_sign(double x, uint32_t sg) {
@@ -473,6 +477,115 @@ __global__ void __launch_bounds__(kUpThreads, kUpMinBlocks) prod_up_kernel(ProdA
   }
 }
 
+constexpr int kUpWThreads = 256;     // column pass, warp tasks: 8 warps per CTA
+constexpr int kUpWMinBlocks = 3;     // CTAs per SM (at most 85 registers)
+constexpr int kUpWChunk = 128;       // columns per warp task (4 per lane, two 16-byte loads)
+constexpr int kUpWBatch = 4;         // up hops per batch: 8 loads of 16 bytes in flight per lane
+
+// Column pass with warp tasks (uniform up hops, Dc even, 16-byte aligned vectors, Uc <= 32768,
+// at most 64 up hops per row): v0[u, chunk] += scale * t_up * sum_up sign * v1[u', chunk].  A
+// task is one row u and 128 columns (lane l: columns 2l, 2l + 1 and 64 + 2l, 65 + 2l, so each
+// load instruction of the warp reads 512 contiguous bytes); tasks run chunk-major (every row of chunk 0, then chunk
+// 1, ...) by static striding over the warps of a grid that is resident at once, so the 1 KB
+// pieces of v1 the rows gather stay in L2.  Each lane holds two 16-bit hop entries of the row
+// and the warp broadcasts them by shuffles (no shared memory, no CTA barrier).
+// part[blockIdx] = sum over the CTA's tasks of v1 . (up hops) v1.
+__global__ void __launch_bounds__(kUpWThreads, kUpWMinBlocks) prod_up_warp_kernel(ProdArgs a, TwoPassArgs b,
+                                                                                 const double *__restrict__ v1,
+                                                                                 double *__restrict__ v0,
+                                                                                 const double *__restrict__ coef,
+                                                                                 double *__restrict__ part) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (int)((blockIdx.x * (unsigned)kUpWThreads + threadIdx.x) >> 5);
+  const int nwarps = (int)(gridDim.x * (unsigned)kUpWThreads) >> 5;
+  const int Dc = a.Dc, Uc = a.Uc;
+  const int nchunk = (Dc + kUpWChunk - 1) / kUpWChunk;
+  const int64_t ntask = (int64_t)nchunk * Uc;
+  const double tup = b.t_up, st = coef[1] * b.t_up;
+  double pr = 0.0;
+  // the row's hop count and packed entries of the next task are loaded one task ahead
+  int64_t task = warp;
+  int nu_n = 0;
+  uint32_t my_n = 0u;
+  auto fetch = [&](int64_t t) {
+    if (t < ntask) {
+      const int un = (int)(t % Uc);
+      nu_n = b.nus[un];
+      my_n = (2 * lane < nu_n) ? __ldg(b.usrc16 + (int64_t)un * b.wu2 + lane) : 0u;
+    }
+  };
+  fetch(task);
+  const uint64_t rowb = (uint64_t)Dc * sizeof(double);
+  for (; task < ntask; task += nwarps) {
+    const int c = (int)(task / Uc), u = (int)(task - (int64_t)c * Uc);
+    const int nu = nu_n;
+    const uint32_t my = my_n;
+    fetch(task + nwarps);
+    const int d = c * kUpWChunk + 2 * lane;     // columns d, d + 1 and d + 64, d + 65
+    const bool ok0 = d < Dc, ok1 = d + 64 < Dc;  // Dc is even: pairs are whole
+    // lanes past the last column read a valid pair (column 0) and discard what they summed
+    const char *base0 = reinterpret_cast<const char *>(v1 + (ok0 ? d : 0));
+    const char *base1 = reinterpret_cast<const char *>(v1 + (ok1 ? d + 64 : 0));
+    double h0 = 0.0, h1 = 0.0, h2 = 0.0, h3 = 0.0;
+    auto hop = [&](uint32_t e, double2 &w0, double2 &w1) {
+      const uint64_t off = (uint64_t)(e & 0x7FFFu) * rowb;
+      w0 = __ldg(reinterpret_cast<const double2 *>(base0 + off));
+      w1 = __ldg(reinterpret_cast<const double2 *>(base1 + off));
+    };
+    auto add = [&](uint32_t e, const double2 &w0, const double2 &w1) {
+      const uint32_t sg = (e & 0x8000u) << 16;
+      h0 += flip_sign(w0.x, sg);
+      h1 += flip_sign(w0.y, sg);
+      h2 += flip_sign(w1.x, sg);
+      h3 += flip_sign(w1.y, sg);
+    };
+    int k = 0;
+    for (; k + kUpWBatch <= nu; k += kUpWBatch) {
+      double2 w0[kUpWBatch], w1[kUpWBatch];
+      uint32_t e[kUpWBatch];
+#pragma unroll
+      for (int q = 0; q < kUpWBatch; q += 2) {
+        const uint32_t word = __shfl_sync(0xFFFFFFFFu, my, ((k + q) >> 1) & 31);
+        e[q] = word & 0xFFFFu;
+        e[q + 1] = word >> 16;
+      }
+#pragma unroll
+      for (int q = 0; q < kUpWBatch; q++) hop(e[q], w0[q], w1[q]);
+#pragma unroll
+      for (int q = 0; q < kUpWBatch; q++) add(e[q], w0[q], w1[q]);
+    }
+    for (; k < nu; k++) {
+      const uint32_t word = __shfl_sync(0xFFFFFFFFu, my, (k >> 1) & 31);
+      const uint32_t e = (k & 1) ? (word >> 16) : (word & 0xFFFFu);
+      double2 w0, w1;
+      hop(e, w0, w1);
+      add(e, w0, w1);
+    }
+    const double *xp = v1 + (int64_t)u * Dc + d;
+    double *yp = v0 + (int64_t)u * Dc + d;
+    // v0 is streamed (read and written once): evict-first, so it does not push the chunk of
+    // v1 that the following rows gather from out of L2
+    if (ok0) {
+      const double2 xv = __ldg(reinterpret_cast<const double2 *>(xp));
+      const double2 yv = __ldcs(reinterpret_cast<const double2 *>(yp));
+      pr += tup * (xv.x * h0 + xv.y * h1);
+      __stcs(reinterpret_cast<double2 *>(yp), make_double2(yv.x + st * h0, yv.y + st * h1));
+    }
+    if (ok1) {
+      const double2 xv = __ldg(reinterpret_cast<const double2 *>(xp + 64));
+      const double2 yv = __ldcs(reinterpret_cast<const double2 *>(yp + 64));
+      pr += tup * (xv.x * h2 + xv.y * h3);
+      __stcs(reinterpret_cast<double2 *>(yp + 64), make_double2(yv.x + st * h2, yv.y + st * h3));
+    }
+  }
+  double v[2] = {pr, 0.0};
+  block_sum<2>(v);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = v[0];
+    part[2 * blockIdx.x + 1] = 0.0;
+  }
+}
+
 __device__ __forceinline__ uint32_t compress_species(uint64_t c, int s, int N) {
   uint32_t x = 0;
   for (int i = 0; i < N; i++) x |= (uint32_t)((c >> (2 * i + s)) & 1ull) << i;
@@ -548,7 +661,8 @@ struct ProdPlan {
   int *counter = nullptr;
   bool two_pass = false;    // real vectors take the two-pass kernels
   TwoPassArgs tp{};
-  int grid_dn = 0, grid_up = 0;
+  int grid_dn = 0, grid_up = 0;  // grid_up: records reserved for the column pass (either kernel)
+  int grid_upw = 0;              // grid of prod_up_warp_kernel (0: not applicable)
   size_t smem_dn = 0;
 };
 
@@ -1024,8 +1138,21 @@ int prod_plan_build(Sector *s, std::string *err) {
         }
         nus[r] = (uint8_t)rows_up[r].size();
       }
+      // packed up-hop table of the warp-task column pass (uniform hops, ranks below 2^15)
+      std::vector<uint32_t> usrc16;
+      b.wu2 = 0;
+      if (b.up_uniform && Uc <= 32768 && wu <= 64) {
+        b.wu2 = std::max(1, (wu + 1) / 2);
+        usrc16.assign((size_t)Uc * b.wu2, 0u);
+        for (int r = 0; r < Uc; r++)
+          for (int k = 0; k < (int)nus[r]; k++) {
+            const uint32_t e = (uint32_t)usrc[(size_t)r * wuu + k];
+            const uint32_t e16 = (e & 0x7FFFu) | ((e >> 31) << 15);
+            usrc16[(size_t)r * b.wu2 + k / 2] |= (k % 2) ? (e16 << 16) : e16;
+          }
+      }
       if (upload(p, gat4, &b.gat, err) || upload(p, wslots, &b.wslots, err) || upload(p, usrc, &b.usrc, err) ||
-          upload(p, ucf, &b.ucf, err) || upload(p, nus, &b.nus, err))
+          upload(p, ucf, &b.ucf, err) || upload(p, nus, &b.nus, err) || upload(p, usrc16, &b.usrc16, err))
         return fail();
       p->smem_dn = (size_t)kRow2Bytes + (size_t)(Dc + 16) * 8;
       if (cudaFuncSetAttribute(prod_down_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_dn) !=
@@ -1033,10 +1160,16 @@ int prod_plan_build(Sector *s, std::string *err) {
         *err = "product plan: shared-memory attribute rejected (row pass)";
         return fail();
       }
-      int up_per_sm = 0;
+      int up_per_sm = 0, upw_per_sm = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&up_per_sm, prod_up_kernel<true, true>, kUpThreads, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&upw_per_sm, prod_up_warp_kernel, kUpWThreads, 0);
       p->grid_dn = std::max(1, std::min((Uc + 1) / 2, s->num_sms));
-      p->grid_up = std::max(1, std::max(1, up_per_sm) * s->num_sms);
+      p->grid_upw = (b.wu2 > 0) ? std::max(1, upw_per_sm) * s->num_sms : 0;
+      {
+        const char *ue = getenv("HPHI_B200_UPPASS");
+        if (ue && std::string(ue) == "block") p->grid_upw = 0;
+      }
+      p->grid_up = std::max(std::max(1, std::max(1, up_per_sm) * s->num_sms), p->grid_upw);
       p->two_pass = true;
       if (2 * (p->grid_dn + p->grid_up) > 2 * Uc) {
         cudaFree(p->part);
@@ -1071,6 +1204,11 @@ void two_pass_launch(Sector *s, const double *v1, double *v0, const double *d_co
   prod_down_kernel<<<p->grid_dn, kDownThreads, p->smem_dn, s->stream>>>(p->args, p->tp, v1, v0, d_coef, d_part);
   const bool vec2 = (p->args.Dc % 2 == 0) && ((((uintptr_t)v1) | ((uintptr_t)v0)) % 16 == 0);
   double *pu = d_part + 2 * p->grid_dn;
+  if (vec2 && p->grid_upw > 0) {
+    prod_up_warp_kernel<<<p->grid_upw, kUpWThreads, 0, s->stream>>>(p->args, p->tp, v1, v0, d_coef, pu);
+    finalize_partials_kernel<2><<<1, 256, 0, s->stream>>>(d_part, p->grid_dn + p->grid_upw, d_out);
+    return;
+  }
   const int g = p->grid_up;
   if (vec2 && p->tp.up_uniform)
     prod_up_kernel<true, true><<<g, kUpThreads, 0, s->stream>>>(p->args, p->tp, v1, v0, d_coef, pu);

@@ -157,6 +157,38 @@ def test_product_and_block_plans_agree_full_size_4x4(tmp_path):
         assert abs(pr - ref_pr) < 1e-11 * abs(ref_pr)
 
 
+@pytest.mark.parametrize("name", ["hub3x4", "hub3x4_doped", "hub4x4"])
+def test_column_pass_kernels_agree(name, tmp_path, monkeypatch):
+    """Two-pass plan, real vectors: the warp-task column pass (default) and the CTA-task
+    column pass (HPHI_B200_UPPASS=block) give the same v0 += H v1 (1e-12) and prdct, on the
+    4x4 sector too (its last 128-column chunk is partial: 12,870 = 100 * 128 + 70)."""
+    if name == "hub4x4":
+        m = expert.hubbard(16, expert.square_bonds(4, 4), 1.0, 8.0, 8, 8)
+    elif name == "hub3x4_doped":   # 495 up x 792 down configurations
+        m = expert.hubbard(12, expert.square_bonds(3, 4), 1.0, 8.0, 4, 5)
+    else:
+        m = MODELS[name]()
+    path = m.write(str(tmp_path))
+    g = torch.Generator(device="cuda").manual_seed(5)
+    res = []
+    for mode in (None, "block"):
+        if mode:
+            monkeypatch.setenv("HPHI_B200_UPPASS", mode)
+        else:
+            monkeypatch.delenv("HPHI_B200_UPPASS", raising=False)
+        H = _open(path)
+        if not res:
+            assert H.info["kernel"] == 3
+            v = torch.rand(H.dim, dtype=torch.float64, device="cuda", generator=g) - 0.5
+            w = torch.rand(H.dim, dtype=torch.float64, device="cuda", generator=g) - 0.5
+        res.append(_hv_device(H, v, w, hphi_b200.REAL64, acc=0.5, scale=2.0))
+        H.close()
+    (ya, pa), (yb, pb) = res
+    err = (ya - yb).abs().max().item() / yb.abs().max().item()
+    assert err < 1e-12, err
+    assert abs(pa - pb) < 1e-12 * abs(pb)
+
+
 def test_full_size_hubbard4x4_block_vs_general(tmp_path):
     """Half-filled 4x4 Hubbard (dim 165,636,900): block kernel == general kernel to 1e-12,
     and H is Hermitian: <u|Hv> = conj(<v|Hu>)."""
