@@ -167,7 +167,7 @@ int hphi_info(const hphi_handle *h, int64_t *info, int n) {
   v[HPHI_INFO_NUM_AVE] = s.model.num_ave;
   v[HPHI_INFO_NATIVE_ORDER] = has_native_order(&s) ? 1 : 0;
   v[HPHI_INFO_EXCT] = s.model.k_exct;
-  v[HPHI_INFO_KERNEL] = s.prod ? (prod_two_pass(&s) ? 3 : 2) : (s.hub ? 1 : 0);
+  v[HPHI_INFO_KERNEL] = s.prod ? (prod_two_pass(&s) ? 3 : 2) : (s.hub ? 1 : (s.rb ? 4 : 0));
   v[HPHI_INFO_N_GREEN_ONE] = (int64_t)s.model.green_one.size();
   v[HPHI_INFO_N_GREEN_TWO] = (int64_t)s.model.green_two.size();
   for (int i = 0; i < n && i < HPHI_INFO_COUNT; i++) info[i] = v[i];

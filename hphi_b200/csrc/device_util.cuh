@@ -3,9 +3,29 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "engine.hpp"
 
 namespace hphi {
+
+// Raises the dynamic shared-memory limit of kernel fn on the current device to at least bytes
+// (never lowers it: plans of several open sectors share one kernel, and a later sector with
+// smaller blocks must not invalidate an earlier one's launches).  Returns the CUDA status.
+inline cudaError_t raise_smem_limit(const void *fn, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, size_t> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  size_t &cur = done[{dev, fn}];
+  if (bytes <= cur) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
+}
 
 __host__ __device__ __forceinline__ cplx cmk(double x, double y) { return cplx{x, y}; }
 __host__ __device__ __forceinline__ cplx operator+(cplx a, cplx b) { return cplx{a.x + b.x, a.y + b.y}; }
@@ -18,6 +38,7 @@ __host__ __device__ __forceinline__ cplx cmul(cplx a, cplx b) {
 // Scalar traits: T is double (real vectors) or cplx (complex128 vectors).
 template <typename T> struct VT;
 template <> struct VT<double> {
+  static constexpr bool kComplex = false;
   static __device__ __forceinline__ double zero() { return 0.0; }
   // coefficient (re, im) times x; real vectors carry real coefficients only
   static __device__ __forceinline__ double cmul_re_im(double re, double, double x) { return re * x; }
@@ -30,6 +51,7 @@ template <> struct VT<double> {
   static __device__ __forceinline__ double add_re(double x, double a) { return x + a; }
 };
 template <> struct VT<cplx> {
+  static constexpr bool kComplex = true;
   static __device__ __forceinline__ cplx zero() { return cplx{0.0, 0.0}; }
   static __device__ __forceinline__ cplx cmul_re_im(double re, double im, cplx x) {
     return cplx{re * x.x - im * x.y, re * x.y + im * x.x};

@@ -18,6 +18,7 @@ namespace hphi {
 
 struct HubPlan;
 struct ProdPlan;
+struct RowBlockPlan;
 
 // Real or complex double scalar for host/device code.
 struct cplx { double x, y; };
@@ -73,6 +74,9 @@ struct Sector {
   HubPlan *hub = nullptr;
   // Product-layout plan (canonical Hubbard); preferred over the block plan when both apply.
   ProdPlan *prod = nullptr;
+  // Row-block plan (spin models, HPhi order): row pass + column pass over the blocks of
+  // rows that share an upper half (hv_rowblock.cu).
+  RowBlockPlan *rb = nullptr;
   SplitPlan split;
   // General spin: the device tables above are indexed by packed digit codes; HPhi's own
   // mixed-radix lists (src/sz.c:795-830, 1564-1590) are kept here for export.

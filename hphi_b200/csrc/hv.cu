@@ -17,6 +17,7 @@
 #include "engine.hpp"
 #include "hv_hubbard.hpp"
 #include "hv_product.hpp"
+#include "hv_rowblock.hpp"
 #include "split.cuh"
 
 namespace hphi {
@@ -98,6 +99,7 @@ int hv_launch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double 
     set_error("H has complex coefficients: real vectors are not allowed");
     return -1;
   }
+  if (rb_applies(s, vt)) return rb_hv_launch(s, vt, d_v1, d_v0, d_coef, d_out);
   if (vt == kReal64) {
     if (s->gc) launch_general<double, true>(s, (const double *)d_v1, (double *)d_v0, d_coef);
     else launch_general<double, false>(s, (const double *)d_v1, (double *)d_v0, d_coef);
@@ -120,6 +122,7 @@ int hv_launch_scratch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const
     set_error("H has complex coefficients: real vectors are not allowed");
     return -1;
   }
+  if (rb_applies(s, vt)) return rb_hv_launch_scratch(s, vt, d_v1, d_v0, d_coef, d_out, d_part);
   const int grid = s->red_blocks;
   const uint64_t lo_mask = s->ihfbit - 1;
   const bool smem_terms = s->split.ngen <= kSmemTermMax;
@@ -156,6 +159,7 @@ int hv_launch_scratch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const
 size_t hv_scratch_doubles(const Sector *s, VecType vt) {
   if (s->prod) return prod_scratch_doubles(s, vt);
   if (s->hub) return hub_scratch_doubles(s);
+  if (rb_applies(s, vt)) return rb_scratch_doubles(s);
   return 2 * (size_t)s->red_blocks;
 }
 

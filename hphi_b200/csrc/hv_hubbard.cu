@@ -628,10 +628,8 @@ int hub_plan_build(Sector *s, std::string *err) {
   plan->smem[0][1] = p0 + sizeof(cplx) * (size_t)maxn;
   plan->smem[1][0] = plan->smem[1][1] = (base + sizeof(uint16_t) * L * nx + 15) & ~(size_t)15;
   if (plan->smem[0][1] > 200 * 1024) { hub_plan_free(plan); return 0; }
-  cudaFuncSetAttribute((const void *)hv_hub_pass<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)plan->smem[0][0]);
-  cudaFuncSetAttribute((const void *)hv_hub_pass<cplx, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)plan->smem[0][1]);
+  raise_smem_limit((const void *)hv_hub_pass<double, 0>, plan->smem[0][0]);
+  raise_smem_limit((const void *)hv_hub_pass<cplx, 0>, plan->smem[0][1]);
   int per_sm0 = 1, per_sm1 = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm0, hv_hub_pass<double, 0>, kThreads, plan->smem[0][0]);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, hv_hub_pass<double, 1>, kThreads, plan->smem[1][0]);

@@ -922,6 +922,14 @@ std::vector<int> balance_positions(const std::vector<std::vector<uint32_t>> &row
 
 }  // namespace
 
+void build_gather_table(const std::vector<std::vector<uint32_t>> &rows, int n, std::vector<uint32_t> *gat,
+                        std::vector<uint8_t> *wslots, int *groups) {
+  // entries carry their sign directly: one hop of coefficient +1, sign bit = (entry >> 16) & 1
+  const std::vector<SpeciesHop> unit{SpeciesHop{0, 0, 1.0, 0.0}};
+  int nslots = 0;
+  build_gather(rows, unit, n, (n + 31) / 32 * 32, gat, wslots, &nslots, groups);
+}
+
 int prod_plan_build(Sector *s, std::string *err) {
   const Model &m = s->model;
   s->prod = nullptr;
@@ -1101,10 +1109,8 @@ int prod_plan_build(Sector *s, std::string *err) {
   }
   p->smem[0] = smem_r;
   p->smem[1] = smem_c;
-  if (cudaFuncSetAttribute(prod_hv_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_r) !=
-          cudaSuccess ||
-      cudaFuncSetAttribute(prod_hv_kernel<cplx>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c) !=
-          cudaSuccess) {
+  if (raise_smem_limit((const void *)prod_hv_kernel<double>, smem_r) != cudaSuccess ||
+      raise_smem_limit((const void *)prod_hv_kernel<cplx>, smem_c) != cudaSuccess) {
     *err = "product plan: shared-memory attribute rejected";
     return fail();
   }
@@ -1155,8 +1161,7 @@ int prod_plan_build(Sector *s, std::string *err) {
           upload(p, ucf, &b.ucf, err) || upload(p, nus, &b.nus, err) || upload(p, usrc16, &b.usrc16, err))
         return fail();
       p->smem_dn = (size_t)kRow2Bytes + (size_t)(Dc + 16) * 8;
-      if (cudaFuncSetAttribute(prod_down_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_dn) !=
-          cudaSuccess) {
+      if (raise_smem_limit((const void *)prod_down_kernel, p->smem_dn) != cudaSuccess) {
         *err = "product plan: shared-memory attribute rejected (row pass)";
         return fail();
       }

@@ -1,6 +1,8 @@
 // Product-layout kernel for canonical Hubbard models (hv_product.cu).
 #pragma once
+#include <cstdint>
 #include <string>
+#include <vector>
 
 #include "engine.hpp"
 
@@ -20,5 +22,12 @@ size_t prod_scratch_doubles(const Sector *s, VecType vt);
 bool prod_two_pass(const Sector *s);
 int prod_permute(Sector *s, VecType vt, const void *in, void *out, bool to_native);
 int prod_observables(Sector *s, VecType vt, const void *v, double *d_out);
+// Edge-coloured gather table of the row pass for n columns (positions): rows[p] lists the
+// sources of column p as (source position | negative << 16).  gat: per warp of 32 columns and
+// group of 8 slots, 32 lanes x 4 words of two 16-bit entries (position | sign << 15);
+// wslots: slots per warp; groups: slot groups per warp in the table.  Empty slots read one of
+// the zero words n .. n + 15 (one per shared-memory bank pair).
+void build_gather_table(const std::vector<std::vector<uint32_t>> &rows, int n, std::vector<uint32_t> *gat,
+                        std::vector<uint8_t> *wslots, int *groups);
 
 }  // namespace hphi

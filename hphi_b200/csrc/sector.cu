@@ -22,6 +22,7 @@
 
 #include "engine.hpp"
 #include "hv_hubbard.hpp"
+#include "hv_rowblock.hpp"
 #include "hv_product.hpp"
 #include "split.cuh"
 
@@ -618,6 +619,9 @@ int sector_build(const Model &m, int device, Sector **out, std::string *err, boo
   if (specialise && kname != "general" && !s->prod) {
     if (hub_plan_build(s, err) != 0) return -1;
   }
+  if (specialise && kname != "general" && !s->prod && !s->hub) {
+    if (rb_plan_build(s, err) != 0) return -1;
+  }
   *out = s;
   return 0;
 }
@@ -632,6 +636,7 @@ void sector_free(Sector *s) {
   cudaFree(s->split.coef); cudaFree(s->split.gen);
   hub_plan_free(s->hub);
   prod_plan_free(s->prod);
+  rb_plan_free(s->rb);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }

@@ -40,7 +40,7 @@ typedef struct hphi_handle hphi_handle;
 #define HPHI_INFO_NUM_AVE 11
 #define HPHI_INFO_NATIVE_ORDER 12 /* 1 if the engine's native vector order differs from HPhi's */
 #define HPHI_INFO_EXCT 13         /* exct: states of LOBPCG / the Lanczos eigenvector index */
-#define HPHI_INFO_KERNEL 14       /* native H*v kernel: 0 general, 1 Hubbard block plan, 2 Hubbard product layout, 3 product layout two-pass (real vectors) */
+#define HPHI_INFO_KERNEL 14       /* native H*v kernel: 0 general, 1 Hubbard block plan, 2 Hubbard product layout, 3 product layout two-pass (real vectors), 4 spin row-block passes */
 #define HPHI_INFO_N_GREEN_ONE 15  /* OneBodyG rows read (NCisAjt) */
 #define HPHI_INFO_N_GREEN_TWO 16  /* TwoBodyG rows read (NCisAjtCkuAlvDC) */
 #define HPHI_INFO_COUNT 17

@@ -37,6 +37,7 @@ def _open(path, general=False, kernel=None):
 
 def _hv_device(H, v1, v0, vt, acc=1.0, scale=1.0):
     out = v0.clone()
+    torch.cuda.synchronize()  # the engine's stream does not wait for torch's
     pr = H.mltply_device(out.data_ptr(), v1.data_ptr(), vt, acc=acc, scale=scale)
     return out, pr
 
@@ -211,3 +212,29 @@ def test_full_size_hubbard4x4_block_vs_general(tmp_path):
     Hg.close()
     err = (Hu - Hug).abs().max().item() / Hug.abs().max().item()
     assert err < 1e-12
+
+
+@pytest.mark.parametrize("big, small", [
+    # product-layout plan: one-pass kernel on complex vectors stages a 128 KB row of the 6+6 sector
+    (lambda: expert.hubbard(16, expert.square_bonds(4, 4), 1.0, 8.0, 6, 6),
+     lambda: expert.hubbard(12, expert.square_bonds(3, 4), 1.0, 8.0, 6, 6)),
+    # spin row-block plan: complex vectors of the 4x7 sector stage 55 KB blocks
+    (lambda: expert.heisenberg(28, expert.square_bonds(4, 7)),
+     lambda: expert.heisenberg(16, expert.chain_bonds(16))),
+])
+def test_shared_memory_limits_survive_a_smaller_sector(big, small, tmp_path):
+    """The kernels' dynamic shared-memory limit is set per kernel, not per sector: opening a
+    sector with smaller rows after a larger one must leave the larger one's launches valid."""
+    Hb = _open(big().write(str(tmp_path / "big")))
+    Hs = _open(small().write(str(tmp_path / "small")))
+    try:
+        for H in (Hb, Hs, Hb):
+            g = torch.Generator(device="cuda").manual_seed(1)
+            v = (torch.rand(H.dim, dtype=torch.complex128, device="cuda", generator=g) - 0.5)
+            out = torch.zeros_like(v)
+            torch.cuda.synchronize()
+            H.mltply_device(out.data_ptr(), v.data_ptr(), hphi_b200.COMPLEX128, acc=0.0)
+            assert torch.isfinite(out.abs()).all()
+    finally:
+        Hb.close()
+        Hs.close()

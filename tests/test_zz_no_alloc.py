@@ -34,8 +34,11 @@ CASES = {
     # block plan of canonical Hubbard sectors (its counter and partial sums live in the array)
     "hubbard3x4_block": (lambda: expert.hubbard(12, expert.square_bonds(3, 4), 1.0, 8.0, 6, 6), False, 1, 1,
                          {"HPHI_B200_KERNEL": "block"}),
+    # row-block plan of spin sectors (row pass and column pass partial sums in the array)
+    "heisenberg_chain16": (lambda: expert.heisenberg(16, expert.chain_bonds(16), 1.0), False, 0, 4, {}),
     # general kernel (native order is HPhi's order)
-    "heisenberg_chain16": (lambda: expert.heisenberg(16, expert.chain_bonds(16), 1.0), False, 0, 0, {}),
+    "heisenberg_chain16_general": (lambda: expert.heisenberg(16, expert.chain_bonds(16), 1.0), False, 0, 0,
+                                   {"HPHI_B200_KERNEL": "general"}),
 }
 
 
