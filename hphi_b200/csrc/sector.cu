@@ -619,7 +619,10 @@ int sector_build(const Model &m, int device, Sector **out, std::string *err, boo
   if (specialise && kname != "general" && !s->prod) {
     if (hub_plan_build(s, err) != 0) return -1;
   }
-  if (specialise && kname != "general" && !s->prod && !s->hub) {
+  // Row-block plan (spin sectors): from 2^24 rows up, where the vectors no longer stay in L2
+  // and the general kernel's scattered gathers go to memory (below that the general kernel is
+  // faster); HPHI_B200_KERNEL=rowblock builds it at any size.
+  if (specialise && kname != "general" && !s->prod && !s->hub && (kname == "rowblock" || s->dim >= (1ll << 24))) {
     if (rb_plan_build(s, err) != 0) return -1;
   }
   *out = s;

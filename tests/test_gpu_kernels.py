@@ -214,19 +214,19 @@ def test_full_size_hubbard4x4_block_vs_general(tmp_path):
     assert err < 1e-12
 
 
-@pytest.mark.parametrize("big, small", [
+@pytest.mark.parametrize("big, small, kernel", [
     # product-layout plan: one-pass kernel on complex vectors stages a 128 KB row of the 6+6 sector
     (lambda: expert.hubbard(16, expert.square_bonds(4, 4), 1.0, 8.0, 6, 6),
-     lambda: expert.hubbard(12, expert.square_bonds(3, 4), 1.0, 8.0, 6, 6)),
-    # spin row-block plan: complex vectors of the 4x7 sector stage 55 KB blocks
+     lambda: expert.hubbard(12, expert.square_bonds(3, 4), 1.0, 8.0, 6, 6), None),
+    # spin row-block plan: complex vectors of the 4x7 sector (40,116,600 rows) stage 55 KB blocks
     (lambda: expert.heisenberg(28, expert.square_bonds(4, 7)),
-     lambda: expert.heisenberg(16, expert.chain_bonds(16))),
+     lambda: expert.heisenberg(16, expert.chain_bonds(16)), "rowblock"),
 ])
-def test_shared_memory_limits_survive_a_smaller_sector(big, small, tmp_path):
+def test_shared_memory_limits_survive_a_smaller_sector(big, small, kernel, tmp_path):
     """The kernels' dynamic shared-memory limit is set per kernel, not per sector: opening a
     sector with smaller rows after a larger one must leave the larger one's launches valid."""
-    Hb = _open(big().write(str(tmp_path / "big")))
-    Hs = _open(small().write(str(tmp_path / "small")))
+    Hb = _open(big().write(str(tmp_path / "big")), kernel=kernel)
+    Hs = _open(small().write(str(tmp_path / "small")), kernel=kernel)
     try:
         for H in (Hb, Hs, Hb):
             g = torch.Generator(device="cuda").manual_seed(1)

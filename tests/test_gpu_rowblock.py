@@ -14,13 +14,14 @@ torch = pytest.importorskip("torch")
 
 
 def _open(path, general, simple=False):
-    """general: the general row kernel; simple: the row-block plan without its fast row pass
-    (HPHI_B200_RB_SIMPLE), which real vectors of Heisenberg-like sectors take by default."""
+    """general: the general row kernel; otherwise the row-block plan (HPHI_B200_KERNEL=rowblock),
+    with simple: without its fast row pass (HPHI_B200_RB_SIMPLE), which real vectors of
+    Heisenberg-like sectors take by default."""
     saved = {k: os.environ.get(k) for k in ("HPHI_B200_KERNEL", "HPHI_B200_RB_SIMPLE")}
     os.environ.pop("HPHI_B200_KERNEL", None)
     os.environ.pop("HPHI_B200_RB_SIMPLE", None)
-    if general:
-        os.environ["HPHI_B200_KERNEL"] = "general"
+    # the plan is built by default from 2^24 rows up; these sectors are smaller
+    os.environ["HPHI_B200_KERNEL"] = "general" if general else "rowblock"
     if simple:
         os.environ["HPHI_B200_RB_SIMPLE"] = "1"
     try:

@@ -35,10 +35,10 @@ CASES = {
     "hubbard3x4_block": (lambda: expert.hubbard(12, expert.square_bonds(3, 4), 1.0, 8.0, 6, 6), False, 1, 1,
                          {"HPHI_B200_KERNEL": "block"}),
     # row-block plan of spin sectors (row pass and column pass partial sums in the array)
-    "heisenberg_chain16": (lambda: expert.heisenberg(16, expert.chain_bonds(16), 1.0), False, 0, 4, {}),
-    # general kernel (native order is HPhi's order)
-    "heisenberg_chain16_general": (lambda: expert.heisenberg(16, expert.chain_bonds(16), 1.0), False, 0, 0,
-                                   {"HPHI_B200_KERNEL": "general"}),
+    "heisenberg_chain16": (lambda: expert.heisenberg(16, expert.chain_bonds(16), 1.0), False, 0, 4,
+                           {"HPHI_B200_KERNEL": "rowblock"}),
+    # general kernel (native order is HPhi's order; the default below 2^24 rows)
+    "heisenberg_chain16_general": (lambda: expert.heisenberg(16, expert.chain_bonds(16), 1.0), False, 0, 0, {}),
 }
 
 
