@@ -699,10 +699,12 @@ def main():
     dim = H.dim
     H_native = bool(H.info.get("native_order"))
     kind = H.info.get("kernel", 0)
-    kname, kdesc = {3: ("prod_two_pass", "prod_down_kernel (row pass) + prod_up_kernel<true> (column pass) + "
+    kname, kdesc = {3: ("prod_two_pass", "prod_down_kernel (row pass) + prod_up_warp_kernel (column pass) + "
                                          "finalize_partials_kernel<2> per step; achieved = B_alg / time of all three"),
                     2: ("prod_hv_kernel", "prod_hv_kernel<double> + finalize_partials_kernel<2> per step"),
-                    1: ("hv_hub_pass", "hv_hub_pass<double,0> + hv_hub_pass<double,1> + finalize per step")}.get(
+                    1: ("hv_hub_pass", "hv_hub_pass<double,0> + hv_hub_pass<double,1> + finalize per step"),
+                    4: ("spin_rowblock", "spin_row_kernel (row pass) + rb_col_kernel<double,0,4> (column pass) + "
+                                         "finalize_partials_kernel<2> per step; achieved = B_alg / time of all three")}.get(
         kind, ("hv_general", "hv_general_kernel + finalize per step"))
     vt = hphi_b200.REAL64
     gen = torch.Generator(device="cuda").manual_seed(1234 + rank)

@@ -93,3 +93,60 @@ def test_rowblock_lanczos_energy_matches_general(tmp_path):
         H.close()
     assert abs(out[0] - out[2]) < 1e-10 * abs(out[2])
     assert abs(out[1] - out[2]) < 1e-10 * abs(out[2])
+
+
+# ---------------------------------------------------------------- pinned to the reference
+import sys  # noqa: E402
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import run_ref  # noqa: E402
+
+REF_CASES = {
+    # fast row pass (one magnitude on every lower-half term)
+    "square4x4": lambda: expert.heisenberg(16, expert.square_bonds(4, 4), lanczos_max=5, initial_iv=-1),
+    # generic row pass (J1 and J2 lower-half terms)
+    "j1j2_18": lambda: expert.j1j2_chain(18, 1.0, 0.4, lanczos_max=5, initial_iv=-1),
+    # grand-canonical rows (SpinGC): exchange and pair-lift terms
+    "kitaev2x3_gc": lambda: expert.kitaev_heisenberg(2, 3, -1.0, 0.2, lanczos_max=5, initial_iv=-1),
+}
+
+
+@pytest.mark.parametrize("name", list(REF_CASES))
+def test_rowblock_accumulating_call_matches_reference(name, tmp_path):
+    """One accumulating mltply call of the reference's own Lanczos (v0 += H v1,
+    src/mltply.c:56-132; oracle/_ref/HPhi_ref run at test time) against the row-block kernels:
+    hphi_mltply on HPhi-layout complex128 host vectors and hphi_mltply_device on real and
+    complex device vectors, to 1e-12."""
+    if not run_ref.available():
+        pytest.skip("oracle/_ref/HPhi_ref is not built (make -C oracle)")
+    m = REF_CASES[name]()
+    ref_dir = str(tmp_path / "ref")
+    m.write(ref_dir)
+    p = run_ref.run(ref_dir, threads=4, dump_call=3, timeout=600, extra_env={"HPHI_DUMP_LISTS": "0"})
+    assert os.path.exists(os.path.join(ref_dir, "hv.bin")), p.stdout[-2000:] + p.stderr[-2000:]
+    v1, v0b, v0a, pr_ref = run_ref.read_hv(ref_dir)
+    H = _open(m.write(str(tmp_path / "eng")), general=False)
+    try:
+        assert H.info["kernel"] == 4
+        v0 = v0b.copy()
+        pr = H.mltply(v0, v1)
+        scale = np.max(np.abs(v0a))
+        assert np.max(np.abs(v0 - v0a)) <= 1e-12 * scale
+        assert abs(pr - pr_ref) <= 1e-12 * max(1.0, abs(pr_ref))
+        vts = [hphi_b200.COMPLEX128]
+        if np.all(v1.imag == 0) and np.all(v0b.imag == 0):
+            vts.append(hphi_b200.REAL64)
+        for vt in vts:
+            if vt == hphi_b200.REAL64:
+                d1 = torch.tensor(v1[1:].real.copy(), device="cuda")
+                d0 = torch.tensor(v0b[1:].real.copy(), device="cuda")
+            else:
+                d1 = torch.tensor(v1[1:].copy(), device="cuda")
+                d0 = torch.tensor(v0b[1:].copy(), device="cuda")
+            torch.cuda.synchronize()
+            prd = H.mltply_device(d0.data_ptr(), d1.data_ptr(), vt, acc=1.0, scale=1.0)
+            out = d0.cpu().numpy()
+            assert np.max(np.abs(out - v0a[1:])) <= 1e-12 * scale, vt
+            assert abs(prd - pr_ref) <= 1e-12 * max(1.0, abs(pr_ref)), (vt, prd, pr_ref)
+    finally:
+        H.close()
