@@ -413,13 +413,13 @@ int hphi_lanczos_steps(hphi_handle *h, int steps, uint64_t seed, double *energie
   if (steps < 2) { set_error("hphi_lanczos_steps: steps must be >= 2"); return -1; }
   Sector *s = h->sector;
   const VecType vt = default_vec_type(*s);
-  std::vector<double> start;
-  if (hashed_start(*s, seed, vt == kComplex128, &start) != 0) return -1;
   LanczosOptions opt;
   opt.fixed_steps = steps;
+  opt.hashed_start = true;
+  opt.hashed_seed = seed;
   LanczosResult &r = h->last_lanczos;
   r = LanczosResult();
-  if (lanczos_run(s, vt, start.data(), opt, &r) != 0) return -1;
+  if (lanczos_run(s, vt, nullptr, opt, &r) != 0) return -1;
   for (int q = 0; energies && q < nev; q++)
     energies[q] = (q < r.steps) ? tridiag_eigenvalue(r.alpha.data(), r.beta.data(), r.steps, q) : 0.0;
   return 0;

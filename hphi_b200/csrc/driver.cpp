@@ -211,30 +211,6 @@ void random_start(const Sector &s, uint64_t seed, bool complex_vec, std::vector<
   for (uint64_t i = 1; i <= dim; i++) { (*v)[2 * i] /= nrm; (*v)[2 * i + 1] /= nrm; }
 }
 
-// Hashed start (start_value of batch.hpp) in HPhi's 1-based complex128 layout, normalised.
-int hashed_start(const Sector &s, uint64_t seed, bool complex_vec, std::vector<double> *v) {
-  const uint64_t dim = (uint64_t)s.dim;
-  std::vector<uint64_t> cfg;
-  if (!s.gc) {
-    cfg.resize(dim);
-    if (cuda_ok(cudaMemcpy(cfg.data(), s.d_list_1, sizeof(uint64_t) * dim, cudaMemcpyDeviceToHost), "read list_1"))
-      return -1;
-  }
-  v->assign(2 * (dim + 1), 0.0);
-  double nrm = 0.0;
-  for (uint64_t i = 0; i < dim; i++) {
-    const uint64_t c = s.gc ? i : cfg[i];
-    const double re = start_value(seed, c, 0);
-    const double im = complex_vec ? start_value(seed, c, 1) : 0.0;
-    (*v)[2 * (i + 1)] = re;
-    (*v)[2 * (i + 1) + 1] = im;
-    nrm += re * re + im * im;
-  }
-  nrm = std::sqrt(nrm);
-  for (uint64_t i = 1; i <= dim; i++) { (*v)[2 * i] /= nrm; (*v)[2 * i + 1] /= nrm; }
-  return 0;
-}
-
 // ------------------------------------------------------- CG eigenvector refinement
 namespace {
 constexpr double kEpsEnergy = 1e-12;  // eps_Energy (src/readdef.c:2703,2707)
@@ -415,8 +391,21 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
   if (!fixed && dim < m.lanczos_target) max_steps = (int)dim;
   RET(cuda_ok(cudaMalloc(&AL.p, sizeof(double) * (max_steps + 2)), "alloc alpha"));
   RET(cuda_ok(cudaMalloc(&BE.p, sizeof(double) * (max_steps + 2)), "alloc beta"));
-  // start vector: HPhi order on the host -> native order on the device
-  RET(vec_from_host_c128(s, vt, h_init, P.p));
+  // start vector: HPhi order on the host (or hashed on the device) -> native order on the device
+  if (opt.hashed_start) {
+    RET(vec_fill_hashed(s, vt, opt.hashed_seed, P.p));
+    RET(vec_norm2(s, vt, P.p, s->d_scal));
+    double n2 = 0.0;
+    RET(cuda_ok(cudaMemcpyAsync(&n2, s->d_scal, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "norm"));
+    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+    if (!(n2 > 0.0)) {
+      set_error("hashed start vector has zero norm");
+      return -1;
+    }
+    RET(vec_scale(s, vt, 1.0 / std::sqrt(n2), P.p));
+  } else {
+    RET(vec_from_host_c128(s, vt, h_init, P.p));
+  }
   RET(to_native(s, vt, P.p, Q.p));
   const bool want_vec = opt.eigenvector;
   if (want_vec) {

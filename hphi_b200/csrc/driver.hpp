@@ -27,6 +27,8 @@ struct LanczosOptions {
   bool restart_out = false;       // fill LanczosResult::restart (ReStart 1 / 2); then a run
                                   // that does not converge is not an error
   const LanczosRestart *resume = nullptr;  // continue from these (ReStart 2 / 3)
+  bool hashed_start = false;      // start from the hashed vector of hashed_seed, made on the
+  uint64_t hashed_seed = 0;       // device (h_init is not read)
 };
 
 // Green's function values of the model's OneBodyG / TwoBodyG rows (expec_cisajs,
@@ -126,10 +128,9 @@ void tridiag_eigenvector(const double *a, const double *b, int n, double lam, st
 VecType default_vec_type(const Sector &s);
 bool single_element_start(const Sector &s, std::vector<double> *v);
 void random_start(const Sector &s, uint64_t seed, bool complex_vec, std::vector<double> *v);
-// start_value (batch.hpp) per configuration, normalised, in HPhi's 1-based complex128 layout.
-int hashed_start(const Sector &s, uint64_t seed, bool complex_vec, std::vector<double> *v);
 
-// h_init: normalised start vector in HPhi's 1-based complex128 layout.
+// h_init: normalised start vector in HPhi's 1-based complex128 layout (not read when
+// opt.hashed_start is set).
 int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOptions &opt, LanczosResult *res);
 int write_lanczos_outputs(const Sector &s, const LanczosResult &r, const std::string &outdir);
 int write_lanczos_restart(const Sector &s, const LanczosRestart &r, const std::string &outdir);

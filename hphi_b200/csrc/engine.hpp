@@ -146,6 +146,9 @@ int vec_tpq_sweep(Sector *s, VecType vt, double cv, double ch, void *v, const vo
 // CG sweep (eigenvector refinement): x += a*p; r -= a*(hp + shift*p); d_out[0] = |r|^2.
 int vec_cg_sweep(Sector *s, VecType vt, double a, double shift, const void *p, const void *hp, void *x, void *r,
                  double *d_out);
+// x = the hashed start vector start_value(seed, configuration of row i, part) (HPhi order, not
+// normalised; imaginary parts only for complex vectors).
+int vec_fill_hashed(Sector *s, VecType vt, uint64_t seed, void *d_x);
 // x[i] += amp * start_value(seed, configuration of row i, 0) on the real part (HPhi order).
 int vec_add_hashed(Sector *s, VecType vt, uint64_t seed, double amp, void *d_x);
 // <v| O_e |v> of compiled Green's function entries (compile_green) on a device vector in

@@ -304,7 +304,27 @@ __global__ void add_hashed_kernel(int64_t n, uint64_t seed, double amp, const ui
   }
 }
 
+// x[i] = start_value(seed, configuration of row i, 0) (+ i start_value(.., 1) for complex
+// vectors), HPhi's row order: the hashed start vector before normalisation.
+template <typename T>
+__global__ void fill_hashed_kernel(int64_t n, uint64_t seed, const uint64_t *__restrict__ list_1, T *__restrict__ x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = list_1 ? list_1[i] : (uint64_t)i;
+    if constexpr (VT<T>::kComplex) x[i] = cplx{start_value(seed, c, 0), start_value(seed, c, 1)};
+    else x[i] = start_value(seed, c, 0);
+  }
+}
+
 }  // namespace
+
+int vec_fill_hashed(Sector *s, VecType vt, uint64_t seed, void *x) {
+  const uint64_t *l1 = s->gc ? nullptr : s->d_list_1;
+  if (vt == kReal64)
+    fill_hashed_kernel<double><<<s->red_blocks, kThreads, 0, s->stream>>>(s->dim, seed, l1, (double *)x);
+  else
+    fill_hashed_kernel<cplx><<<s->red_blocks, kThreads, 0, s->stream>>>(s->dim, seed, l1, (cplx *)x);
+  return check_launch("vec_fill_hashed");
+}
 
 int lanczos_scalars(Sector *s, int phase, int k, double *st, double *alpha, double *beta) {
   lanczos_scalars_kernel<<<1, 32, 0, s->stream>>>(phase, k, st, alpha, beta);
