@@ -45,7 +45,7 @@ EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi
                     "hphi_batch_free", "hphi_server_create", "hphi_server_submit", "hphi_server_step",
                     "hphi_server_poll", "hphi_server_clock", "hphi_server_free", "hphi_lobpcg",
                     "hphi_reference_start", "hphi_expec_green", "hphi_expec_cisajs", "hphi_expec_cisajscktaltdc",
-                    "hphi_inspect_green", "hphi_expec_green_device"]
+                    "hphi_inspect_green", "hphi_expec_green_device", "hphi_spectrum"]
 FP64 = 0
 FP32 = 1
 BATCH_GRAPH = 1
@@ -94,6 +94,7 @@ def load_library() -> ctypes.CDLL:
     lib.hphi_tpq.argtypes = [P, pd, ctypes.c_char_p, pd, I]
     lib.hphi_tem.argtypes = [P, pd, ctypes.c_char_p, pd, I]
     lib.hphi_run.argtypes = [P, ctypes.c_char_p]
+    lib.hphi_spectrum.argtypes = [P, pd, ctypes.c_char_p, pd, I]
     lib.hphi_mltply_device_async.argtypes = [P, I, VP, VP, VP, VP]
     lib.hphi_mltply_device_noalloc.argtypes = [P, I, VP, VP, D, D, pd]
     lib.hphi_to_native.argtypes = [P, I, VP, VP]
@@ -404,6 +405,20 @@ class Hamiltonian:
         _check(load_library().hphi_tem(self._h, None if buf is None else _dptr(buf.view(np.float64)),
                                        None if output_dir is None else os.fsencode(output_dir), _dptr(res), n))
         return res
+
+    def calc_spectrum(self, vec: Optional[np.ndarray] = None, output_dir: Optional[str] = None,
+                      n_omega: int = 0) -> np.ndarray:
+        """Dynamical Green's function (CalcSpectrum with CalcSpec 1, Lanczos): the excitation
+        operators of the input act on vec (HPhi layout, dim+1 complex128) or, when None, on
+        <SpectrumVec>_rank_0.dat in output_dir; writes <head>_DynamicalGreen.dat and
+        <head>_TMComponents.dat.  Returns (n_omega, 2) complex: omega (OmegaOrg included), G."""
+        res = np.zeros(4 * max(n_omega, 0))
+        buf = None if vec is None else np.ascontiguousarray(_as_hphi_vector(vec, self.dim))
+        _check(load_library().hphi_spectrum(self._h, None if buf is None else _dptr(buf.view(np.float64)),
+                                            None if output_dir is None else os.fsencode(output_dir),
+                                            _dptr(res) if n_omega > 0 else None, int(n_omega)))
+        r = res.reshape(-1, 4)
+        return np.stack([r[:, 0] + 1j * r[:, 1], r[:, 2] + 1j * r[:, 3]], axis=1)
 
     def calc_by_lobpcg(self, v_init: Optional[Sequence[np.ndarray]] = None,
                        output_dir: Optional[str] = None) -> dict:

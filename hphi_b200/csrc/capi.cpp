@@ -739,9 +739,52 @@ int hphi_tem(hphi_handle *h, const double *v_init, const char *output_dir, doubl
   return 0;
 }
 
+int hphi_spectrum(hphi_handle *h, const double *h_vec, const char *output_dir, double *result, int nresult) {
+  CHECK_HANDLE(h);
+  Sector *s = h->sector;
+  const Model &m = s->model;
+  const std::string out = output_dir ? output_dir : "output";
+  if (m.calc_type != kLanczos) {
+    set_error("spectrum: only the Lanczos method (CalcType 0) is supported");
+    return -1;
+  }
+  std::vector<double> vec;
+  if (!h_vec) {
+    // the input vector <SpectrumVec>_rank_0.dat in the output folder (src/CalcSpectrum.c:153-182)
+    const std::string path = out + "/" + m.spectrum_vec + "_rank_0.dat";
+    FILE *fin = m.spectrum_vec.empty() ? nullptr : fopen(path.c_str(), "rb");
+    if (!fin) {
+      set_error("Error: A file of Input vector does not exist.");
+      return -1;
+    }
+    const int64_t stride = 2 * (s->dim + 1);
+    int stp = 0;
+    long dim = 0;
+    vec.assign(stride, 0.0);
+    const bool ok = fread(&stp, sizeof(int), 1, fin) == 1 && fread(&dim, sizeof(long), 1, fin) == 1 &&
+                    dim == (long)s->dim && fread(vec.data(), sizeof(double), stride, fin) == (size_t)stride;
+    fclose(fin);
+    if (!ok) {
+      set_error("Error: A file of Input vector is incorrect.");
+      return -1;
+    }
+    h_vec = vec.data();
+  }
+  SpectrumResult r;
+  if (spectrum_run(s, h_vec, out, &r) != 0) return -1;
+  for (int i = 0; result && i < nresult && i < (int)r.omega.size(); i++) {
+    result[4 * i] = r.omega[i].real();
+    result[4 * i + 1] = r.omega[i].imag();
+    result[4 * i + 2] = r.green[i].real();
+    result[4 * i + 3] = r.green[i].imag();
+  }
+  return 0;
+}
+
 int hphi_run(hphi_handle *h, const char *output_dir) {
   CHECK_HANDLE(h);
   const std::string out = output_dir ? output_dir : "output";
+  if (h->sector->model.calc_spec == 1) return hphi_spectrum(h, nullptr, out.c_str(), nullptr, 0);
   switch (h->sector->model.calc_type) {
     case kLanczos: return hphi_lanczos(h, nullptr, out.c_str(), nullptr, 0);
     case kTPQ:

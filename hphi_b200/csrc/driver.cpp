@@ -403,6 +403,8 @@ int lanczos_run(Sector *s, VecType vt, const double *h_init, const LanczosOption
       return -1;
     }
     RET(vec_scale(s, vt, 1.0 / std::sqrt(n2), P.p));
+  } else if (opt.device_start) {
+    RET(cuda_ok(cudaMemcpyAsync(P.p, opt.device_start, esz * dim, cudaMemcpyDeviceToDevice, s->stream), "start"));
   } else {
     RET(vec_from_host_c128(s, vt, h_init, P.p));
   }

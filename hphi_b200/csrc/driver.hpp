@@ -1,5 +1,6 @@
 // Lanczos / TPQ drivers over a device Sector.
 #pragma once
+#include <complex>
 #include <string>
 #include <vector>
 
@@ -29,6 +30,7 @@ struct LanczosOptions {
   const LanczosRestart *resume = nullptr;  // continue from these (ReStart 2 / 3)
   bool hashed_start = false;      // start from the hashed vector of hashed_seed, made on the
   uint64_t hashed_seed = 0;       // device (h_init is not read)
+  const void *device_start = nullptr;  // start from this normalised device vector in HPhi's order
 };
 
 // Green's function values of the model's OneBodyG / TwoBodyG rows (expec_cisajs,
@@ -119,6 +121,19 @@ struct TeResult {
   std::vector<double> time, energy, norm;
   int final_step = 0;
 };
+
+// Dynamical Green's function (spectrum.cu): the frequencies (omega, OmegaOrg included), the
+// Green's function on them, the excited state's norm and the Lanczos components a[1..steps],
+// b[1..steps].
+struct SpectrumResult {
+  std::vector<std::complex<double>> omega, green;
+  double dnorm = 0.0;
+  int steps = 0;
+  std::vector<double> alpha, beta;
+};
+// CalcSpectrum with CalcSpec 1 and the Lanczos method for the input vector h_vec (HPhi's
+// 1-based complex128 layout, org's sector); writes the output files to outdir.
+int spectrum_run(Sector *org, const double *h_vec, const std::string &outdir, SpectrumResult *res);
 
 // k-th smallest eigenvalue (0-based) of the symmetric tridiagonal matrix with diagonal
 // a[0..n) and off-diagonal b[0..n-1), by Sturm bisection; its eigenvector by inverse iteration.

@@ -367,7 +367,7 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
   }
   for (const char *must : {"calcmod", "modpara", "locspin"})
     if (!files.count(must)) { *err = std::string("namelist.def: missing ") + must; return -1; }
-  for (const char *unsupported : {"boost", "laser", "singleexcitation", "pairexcitation"})
+  for (const char *unsupported : {"boost", "laser"})
     if (files.count(unsupported)) {
       *err = std::string("namelist.def: keyword not supported by this engine: ") + unsupported;
       return -1;
@@ -393,9 +393,17 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       else if (k == "inputeigenvec" || k == "iev") m->input_eigenvec = (int)v;
       else if (k == "restart") m->restart = (int)v;
       else if (k == "flgfinitetemperature") m->flg_finite_temperature = (int)v;
-      else if (k == "outputham" || k == "inputham" || k == "outputexcitedvec" || k == "outputexvec" ||
-               k == "calcspec" || k == "calcspectrum" || k == "ngpu" || k == "scalapack") {
-        if ((k == "calcspec" || k == "calcspectrum" || k == "inputham") && v != 0) {
+      else if (k == "calcspec" || k == "calcspectrum") {
+        if (v != 0 && v != 1) {
+          *err = "calcmod.def: " + kw + " " + std::to_string(v) +
+                 " is not supported by this engine (0, or 1: spectrum from an input vector)";
+          return -1;
+        }
+        m->calc_spec = (int)v;
+      } else if (k == "outputexcitedvec" || k == "outputexvec") {
+        m->output_exvec = (int)v;
+      } else if (k == "outputham" || k == "inputham" || k == "ngpu" || k == "scalapack") {
+        if (k == "inputham" && v != 0) {
           *err = "calcmod.def: " + kw + " is not supported by this engine";
           return -1;
         }
@@ -421,9 +429,10 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
     while (std::getline(f, line)) {
       std::istringstream ss(line);
       std::string kw;
-      double v = 0.0;
+      double v = 0.0, v2 = 0.0;
       if (!(ss >> kw)) continue;
       if (!(ss >> v)) { *err = "modpara.def: malformed line: " + line; return -1; }
+      if (!(ss >> v2)) v2 = 0.0;  // second number (imaginary part of OmegaMax / OmegaMin / OmegaOrg)
       const std::string k = lower(kw);
       if (k == "nsite") m->nsite = (int)v;
       else if (k == "nup") m->nup = (int)v;
@@ -446,9 +455,12 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       else if (k == "precg") m->pre_cg = (int)v;
       else if (k == "expandcoef") m->expand_coef = (int)v;
       else if (k == "outputinterval") m->output_interval = (int)v;
-      else if (k == "timeslice" || k == "tinit" ||
-               k == "omegamax" || k == "omegamin" || k == "omegaim" || k == "omegaorg" || k == "nomega" ||
-               k == "targettpqrand") {
+      else if (k == "omegamax") { m->omega_max[0] = v; m->omega_max[1] = v2; m->omega_max_set = true; }
+      else if (k == "omegamin") { m->omega_min[0] = v; m->omega_min[1] = v2; m->omega_min_set = true; }
+      else if (k == "omegaim") { m->omega_org[1] += v; m->omega_org_set = true; }
+      else if (k == "omegaorg") { m->omega_org[0] += v; m->omega_org[1] += v2; m->omega_org_set = true; }
+      else if (k == "nomega") m->n_omega = (int)v;
+      else if (k == "timeslice" || k == "tinit" || k == "targettpqrand") {
         // accepted and ignored: parameters of modes outside this engine
       } else {
         *err = "modpara.def: unknown keyword " + kw;
@@ -897,6 +909,97 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
     }
     if ((int)m->te_time.size() != nsteps) { *err = fn + ": fewer time indices than AllTimeStep"; return -1; }
     m->te_kind = one ? 1 : 2;
+  }
+  // ---- SingleExcitation / PairExcitation (src/readdef.c:1943-2007): operators of the
+  // excited state A|v> for the dynamical Green's function, compiled in gather form on the
+  // excited sector's configurations.  Single: c+_{i s} (type 1) or c_{i s} (type 0), Hubbard
+  // models only.  Pair: c+_{i s1} c_{j s2} (type 1) or c_{i s1} c+_{j s2} (type 0; the
+  // reference stores it as -c+_{j s2} c_{i s1}, or 1 - n for i = j, s1 = s2); on spins the
+  // sites must agree and the pair is the one-site transition |s1><s2| (type 1), 1 - n_{s1}
+  // (type 0, s1 = s2) or -|s2><s1| (type 0, s1 != s2) (src/PairExSpin.c:251-330).
+  if (files.count("singleexcitation") || files.count("pairexcitation")) {
+    if (files.count("singleexcitation") && files.count("pairexcitation")) {
+      *err = "Error: Both single and pair excitation operators exist.";
+      return -1;
+    }
+    const bool spin = m->is_spin();
+    if (m->general_spin || m->is_kondo() || m->calc_model == kHubbardNConserved) {
+      *err = "excitation operators: supported for Hubbard, HubbardGC and spin-1/2 Spin / SpinGC models";
+      return -1;
+    }
+    const bool single = files.count("singleexcitation") > 0;
+    const std::string fn = files[single ? "singleexcitation" : "pairexcitation"];
+    if (!read_table(*m, fn, &rows, single ? 5 : 7, err)) return -1;
+    if (single && spin) { *err = "SingleExcitation is not allowed for spin system."; return -1; }
+    auto fbit = [](int site, int sg) { return 2 * site + sg; };
+    const uint64_t even = 0x5555555555555555ull;
+    int dup = 0, ddn = 0;
+    bool first = true;
+    for (const auto &r : rows) {
+      const int i = (int)r[0], s1 = (int)r[1];
+      uint64_t rm = 0, rv = 0, fl = 0, sm = 0;
+      int s0 = 0;
+      std::complex<double> coef;
+      bool ok;
+      if (single) {
+        const int type = (int)r[2];
+        coef = std::complex<double>(r[3], r[4]);
+        if (!check_site(i) || s1 < 0 || s1 > 1 || (type != 0 && type != 1)) { *err = fn + ": bad line"; return -1; }
+        // the reference's single-operator sign counts the occupied modes above the mode
+        // (child_Cis / child_Ajt, GC_Cis / GC_Ajt: src/mltplyHubbardCore.c:980-1180)
+        const uint64_t b = 1ull << fbit(i, s1);
+        rm = b;
+        rv = (type == 1) ? 0 : b;
+        fl = b;
+        sm = ~((b << 1) - 1);
+        ok = true;
+      } else {
+        const int j = (int)r[2], s2 = (int)r[3], type = (int)r[4];
+        coef = std::complex<double>(r[5], r[6]);
+        if (!check_site(i) || !check_site(j) || s1 < 0 || s1 > 1 || s2 < 0 || s2 > 1 || (type != 0 && type != 1)) {
+          *err = fn + ": bad line";
+          return -1;
+        }
+        if (spin) {
+          if (i != j) { *err = "Error: isite1 must be equal to isite2 for Spin system."; return -1; }
+          SpinOp op{i, s1, s2};
+          if (type == 0) {
+            if (s1 == s2) op = SpinOp{i, 1 - s1, 1 - s1};
+            else { op = SpinOp{i, s2, s1}; coef = -coef; }
+          }
+          ok = compile_spin({op}, 1, &rm, &rv, &fl);
+        } else if (type == 1) {
+          ok = compile_fermion({{fbit(i, s1), true}, {fbit(j, s2), false}}, &rm, &rv, &fl, &sm, &s0);
+        } else {
+          ok = compile_fermion({{fbit(i, s1), false}, {fbit(j, s2), true}}, &rm, &rv, &fl, &sm, &s0);
+        }
+      }
+      if (!ok) continue;  // identically zero (e.g. c c on one mode)
+      // particle change of the operator: the flipped bits before (rv & fl) and after
+      const uint64_t before = rv & fl, after = (rv ^ fl) & fl;
+      const int du = spin ? __builtin_popcountll(after) - __builtin_popcountll(before)
+                          : __builtin_popcountll(after & even) - __builtin_popcountll(before & even);
+      const int dd = spin ? 0 : __builtin_popcountll(after & ~even) - __builtin_popcountll(before & ~even);
+      if (first) { dup = du; ddn = dd; first = false; }
+      else if (!m->is_gc() && (du != dup || dd != ddn)) {
+        *err = fn + ": the operators lead to different sectors";
+        return -1;
+      }
+      if (s0) coef = -coef;
+      if (parity64(fl & sm)) coef = -coef;
+      m->excitation.push_back(BitTerm{rm, rv ^ (fl & rm), fl, sm, coef.real(), coef.imag()});
+    }
+    (single ? m->n_single_ex : m->n_pair_ex) = (int)rows.size();
+    m->ex_nup = m->nup;
+    m->ex_ndown = m->ndown;
+    m->ex_ne = m->ne;
+    m->ex_2sz = m->total_2sz;
+    if (!m->is_gc()) {
+      m->ex_nup += dup;
+      m->ex_ndown += ddn;
+      m->ex_ne += spin ? dup : dup + ddn;
+      m->ex_2sz += spin ? 2 * dup : dup - ddn;
+    }
   }
   canonicalize_terms(m);
   return 0;

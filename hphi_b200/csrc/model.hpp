@@ -87,6 +87,18 @@ struct Model {
   std::vector<std::vector<BitTerm>> te_offdiag;  // per step
   std::vector<std::vector<DiagTerm>> te_diag;    // per step
   std::string spectrum_vec;                      // SpectrumVec: head of the input vector file
+  // Dynamical Green's function (CalcSpec 1, src/CalcSpectrum.c:90-312): the SingleExcitation or
+  // PairExcitation operators compiled in gather form on the excited sector (flip 0 allowed),
+  // that sector's particle numbers (MakeExcitedList, :438-634) and the frequency grid
+  // (modpara OmegaMax / OmegaMin / OmegaIm / OmegaOrg / NOmega, src/readdef.c:624-642).
+  int calc_spec = 0;
+  int output_exvec = 0;
+  int n_single_ex = 0, n_pair_ex = 0;
+  std::vector<BitTerm> excitation;
+  int ex_nup = 0, ex_ndown = 0, ex_ne = 0, ex_2sz = 0;
+  bool omega_max_set = false, omega_min_set = false, omega_org_set = false;
+  double omega_max[2] = {0.0, 0.0}, omega_min[2] = {0.0, 0.0}, omega_org[2] = {0.0, 0.0};
+  int n_omega = 1000;
   int output_interval = 0;                       // OutputInterval (eigenvector files)
   // Raw term counts as read (for logs).
   int n_trans = 0, n_coulomb_intra = 0, n_coulomb_inter = 0, n_hund = 0, n_exchange = 0;

@@ -87,6 +87,17 @@ class ExpertModel:
     input_eigenvec: int = 0
     expand_coef: int = 0
     output_interval: int = 0
+    # dynamical Green's function (calc_spec 1, src/CalcSpectrum.c): SingleExcitation rows
+    # (i, s, type, re, im) or PairExcitation rows (i, s1, j, s2, type, re, im)
+    # (src/readdef.c:1943-2007) and the frequency grid (complex OmegaMax / OmegaMin, OmegaIm)
+    calc_spec: int = 0
+    single_excitation: List[Tuple] = field(default_factory=list)
+    pair_excitation: List[Tuple] = field(default_factory=list)
+    omega_max: Optional[complex] = None
+    omega_min: Optional[complex] = None
+    omega_im: Optional[float] = None
+    n_omega: Optional[int] = None
+    output_exvec: int = 0
 
     # ------------------------------------------------------------------ writers
     def write(self, directory: str) -> str:
@@ -114,6 +125,10 @@ class ExpertModel:
             ("ThreeBodyG", "greenthree.def", "NThreeBody", self.greenthree, " ".join(["{:d}"] * 12)),
             ("FourBodyG", "greenfour.def", "NFourBody", self.greenfour, " ".join(["{:d}"] * 16)),
             ("SixBodyG", "greensix.def", "NSixBody", self.greensix, " ".join(["{:d}"] * 24)),
+            ("SingleExcitation", "single.def", "NSingle", self.single_excitation,
+             "{:d} {:d} {:d} {:.17g} {:.17g}"),
+            ("PairExcitation", "pair.def", "NPair", self.pair_excitation,
+             "{:d} {:d} {:d} {:d} {:d} {:.17g} {:.17g}"),
         ]
         for kw, fname, head, rows, fmt in tables:
             if not rows:
@@ -158,6 +173,10 @@ class ExpertModel:
                 f.write(f"InputEigenVec {self.input_eigenvec}\n")
             if self.restart:
                 f.write(f"ReStart {self.restart}\n")
+            if self.calc_spec:
+                f.write(f"CalcSpec {self.calc_spec}\n")
+            if self.output_exvec:
+                f.write(f"OutputExVec {self.output_exvec}\n")
 
     def _write_modpara(self, path: str) -> None:
         lines = ["--------------------", "Model_Parameters   0", "--------------------",
@@ -181,6 +200,14 @@ class ExpertModel:
             lines.append(f"ExpandCoef     {self.expand_coef}")
         if self.output_interval:
             lines.append(f"OutputInterval {self.output_interval}")
+        if self.omega_max is not None:
+            lines.append(f"OmegaMax       {complex(self.omega_max).real!r} {complex(self.omega_max).imag!r}")
+        if self.omega_min is not None:
+            lines.append(f"OmegaMin       {complex(self.omega_min).real!r} {complex(self.omega_min).imag!r}")
+        if self.omega_im is not None:
+            lines.append(f"OmegaIm        {self.omega_im!r}")
+        if self.n_omega is not None:
+            lines.append(f"NOmega         {self.n_omega}")
         with open(path, "w") as f:
             f.write("\n".join(lines) + "\n")
 

@@ -120,6 +120,21 @@ int hphi_mltply_device_async(hphi_handle *h, int vec_type, void *d_v0, const voi
                              double *d_prdct);
 
 /*
+ * Dynamical Green's function by the Lanczos method: CalcSpectrum with CalcSpec 1
+ * (src/CalcSpectrum.c:90-312) and CalcSpectrumByLanczos (src/CalcSpectrumByLanczos.c:43-163).
+ * The excitation operators of the input (SingleExcitation / PairExcitation) act on h_vec
+ * (HPhi-layout complex128, 2*(dim+1) doubles; NULL: <SpectrumVec>_rank_0.dat in output_dir),
+ * the Lanczos tridiagonal components of the normalised excited state are computed on its
+ * sector and G(omega) = |A v|^2 / (omega - a_1 - b_1^2 / (omega - a_2 - ...)) is evaluated on the
+ * modpara frequency grid (OmegaMax, OmegaMin, OmegaIm / OmegaOrg, NOmega; without OmegaMax /
+ * OmegaMin, from <head>_Lanczos_Step.dat as the reference's SetOmega does).  Writes
+ * <head>_DynamicalGreen.dat, <head>_TMComponents.dat and, with OutputExVec 1,
+ * <head>_excitedvec_rank_0.dat.  result (optional): per frequency Re omega, Im omega (OmegaOrg
+ * included), Re G, Im G, for the first nresult frequencies.
+ */
+int hphi_spectrum(hphi_handle *h, const double *h_vec, const char *output_dir, double *result, int nresult);
+
+/*
  * The H*v of hphi_mltply_device_async for callers that may not allocate device memory
  * when they call it: code whose device memory belongs to another allocator's budget, or a
  * latency-bound loop that cannot take cudaMalloc's device-wide synchronisation.  Same
