@@ -27,7 +27,8 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-__all__ = ["Hamiltonian", "Batch", "Server", "HPhiError", "inspect_terms", "inspect_green", "load_library",
+__all__ = ["Hamiltonian", "Batch", "Server", "HPhiError", "inspect_terms", "inspect_green", "standard_mode",
+           "load_library",
            "library_path", "REAL64", "COMPLEX128", "INFO_FIELDS", "EXPORTED_SYMBOLS"]
 
 REAL64 = 0
@@ -45,7 +46,8 @@ EXPORTED_SYMBOLS = ["hphi_version", "hphi_last_error", "hphi_open_expert", "hphi
                     "hphi_batch_free", "hphi_server_create", "hphi_server_submit", "hphi_server_step",
                     "hphi_server_poll", "hphi_server_clock", "hphi_server_free", "hphi_lobpcg",
                     "hphi_reference_start", "hphi_expec_green", "hphi_expec_cisajs", "hphi_expec_cisajscktaltdc",
-                    "hphi_inspect_green", "hphi_expec_green_device", "hphi_spectrum"]
+                    "hphi_inspect_green", "hphi_expec_green_device", "hphi_spectrum",
+                    "hphi_stdface"]
 FP64 = 0
 FP32 = 1
 BATCH_GRAPH = 1
@@ -162,6 +164,16 @@ def reference_start(dim: int, kind: int = REF_LANCZOS, initial_iv: int = -1, sam
     _check(load_library().hphi_reference_start(int(dim), int(kind), int(initial_iv), int(sample), int(vec_type),
                                                int(threads), int(count), _dptr(v.view(np.float64))))
     return v
+
+
+def standard_mode(stan_in: str, out_dir: str) -> str:
+    """Standard mode (`HPhi -sdry stan.in`): writes the expert-mode files of the keyword file
+    `stan_in` into `out_dir`; returns the path of the namelist.def written there.  Host only."""
+    lib = load_library()
+    lib.hphi_stdface.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+    os.makedirs(out_dir, exist_ok=True)
+    _check(lib.hphi_stdface(stan_in.encode(), out_dir.encode()))
+    return os.path.join(out_dir, "namelist.def")
 
 
 def inspect_terms(namelist_def: str):

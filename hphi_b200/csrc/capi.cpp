@@ -15,6 +15,7 @@
 #include "hv_product.hpp"
 #include "refrand.hpp"
 #include "model.hpp"
+#include "stdface.hpp"
 
 namespace hphi {
 namespace {
@@ -91,6 +92,13 @@ int hphi_open_expert(const char *namelist_def, int device, hphi_handle **out) {
   h->sector = s;
   if (cuda_fail(cudaMalloc(&h->d_scal, sizeof(double) * 8), "alloc")) { hphi_close(h); return -1; }
   *out = h;
+  return 0;
+}
+
+int hphi_stdface(const char *stan_in, const char *out_dir) {
+  if (!stan_in || !out_dir) { set_error("null argument"); return -1; }
+  std::string err;
+  if (stdface::generate(stan_in, out_dir, &err) != 0) { set_error(err); return -1; }
   return 0;
 }
 

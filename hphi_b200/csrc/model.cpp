@@ -580,9 +580,6 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       if (!check_site(i) || !check_site(j) || !sigma_ok(i, s1) || !sigma_ok(j, s2)) {
         *err = files["trans"] + ": bad site or spin index"; return -1;
       }
-      if (m->general_spin && m->calc_model == kSpin && s1 != s2) {
-        *err = files["trans"] + ": a canonical general-spin model only takes diagonal transfers"; return -1;
-      }
       if (i == j && s1 == s2 && std::fabs(r[5]) > 1e-12) {
         *err = files["trans"] + ": diagonal transfer with an imaginary part"; return -1;
       }
@@ -608,6 +605,9 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       int i, s1, j, s2;
       std::tie(i, s1, j, s2) = key;
       const std::complex<double> t = tr[key];
+      // A canonical spin sector keeps Sz: the reference's multiply absorbs only the diagonal
+      // transfers and never applies spin-flip ones (src/mltplySpin.c:208-211, 327-329).
+      if (m->calc_model == kSpin && s1 != s2) continue;
       if (spin) add_spin_string(m, {{i, s1, s2}}, -t);
       else add_fermion_string(m, {{fbit(i, s1), true}, {fbit(j, s2), false}}, -t);
     }

@@ -61,6 +61,15 @@ const char *hphi_last_error(void);
 int hphi_open_expert(const char *namelist_def, int device, hphi_handle **out);
 
 /*
+ * Standard mode: reads the keyword file stan_in (lattice = chain / ladder / square /
+ * triangular / honeycomb / kagome; model = Hubbard / Spin / Kondo and their GC forms;
+ * method = Lanczos / CG / TPQ / cTPQ; their parameters) and writes namelist.def and the
+ * expert-mode files it lists into out_dir, which then open with hphi_open_expert.  Host only.
+ * Replaces: StdFace_main (called at src/HPhiMain.c:212-214 for `HPhi -s` / `HPhi -sdry`).
+ */
+int hphi_stdface(const char *stan_in, const char *out_dir);
+
+/*
  * Reads an expert-mode input on the host only (no device needed) and exports the
  * compiled Hamiltonian: counts[0] = off-diagonal terms, counts[1] = diagonal terms.
  * Off-diagonal term k (gather form, for an output configuration t): applies iff

@@ -1,0 +1,22 @@
+"""The reference's standard-mode test scripts (test/*.sh, replayed from tests/golden/stdface/)
+end to end on the engine: `HPhi_b200 -s stan.in` (the standard-mode generator, then the
+engine's drivers on the GPU) must print what each script checks, by the script's own
+criteria: energies, one- and two-body correlation functions, multi-body Green's functions and
+dynamical Green's functions summed |difference| < 5e-7 per block, restarted runs, and TPQ
+averages within twice the reference's error bars.  The reference computes the spectra of these
+scripts (method CG) by shifted BiCG; the engine's Lanczos continued fraction of the same
+Green's function matches them to the printed digits.  Full diagonalisation is outside the
+engine (its scripts pin the generator on the CPU, tests/test_stdface_cpu.py)."""
+import pytest
+
+import stdface_runner as R
+
+pytestmark = pytest.mark.gpu
+
+ENGINE_CASES = [n for n in R.names() if not n.startswith(("fulldiag_", "te_"))]
+
+
+@pytest.mark.parametrize("name", ENGINE_CASES)
+def test_engine_reproduces_standard_mode_test(name, tmp_path):
+    problems = R.run(name, str(tmp_path / name), backend="engine")
+    assert not problems, problems
