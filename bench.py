@@ -25,6 +25,8 @@ metric (solves/s and latency against the plain FP64 GPU path):
              half-filled Hubbard chains L=10..14 (U in [2,10]) and 24-site Kitaev-Heisenberg
              honeycomb (SpinGC, complex) through the continuous-batching server: solves/s,
              p50/p99 latency, |dE| against each request solved alone by the plain driver.
+  tpq        mTPQ on a 26-site J1-J2 chain (dim 10,400,600): NumAve = 8 samples in lockstep with
+             one block H*V per step against the same samples one after another.
   green      expec_cisajs on the 4x4 Hubbard sector: the 512 spin-conserving one-body rows of a
              normalised random vector (rows x sector rows per second), the reference's
              expec_cisajs timed on 8 of the rows as the CPU baseline.
@@ -558,6 +560,57 @@ def run_tem_mode(args):
     print(json.dumps(out))
 
 
+def run_tpq_mode(args):
+    """mTPQ with its NumAve = 8 samples in lockstep (one block H*V over the samples per step,
+    hv_block_native) against the same samples one after another, on a 26-site J1-J2 chain
+    (2Sz = 0, dim 10,400,600, complex vectors, the general kernel): K timed steps each, host
+    clock around calc_by_tpq with W and W + K steps (difference / K).  Both runs write the
+    same files; the first step lines are compared."""
+    import hphi_b200
+    from hphi_b200 import expert
+    W, K = max(args.warmup, 3), max(args.steps // 25, 10)
+    L, nave = 26, 8
+    bonds = expert.chain_bonds(L) + expert.chain_bonds(L, 2)
+    tmp = tempfile.mkdtemp()
+    res = {}
+    first_lines = {}
+    for mode in ("serial", "block"):
+        os.environ["HPHI_B200_TPQ_BLOCK"] = "1" if mode == "block" else "0"
+        times = {}
+        for n in (W, W + K):
+            m = expert.heisenberg(L, bonds, J=[1.0] * L + [0.35] * L, calc_type="TPQ", lanczos_max=n, num_ave=nave,
+                                  large_value=2.0, expec_interval=100000)
+            d = os.path.join(tmp, f"{mode}{n}")
+            with hphi_b200.Hamiltonian(m.write(d)) as H:
+                dim = H.dim
+                if n == W and mode == "serial":
+                    H.calc_by_tpq(output_dir=os.path.join(d, "warm"))   # first-call setup
+                    clocks = _clock_start()
+                t0 = time.perf_counter()
+                H.calc_by_tpq(output_dir=os.path.join(d, "output"))
+                times[n] = time.perf_counter() - t0
+        res[mode] = (times[W + K] - times[W]) / K
+        with open(os.path.join(tmp, f"{mode}{W + K}", "output", "SS_rand7.dat")) as f:
+            first_lines[mode] = f.read().split("\n")[:6]
+    os.environ.pop("HPHI_B200_TPQ_BLOCK", None)
+    cl = clocks.stop()
+    shutil.rmtree(tmp, ignore_errors=True)
+    hv_bytes = nave * 3.0 * dim * 16
+    out = {"metric": METRIC, "mode": "tpq", "value": nave / res["block"], "unit": "sample-steps/s", "n_gpus": 1,
+           "steps": K, "warmup": W, "ms_per_step": 1e3 * res["block"], "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+           "config": {"workload": "J1-J2 chain L=26 (J2=0.35), 2Sz=0, mTPQ", "dim": dim, "samples": nave,
+                      "timing": "host clock around calc_by_tpq with W and W+K steps (difference / K); "
+                                "each step reads its norms and energies to the host and appends the files",
+                      "l2": "vectors (166 MB each) exceed L2 together; no flush"},
+           "serial_ms_per_step": 1e3 * res["serial"], "block_ms_per_step": 1e3 * res["block"],
+           "speedup_block_vs_serial": res["serial"] / res["block"],
+           "hv_equivalent_gbs_block": hv_bytes / res["block"] / 1e9,
+           "hv_equivalent_gbs_serial": hv_bytes / res["serial"] / 1e9,
+           "files_equal": first_lines["serial"] == first_lines["block"], "clocks": cl}
+    print(json.dumps(out))
+
+
 def serve_requests(n: int, seed: int = 50):
     from hphi_b200 import expert
     rng = np.random.default_rng(seed)
@@ -643,7 +696,7 @@ def run_serve_mode(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", default="hv", choices=["hv", "batch", "precision", "serve", "green", "tem"])
+    ap.add_argument("--mode", default="hv", choices=["hv", "batch", "precision", "serve", "green", "tem", "tpq"])
     ap.add_argument("--batch-size", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=300)
     ap.add_argument("--precision-steps", type=int, default=300)
@@ -672,7 +725,7 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         {"batch": run_batch_mode, "precision": run_precision_mode, "serve": run_serve_mode,
-         "green": run_green_mode, "tem": run_tem_mode}[args.mode](args)
+         "green": run_green_mode, "tem": run_tem_mode, "tpq": run_tpq_mode}[args.mode](args)
         return
 
     import torch

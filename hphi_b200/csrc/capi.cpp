@@ -530,21 +530,58 @@ int hphi_tpq(hphi_handle *h, const double *v_init, const char *output_dir, doubl
   const std::string out = output_dir ? output_dir : "output";
   const int64_t stride = 2 * (s->dim + 1);
   TpqResult r;
-  std::vector<double> start;
   const int restart = s->model.restart;  // RESTART_OUT 1, RESTART_INOUT 2, RESTART_IN 3
-  for (int rand_i = 0; rand_i < s->model.num_ave; rand_i++) {
-    TpqOptions opt;
-    opt.keep_vector = restart == 1 || restart == 2;
-    const double *v = nullptr;
+  TpqOptions opt;
+  opt.keep_vector = restart == 1 || restart == 2;
+  auto tmpvec = [&](int rand_i) {
     char vname[256];
     snprintf(vname, sizeof(vname), "tmpvec_set%d_rank_%d.dat", rand_i, 0);
-    const std::string vpath = out + "/" + vname;
+    return out + "/" + vname;
+  };
+  auto save = [&](int rand_i, const TpqResult &rr) -> int {
+    // tmpvec_set%d_rank_%d.dat after the loop (src/CalcByTPQ.c:275-290)
+    FILE *fo = fopen(tmpvec(rand_i).c_str(), "wb");
+    if (!fo) {
+      set_error("cannot write " + tmpvec(rand_i));
+      return -1;
+    }
+    const int stp = rr.final_step;
+    const long dim = (long)s->dim;
+    fwrite(&stp, sizeof(int), 1, fo);
+    fwrite(&dim, sizeof(long), 1, fo);
+    fwrite(rr.final_vector.data(), sizeof(double), rr.final_vector.size(), fo);
+    fclose(fo);
+    return 0;
+  };
+  // The samples of the reference's loop (src/CalcByTPQ.c:76) run in blocks of up to
+  // kHvBlockMax in lockstep, sharing each H application (one block H*V), where the sector's
+  // H*v is the general kernel; a sample continued from a stored state runs alone.
+  const char *blk_env = std::getenv("HPHI_B200_TPQ_BLOCK");
+  const bool block_ok = hv_block_applies(s, vt) && !(blk_env && std::strcmp(blk_env, "0") == 0);
+  const int block_max = block_ok ? kHvBlockMax : 1;
+  std::vector<std::vector<double>> starts;
+  std::vector<int> pending;
+  auto run_pending = [&]() -> int {
+    if (pending.empty()) return 0;
+    std::vector<const double *> hv;
+    for (size_t b = 0; b < pending.size(); b++) hv.push_back(starts[b].empty() ? v_init + stride * pending[b] : starts[b].data());
+    std::vector<TpqResult> rr;
+    if (tpq_run_samples(s, vt, hv, pending, out, &rr, opt, block_ok && pending.size() > 1) != 0) return -1;
+    for (size_t b = 0; b < pending.size(); b++)
+      if (opt.keep_vector && save(pending[b], rr[b]) != 0) return -1;
+    r = std::move(rr.back());
+    pending.clear();
+    starts.clear();
+    return 0;
+  };
+  for (int rand_i = 0; rand_i < s->model.num_ave; rand_i++) {
+    const std::string vpath = tmpvec(rand_i);
     FILE *fin = (restart == 2 || restart == 3) ? fopen(vpath.c_str(), "rb") : nullptr;
     if (fin) {
       // stored state: int step, long dim, complex128[dim+1] (src/CalcByTPQ.c:86-104)
       int stp = 0;
       long dim = 0;
-      start.assign(stride, 0.0);
+      std::vector<double> start(stride, 0.0);
       const bool ok = fread(&stp, sizeof(int), 1, fin) == 1 && fread(&dim, sizeof(long), 1, fin) == 1 &&
                       dim == (long)s->dim && fread(start.data(), sizeof(double), stride, fin) == (size_t)stride;
       fclose(fin);
@@ -552,33 +589,24 @@ int hphi_tpq(hphi_handle *h, const double *v_init, const char *output_dir, doubl
         set_error("Error: A file of Inputvector is incorrect.");
         return -1;
       }
-      opt.resume_step = stp;
-      v = start.data();
-    } else if (v_init) {
+      if (run_pending() != 0) return -1;
+      TpqOptions o = opt;
+      o.resume_step = stp;
+      if (tpq_run(s, vt, start.data(), rand_i, out, &r, o) != 0) return -1;
+      if (opt.keep_vector && save(rand_i, r) != 0) return -1;
+      continue;
+    }
+    pending.push_back(rand_i);
+    starts.emplace_back();
+    if (!v_init) {
       // a missing stored state starts the sample normally, as the reference announces
       // (src/CalcByTPQ.c:93-96; it then reads from the missing file, here it does not)
-      v = v_init + stride * rand_i;
-    } else {
       reference_random_start(s->dim, kRefTPQ, s->model.initial_iv, rand_i, s->model.initial_vec_type,
-                             reference_threads(), 1, &start);
-      v = start.data();
+                             reference_threads(), 1, &starts.back());
     }
-    if (tpq_run(s, vt, v, rand_i, out, &r, opt) != 0) return -1;
-    if (opt.keep_vector) {
-      // tmpvec_set%d_rank_%d.dat after the loop (src/CalcByTPQ.c:275-290)
-      FILE *fo = fopen(vpath.c_str(), "wb");
-      if (!fo) {
-        set_error("cannot write " + vpath);
-        return -1;
-      }
-      const int stp = r.final_step;
-      const long dim = (long)s->dim;
-      fwrite(&stp, sizeof(int), 1, fo);
-      fwrite(&dim, sizeof(long), 1, fo);
-      fwrite(r.final_vector.data(), sizeof(double), r.final_vector.size(), fo);
-      fclose(fo);
-    }
+    if ((int)pending.size() == block_max && run_pending() != 0) return -1;
   }
+  if (run_pending() != 0) return -1;
   if (result)
     for (int i = 0; i < nresult && i < (int)r.energy.size(); i++) result[i] = r.energy[i];
   return 0;

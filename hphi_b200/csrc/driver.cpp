@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -817,83 +818,132 @@ int write_lanczos_outputs(const Sector &s, const LanczosResult &r, const std::st
 // ------------------------------------------------------------------------ TPQ
 int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::string &outdir, TpqResult *res,
             const TpqOptions &opt) {
+  std::vector<TpqResult> r(1);
+  const int rc = tpq_run_samples(s, vt, {h_init}, {rand_i}, outdir, &r, opt, false);
+  *res = std::move(r[0]);
+  return rc;
+}
+
+int tpq_run_samples(Sector *s, VecType vt, const std::vector<const double *> &h_init, const std::vector<int> &rand_i,
+                    const std::string &outdir, std::vector<TpqResult> *res, const TpqOptions &opt, bool block) {
+  // Samples run in lockstep: every H application of a step is one block H*V over all of them
+  // (hv_block_native) when `block`, else one launch per sample; everything else is per sample.
   const Model &m = s->model;
+  const int nb = (int)h_init.size();
   const int64_t dim = s->dim;
   const size_t esz = (vt == kReal64) ? sizeof(double) : sizeof(cplx);
   const double Ns = (double)m.nsite;
   const double L = m.large_value;
-  RET(cuda_ok(cudaSetDevice(s->device), "cudaSetDevice"));
-  DevBuf V, H, ST;
-  RET(cuda_ok(cudaMalloc(&V.p, esz * dim), "alloc V"));
-  RET(cuda_ok(cudaMalloc(&H.p, esz * dim), "alloc H"));
-  RET(cuda_ok(cudaMalloc(&ST.p, sizeof(double) * 32), "alloc scalars"));
-  double *st = (double *)ST.p;
-  // h_init is the un-normalised start vector; its norm is global_1st_norm.
-  RET(vec_from_host_c128(s, vt, h_init, H.p));
-  RET(to_native(s, vt, H.p, V.p));
-  double n0 = 0.0;
-  RET(vec_norm2(s, vt, V.p, st + 0));
-  RET(cuda_ok(cudaMemcpyAsync(&n0, st, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "read"));
-  RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
-  const bool resumed = opt.resume_step > 0;
-  // global_1st_norm is only set by MakeIniVec, so a continued run prints 0 (its initial value)
-  const double first_norm = resumed ? 0.0 : std::sqrt(n0);
-  double sv = 1.0 / std::sqrt(n0);  // V holds the current vector times 1/sv
-  RET(ensure_dir(outdir));
-  char name[256];
-  snprintf(name, sizeof(name), "SS_rand%d.dat", rand_i);
-  const std::string ss_file = join(outdir, name);
-  snprintf(name, sizeof(name), "Norm_rand%d.dat", rand_i);
-  const std::string norm_file = join(outdir, name);
-  snprintf(name, sizeof(name), "Flct_rand%d.dat", rand_i);
-  const std::string flct_file = join(outdir, name);
-  const char *mode = resumed ? "a" : "w";  // a continued run appends (src/CalcByTPQ.c:118-136)
-  FILE *fss = fopen(ss_file.c_str(), mode), *fnorm = fopen(norm_file.c_str(), mode), *fflct = fopen(flct_file.c_str(), mode);
-  if (!fss || !fnorm || !fflct) {
-    if (fss) fclose(fss);
-    if (fnorm) fclose(fnorm);
-    if (fflct) fclose(fflct);
-    set_error("cannot write TPQ output files in " + outdir);
+  if (nb < 1 || (int)rand_i.size() != nb || (block && (nb > kHvBlockMax || !hv_block_applies(s, vt))) ||
+      (nb > 1 && opt.resume_step > 0)) {
+    set_error("tpq_run_samples: bad sample block");
     return -1;
   }
-  if (!resumed) {
-    fprintf(fss, " # inv_tmp, energy, phys_var, phys_doublon, phys_num, step_i\n");
-    fprintf(fnorm, " # inv_temp, global_norm, global_1st_norm, step_i \n");
-    fprintf(fflct, " # inv_temp, N, N^2, D, D^2, Sz, Sz^2, step_i \n");
+  res->assign(nb, TpqResult());
+  RET(cuda_ok(cudaSetDevice(s->device), "cudaSetDevice"));
+  constexpr int kSlots = 32;  // per-sample scalar slots (coefficients, sums)
+  DevBuf V, H, ST, PART;
+  RET(cuda_ok(cudaMalloc(&V.p, esz * dim * nb), "alloc V"));
+  RET(cuda_ok(cudaMalloc(&H.p, esz * dim * nb), "alloc H"));
+  RET(cuda_ok(cudaMalloc(&ST.p, sizeof(double) * kSlots * nb), "alloc scalars"));
+  if (block) RET(cuda_ok(cudaMalloc(&PART.p, sizeof(double) * 2 * nb * (size_t)s->red_blocks), "alloc partials"));
+  auto vec = [&](void *base, int b) { return (void *)((char *)base + esz * dim * b); };
+  auto slot = [&](int b) { return (double *)ST.p + kSlots * b; };
+  // h_init[b] is the un-normalised start vector of sample b; its norm is global_1st_norm.
+  for (int b = 0; b < nb; b++) {
+    RET(vec_from_host_c128(s, vt, h_init[b], vec(H.p, b)));
+    RET(to_native(s, vt, vec(H.p, b), vec(V.p, b)));
+    RET(vec_norm2(s, vt, vec(V.p, b), slot(b)));
   }
-  // expec_energy_flct on the current vector (sv*V): observables, H = H*(sv V), E, var.
-  double ob[6], E = 0.0, var = 0.0;
-  auto expec = [&]() -> int {
-    RET(native_observables(s, vt, V.p, st + 16));
-    const double coef[2] = {0.0, sv};
-    RET(cuda_ok(cudaMemcpyAsync(st + 4, coef, sizeof(coef), cudaMemcpyHostToDevice, s->stream), "coef"));
-    RET(hv_native(s, vt, V.p, H.p, st + 4, st + 6, false));
-    RET(vec_norm2(s, vt, H.p, st + 8));
-    double sc[3];
-    RET(cuda_ok(cudaMemcpyAsync(sc, st + 6, sizeof(double) * 3, cudaMemcpyDeviceToHost, s->stream), "read"));
-    RET(cuda_ok(cudaMemcpyAsync(ob, st + 16, sizeof(double) * 6, cudaMemcpyDeviceToHost, s->stream), "read"));
-    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
-    const double w2 = sv * sv;
-    for (double &o : ob) o *= w2;
-    E = sc[0] * sv * sv;
-    var = sc[2];
+  std::vector<double> host(kSlots * nb);
+  auto read_slots = [&]() -> int {
+    RET(cuda_ok(cudaMemcpyAsync(host.data(), ST.p, sizeof(double) * kSlots * nb, cudaMemcpyDeviceToHost, s->stream),
+                "read"));
+    return cuda_ok(cudaStreamSynchronize(s->stream), "sync");
+  };
+  RET(read_slots());
+  const bool resumed = opt.resume_step > 0;
+  // global_1st_norm is only set by MakeIniVec, so a continued run prints 0 (its initial value)
+  std::vector<double> first_norm(nb), sv(nb);  // V_b holds the current vector times 1/sv[b]
+  for (int b = 0; b < nb; b++) {
+    first_norm[b] = resumed ? 0.0 : std::sqrt(host[kSlots * b]);
+    sv[b] = 1.0 / std::sqrt(host[kSlots * b]);
+  }
+  RET(ensure_dir(outdir));
+  std::vector<FILE *> fss(nb, nullptr), fnorm(nb, nullptr), fflct(nb, nullptr);
+  struct Closer {
+    std::vector<FILE *> *f[3];
+    ~Closer() {
+      for (auto *v : f)
+        for (FILE *x : *v)
+          if (x) fclose(x);
+    }
+  } closer{{&fss, &fnorm, &fflct}};
+  const char *mode = resumed ? "a" : "w";  // a continued run appends (src/CalcByTPQ.c:118-136)
+  for (int b = 0; b < nb; b++) {
+    char name[256];
+    snprintf(name, sizeof(name), "SS_rand%d.dat", rand_i[b]);
+    fss[b] = fopen(join(outdir, name).c_str(), mode);
+    snprintf(name, sizeof(name), "Norm_rand%d.dat", rand_i[b]);
+    fnorm[b] = fopen(join(outdir, name).c_str(), mode);
+    snprintf(name, sizeof(name), "Flct_rand%d.dat", rand_i[b]);
+    fflct[b] = fopen(join(outdir, name).c_str(), mode);
+    if (!fss[b] || !fnorm[b] || !fflct[b]) {
+      set_error("cannot write TPQ output files in " + outdir);
+      return -1;
+    }
+    if (!resumed) {
+      fprintf(fss[b], " # inv_tmp, energy, phys_var, phys_doublon, phys_num, step_i\n");
+      fprintf(fnorm[b], " # inv_temp, global_norm, global_1st_norm, step_i \n");
+      fprintf(fflct[b], " # inv_temp, N, N^2, D, D^2, Sz, Sz^2, step_i \n");
+    }
+  }
+  // H applied to every sample: dst_b = acc_b dst_b + scale_b H src_b with (acc, scale) in slot
+  // c0 and <src_b|H src_b> into slot c0 + 2 of each sample
+  auto apply_h = [&](void *src, void *dst, int c0) -> int {
+    if (block)
+      return hv_block_native(s, vt, nb, dim, src, dst, slot(0) + c0, kSlots, slot(0) + c0 + 2, kSlots,
+                             (double *)PART.p);
+    for (int b = 0; b < nb; b++) RET(hv_native(s, vt, vec(src, b), vec(dst, b), slot(b) + c0, slot(b) + c0 + 2, false));
     return 0;
   };
-  auto write_lines = [&](double inv_temp, double gnorm, int step, bool flct) {
-    fprintf(fss, "%.16lf  %.16lf %.16lf %.16lf %.16lf %d\n", inv_temp, E, var, ob[0], ob[2], step);
-    fprintf(fnorm, "%.16lf %.16lf %.16lf %d\n", inv_temp, gnorm, first_norm, step);
-    if (flct)
-      fprintf(fflct, "%.16lf %.16lf %.16lf %.16lf %.16lf %.16lf %.16lf %d\n", inv_temp, ob[2], ob[3], ob[0], ob[1],
-              ob[4], ob[5], step);
+  // expec_energy_flct on every sample's current vector sv*V: observables, H = H*(sv V), E, var.
+  std::vector<std::array<double, 6>> ob(nb);
+  std::vector<double> E(nb, 0.0), var(nb, 0.0);
+  auto expec = [&]() -> int {
+    for (int b = 0; b < nb; b++) {
+      RET(native_observables(s, vt, vec(V.p, b), slot(b) + 16));
+      const double coef[2] = {0.0, sv[b]};
+      RET(cuda_ok(cudaMemcpyAsync(slot(b) + 4, coef, sizeof(coef), cudaMemcpyHostToDevice, s->stream), "coef"));
+    }
+    RET(apply_h(V.p, H.p, 4));
+    for (int b = 0; b < nb; b++) RET(vec_norm2(s, vt, vec(H.p, b), slot(b) + 8));
+    RET(read_slots());
+    for (int b = 0; b < nb; b++) {
+      const double *h = host.data() + kSlots * b;
+      const double w2 = sv[b] * sv[b];
+      for (int k = 0; k < 6; k++) ob[b][k] = h[16 + k] * w2;
+      E[b] = h[6] * sv[b] * sv[b];
+      var[b] = h[8];
+    }
+    return 0;
   };
-  auto multiply = [&](double *gnorm) -> int {
+  auto write_lines = [&](int b, double inv_temp, double gnorm, int step, bool flct) {
+    fprintf(fss[b], "%.16lf  %.16lf %.16lf %.16lf %.16lf %d\n", inv_temp, E[b], var[b], ob[b][0], ob[b][2], step);
+    fprintf(fnorm[b], "%.16lf %.16lf %.16lf %d\n", inv_temp, gnorm, first_norm[b], step);
+    if (flct)
+      fprintf(fflct[b], "%.16lf %.16lf %.16lf %.16lf %.16lf %.16lf %.16lf %d\n", inv_temp, ob[b][2], ob[b][3],
+              ob[b][0], ob[b][1], ob[b][4], ob[b][5], step);
+  };
+  std::vector<double> gnorm(nb, 0.0), inv_temp(nb, 0.0);
+  auto multiply = [&]() -> int {
     // v = L*v - H v / Ns with v = sv V: V <- (L sv) V - (1/Ns) H, then normalise lazily.
-    RET(vec_tpq_sweep(s, vt, L * sv, 1.0 / Ns, V.p, H.p, st + 10));
-    double n2 = 0.0;
-    RET(cuda_ok(cudaMemcpyAsync(&n2, st + 10, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "read"));
-    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
-    *gnorm = std::sqrt(n2);
-    sv = 1.0 / *gnorm;
+    for (int b = 0; b < nb; b++) RET(vec_tpq_sweep(s, vt, L * sv[b], 1.0 / Ns, vec(V.p, b), vec(H.p, b), slot(b) + 10));
+    RET(read_slots());
+    for (int b = 0; b < nb; b++) {
+      gnorm[b] = std::sqrt(host[kSlots * b + 10]);
+      sv[b] = 1.0 / gnorm[b];
+    }
     return 0;
   };
   // Green's functions of the normalised state sv*V at step 0 and at every ExpecInterval-th
@@ -903,15 +953,16 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
   DevBuf GV;
   if (green) RET(cuda_ok(cudaMalloc(&GV.p, esz * dim), "alloc Green's function staging"));
   auto green_step = [&](int step) -> int {
-    RET(from_native(s, vt, V.p, GV.p));
-    GreenValues g;
-    RET(model_green(s, vt, GV.p, sv * sv, &g));
-    char suffix[64];
-    snprintf(suffix, sizeof(suffix), "_set%dstep%d", rand_i, step);
-    return write_green_files(m, g, outdir, suffix);
+    for (int b = 0; b < nb; b++) {
+      RET(from_native(s, vt, vec(V.p, b), GV.p));
+      GreenValues g;
+      RET(model_green(s, vt, GV.p, sv[b] * sv[b], &g));
+      char suffix[64];
+      snprintf(suffix, sizeof(suffix), "_set%dstep%d", rand_i[b], step);
+      RET(write_green_files(m, g, outdir, suffix));
+    }
+    return 0;
   };
-  res->energy.clear();
-  res->inv_temp.clear();
   // canonical TPQ (CalcType 5, CalcByCanonicalTPQ src/CalcByCanonicalTPQ.c:52-287): the step
   // is v <- exp(-dtau H / 2) v / |.|, dtau = 1/LargeValue, by a Taylor sum of ExpandCoef terms
   // (MultiplyForCanonicalTPQ src/Multiply.c:162-203), and the inverse temperature grows by dtau
@@ -920,38 +971,44 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
   const double dtau = 1.0 / L;
   DevBuf CA, CT, CU;
   if (canonical) {
-    RET(cuda_ok(cudaMalloc(&CA.p, esz * dim), "alloc cTPQ sum"));
-    RET(cuda_ok(cudaMalloc(&CT.p, esz * dim), "alloc cTPQ term"));
-    RET(cuda_ok(cudaMalloc(&CU.p, esz * dim), "alloc cTPQ term"));
+    RET(cuda_ok(cudaMalloc(&CA.p, esz * dim * nb), "alloc cTPQ sum"));
+    RET(cuda_ok(cudaMalloc(&CT.p, esz * dim * nb), "alloc cTPQ term"));
+    RET(cuda_ok(cudaMalloc(&CU.p, esz * dim * nb), "alloc cTPQ term"));
   }
-  auto ctpq_multiply = [&](double *gnorm_out) -> int {
+  auto ctpq_multiply = [&]() -> int {
     // x = sv V and h = H x (expec left H x in H): sum = x + a h + sum_c a^c/c! H^c x;
     // scalar slots [26, 31) (expec and the observables use [0, 22))
     const double a = -0.5 * dtau;
-    RET(cuda_ok(cudaMemcpyAsync(CA.p, V.p, esz * dim, cudaMemcpyDeviceToDevice, s->stream), "copy"));
-    RET(vec_scale(s, vt, sv, CA.p));
-    RET(vec_axpby(s, vt, a, H.p, 1.0, CA.p));
-    RET(cuda_ok(cudaMemcpyAsync(CT.p, H.p, esz * dim, cudaMemcpyDeviceToDevice, s->stream), "copy"));
+    RET(cuda_ok(cudaMemcpyAsync(CA.p, V.p, esz * dim * nb, cudaMemcpyDeviceToDevice, s->stream), "copy"));
+    for (int b = 0; b < nb; b++) {
+      RET(vec_scale(s, vt, sv[b], vec(CA.p, b)));
+      RET(vec_axpby(s, vt, a, vec(H.p, b), 1.0, vec(CA.p, b)));
+    }
+    RET(cuda_ok(cudaMemcpyAsync(CT.p, H.p, esz * dim * nb, cudaMemcpyDeviceToDevice, s->stream), "copy"));
     double coeff = a;
     const double c01[2] = {0.0, 1.0};
-    RET(cuda_ok(cudaMemcpyAsync(st + 26, c01, sizeof(c01), cudaMemcpyHostToDevice, s->stream), "coef"));
+    for (int b = 0; b < nb; b++)
+      RET(cuda_ok(cudaMemcpyAsync(slot(b) + 26, c01, sizeof(c01), cudaMemcpyHostToDevice, s->stream), "coef"));
     for (int c = 2; c <= expand; c++) {
       coeff *= a / (double)c;
-      RET(hv_native(s, vt, CT.p, CU.p, st + 26, st + 28, false));
-      RET(vec_axpby(s, vt, coeff, CU.p, 1.0, CA.p));
+      RET(apply_h(CT.p, CU.p, 26));
+      for (int b = 0; b < nb; b++) RET(vec_axpby(s, vt, coeff, vec(CU.p, b), 1.0, vec(CA.p, b)));
       std::swap(CT.p, CU.p);
     }
-    RET(vec_norm2(s, vt, CA.p, st + 30));
-    double n2 = 0.0;
-    RET(cuda_ok(cudaMemcpyAsync(&n2, st + 30, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "read"));
-    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
-    *gnorm_out = std::sqrt(n2);
+    for (int b = 0; b < nb; b++) RET(vec_norm2(s, vt, vec(CA.p, b), slot(b) + 30));
+    RET(read_slots());
+    for (int b = 0; b < nb; b++) {
+      gnorm[b] = std::sqrt(host[kSlots * b + 30]);
+      sv[b] = 1.0 / gnorm[b];
+    }
     std::swap(V.p, CA.p);
-    sv = 1.0 / *gnorm_out;
     return 0;
   };
+  auto record = [&](int b) {
+    (*res)[b].energy.push_back(E[b]);
+    (*res)[b].inv_temp.push_back(inv_temp[b]);
+  };
   if (canonical && m.expand_coef <= 0) printf("In cTPQ calc., the default value of ExpandCoef (=10) is used. \n");
-  double gnorm = 0.0, inv_temp = 0.0;
   int step = 2;
   if (resumed) {
     // expec_energy_flct on the stored state, then the loop from its step (src/CalcByTPQ.c:107-113);
@@ -959,55 +1016,58 @@ int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::
     // leaves it unset on this path)
     RET(expec());
     step = opt.resume_step;
-    if (canonical) inv_temp = (step - 1) * dtau;
+    if (canonical) inv_temp[0] = (step - 1) * dtau;
   } else if (canonical) {
     // step 0: the normalised start vector, its Green's functions, expec (with the Flct line)
     RET(expec());
     if (green) RET(green_step(0));
-    write_lines(0.0, first_norm, 0, true);
-    res->energy.push_back(E);
-    res->inv_temp.push_back(0.0);
+    for (int b = 0; b < nb; b++) {
+      write_lines(b, 0.0, first_norm[b], 0, true);
+      record(b);
+    }
     step = 1;
   } else {
     // FirstMultiply: expec on the start vector, then v = (L - H/Ns) v normalised.
     RET(expec());
     if (green) RET(green_step(0));
-    RET(multiply(&gnorm));
-    write_lines(0.0, first_norm, 0, false);
-    res->energy.push_back(E);
-    res->inv_temp.push_back(0.0);
+    RET(multiply());
+    for (int b = 0; b < nb; b++) {
+      write_lines(b, 0.0, first_norm[b], 0, false);
+      record(b);
+    }
     RET(expec());
-    inv_temp = (2.0 / Ns) / (L - E / Ns);
-    write_lines(inv_temp, gnorm, 1, true);
-    res->energy.push_back(E);
-    res->inv_temp.push_back(inv_temp);
+    for (int b = 0; b < nb; b++) {
+      inv_temp[b] = (2.0 / Ns) / (L - E[b] / Ns);
+      write_lines(b, inv_temp[b], gnorm[b], 1, true);
+      record(b);
+    }
   }
   for (; step < m.lanczos_max; step++) {
     if (canonical) {
-      RET(ctpq_multiply(&gnorm));
+      RET(ctpq_multiply());
       RET(expec());
-      inv_temp += dtau;
+      for (int b = 0; b < nb; b++) inv_temp[b] += dtau;
     } else {
-      RET(multiply(&gnorm));
+      RET(multiply());
       RET(expec());
-      inv_temp = (2.0 * step / Ns) / (L - E / Ns);
+      for (int b = 0; b < nb; b++) inv_temp[b] = (2.0 * step / Ns) / (L - E[b] / Ns);
     }
-    write_lines(inv_temp, gnorm, step, true);
-    res->energy.push_back(E);
-    res->inv_temp.push_back(inv_temp);
+    for (int b = 0; b < nb; b++) {
+      write_lines(b, inv_temp[b], gnorm[b], step, true);
+      record(b);
+    }
     if (green && m.expec_interval > 0 && step % m.expec_interval == 0) RET(green_step(step));
   }
-  fclose(fss);
-  fclose(fnorm);
-  fclose(fflct);
-  res->final_step = step;
-  if (opt.keep_vector) {
-    // the normalised state sv*V in HPhi's order
-    RET(from_native(s, vt, V.p, H.p));
-    res->final_vector.assign(2 * (dim + 1), 0.0);
-    RET(vec_to_host_c128(s, vt, H.p, res->final_vector.data()));
-    RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
-    for (double &x : res->final_vector) x *= sv;
+  for (int b = 0; b < nb; b++) {
+    (*res)[b].final_step = step;
+    if (opt.keep_vector) {
+      // the normalised state sv*V in HPhi's order
+      RET(from_native(s, vt, vec(V.p, b), vec(H.p, b)));
+      (*res)[b].final_vector.assign(2 * (dim + 1), 0.0);
+      RET(vec_to_host_c128(s, vt, vec(H.p, b), (*res)[b].final_vector.data()));
+      RET(cuda_ok(cudaStreamSynchronize(s->stream), "sync"));
+      for (double &x : (*res)[b].final_vector) x *= sv[b];
+    }
   }
   return 0;
 }

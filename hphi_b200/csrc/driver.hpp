@@ -153,6 +153,12 @@ int read_lanczos_restart(const Sector &s, const std::string &outdir, LanczosRest
 // h_init: start vector (any norm) of sample rand_i; writes SS/Norm/Flct_rand<rand_i>.dat.
 int tpq_run(Sector *s, VecType vt, const double *h_init, int rand_i, const std::string &outdir, TpqResult *res,
             const TpqOptions &opt = TpqOptions());
+// Several TPQ samples in lockstep (rand_i[b] from start h_init[b]), with every H application
+// of a step one block H*V over the samples when `block` (hv_block_applies, at most
+// kHvBlockMax samples), else one launch per sample.  Output files and results per sample are
+// those of tpq_run; resume_step > 0 takes a single sample.
+int tpq_run_samples(Sector *s, VecType vt, const std::vector<const double *> &h_init, const std::vector<int> &rand_i,
+                    const std::string &outdir, std::vector<TpqResult> *res, const TpqOptions &opt, bool block);
 // h_init: the input state (SpectrumVec file contents, HPhi's 1-based complex128 layout);
 // step_initial: the first time index (the file's step on a ReStart 2 / 3 run, else 0).
 int te_run(Sector *s, const double *h_init, int step_initial, const std::string &outdir, TeResult *res);

@@ -107,6 +107,14 @@ int hv_launch(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double 
 // exact per-block permutation of it).  hv_native runs the fastest kernel on native
 // vectors; to_native / from_native convert (they copy when the orders coincide).
 bool has_native_order(const Sector *s);
+// Block H*V over nb <= kHvBlockMax vectors at d_v1 + b * stride (general kernel path only,
+// hv_block_applies): v0_b = acc_b * v0_b + scale_b * H v1_b with (acc_b, scale_b) at
+// d_coef + b * cstride and <v1_b|H v1_b> at d_out + b * ostride; d_part holds
+// 2 * nb * red_blocks doubles.
+constexpr int kHvBlockMax = 8;
+bool hv_block_applies(const Sector *s, VecType vt);
+int hv_block_native(Sector *s, VecType vt, int nb, int64_t stride, const void *d_v1, void *d_v0,
+                    const double *d_coef, int cstride, double *d_out, int ostride, double *d_part);
 int hv_native(Sector *s, VecType vt, const void *d_v1, void *d_v0, const double *d_coef, double *d_out,
               bool acc_read = true);
 int to_native(Sector *s, VecType vt, const void *d_hphi, void *d_native);

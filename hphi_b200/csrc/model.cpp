@@ -923,8 +923,8 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       return -1;
     }
     const bool spin = m->is_spin();
-    if (m->general_spin || m->is_kondo() || m->calc_model == kHubbardNConserved) {
-      *err = "excitation operators: supported for Hubbard, HubbardGC and spin-1/2 Spin / SpinGC models";
+    if (m->calc_model == kHubbardNConserved) {
+      *err = "excitation operators: not supported for HubbardNConserved";
       return -1;
     }
     const bool single = files.count("singleexcitation") > 0;
@@ -956,9 +956,36 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       } else {
         const int j = (int)r[2], s2 = (int)r[3], type = (int)r[4];
         coef = std::complex<double>(r[5], r[6]);
-        if (!check_site(i) || !check_site(j) || s1 < 0 || s1 > 1 || s2 < 0 || s2 > 1 || (type != 0 && type != 1)) {
+        const int smax = spin ? m->locspn[i] : 1;
+        if (!check_site(i) || !check_site(j) || s1 < 0 || s1 > smax || s2 < 0 || s2 > smax || (type != 0 && type != 1)) {
           *err = fn + ": bad line";
           return -1;
+        }
+        if (spin && m->general_spin) {
+          // general spin (src/PairExSpin.c:353-440): |s1><s2| whatever the type when s1 != s2;
+          // n_{s1} (type 1) or -(1 - n_{s1}) (type 0) when s1 == s2
+          if (i != j) { *err = "ERROR: hopping is not allowed in localized spin system"; return -1; }
+          std::vector<std::pair<int, std::complex<double>>> ops;  // (state, coefficient) of diagonal parts
+          if (s1 != s2) {
+            uint64_t grm, grv, gfl;
+            if (compile_spin({SpinOp{i, s1, s2}}, m->site_bits, &grm, &grv, &gfl))
+              m->excitation.push_back(BitTerm{grm, grv ^ (gfl & grm), gfl, 0, coef.real(), coef.imag()});
+          } else if (type == 1) {
+            ops.push_back({s1, coef});
+          } else {
+            for (int t = 0; t <= m->locspn[i]; t++)
+              if (t != s1) ops.push_back({t, -coef});
+          }
+          for (const auto &o : ops) {
+            uint64_t grm, grv, gfl;
+            if (compile_spin({SpinOp{i, o.first, o.first}}, m->site_bits, &grm, &grv, &gfl))
+              m->excitation.push_back(BitTerm{grm, grv ^ (gfl & grm), gfl, 0, o.second.real(), o.second.imag()});
+          }
+          // Sz change of the operator: s counts down from m = S
+          const int d2 = 2 * (s2 - s1) / 2;
+          if (first) { dup = d2; ddn = 0; first = false; }
+          else if (!m->is_gc() && d2 != dup) { *err = fn + ": the operators lead to different sectors"; return -1; }
+          continue;
         }
         if (spin) {
           if (i != j) { *err = "Error: isite1 must be equal to isite2 for Spin system."; return -1; }

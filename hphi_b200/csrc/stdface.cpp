@@ -647,6 +647,22 @@ int generate(const std::string &stan_in, const std::string &dir, std::string *er
 
     const double phase[2] = {k.real_or("phase0", 0.0), k.real_or("phase1", 0.0)};
     const bool simplified_ok = lat.kind != "ladder";
+    // Time evolution: PumpType "Quench" adds U_quench sum_i n_i,up n_i,down to H for t >= 0;
+    // the lasers replace every hopping by its Peierls-substituted form at each time step.
+    std::string pump;
+    if (P.calc_type == 4) {
+      pump = k.str_or("pumptype", "quench");
+      if (pump != "quench" && pump != "pulselaser" && pump != "aclaser" && pump != "dclaser")
+        throw Fail("PumpType: Quench, Pulse Laser, AC Laser or DC Laser");
+      if (P.model == kSpinM) throw Fail("time evolution from the standard mode needs electrons");
+    }
+    const bool laser = P.calc_type == 4 && pump != "quench";
+    struct Hop {
+      int oi, oj;      // H gets -t c+_{oj s} c_{oi s} + h.c.
+      cplx t;
+      double dr[2];    // r_oj - r_oi, fractional
+    };
+    std::vector<Hop> hops;
 
     // ---------------------------------------------------------------- one-site terms
     const double mu = (P.model == kSpinM) ? 0.0 : k.real_or("mu", 0.0);
@@ -712,6 +728,12 @@ int generate(const std::string &stan_in, const std::string &dir, std::string *er
           const double th = (phase[0] * n0 + phase[1] * n1) * kPi / 180.0;
           const cplx te = t * std::polar(1.0, th);
           const int oi = P.orb_site(i), oj = P.orb_site(j);
+          if (laser && te != 0.0) {
+            const double dr0 = b.dw + lat.tau[b.sj][0] - lat.tau[b.si][0];
+            const double dr1 = b.dl + lat.tau[b.sj][1] - lat.tau[b.si][1];
+            hops.push_back({oi, oj, te, {dr0, dr1}});
+            continue;
+          }
           for (int s = 0; s < 2; s++) {
             T.add_trans(oj, s, oi, s, te);
             T.add_trans(oi, s, oj, s, std::conj(te));
@@ -746,6 +768,7 @@ int generate(const std::string &stan_in, const std::string &dir, std::string *er
     const long num_ave = k.int_or("numave", 5);
     const long expec_interval = k.int_or("expecinterval", 20);
     const long n_omega = k.int_or("nomega", 200);
+    const long expand_coef = k.int_or("expandcoef", 10);
     const double omega_max = k.real_or("omegamax", large_value * nsite);
     const double omega_min = k.real_or("omegamin", -large_value * nsite);
     const double omega_org = k.real_or("omegaorg", 0.0);
@@ -786,8 +809,46 @@ int generate(const std::string &stan_in, const std::string &dir, std::string *er
     const int hamio = pick("hamio", {{"none", 0}, {"in", 1}, {"out", 2}}, 0);
     const int exvec = pick("outputexcitedvec", {{"none", 0}, {"out", 1}}, 0);
 
-    if (P.calc_type == 4 || k.has("pumptype") || k.has("dt"))
-      throw Fail("time evolution from the standard mode is not supported by this generator");
+    // time-dependent terms, one list per step at t = step * dt (src/CalcByTEM.c:141-165 reads
+    // them as TETime / TEOneBody / TETwoBody); the vector potential of a laser is
+    // A0 exp(-(t - t0)^2 / (2 tdump^2)) cos(freq (t - t0)) (Pulse), A0 sin(freq (t - t0)) (AC) or
+    // A0 t (DC), with A0 = (VecPotW, VecPotL) and t0 = tshift
+    std::vector<std::pair<double, std::vector<std::tuple<int, int, int, int, cplx>>>> te_one;
+    std::vector<std::pair<double, std::vector<std::pair<std::array<int, 8>, cplx>>>> te_two;
+    if (P.calc_type == 4) {
+      const double dt = k.real_or("dt", 0.1), tshift = k.real_or("tshift", 0.0), tdump = k.real_or("tdump", 0.1);
+      const double freq = k.real_or("freq", 0.1), uquench = k.real_or("uquench", 0.0);
+      const double A0[2] = {k.real_or("vecpotw", 0.0), k.real_or("vecpotl", 0.0)};
+      for (long step = 0; step < lanczos_max; step++) {
+        const double t = dt * step;
+        const double ta = t;
+        if (!laser) {
+          std::vector<std::pair<std::array<int, 8>, cplx>> rows;
+          if (uquench != 0.0)
+            for (int n = 0; n < P.nc; n++) {
+              const int o = P.orb_site(n);
+              rows.push_back({{o, 0, o, 0, o, 1, o, 1}, uquench});
+            }
+          te_two.push_back({t, rows});
+          continue;
+        }
+        double a;  // A(t) / A0
+        if (pump == "pulselaser") a = std::exp(-(ta - tshift) * (ta - tshift) / (2.0 * tdump * tdump)) * std::cos(freq * (ta - tshift));
+        else if (pump == "aclaser") a = std::sin(freq * (ta - tshift));
+        else a = ta;
+        std::vector<std::tuple<int, int, int, int, cplx>> rows;
+        for (const Hop &h : hops) {
+          // A(t) = A0 a(t) in units of the reciprocal lattice vectors: the hop from r_i to r_j
+          // picks up exp(i A(t).(r_j - r_i) / 2 pi) = exp(i a(t) (A0W dr_W + A0L dr_L))
+          const cplx te = h.t * std::polar(1.0, a * (A0[0] * h.dr[0] + A0[1] * h.dr[1]));
+          for (int s = 0; s < 2; s++) {
+            rows.emplace_back(h.oj, s, h.oi, s, te);
+            rows.emplace_back(h.oi, s, h.oj, s, std::conj(te));
+          }
+        }
+        te_one.push_back({t, rows});
+      }
+    }
     const std::string spectrum_type = k.str_or("spectrumtype", "szsz");
     const double qw = k.real_or("spectrumqw", 0.0), ql = k.real_or("spectrumql", 0.0);
     if (calc_spec != 0) make_excitation(&P, spectrum_type, qw, ql);
@@ -881,7 +942,32 @@ int generate(const std::string &stan_in, const std::string &dir, std::string *er
       std::fclose(f);
       names.push_back({"PairExcitation", "pair.def"});
     }
-    if (calc_spec != 0) names.push_back({"SpectrumVec", "zvo_eigenvec_0"});
+    if (!te_one.empty()) {
+      FILE *f = open_out(dir, "teone.def");
+      write_table_head(f, "AllTimeStep", te_one.size());
+      for (const auto &st : te_one) {
+        std::fprintf(f, "%.15f %zu\n", st.first, st.second.size());
+        for (const auto &e : st.second)
+          std::fprintf(f, "%5d %5d %5d %5d %25.15f %25.15f\n", std::get<0>(e), std::get<1>(e), std::get<2>(e),
+                       std::get<3>(e), std::get<4>(e).real(), std::get<4>(e).imag());
+      }
+      std::fclose(f);
+      names.push_back({"TEOneBody", "teone.def"});
+    }
+    if (!te_two.empty()) {
+      FILE *f = open_out(dir, "tetwo.def");
+      write_table_head(f, "AllTimeStep", te_two.size());
+      for (const auto &st : te_two) {
+        std::fprintf(f, "%.15f %zu\n", st.first, st.second.size());
+        for (const auto &e : st.second) {
+          for (int q = 0; q < 8; q++) std::fprintf(f, "%5d ", e.first[q]);
+          std::fprintf(f, "%25.15f %25.15f\n", e.second.real(), e.second.imag());
+        }
+      }
+      std::fclose(f);
+      names.push_back({"TETwoBody", "tetwo.def"});
+    }
+    if (calc_spec != 0 || P.calc_type == 4) names.push_back({"SpectrumVec", "zvo_eigenvec_0"});
     {
       int calc_model;
       if (P.model == kHubbardM) calc_model = P.gc ? 3 : 0;
@@ -912,6 +998,7 @@ int generate(const std::string &stan_in, const std::string &dir, std::string *er
       std::fprintf(f, "LanczosTarget  %ld\nLargeValue     %.15e\nNumAve         %ld\nExpecInterval  %ld\n",
                    lanczos_target, large_value, num_ave, expec_interval);
       std::fprintf(f, "NOmega         %ld\n", n_omega);
+      std::fprintf(f, "ExpandCoef     %ld\n", expand_coef);
       std::fprintf(f, "OmegaMax       %.15e %.15e\n", omega_max + omega_org, omega_im);
       std::fprintf(f, "OmegaMin       %.15e %.15e\n", omega_min + omega_org, omega_im);
       std::fprintf(f, "OmegaOrg       %.15e %.15e\n", omega_org, 0.0);

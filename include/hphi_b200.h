@@ -63,8 +63,10 @@ int hphi_open_expert(const char *namelist_def, int device, hphi_handle **out);
 /*
  * Standard mode: reads the keyword file stan_in (lattice = chain / ladder / square /
  * triangular / honeycomb / kagome; model = Hubbard / Spin / Kondo and their GC forms;
- * method = Lanczos / CG / TPQ / cTPQ; their parameters) and writes namelist.def and the
- * expert-mode files it lists into out_dir, which then open with hphi_open_expert.  Host only.
+ * method = Lanczos / CG / TPQ / cTPQ / FullDiag / Time-Evolution with quench or laser pumps;
+ * CalcSpec with SpectrumType SzSz / S+S- / Density / Up / Down; their parameters) and writes
+ * namelist.def and the expert-mode files it lists into out_dir, which then open with
+ * hphi_open_expert.  Host only.
  * Replaces: StdFace_main (called at src/HPhiMain.c:212-214 for `HPhi -s` / `HPhi -sdry`).
  */
 int hphi_stdface(const char *stan_in, const char *out_dir);

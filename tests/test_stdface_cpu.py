@@ -73,3 +73,12 @@ def test_cell_enumeration_and_bond_folding(tmp_path):
 def test_reference_reproduces_its_test_values_from_generated_inputs(name, tmp_path):
     problems = R.run(name, str(tmp_path / name), backend="reference", env={"OMP_NUM_THREADS": "4"})
     assert not problems, problems
+
+
+@pytest.mark.skipif(not os.path.exists(R.REF_EXE), reason="reference binary oracle/_ref/HPhi_ref not built")
+def test_reference_reproduces_time_evolution_tests_from_generated_inputs(tmp_path):
+    """te_ac_hubbard_square computes the ground state the other three scripts start from."""
+    for name in ("te_ac_hubbard_square", "te_dc_hubbard_square", "te_pulse_hubbard_square",
+                 "te_quench_hubbard_square"):
+        problems = R.run(name, str(tmp_path / name), backend="reference", env={"OMP_NUM_THREADS": "4"})
+        assert not problems, (name, problems)
