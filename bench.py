@@ -569,7 +569,7 @@ def run_tpq_mode(args):
     import hphi_b200
     from hphi_b200 import expert
     W, K = max(args.warmup, 3), max(args.steps // 25, 10)
-    L, nave = 26, 8
+    L, nave = args.tpq_sites, 8
     bonds = expert.chain_bonds(L) + expert.chain_bonds(L, 2)
     tmp = tempfile.mkdtemp()
     res = {}
@@ -599,10 +599,10 @@ def run_tpq_mode(args):
     out = {"metric": METRIC, "mode": "tpq", "value": nave / res["block"], "unit": "sample-steps/s", "n_gpus": 1,
            "steps": K, "warmup": W, "ms_per_step": 1e3 * res["block"], "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-           "config": {"workload": "J1-J2 chain L=26 (J2=0.35), 2Sz=0, mTPQ", "dim": dim, "samples": nave,
+           "config": {"workload": f"J1-J2 chain L={L} (J2=0.35), 2Sz=0, mTPQ", "dim": dim, "samples": nave,
                       "timing": "host clock around calc_by_tpq with W and W+K steps (difference / K); "
                                 "each step reads its norms and energies to the host and appends the files",
-                      "l2": "vectors (166 MB each) exceed L2 together; no flush"},
+                      "l2": f"the {nave} samples' vectors ({nave * dim * 16 / 1e9:.2f} GB) exceed L2; no flush"},
            "serial_ms_per_step": 1e3 * res["serial"], "block_ms_per_step": 1e3 * res["block"],
            "speedup_block_vs_serial": res["serial"] / res["block"],
            "hv_equivalent_gbs_block": hv_bytes / res["block"] / 1e9,
@@ -703,6 +703,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=100)
     ap.add_argument("--serve-slots", type=int, default=64)
     ap.add_argument("--plain-sample", type=int, default=256)
+    ap.add_argument("--tpq-sites", type=int, default=26, help="--mode tpq: sites of the J1-J2 chain")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=250)  # ~1 s timed: several clock samples
     ap.add_argument("--warmup", type=int, default=3)

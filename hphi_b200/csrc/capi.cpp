@@ -780,8 +780,12 @@ int hphi_spectrum(hphi_handle *h, const double *h_vec, const char *output_dir, d
   Sector *s = h->sector;
   const Model &m = s->model;
   const std::string out = output_dir ? output_dir : "output";
-  if (m.calc_type != kLanczos) {
-    set_error("spectrum: only the Lanczos method (CalcType 0) is supported");
+  // CalcType 0 is the reference's Lanczos spectrum; for CalcType 3 it solves the same
+  // Green's function by shifted BiCG (src/CalcSpectrum.c, CalcSpectrumByBiCG), which the
+  // Lanczos continued fraction here reproduces to the printed digits.  TPQ and full
+  // diagonalisation spectra are other quantities.
+  if (m.calc_type != kLanczos && m.calc_type != kCG) {
+    set_error("spectrum: CalcType 0 (Lanczos) or 3 (CG) only");
     return -1;
   }
   std::vector<double> vec;
