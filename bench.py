@@ -563,7 +563,8 @@ def run_tem_mode(args):
 def run_tpq_mode(args):
     """mTPQ with its NumAve = 8 samples in lockstep (one block H*V over the samples per step,
     hv_block_native) against the same samples one after another, on a 26-site J1-J2 chain
-    (2Sz = 0, dim 10,400,600, complex vectors, the general kernel): K timed steps each, host
+    (2Sz = 0, dim 10,400,600, complex vectors as the reference's default InitialVecType, the
+    general kernel): K timed steps each, host
     clock around calc_by_tpq with W and W + K steps (difference / K).  Both runs write the
     same files; the first step lines are compared."""
     import hphi_b200
@@ -579,7 +580,7 @@ def run_tpq_mode(args):
         times = {}
         for n in (W, W + K):
             m = expert.heisenberg(L, bonds, J=[1.0] * L + [0.35] * L, calc_type="TPQ", lanczos_max=n, num_ave=nave,
-                                  large_value=2.0, expec_interval=100000)
+                                  large_value=2.0, expec_interval=100000, initial_vec_type=0)
             d = os.path.join(tmp, f"{mode}{n}")
             with hphi_b200.Hamiltonian(m.write(d)) as H:
                 dim = H.dim
@@ -833,10 +834,11 @@ def _mode_line(argv, timeout):
 
 
 def run_modes():
-    """Bounded runs of the batching, serving and precision workloads after the timed H*v, so
-    the default line carries their solves/s, latency and accuracy: batch with 64 of the 256
-    J1-J2 chains (300 steps), serve with 40 Poisson requests, precision on the full 4x8
-    Heisenberg sector (300 steps).  The full-size runs are --mode batch / serve."""
+    """Bounded runs of the batching, serving, TPQ-block and precision workloads after the timed
+    H*v, so the default line carries their solves/s, latency and accuracy: batch with 64 of the
+    256 J1-J2 chains (300 steps), serve with 40 Poisson requests, 8 TPQ samples in lockstep
+    against one after another, precision on the full 4x8 Heisenberg sector (300 steps).  The
+    full-size runs are --mode batch / serve."""
     modes = {}
     b = _mode_line(["--mode", "batch", "--batch-size", "64", "--plain-sample", "16"], 600)
     if "error" in b:
@@ -852,6 +854,12 @@ def run_modes():
     else:
         modes["serve"] = {k: sv[k] for k in ("config", "fp64", "fp32", "plain_fp64_solves_per_s", "plain_sample",
                                              "clocks")}
+    tq = _mode_line(["--mode", "tpq"], 600)
+    if "error" in tq:
+        modes["tpq"] = tq
+    else:
+        modes["tpq"] = {k: tq[k] for k in ("config", "value", "unit", "serial_ms_per_step", "block_ms_per_step",
+                                           "speedup_block_vs_serial", "files_equal", "clocks")}
     pr = _mode_line(["--mode", "precision"], 900)
     if "error" in pr:
         modes["precision"] = pr

@@ -923,10 +923,6 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       return -1;
     }
     const bool spin = m->is_spin();
-    if (m->calc_model == kHubbardNConserved) {
-      *err = "excitation operators: not supported for HubbardNConserved";
-      return -1;
-    }
     const bool single = files.count("singleexcitation") > 0;
     const std::string fn = files[single ? "singleexcitation" : "pairexcitation"];
     if (!read_table(*m, fn, &rows, single ? 5 : 7, err)) return -1;
@@ -981,8 +977,9 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
             if (compile_spin({SpinOp{i, o.first, o.first}}, m->site_bits, &grm, &grv, &gfl))
               m->excitation.push_back(BitTerm{grm, grv ^ (gfl & grm), gfl, 0, o.second.real(), o.second.imag()});
           }
-          // Sz change of the operator: s counts down from m = S
-          const int d2 = 2 * (s2 - s1) / 2;
+          // Sz change of the operator: a spin state's digit counts up from m = -S, so
+          // |s1><s2| changes 2Sz by 2 (s1 - s2) (src/CalcSpectrum.c:588-589)
+          const int d2 = s1 - s2;
           if (first) { dup = d2; ddn = 0; first = false; }
           else if (!m->is_gc() && d2 != dup) { *err = fn + ": the operators lead to different sectors"; return -1; }
           continue;
@@ -1007,8 +1004,10 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
       const int du = spin ? __builtin_popcountll(after) - __builtin_popcountll(before)
                           : __builtin_popcountll(after & even) - __builtin_popcountll(before & even);
       const int dd = spin ? 0 : __builtin_popcountll(after & ~even) - __builtin_popcountll(before & ~even);
+      // HubbardNConserved keeps only the particle number (src/CalcSpectrum.c:521-527)
+      const bool n_only = m->calc_model == kHubbardNConserved;
       if (first) { dup = du; ddn = dd; first = false; }
-      else if (!m->is_gc() && (du != dup || dd != ddn)) {
+      else if (!m->is_gc() && (n_only ? du + dd != dup + ddn : (du != dup || dd != ddn))) {
         *err = fn + ": the operators lead to different sectors";
         return -1;
       }
@@ -1021,7 +1020,9 @@ int read_expert(const std::string &namelist, Model *m, std::string *err) {
     m->ex_ndown = m->ndown;
     m->ex_ne = m->ne;
     m->ex_2sz = m->total_2sz;
-    if (!m->is_gc()) {
+    if (m->calc_model == kHubbardNConserved) {
+      m->ex_ne += dup + ddn;
+    } else if (!m->is_gc()) {
       m->ex_nup += dup;
       m->ex_ndown += ddn;
       m->ex_ne += spin ? dup : dup + ddn;

@@ -32,8 +32,6 @@
 #include <cstdlib>
 #include <fstream>
 #include <map>
-#include <set>
-#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <tuple>
@@ -618,10 +616,15 @@ int generate(const std::string &stan_in, const std::string &dir, std::string *er
     if (model == "hubbard" || model == "fermionhubbard") P.model = kHubbardM;
     else if (model == "hubbardgc" || model == "fermionhubbardgc") { P.model = kHubbardM; P.gc = true; }
     else if (model == "spin") P.model = kSpinM;
-    else if (model == "spingc") { P.model = kSpinM; P.gc = true; }
+    else if (model == "spingc" || model == "spingccma") {
+      // SpinGCCMA is the SpinGC Hamiltonian computed by the reference's cluster-multiplication
+      // algorithm; the engine's general kernel computes the same system
+      P.model = kSpinM;
+      P.gc = true;
+    }
     else if (model == "kondo" || model == "kondolattice") P.model = kKondoM;
     else if (model == "kondogc" || model == "kondolatticegc") { P.model = kKondoM; P.gc = true; }
-    else throw Fail("model not supported: '" + model + "' (Hubbard, Spin, Kondo and their GC forms are)");
+    else throw Fail("model not supported: '" + model + "' (Hubbard, Spin, Kondo, their GC forms and SpinGCCMA are)");
     const std::string method = k.str_or("method", "");
     if (method == "lanczos") P.calc_type = 0;
     else if (method == "tpq") P.calc_type = 1;

@@ -57,6 +57,11 @@ def _cases():
     m.trans += [(i, s, i, s, 1.2, 0.0) for i in range(4) for s in (0, 1)]
     c["hubgc_single_2x2"] = (m, dict(single_excitation=[(2, 1, 1, 1.0, 0.0)],
                                      omega_min=-4.0, omega_max=6.0, omega_im=0.1, n_omega=40))
+    # removal of an up electron from a Hubbard chain with the particle number only (HubbardNConserved)
+    m = expert.hubbard(6, expert.chain_bonds(6), 1.0, 4.0, 3, 3, lanczos_max=500)
+    m.two_sz = None
+    c["hubnc_single_chain6"] = (m, dict(single_excitation=[(0, 0, 0, 1.0, 0.0), (3, 1, 0, 0.5, 0.2)],
+                                        omega_min=-6.0, omega_max=6.0, omega_im=0.1, n_omega=36))
     return c
 
 

@@ -14,11 +14,12 @@ pytestmark = pytest.mark.gpu
 
 def _models():
     out = {}
-    # microcanonical TPQ, complex vectors, 10 samples: blocks of 8 and 2
+    # microcanonical TPQ, complex vectors (the reference's default), 10 samples: blocks of 8 and 2
     m = expert.heisenberg(12, expert.chain_bonds(12) + expert.chain_bonds(12, 2), J=[1.0] * 12 + [0.4] * 12,
-                          calc_type="TPQ", lanczos_max=60, num_ave=10, large_value=3.0, expec_interval=20)
+                          calc_type="TPQ", lanczos_max=60, num_ave=10, large_value=3.0, expec_interval=20,
+                          initial_vec_type=0)
     out["tpq_j1j2_chain12"] = m
-    # canonical TPQ on a grand-canonical spin model with a field
+    # canonical TPQ on a grand-canonical spin model, real vectors
     m = expert.kitaev_heisenberg(2, 2, 1.0, 0.3, calc_type="cTPQ", lanczos_max=30, num_ave=3, large_value=5.0)
     out["ctpq_kitaev2x2"] = m
     # a grand-canonical Hubbard sector with Green's functions every ExpecInterval steps
