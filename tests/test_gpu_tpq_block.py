@@ -1,7 +1,8 @@
 """TPQ samples in lockstep (hphi_tpq groups the NumAve samples of the reference's loop,
 src/CalcByTPQ.c:76, into blocks that share one H*V per H application, hv_block_native):
 every output file must equal the one-sample-at-a-time run (HPHI_B200_TPQ_BLOCK=0) digit for
-digit, since per vector the block kernel does the general kernel's arithmetic in its order."""
+digit, since per vector the block kernel does the general kernel's arithmetic in its order.
+HPHI_B200_TPQ_BLOCK caps the block size (0: one sample at a time)."""
 import os
 
 import pytest
@@ -39,7 +40,7 @@ def test_block_samples_equal_serial_samples(name, tmp_path, monkeypatch):
     d = tmp_path / "in"
     MODELS[name].write(str(d))
     outs = {}
-    for mode in ("0", "1"):
+    for mode in ("0", "8", "3"):  # one after another; blocks of up to 8; blocks of up to 3
         monkeypatch.setenv("HPHI_B200_TPQ_BLOCK", mode)
         o = tmp_path / f"out{mode}"
         with hphi_b200.Hamiltonian(str(d / "namelist.def")) as H:
@@ -47,9 +48,8 @@ def test_block_samples_equal_serial_samples(name, tmp_path, monkeypatch):
             H.calc_by_tpq(output_dir=str(o))
         outs[mode] = o
     files = sorted(os.listdir(outs["0"]))
-    assert files == sorted(os.listdir(outs["1"]))
     assert any(f.startswith("SS_rand") for f in files)
-    for f in files:
-        a = (outs["0"] / f).read_text()
-        b = (outs["1"] / f).read_text()
-        assert a == b, f
+    for mode in ("8", "3"):
+        assert files == sorted(os.listdir(outs[mode]))
+        for f in files:
+            assert (outs["0"] / f).read_text() == (outs[mode] / f).read_text(), (mode, f)
