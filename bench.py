@@ -626,7 +626,7 @@ def run_tpq_mode(args):
                       "timing": "host clock around calc_by_tpq with W and W+K steps from the same seeded start "
                                 "vectors (difference of the medians of 3 runs / K); each step reads its norms and "
                                 "energies to the host and appends the files",
-                      "default_block": "8 real / 4 complex samples",
+                      "default_block": "8 samples",
                       "l2": f"the {nave} samples' vectors exceed L2; no flush"},
            "complex": results["c128"], "real": results["f64"], "clocks": cl}
     print(json.dumps(out))

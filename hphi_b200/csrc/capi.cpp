@@ -556,12 +556,10 @@ int hphi_tpq(hphi_handle *h, const double *v_init, const char *output_dir, doubl
   // The samples of the reference's loop (src/CalcByTPQ.c:76) run in blocks of up to
   // kHvBlockMax in lockstep, sharing each H application (one block H*V), where the sector's
   // H*v is the general kernel; a sample continued from a stored state runs alone.
-  // HPHI_B200_TPQ_BLOCK: 0 runs the samples one after another, N in 2..8 caps the block size.
-  // By default blocks hold 8 real or 4 complex samples: past 4 complex samples the block's
-  // source rows (4 x 16 B per gathered element) stop fitting the L2 working set and the
-  // block is no faster (measured on a 26-site chain, 10.4M rows).
+  // HPHI_B200_TPQ_BLOCK: 0 runs the samples one after another, N in 2..8 caps the block size
+  // (default 8).
   const char *blk_env = std::getenv("HPHI_B200_TPQ_BLOCK");
-  int block_cap = (vt == kReal64) ? kHvBlockMax : 4;
+  int block_cap = kHvBlockMax;
   if (blk_env && *blk_env) block_cap = std::max(0, std::min(kHvBlockMax, std::atoi(blk_env)));
   const bool block_ok = hv_block_applies(s, vt) && block_cap > 1;
   const int block_max = block_ok ? block_cap : 1;
