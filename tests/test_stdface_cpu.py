@@ -82,3 +82,66 @@ def test_reference_reproduces_time_evolution_tests_from_generated_inputs(tmp_pat
                  "te_quench_hubbard_square"):
         problems = R.run(name, str(tmp_path / name), backend="reference", env={"OMP_NUM_THREADS": "4"})
         assert not problems, (name, problems)
+
+
+def _neighbours(tmp_path, lattice, extra, model="SpinGC"):
+    """Sites and, per site, the set of sites it shares an InterAll (spin) bond with."""
+    p = tmp_path / "stan.in"
+    # the ladder has no direction-free J (rungs J0, legs J1)
+    coupling = "J0 = 1.0\nJ1 = 1.0\n" if lattice == "ladder" else "J = 1.0\n"
+    p.write_text(f'model = "{model}"\nmethod = "Lanczos"\nlattice = "{lattice}"\n' + coupling + extra)
+    hphi_b200.standard_mode(str(p), str(tmp_path))
+    mod = dict(l.split()[:2] for l in open(tmp_path / "modpara.def") if len(l.split()) >= 2)
+    n = int(mod["Nsite"])
+    nb = {i: set() for i in range(n)}
+    for l in open(tmp_path / "interall.def").read().split("\n")[5:]:
+        r = l.split()
+        if len(r) == 10 and r[0] != r[4]:
+            nb[int(r[0])].add(int(r[4]))
+            nb[int(r[4])].add(int(r[0]))
+    return n, nb
+
+
+@pytest.mark.parametrize("lattice,extra,nsite,z", [
+    ("chain", "L = 8\n", 8, 2),
+    ("ladder", "L = 4\nW = 2\n", 8, 3),
+    ("square", "W = 4\nL = 4\n", 16, 4),
+    ("triangular", "W = 3\nL = 3\n", 9, 6),
+    ("honeycomb", "W = 3\nL = 3\n", 18, 3),
+    ("kagome", "W = 2\nL = 2\n", 12, 4),
+])
+def test_nearest_neighbour_coordination(lattice, extra, nsite, z, tmp_path):
+    """Every site of the periodic clusters has the lattice's coordination number, and the
+    couplings are symmetric (checked through the written InterAll bonds)."""
+    n, nb = _neighbours(tmp_path, lattice, extra)
+    assert n == nsite
+    assert all(len(v) == z for v in nb.values()), {i: len(v) for i, v in nb.items()}
+
+
+def test_kondo_lattice_layout(tmp_path):
+    """Kondo chain: local spins 0..L-1 first, conduction orbitals L..2L-1, local spin n coupled to
+    orbital L + n, hoppings only between conduction orbitals."""
+    p = tmp_path / "stan.in"
+    p.write_text('L = 4\nmodel = "Kondo"\nmethod = "Lanczos"\nlattice = "chain"\nt = 1.0\nJ = 4.0\n'
+                 'nelec = 4\n2Sz = 0\n')
+    hphi_b200.standard_mode(str(p), str(tmp_path))
+    loc = [l.split() for l in open(tmp_path / "locspn.def").read().split("\n")[5:] if l.strip()]
+    assert [int(r[1]) for r in loc] == [1, 1, 1, 1, 0, 0, 0, 0]
+    hops = [l.split() for l in open(tmp_path / "trans.def").read().split("\n")[5:] if l.strip()]
+    assert hops and all(int(r[0]) >= 4 and int(r[2]) >= 4 for r in hops)
+    pairs = {tuple(sorted((int(r[0]), int(r[4])))) for r in
+             (l.split() for l in open(tmp_path / "interall.def").read().split("\n")[5:]) if len(r) == 10}
+    assert pairs == {(n, 4 + n) for n in range(4)}
+
+
+def test_command_line_dry_run_writes_the_expert_files(tmp_path):
+    """`HPhi_b200 -sdry stan.in` only writes the files (no device is touched)."""
+    import subprocess
+    (tmp_path / "stan.in").write_text('L = 6\nmodel = "Spin"\nmethod = "TPQ"\nlattice = "chain"\nJ = 1.0\n'
+                                      '2Sz = 0\nNumAve = 3\n')
+    p = subprocess.run([R.ENGINE_EXE, "-sdry", "stan.in"], cwd=tmp_path, capture_output=True, text=True)
+    assert p.returncode == 0, p.stderr
+    names = [l.split()[1] for l in open(tmp_path / "namelist.def") if l.strip()]
+    assert {"modpara.def", "calcmod.def", "locspn.def", "trans.def", "interall.def"} <= set(names)
+    calc = dict(l.split()[:2] for l in open(tmp_path / "calcmod.def") if l[0] != "#" and len(l.split()) >= 2)
+    assert calc["CalcType"] == "1" and calc["CalcModel"] == "1"
