@@ -2,7 +2,8 @@
 // the StdFace library's StdFace_main): a keyword file that names a lattice, a model and a
 // method becomes the expert-mode input that the engine reads (namelist.def, calcmod.def,
 // modpara.def, locspn.def, trans.def, interall.def, coulombintra.def, coulombinter.def,
-// greenone.def, greentwo.def, and pair.def / single.def for spectra).
+// greenone.def, greentwo.def, pair.def / single.def for spectra, teone.def / tetwo.def for time
+// evolution, and geometry.dat for the Fourier utility).
 //
 // StdFace's own sources are an empty submodule of the reference tree.  The conventions below
 // follow the reference's documentation (doc/en/source/filespecification/standardmode_en/*.rst,
@@ -1005,6 +1006,25 @@ int generate(const std::string &stan_in, const std::string &dir, std::string *er
       std::fprintf(f, "OmegaMax       %.15e %.15e\n", omega_max + omega_org, omega_im);
       std::fprintf(f, "OmegaMin       %.15e %.15e\n", omega_min + omega_org, omega_im);
       std::fprintf(f, "OmegaOrg       %.15e %.15e\n", omega_org, 0.0);
+      std::fclose(f);
+    }
+    {
+      // geometry.dat for HPhi's Fourier utility (doc/en/source/fourier/format.rst): the unit
+      // lattice vectors, the boundary phases, the three integer vectors of the numerical cell
+      // and, per site, its cell (W, L, H) and orbital (a Kondo lattice's conduction orbitals
+      // follow its local spins as orbitals nsub .. 2 nsub - 1).  The k path the utility also
+      // reads is the user's to append.
+      FILE *f = open_out(dir, "geometry.dat");
+      for (int d = 0; d < 2; d++) std::fprintf(f, "%25.15e %25.15e %25.15e\n", lat.cart[d][0], lat.cart[d][1], 0.0);
+      std::fprintf(f, "%25.15e %25.15e %25.15e\n", 0.0, 0.0, 1.0);
+      std::fprintf(f, "%25.15e %25.15e %25.15e\n", phase[0], phase[1], 0.0);
+      for (int d = 0; d < 2; d++) std::fprintf(f, "%ld %ld %d\n", lat.a[d][0], lat.a[d][1], 0);
+      std::fprintf(f, "0 0 1\n");
+      const int copies = P.model == kKondoM ? 2 : 1;
+      for (int k = 0; k < copies; k++)
+        for (int c = 0; c < ncell; c++)
+          for (int o = 0; o < lat.nsub; o++)
+            std::fprintf(f, "%ld %ld 0 %d\n", lat.cells[c][0], lat.cells[c][1], o + k * lat.nsub);
       std::fclose(f);
     }
     {

@@ -145,3 +145,18 @@ def test_command_line_dry_run_writes_the_expert_files(tmp_path):
     assert {"modpara.def", "calcmod.def", "locspn.def", "trans.def", "interall.def"} <= set(names)
     calc = dict(l.split()[:2] for l in open(tmp_path / "calcmod.def") if l[0] != "#" and len(l.split()) >= 2)
     assert calc["CalcType"] == "1" and calc["CalcModel"] == "1"
+
+
+def test_geometry_file_matches_the_documented_example(tmp_path):
+    """The Fourier utility's geometry.dat for a0 = (2, 2), a1 = (-2, 2) on the square lattice,
+    as printed in doc/en/source/fourier/format.rst: unit vectors, phases, the numerical cell
+    and the eight cells in the order the standard mode numbers them."""
+    p = tmp_path / "stan.in"
+    p.write_text('a0W = 2\na0L = 2\na1W = -2\na1L = 2\nmodel = "Hubbard"\nmethod = "Lanczos"\n'
+                 'lattice = "square"\nt = 1.0\nU = 4.0\nnelec = 8\n2Sz = 0\n')
+    hphi_b200.standard_mode(str(p), str(tmp_path))
+    rows = [l.split() for l in open(tmp_path / "geometry.dat") if l.strip()]
+    assert [[float(x) for x in r] for r in rows[:4]] == [[1, 0, 0], [0, 1, 0], [0, 0, 1], [0, 0, 0]]
+    assert rows[4:7] == [["2", "2", "0"], ["-2", "2", "0"], ["0", "0", "1"]]
+    assert [" ".join(r) for r in rows[7:]] == ["0 0 0 0", "-1 1 0 0", "0 1 0 0", "1 1 0 0", "-1 2 0 0",
+                                              "0 2 0 0", "1 2 0 0", "0 3 0 0"]
