@@ -617,6 +617,36 @@ __global__ void prod_permute_kernel(int64_t dim, int N, int Dc, const uint64_t *
   }
 }
 
+// HPhi order -> native order as a gather over the native positions: position (up rank ua, down
+// position da) holds the configuration c with the up spins of unrank_up[ua] on the even bits
+// and the down spins of unrank_dn[da] on the odd bits, whose HPhi row is
+// list_2_1[c & lo_mask] + list_2_2[c >> lo_bits] - 3.  Writes are coalesced and only the reads
+// scattered, where the row-ordered form above scatters its writes.
+__device__ __forceinline__ uint64_t spread_even_bits(uint64_t x) {  // bit i -> bit 2i, x < 2^32
+  x &= 0xFFFFFFFFull;
+  x = (x | (x << 16)) & 0x0000FFFF0000FFFFull;
+  x = (x | (x << 8)) & 0x00FF00FF00FF00FFull;
+  x = (x | (x << 4)) & 0x0F0F0F0F0F0F0F0Full;
+  x = (x | (x << 2)) & 0x3333333333333333ull;
+  x = (x | (x << 1)) & 0x5555555555555555ull;
+  return x;
+}
+
+template <typename T>
+__global__ void prod_to_native_gather_kernel(int64_t n, int N, int Dc, const uint16_t *__restrict__ unrank_up,
+                                             const uint16_t *__restrict__ unrank_dn, const uint32_t *__restrict__ l21,
+                                             const uint32_t *__restrict__ l22, int lo_bits, uint64_t lo_mask,
+                                             const T *__restrict__ in, T *__restrict__ out) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t ua = p / Dc;
+    const int64_t da = p - ua * Dc;
+    const uint64_t c = spread_even_bits(__ldg(unrank_up + ua)) | (spread_even_bits(__ldg(unrank_dn + da)) << 1);
+    const int64_t r = (int64_t)__ldg(l21 + (c & lo_mask)) + (int64_t)__ldg(l22 + (c >> lo_bits)) - 3;
+    const double sg = species_parity(c, N) ? -1.0 : 1.0;
+    out[p] = VT<T>::scale(sg, in[r]);
+  }
+}
+
 // Diagonal observables in native order (expec_energy_flct_Hubbard, src/expec_energy_flct.c:259-330).
 template <typename T>
 __global__ void prod_obs_kernel(ProdArgs a, const T *__restrict__ v, double *__restrict__ part) {
@@ -1276,6 +1306,18 @@ int prod_permute(Sector *s, VecType vt, const void *in, void *out, bool to_nativ
   ProdPlan *p = s->prod;
   const unsigned nb = (unsigned)std::min<int64_t>((s->dim + 255) / 256, (int64_t)s->num_sms * 16);
   const int N = p->args.N, Dc = p->args.Dc;
+  if (to_native && s->d_list_2_1 && s->d_list_2_2) {
+    const uint64_t lo_mask = s->ihfbit - 1;
+    if (vt == kReal64)
+      prod_to_native_gather_kernel<double><<<nb, 256, 0, s->stream>>>(
+          s->dim, N, Dc, p->args.unrank_up, p->args.unrank_dn, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask,
+          (const double *)in, (double *)out);
+    else
+      prod_to_native_gather_kernel<cplx><<<nb, 256, 0, s->stream>>>(
+          s->dim, N, Dc, p->args.unrank_up, p->args.unrank_dn, s->d_list_2_1, s->d_list_2_2, s->lo_bits, lo_mask,
+          (const cplx *)in, (cplx *)out);
+    return cuda_ok(cudaGetLastError(), "permute");
+  }
   if (vt == kReal64) {
     if (to_native)
       prod_permute_kernel<double, true, true><<<nb, 256, 0, s->stream>>>(s->dim, N, Dc, s->d_list_1, p->args.rank, p->args.pos_dn,
