@@ -160,3 +160,63 @@ def test_geometry_file_matches_the_documented_example(tmp_path):
     assert rows[4:7] == [["2", "2", "0"], ["-2", "2", "0"], ["0", "0", "1"]]
     assert [" ".join(r) for r in rows[7:]] == ["0 0 0 0", "-1 1 0 0", "0 1 0 0", "1 1 0 0", "-1 2 0 0",
                                               "0 2 0 0", "1 2 0 0", "0 3 0 0"]
+
+
+# Lattice geometry (primitive vectors, orbital positions in fractional coordinates) and the
+# distances of the first three neighbour shells, from the lattice figures of the reference's
+# documentation; used to build hopping matrices independently of the generator's bond tables.
+_TRI = [[1.0, 0.0], [0.5, 3 ** 0.5 / 2]]
+_GEOMETRY = {
+    "chain": ([[1.0, 0.0], [0.0, 1.0]], [[0, 0]], [1.0, 2.0, 3.0]),
+    "square": ([[1.0, 0.0], [0.0, 1.0]], [[0, 0]], [1.0, 2 ** 0.5, 2.0]),
+    "triangular": (_TRI, [[0, 0]], [1.0, 3 ** 0.5, 2.0]),
+    "honeycomb": (_TRI, [[0, 0], [1 / 3, 1 / 3]], [1 / 3 ** 0.5, 1.0, 2 / 3 ** 0.5]),
+    "kagome": (_TRI, [[0, 0], [0.5, 0], [0, 0.5]], [0.5, 3 ** 0.5 / 2]),
+}
+
+
+@pytest.mark.parametrize("lattice,cell", [
+    ("chain", "L = 7\n"),
+    ("square", "W = 4\nL = 3\n"),
+    ("square", "a0W = 2\na0L = 2\na1W = -2\na1L = 2\n"),
+    ("triangular", "a0W = 3\na0L = 0\na1W = -1\na1L = 2\n"),
+    ("triangular", "W = 4\nL = 4\n"),
+    ("honeycomb", "W = 3\nL = 2\n"),
+    ("honeycomb", "a0W = 2\na0L = 2\na1W = 1\na1L = -2\n"),
+    ("kagome", "a0W = 1\na0L = 1\na1W = -1\na1L = 2\n"),
+    ("kagome", "W = 3\nL = 2\n"),
+])
+def test_hoppings_follow_the_lattice_geometry(lattice, cell, tmp_path):
+    """The one-body matrix the generator writes (t, t', t'' = 1, 0.3, 0.17) equals the one built
+    from the site positions alone: every pair of sites, periodic images included, at the first,
+    second or third neighbour distance is joined by -t of that shell."""
+    import numpy as np
+    prim, orbs, shells = _GEOMETRY[lattice]
+    ts = [1.0, 0.3, 0.17][:len(shells)]
+    p = tmp_path / "stan.in"
+    hop = "".join(f"t{q} = {v}\n" for q, v in zip(["", "'", "''"], ts))
+    p.write_text(f'model = "HubbardGC"\nmethod = "Lanczos"\nlattice = "{lattice}"\n' + hop + cell)
+    hphi_b200.standard_mode(str(p), str(tmp_path))
+    geo = [l.split() for l in open(tmp_path / "geometry.dat") if l.strip()]
+    box = np.array([[float(x) for x in r[:2]] for r in geo[4:6]])
+    sites = [(float(r[0]), float(r[1]), int(r[3])) for r in geo[7:]]
+    n = len(sites)
+    h_gen = np.zeros((n, n), dtype=complex)
+    for r in open(tmp_path / "trans.def").read().split("\n")[5:]:
+        r = r.split()
+        if len(r) == 6 and r[1] == "0" and r[3] == "0":
+            h_gen[int(r[0]), int(r[2])] -= complex(float(r[4]), float(r[5]))
+    prim = np.array(prim)
+    pos = np.array([(np.array([w, l]) + np.array(orbs[o])) @ prim for w, l, o in sites])
+    h_geo = np.zeros((n, n))
+    for i in range(n):
+        for j in range(n):
+            for n0 in range(-3, 4):
+                for n1 in range(-3, 4):
+                    if lattice == "chain" and n1 != 0:
+                        continue
+                    d = np.linalg.norm(pos[j] + (n0 * box[0] + n1 * box[1]) @ prim - pos[i])
+                    for shell, t in zip(shells, ts):
+                        if abs(d - shell) < 1e-9:
+                            h_geo[i, j] -= t
+    np.testing.assert_allclose(h_gen, h_geo, atol=1e-12)
