@@ -220,3 +220,44 @@ def test_hoppings_follow_the_lattice_geometry(lattice, cell, tmp_path):
                         if abs(d - shell) < 1e-9:
                             h_geo[i, j] -= t
     np.testing.assert_allclose(h_gen, h_geo, atol=1e-12)
+
+
+# Bond direction of each direction-resolved hopping (t0, t1, t2 and their primed forms) in
+# fractional coordinates, as drawn in the reference's lattice figures (doc/figs/*.png).
+_LABELS = {
+    "square": {"t0": (1, 0), "t1": (0, 1), "t0'": (1, 1), "t1'": (1, -1), "t0''": (2, 0), "t1''": (0, 2)},
+    "triangular": {"t0": (1, 0), "t1": (0, 1), "t2": (-1, 1), "t0'": (-1, 2), "t1'": (2, -1), "t2'": (1, 1),
+                   "t0''": (2, 0), "t1''": (0, 2), "t2''": (-2, 2)},
+    "honeycomb": {"t0": (1 / 3, 1 / 3), "t1": (2 / 3, -1 / 3), "t2": (-1 / 3, 2 / 3)},
+    "kagome": {"t0": (-0.5, 0.5), "t1": (0, 0.5), "t2": (0.5, 0)},
+}
+
+
+@pytest.mark.parametrize("lattice", sorted(_LABELS))
+def test_direction_resolved_hoppings_follow_the_figures(lattice, tmp_path):
+    """Each direction-resolved hopping joins sites displaced along the bond its figure shows."""
+    import numpy as np
+    prim, orbs, _ = _GEOMETRY[lattice]
+    labels = _LABELS[lattice]
+    value = {lab: 1.0 + 0.1 * k for k, lab in enumerate(labels)}
+    p = tmp_path / "stan.in"
+    p.write_text(f'model = "HubbardGC"\nmethod = "Lanczos"\nlattice = "{lattice}"\nW = 5\nL = 5\n' +
+                 "".join(f"{lab} = {v}\n" for lab, v in value.items()))
+    hphi_b200.standard_mode(str(p), str(tmp_path))
+    geo = [l.split() for l in open(tmp_path / "geometry.dat") if l.strip()]
+    box = np.array([[float(x) for x in r[:2]] for r in geo[4:6]])
+    frac = np.array([[float(r[0]) + orbs[int(r[3])][0], float(r[1]) + orbs[int(r[3])][1]] for r in geo[7:]])
+    seen = set()
+    for r in open(tmp_path / "trans.def").read().split("\n")[5:]:
+        r = r.split()
+        if len(r) != 6 or r[1] != "0" or r[3] != "0" or r[0] == r[2]:
+            continue
+        i, j, t = int(r[0]), int(r[2]), float(r[4])
+        d = frac[i] - frac[j]   # the entry is -t c+_i c_j: a hop from j to i
+        d = d - np.round(np.linalg.solve(box.T, d)) @ box    # minimal image in the 5x5 cell
+        match = [lab for lab, v in labels.items() if np.allclose(np.abs(d), np.abs(v)) and
+                 (np.allclose(d, v) or np.allclose(d, -np.array(v)))]
+        assert len(match) == 1, (i, j, d)
+        assert abs(t - value[match[0]]) < 1e-12, (match[0], t)
+        seen.add(match[0])
+    assert seen == set(labels)
